@@ -1,0 +1,113 @@
+/*
+ * xkb_cuda.h -- the thin C ABI between the host runtime and the sm_100a
+ * kernels of libxkblas.so.  Plain pointers (DEVICE addresses) and sizes; the
+ * stream is a cudaStream_t passed as void* (NULL = the library's stream).
+ *
+ * It replaces the reference's per-tile GPU task bodies, which hand each tile
+ * to cuBLAS:
+ *   xkb_cuda_gemm       <- blas/ztask_gemm.c:176-216   (cublasZgemm, :206),
+ *                          blas/ztask_gemmt.c:213, ztask_syrk.c:130,
+ *                          ztask_herk.c:130, ztask_syr2k.c:138,
+ *                          ztask_her2k.c:138 (triangle-masked variants)
+ *   xkb_cuda_trsm       <- blas/ztask_trsm.c:162-180   (cublasZtrsm, :172)
+ *   xkb_cuda_trmm       <- blas/ztask_trmm.c:156       (cublasZtrmm)
+ *   xkb_cuda_symm       <- blas/ztask_symm.c:133, ztask_hemm.c:132
+ *   xkb_cuda_ozaki_dgemm / xkb_cuda_ozaki_zgemm: no counterpart in the
+ *                          reference (FP64 contraction on INT8 tensor cores).
+ * Every function returns 0 or a negative XKB_E* code; nothing aborts.
+ */
+#ifndef XKB_CUDA_H
+#define XKB_CUDA_H
+#include <stddef.h>
+#include <stdint.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* element types */
+#define XKB_S 0   /* float            */
+#define XKB_D 1   /* double           */
+#define XKB_C 2   /* float complex    */
+#define XKB_Z 3   /* double complex   */
+/* op codes */
+#define XKB_OP_N 0
+#define XKB_OP_T 1
+#define XKB_OP_C 2
+/* triangle masks on C */
+#define XKB_FULL 0
+#define XKB_LOWER 1
+#define XKB_UPPER 2
+
+/* error codes */
+#define XKB_OK 0
+#define XKB_EINVAL -1     /* bad argument (size, alignment, op)         */
+#define XKB_ECUDA -2      /* CUDA runtime error                          */
+#define XKB_ENOMEM -3     /* device allocation failed                    */
+#define XKB_ENODEV -4     /* no usable sm_100 device                     */
+#define XKB_ETIMEDOUT -5  /* a bounded device-side wait gave up          */
+#define XKB_ERANGE -6     /* size beyond a documented maximum            */
+
+typedef struct xkb_gemm_args {
+  int dtype;          /* XKB_S/D/C/Z                                          */
+  int opA, opB;       /* XKB_OP_N/T/C                                         */
+  int M, N, K;        /* C is M x N, op(A) M x K, op(B) K x N                 */
+  const void* A; long lda;   /* column-major device matrices               */
+  const void* B; long ldb;
+  void* C; long ldc;
+  double alpha[2];    /* (re, im); im ignored for real types                  */
+  double beta[2];
+  int uplo;           /* XKB_FULL / XKB_LOWER / XKB_UPPER: written part of C  */
+  int herm_diag;      /* complex: force Im(C(i,i)) = 0 (herk/her2k contract)  */
+  long diag;          /* C(i,j) lies on the diagonal when i + diag == j       */
+} xkb_gemm_args;
+
+/* C <- alpha*op(A)*op(B) + beta*C on the masked part of C, FP64 DMMA
+ * tensor cores (float storage computed in double and rounded once). */
+int xkb_cuda_gemm(const xkb_gemm_args* a, void* stream);
+
+/* Triangular solve, all side/uplo/trans/diag cases:
+ *   side L: B <- alpha * op(A)^-1 * B   (A is M x M)
+ *   side R: B <- alpha * B * op(A)^-1   (A is N x N)
+ * FP64 diagonal-block substitution + DMMA GEMM updates (or Ozaki updates
+ * when ozaki != 0 and dtype is XKB_D/XKB_Z). */
+int xkb_cuda_trsm(int dtype, int side, int uplo, int trans, int diag, int M,
+                  int N, const double* alpha, const void* A, long lda, void* B,
+                  long ldb, int ozaki, void* stream);
+
+/* B <- alpha * op(A) * B (side L) or alpha * B * op(A) (side R). */
+int xkb_cuda_trmm(int dtype, int side, int uplo, int trans, int diag, int M,
+                  int N, const double* alpha, const void* A, long lda, void* B,
+                  long ldb, void* stream);
+
+/* C <- alpha*A*B + beta*C (side L) or alpha*B*A + beta*C, A symmetric
+ * (herm = 0) or Hermitian (herm = 1) stored in its uplo triangle. */
+int xkb_cuda_symm(int dtype, int herm, int side, int uplo, int M, int N,
+                  const double* alpha, const void* A, long lda, const void* B,
+                  long ldb, const double* beta, void* C, long ldc,
+                  void* stream);
+
+/* C <- beta*C on the masked part (used for K == 0 / alpha == 0). */
+int xkb_cuda_scale(int dtype, int M, int N, const double* beta, void* C,
+                   long ldc, int uplo, int herm_diag, long diag, void* stream);
+
+/* Ozaki scheme II: FP64 (or complex128) C <- alpha*op(A)*op(B) + beta*C
+ * computed as nmod INT8 tensor-core products modulo pairwise coprime
+ * moduli (tcgen05, exact INT32 accumulation) and a Chinese-remainder
+ * reconstruction.  nmod = 0 picks the count from K for FP64 accuracy.
+ * uplo/herm_diag/diag mask C as in xkb_gemm_args.  dtype XKB_D or XKB_Z. */
+int xkb_cuda_ozaki_gemm(const xkb_gemm_args* a, int nmod, void* stream);
+
+/* Number of moduli the Ozaki path uses for contraction length K (0 if K is
+ * beyond the exact-INT32 limit). */
+int xkb_ozaki_default_moduli(long K);
+
+/* Device error word written by bounded waits (0 = none); clears it. */
+int xkb_cuda_take_device_error(void);
+
+/* Kernels launched by the library since load (for launch accounting). */
+uint64_t xkb_cuda_kernel_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,260 @@
+/*
+ * xkblas.h -- public C interface of the B200 level-3 BLAS tile library.
+ *
+ * Drop-in for the XKBlas C API: the same symbol names, argument orders,
+ * enum values and return conventions as XKBlas 0.6 (blas/xkblas.h:70-511 and
+ * blas/zxkblas.h:45-151 of the reference).  Every declaration below names the
+ * reference declaration it replaces.
+ *
+ * Semantics kept from the reference:
+ *   - matrices are host resident, column major, owned by the caller;
+ *   - xkblas_?xxx_async() enqueues work and returns 0, or -i when the i-th
+ *     argument is invalid (reference e.g. blas/zgemm.c:132-181);
+ *   - results are copied back to the host only on request:
+ *     xkblas_memory_coherent_async() followed by xkblas_sync();
+ *   - device copies stay cached (keyed by the host pointer) until
+ *     xkblas_memory_invalidate*() or xkblas_memory_free().
+ * Divergence: argument errors are reported by return code only; the library
+ * never aborts the process (the reference prints and aborts).
+ *
+ * All compute runs on the GPU (FP64 DMMA tensor-core kernels, or the Ozaki
+ * INT8 tensor-core form under XKBLAS_TENSOR_OP_MATH).  The *_native entry
+ * points are the reference's CPU-BLAS pass-through and are never used by the
+ * *_async path.
+ */
+#ifndef XKBLAS_B200_XKBLAS_H
+#define XKBLAS_B200_XKBLAS_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+#include <complex>
+typedef std::complex<float>  Complex32_t;
+typedef std::complex<double> Complex64_t;
+extern "C" {
+#else
+#include <complex.h>
+typedef float _Complex  Complex32_t;
+typedef double _Complex Complex64_t;
+#endif
+typedef double CFloat64_t;
+typedef float  CFloat32_t;
+
+#define __XKBLAS__ 0
+#define __XKBLAS_MINOR__ 6
+#define __XKBLAS_PATCHLEVEL__ 0
+
+/* ---- enums: values identical to the reference (blas/xkblas.h:100-119) --- */
+typedef enum { XKBLAS_DEFAULT_MATH, XKBLAS_TENSOR_OP_MATH } xkblas_mode_math_t;
+
+#ifndef KAAPI_NO_DEFAULT_BLAS_ENUM
+typedef enum { CblasRowMajor = 101, CblasColMajor = 102 } CBLAS_ORDER;
+typedef enum { CblasNoTrans = 111, CblasTrans = 112, CblasConjTrans = 113,
+               CblasConjNoTrans = 114 } CBLAS_TRANSPOSE;
+typedef enum { CblasUpper = 121, CblasLower = 122 } CBLAS_UPLO;
+typedef enum { CblasNonUnit = 131, CblasUnit = 132 } CBLAS_DIAG;
+typedef enum { CblasLeft = 141, CblasRight = 142 } CBLAS_SIDE;
+typedef CBLAS_ORDER CBLAS_LAYOUT;
+#endif
+
+/* reference blas/xkblas.h:124-138 */
+typedef enum {
+  KERN_VOID, KERN_GEMM, KERN_GEMMT, KERN_TRMM, KERN_TRSM, KERN_SYMM,
+  KERN_SYRK, KERN_SYR2K, KERN_HEMM, KERN_HERK, KERN_HER2K, KERN_SWAP,
+  KERN_COPYSCALE
+} xkblas_kernel_t;
+
+/* reference blas/xkblas.h:221-243 */
+typedef struct xkblas_dev_prop_t {
+  int arch;
+  int has_unified;
+  int device_count;
+} xkblas_dev_prop_t;
+
+typedef enum xkblas_dev_arch_t {
+  XKBLAS_ARCH_UNDEF = -1, XKBLAS_ARCH_UNKNOWN = 0, XKBLAS_ARCH_V100 = 1,
+  XKBLAS_ARCH_A100 = 2, XKBLAS_ARCH_RESERVED0 = 3, XKBLAS_ARCH_GRACEHOPPER = 4,
+  XKBLAS_ARCH_MI50 = 101, XKBLAS_ARCH_RESERVED1 = 102,
+  XKBLAS_ARCH_RESERVED2 = 103, XKBLAS_ARCH_MI250 = 104,
+  XKBLAS_ARCH_RESERVED3 = 105, XKBLAS_ARCH_MI300A = 106,
+  /* added: Blackwell data-centre part this library is built for */
+  XKBLAS_ARCH_B200 = 5
+} xkblas_dev_arch_t;
+
+struct xkblas_context;
+typedef struct xkblas_context xkblas_context_t;
+struct xkblas_matrix_descr;
+typedef struct xkblas_matrix_descr xkblas_matrix_descr_t;
+
+/* ---- lifecycle (reference blas/xkblas.h:95-498) ------------------------- */
+int  xkblas_get_devicecount(void);                         /* :203 */
+int  xkblas_init(void);                                    /* :207; ref-counted */
+int  xkblas_finalize(void);                                /* :211 */
+int  xkblas_get_device_count(int* count);                  /* :217 */
+int  xkblas_get_device_properties(struct xkblas_dev_prop_t* prop); /* :256 */
+int  xkblas_force_set_unified(void);                       /* :267; EINVAL here */
+const char* xkblas_get_configuration(void);                /* :273 */
+void xkblas_load_sym(void** ptr, const char* name);        /* :278 */
+int  xkblas_sync(void);                                    /* :282 */
+xkblas_context_t* xkblas_context_get(void);                /* :95 */
+void xkblas_set_modemath(xkblas_mode_math_t mode);         /* :107 */
+size_t xkblas_get_param(void);                             /* :470 */
+void xkblas_set_param(size_t nb, size_t p);                /* :484 */
+int  xkblas_get_ngpus(void);                               /* :476 */
+int  xkblas_set_ngpus(int ngpus);                          /* :480 */
+uint64_t xkblas_elapsedns(void);                           /* :492 */
+double   xkblas_elapsedtime(void);                         /* :498 */
+
+/* ---- matrix descriptors (reference blas/xkblas.h:287-312) --------------- */
+xkblas_matrix_descr_t* xkblas_find(const void* A);
+int xkblas_matrix_descr_isinit(xkblas_matrix_descr_t* Ah);
+int xkblas_init_matrix_handle(xkblas_matrix_descr_t* Ah, void* A, size_t M,
+                              size_t N, size_t LD, size_t eltsize, size_t MB,
+                              size_t NB);
+size_t xkblas_auto_tilesize(xkblas_context_t* ctx, xkblas_kernel_t kernel,
+                            size_t M, size_t N, size_t K);
+
+/* ---- host memory (reference blas/xkblas.h:70-85, 318-365, 500-511) ----- */
+void*    xkblas_malloc(size_t sz);                 /* pinned host memory */
+void     xkblas_free(void* ptr, size_t sz);
+int      xkblas_malloc_unified(void** ptr, size_t size);
+int      xkblas_free_unified(void* ptr);
+void     xkblas_activate_custom_alloc(void);
+void     xkblas_deactivate_custom_alloc(void);
+uint64_t xkblas_register_memory_async(void* ptr, size_t sz);
+uint64_t xkblas_unregister_memory_async(void* ptr, size_t sz);
+int      xkblas_register_memory_test(uint64_t handle);
+int      xkblas_register_memory_wait(uint64_t handle);
+int      xkblas_register_memory_waitall(void);
+int      xkblas_register_memory(void* ptr, size_t sz);
+int      xkblas_unregister_memory(void* ptr, size_t sz);
+void     xkblas_memset(void* ptr, int v, size_t sz);
+void     xkblas_memcpy(void* dst, void* src, size_t sz);
+void     xkblas_register_work_buffer(void* ptr, size_t sz);
+void     xkblas_unregister_work_buffer(void* ptr);
+void*    xkblas_get_work_pos(size_t sz);
+void     xkblas_free_work_pos(void* ptr);
+void     xkblas_bind_cpu(void* ptr, size_t sz);
+void     xkblas_host_register_direct(void* ptr, size_t sz);
+void     xkblas_host_unregister_direct(void* ptr);
+
+/* ---- debug and multi-device placement (reference xkblas.h:371-430) -----
+ * One GPU: placement calls validate their arguments and return 0. */
+int  xkblas_dbg_setname(const char* name, xkblas_matrix_descr_t* Mh);
+int  xkblas_dbg_setname_with_flags(const char* name, xkblas_matrix_descr_t* Mh,
+                                   uint32_t flags);
+void xkblas_dbg_dump_graph(const char* name);
+int  xkblas_map_2Dblock_cyclic(xkblas_context_t* ctx, int hlevel, int storage,
+                               size_t m, size_t n, const void* A, size_t ld,
+                               size_t eltsize, size_t Bp, size_t Bq, size_t Gp,
+                               size_t Gq, int force);
+int  xkblas_map_1Dblock_cyclic(xkblas_context_t* ctx, int hlevel, int storage,
+                               int colrow, size_t m, size_t n, const void* A,
+                               size_t ld, size_t eltsize, size_t B, size_t G,
+                               int force);
+int  xkblas_distribute_2Dblock_cyclic_async(int hlevel, int storage, int uplo,
+                               size_t NB, size_t m, size_t n, const void* A,
+                               size_t ld, size_t eltsize, size_t Bp, size_t Bq,
+                               size_t Gp, size_t Gq);
+int  xkblas_distribute_1Dblock_cyclic_async(int hlevel, int storage, int uplo,
+                               int colrow, size_t NB, size_t m, size_t n,
+                               const void* A, size_t ld, size_t eltsize,
+                               size_t B, size_t G);
+
+/* ---- coherence (reference blas/xkblas.h:441-466) ------------------------
+ * uplo 0: whole matrix; CblasUpper/CblasLower: that triangle (diagonal
+ * tiles included).  memflag 1: the other triangle's device copy is dropped. */
+int xkblas_memory_coherent_async(int uplo, int memflag, size_t M, size_t N,
+                                 void* A, size_t ld, size_t elsize);
+int xkblas_memory_syncall(void);
+int xkblas_memory_invalidate(const void* A);
+int xkblas_memory_invalidate_caches(void);
+int xkblas_memory_free(void);
+
+/* ---- level-3 operations (reference blas/zxkblas.h:45-151, generated for
+ * s/d/c/z).  Scalars by pointer; CBLAS enum ints; int dims and ld. -------- */
+#define XKBLAS_DECL_OPS(p, T, R)                                               \
+  int xkblas_##p##gemm_async(int transA, int transB, int M, int N, int K,      \
+      const T* alpha, const T* A, int LDA, const T* B, int LDB,                \
+      const T* beta, T* C, int LDC);                                           \
+  int xkblas_##p##gemm_native(int transA, int transB, int M, int N, int K,     \
+      const T* alpha, const T* A, int LDA, const T* B, int LDB,                \
+      const T* beta, T* C, int LDC);                                           \
+  int xkblas_##p##gemmt_async(int uplo, int transA, int transB, int N, int K,  \
+      const T* alpha, const T* A, int LDA, const T* B, int LDB,                \
+      const T* beta, T* C, int LDC);                                           \
+  int xkblas_##p##gemmt_native(int uplo, int transA, int transB, int N, int K, \
+      const T* alpha, const T* A, int LDA, const T* B, int LDB,                \
+      const T* beta, T* C, int LDC);                                           \
+  int xkblas_##p##trsm_async(int side, int uplo, int transA, int diag, int N,  \
+      int NRHS, const T* alpha, const T* A, int LDA, T* B, int LDB);           \
+  int xkblas_##p##trsm_native(int side, int uplo, int transA, int diag, int N, \
+      int NRHS, const T* alpha, const T* A, int LDA, T* B, int LDB);           \
+  int xkblas_##p##trmm_async(int side, int uplo, int transA, int diag, int N,  \
+      int NRHS, const T* alpha, const T* A, int LDA, T* B, int LDB);           \
+  int xkblas_##p##trmm_native(int side, int uplo, int transA, int diag, int N, \
+      int NRHS, const T* alpha, const T* A, int LDA, T* B, int LDB);           \
+  int xkblas_##p##symm_async(int side, int uplo, int M, int N, const T* alpha, \
+      const T* A, int LDA, const T* B, int LDB, const T* beta, T* C, int LDC); \
+  int xkblas_##p##symm_native(int side, int uplo, int M, int N,                \
+      const T* alpha, const T* A, int LDA, const T* B, int LDB,                \
+      const T* beta, T* C, int LDC);                                           \
+  int xkblas_##p##syrk_async(int uplo, int trans, int N, int K,                \
+      const T* alpha, const T* A, int LDA, const T* beta, T* C, int LDC);      \
+  int xkblas_##p##syrk_native(int uplo, int trans, int N, int K,               \
+      const T* alpha, const T* A, int LDA, const T* beta, T* C, int LDC);      \
+  int xkblas_##p##syr2k_async(int uplo, int trans, int N, int K,               \
+      const T* alpha, const T* A, int LDA, const T* B, int LDB,                \
+      const T* beta, T* C, int LDC);                                           \
+  int xkblas_##p##syr2k_native(int uplo, int trans, int N, int K,              \
+      const T* alpha, const T* A, int LDA, const T* B, int LDB,                \
+      const T* beta, T* C, int LDC);
+
+/* hemm/herk/her2k exist for c and z only (reference gen_internal_register.sh:10-20) */
+#define XKBLAS_DECL_HE_OPS(p, T, R)                                            \
+  int xkblas_##p##hemm_async(int side, int uplo, int M, int N, const T* alpha, \
+      const T* A, int LDA, const T* B, int LDB, const T* beta, T* C, int LDC); \
+  int xkblas_##p##hemm_native(int side, int uplo, int M, int N,                \
+      const T* alpha, const T* A, int LDA, const T* B, int LDB,                \
+      const T* beta, T* C, int LDC);                                           \
+  int xkblas_##p##herk_async(int uplo, int trans, int N, int K,                \
+      const R* alpha, const T* A, int LDA, const R* beta, T* C, int LDC);      \
+  int xkblas_##p##herk_native(int uplo, int trans, int N, int K,               \
+      const R* alpha, const T* A, int LDA, const R* beta, T* C, int LDC);      \
+  int xkblas_##p##her2k_async(int uplo, int trans, int N, int K,               \
+      const T* alpha, const T* A, int LDA, const T* B, int LDB,                \
+      const R* beta, T* C, int LDC);                                           \
+  int xkblas_##p##her2k_native(int uplo, int trans, int N, int K,              \
+      const T* alpha, const T* A, int LDA, const T* B, int LDB,                \
+      const R* beta, T* C, int LDC);
+
+XKBLAS_DECL_OPS(s, float, float)
+XKBLAS_DECL_OPS(d, double, double)
+XKBLAS_DECL_OPS(c, Complex32_t, float)
+XKBLAS_DECL_OPS(z, Complex64_t, double)
+XKBLAS_DECL_HE_OPS(c, Complex32_t, float)
+XKBLAS_DECL_HE_OPS(z, Complex64_t, double)
+
+/* ---- added: per-call counters (reference XKBLAS_VERBOSE statistics,
+ * blas/xkblas.c:1635-1700, as a queryable record) ------------------------ */
+typedef struct xkblas_stats_t {
+  uint64_t calls;          /* level-3 calls accepted */
+  uint64_t kernels;        /* kernels launched by the library */
+  uint64_t h2d_bytes;      /* bytes copied host -> device */
+  uint64_t d2h_bytes;      /* bytes copied device -> host */
+  uint64_t tile_hits;      /* tiles found valid on the device */
+  uint64_t tile_misses;    /* tiles fetched from the host */
+  uint64_t ozaki_calls;    /* contractions run in the Ozaki INT8 form */
+  uint64_t ozaki_moduli;   /* sum over those calls of the moduli used */
+  double   flops;          /* algorithmic flops (reference blas/flops.h) */
+} xkblas_stats_t;
+int  xkblas_get_stats(xkblas_stats_t* st);
+void xkblas_reset_stats(void);
+/* Last device-side error word (0 = none); set by bounded waits in kernels. */
+int  xkblas_last_device_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* XKBLAS_B200_XKBLAS_H */

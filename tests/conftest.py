@@ -1,0 +1,29 @@
+import os
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a B200 (sm_100a) GPU")
+    config.addinivalue_line("markers", "slow: large sizes, minutes of CPU")
+
+
+@pytest.fixture(scope="session")
+def xk():
+    """The library under test, initialised on the GPU."""
+    import xkblas_b200 as X
+    X.init()
+    yield X
+    X.lib().xkblas_memory_invalidate_caches()
+
+
+@pytest.fixture(scope="session")
+def orc():
+    import oracle as O
+    O.lib()
+    return O

@@ -1,0 +1,504 @@
+// api_ops.cpp -- the level-3 entry points of xkblas.h (s/d/c/z):
+// argument checking with the reference's -i codes, quick returns, tile
+// directory acquisition, and the device call that replaces the reference's
+// tile-task insertion loops.
+//
+// Reference drivers (argument checks / quick returns / tile loops):
+//   gemm  blas/zgemm.c:118-370      gemmt blas/zgemmt.c:114-390
+//   trsm  blas/ztrsm.c:102-499      trmm  blas/ztrmm.c:101-460
+//   symm  blas/zsymm.c:107-400      hemm  blas/zhemm.c:106-390
+//   syrk  blas/zsyrk.c:97-319       herk  blas/zherk.c:97-320
+//   syr2k blas/zsyr2k.c:107-330     her2k blas/zher2k.c:107-383
+// Instead of one task per NB x NB tile, each call becomes one (or, for
+// trsm, a short sequence of) whole-matrix kernel launch on the compute
+// stream; the tile directory supplies the operands and records what the
+// call wrote.  Divergences from the reference, all deliberate:
+//   * errors are returned, never abort();
+//   * gemmt writes only the uplo triangle (the reference's GPU body writes
+//     the whole diagonal tile, blas/ztask_gemmt.c:213);
+//   * float / complex-float operands are computed in FP64 and rounded once.
+#include <algorithm>
+#include <cerrno>
+#include <cmath>
+#include <complex>
+
+#include "runtime.hpp"
+
+using namespace xkbrt;
+
+namespace {
+
+template <class T>
+struct HT;
+template <>
+struct HT<float> {
+  static constexpr int dt = XKB_S;
+  static constexpr bool cplx = false;
+};
+template <>
+struct HT<double> {
+  static constexpr int dt = XKB_D;
+  static constexpr bool cplx = false;
+};
+template <>
+struct HT<Complex32_t> {
+  static constexpr int dt = XKB_C;
+  static constexpr bool cplx = true;
+};
+template <>
+struct HT<Complex64_t> {
+  static constexpr int dt = XKB_Z;
+  static constexpr bool cplx = true;
+};
+
+template <class T>
+void sc(const T& v, double out[2]) {
+  if constexpr (HT<T>::cplx) {
+    out[0] = (double)v.real();
+    out[1] = (double)v.imag();
+  } else {
+    out[0] = (double)v;
+    out[1] = 0.0;
+  }
+}
+template <class T>
+bool is_zero(const T& v) {
+  return v == T(0);
+}
+template <class T>
+bool is_one(const T& v) {
+  return v == T(1);
+}
+
+int opcode(int t) { return t == CblasNoTrans ? XKB_OP_N : (t == CblasTrans ? XKB_OP_T : XKB_OP_C); }
+int maskcode(int uplo) { return uplo == CblasLower ? XKB_LOWER : XKB_UPPER; }
+
+// Host error mapping: argument errors are -i; runtime failures are positive
+// errno values so they never collide with an argument index.
+int rt_error(int xkb) {
+  switch (xkb) {
+    case XKB_OK: return 0;
+    case XKB_ENODEV: return ENODEV;
+    case XKB_ENOMEM: return ENOMEM;
+    case XKB_ETIMEDOUT: return ETIMEDOUT;
+    case XKB_ERANGE: return ERANGE;
+    default: return EIO;
+  }
+}
+
+struct Guard {
+  std::lock_guard<std::recursive_mutex> g;
+  Guard() : g(rt().mu) {}
+};
+
+bool use_ozaki(int dt, long m, long n, long k) {
+  Runtime& R = rt();
+  if (R.math != XKBLAS_TENSOR_OP_MATH) return false;
+  if (dt != XKB_D && dt != XKB_Z) return false;
+  return std::min(m, std::min(n, k)) >= R.ozaki_min_dim && xkb_ozaki_default_moduli(k) > 0;
+}
+
+// One contraction on device operands: plain DMMA or Ozaki.
+int run_gemm(xkb_gemm_args& a) {
+  Runtime& R = rt();
+  if (use_ozaki(a.dtype, a.M, a.N, a.K)) {
+    int nm = R.ozaki_moduli ? R.ozaki_moduli : xkb_ozaki_default_moduli(a.K);
+    int e = xkb_cuda_ozaki_gemm(&a, nm, R.s_comp);
+    if (e == XKB_OK) {
+      R.stats.ozaki_calls++;
+      R.stats.ozaki_moduli += (uint64_t)nm;
+      return e;
+    }
+    if (e != XKB_ERANGE) return e;
+  }
+  return xkb_cuda_gemm(&a, R.s_comp);
+}
+
+template <class T>
+xkb_gemm_args base_args(int opA, int opB, int M, int N, int K, const T* alpha, const T* beta) {
+  xkb_gemm_args a{};
+  a.dtype = HT<T>::dt;
+  a.opA = opA;
+  a.opB = opB;
+  a.M = M;
+  a.N = N;
+  a.K = K;
+  sc(*alpha, a.alpha);
+  sc(*beta, a.beta);
+  a.uplo = XKB_FULL;
+  a.herm_diag = 0;
+  a.diag = 0;
+  return a;
+}
+
+// ---------------------------------------------------------------------------
+template <class T>
+int gemm_async(int transA, int transB, int M, int N, int K, const T* alpha, const T* A, int LDA,
+               const T* B, int LDB, const T* beta, T* C, int LDC) {
+  if (transA < CblasNoTrans || transA > CblasConjTrans) return -1;
+  if (transB < CblasNoTrans || transB > CblasConjTrans) return -2;
+  const int Am = transA == CblasNoTrans ? M : K, An = transA == CblasNoTrans ? K : M;
+  const int Bm = transB == CblasNoTrans ? K : N, Bn = transB == CblasNoTrans ? N : K;
+  if (M < 0) return -3;
+  if (N < 0) return -4;
+  if (K < 0) return -5;
+  if (LDA < std::max(1, Am)) return -8;
+  if (LDB < std::max(1, Bm)) return -10;
+  if (LDC < std::max(1, M)) return -13;
+  if (M == 0 || N == 0 || ((is_zero(*alpha) || K == 0) && is_one(*beta))) return 0;
+  Guard g;
+  if (int e = ensure_init()) return rt_error(e);
+  Runtime& R = rt();
+  R.stats.calls++;
+  R.stats.flops += (HT<T>::cplx ? 8.0 : 2.0) * M * (double)N * K;
+  const size_t NB = auto_tilesize(KERN_GEMM, M, N, K), es = sizeof(T);
+  int err;
+  const bool need_ab = !is_zero(*alpha) && K > 0;
+  Desc *dA = nullptr, *dB = nullptr;
+  if (need_ab) {
+    dA = get_desc(A, Am, An, LDA, es, NB, &err);
+    if (!dA) return rt_error(err);
+    if ((err = make_valid(dA, 0, Am, 0, An))) return rt_error(err);
+    dB = get_desc(B, Bm, Bn, LDB, es, NB, &err);
+    if (!dB) return rt_error(err);
+    if ((err = make_valid(dB, 0, Bm, 0, Bn))) return rt_error(err);
+  }
+  Desc* dC = get_desc(C, M, N, LDC, es, NB, &err);
+  if (!dC) return rt_error(err);
+  if (!is_zero(*beta)) {
+    if ((err = make_valid(dC, 0, M, 0, N))) return rt_error(err);
+  }
+  xkb_gemm_args a = base_args<T>(opcode(transA), opcode(transB), M, N, K, alpha, beta);
+  a.A = dA ? dev_ptr(dA, 0, 0) : nullptr;
+  a.lda = dA ? (long)dA->dld : 1;
+  a.B = dB ? dev_ptr(dB, 0, 0) : nullptr;
+  a.ldb = dB ? (long)dB->dld : 1;
+  a.C = dev_ptr(dC, 0, 0);
+  a.ldc = (long)dC->dld;
+  if (!need_ab) a.K = 0;
+  if ((err = run_gemm(a))) return rt_error(err);
+  mark_full_overwrite(dC, 0, M, 0, N);
+  return 0;
+}
+
+template <class T>
+int gemmt_async(int uplo, int transA, int transB, int N, int K, const T* alpha, const T* A,
+                int LDA, const T* B, int LDB, const T* beta, T* C, int LDC) {
+  // reference blas/zgemmt.c:114-190 (uplo 0 = full product, an XKBlas extension)
+  // argument codes follow the reference (transA -1, transB -2, N -4, ...);
+  // the reference does not check uplo, an invalid one is reported as -1 here.
+  if (transA < CblasNoTrans || transA > CblasConjTrans) return -1;
+  if (transB < CblasNoTrans || transB > CblasConjTrans) return -2;
+  if (uplo != 0 && uplo != CblasUpper && uplo != CblasLower) return -1;
+  const int Am = transA == CblasNoTrans ? N : K, An = transA == CblasNoTrans ? K : N;
+  const int Bm = transB == CblasNoTrans ? K : N, Bn = transB == CblasNoTrans ? N : K;
+  if (N < 0) return -4;
+  if (K < 0) return -5;
+  if (LDA < std::max(1, Am)) return -8;
+  if (LDB < std::max(1, Bm)) return -10;
+  if (LDC < std::max(1, N)) return -13;
+  if (N == 0 || ((is_zero(*alpha) || K == 0) && is_one(*beta))) return 0;
+  if (uplo == 0) return gemm_async<T>(transA, transB, N, N, K, alpha, A, LDA, B, LDB, beta, C, LDC);
+  Guard g;
+  if (int e = ensure_init()) return rt_error(e);
+  Runtime& R = rt();
+  R.stats.calls++;
+  R.stats.flops += (HT<T>::cplx ? 4.0 : 1.0) * N * (double)(N + 1) * K;
+  const size_t NB = auto_tilesize(KERN_GEMMT, N, N, K), es = sizeof(T);
+  int err;
+  const bool need_ab = !is_zero(*alpha) && K > 0;
+  Desc *dA = nullptr, *dB = nullptr;
+  if (need_ab) {
+    if (!(dA = get_desc(A, Am, An, LDA, es, NB, &err))) return rt_error(err);
+    if ((err = make_valid(dA, 0, Am, 0, An))) return rt_error(err);
+    if (!(dB = get_desc(B, Bm, Bn, LDB, es, NB, &err))) return rt_error(err);
+    if ((err = make_valid(dB, 0, Bm, 0, Bn))) return rt_error(err);
+  }
+  Desc* dC = get_desc(C, N, N, LDC, es, NB, &err);
+  if (!dC) return rt_error(err);
+  if ((err = make_valid(dC, 0, N, 0, N))) return rt_error(err);  // other triangle kept
+  xkb_gemm_args a = base_args<T>(opcode(transA), opcode(transB), N, N, need_ab ? K : 0, alpha, beta);
+  a.A = dA ? dev_ptr(dA, 0, 0) : nullptr;
+  a.lda = dA ? (long)dA->dld : 1;
+  a.B = dB ? dev_ptr(dB, 0, 0) : nullptr;
+  a.ldb = dB ? (long)dB->dld : 1;
+  a.C = dev_ptr(dC, 0, 0);
+  a.ldc = (long)dC->dld;
+  a.uplo = maskcode(uplo);
+  if ((err = run_gemm(a))) return rt_error(err);
+  mark_written(dC, 0, N, 0, N, uplo);
+  return 0;
+}
+
+// syrk / herk (herm = 1: alpha, beta real, A^H, real diagonal)
+template <class T>
+int rk_async(int herm, int uplo, int trans, int N, int K, const T& alpha, const T* A, int LDA,
+             const T& beta, T* C, int LDC) {
+  if (uplo != CblasUpper && uplo != CblasLower) return -1;
+  // reference: syrk/syr2k accept N or T, herk/her2k N or C (all precisions)
+  if (herm) {
+    if (trans != CblasNoTrans && trans != CblasConjTrans) return -2;
+  } else {
+    if (trans != CblasNoTrans && trans != CblasTrans) return -2;
+  }
+  const int Am = trans == CblasNoTrans ? N : K, An = trans == CblasNoTrans ? K : N;
+  if (N < 0) return -3;
+  if (K < 0) return -4;
+  if (LDA < std::max(1, Am)) return -7;
+  if (LDC < std::max(1, N)) return -10;
+  if (N == 0 || ((is_zero(alpha) || K == 0) && is_one(beta))) return 0;
+  Guard g;
+  if (int e = ensure_init()) return rt_error(e);
+  Runtime& R = rt();
+  R.stats.calls++;
+  R.stats.flops += (HT<T>::cplx ? 4.0 : 1.0) * N * (double)(N + 1) * K;
+  const size_t NB = auto_tilesize(herm ? KERN_HERK : KERN_SYRK, N, N, K), es = sizeof(T);
+  int err;
+  const bool need_a = !is_zero(alpha) && K > 0;
+  Desc* dA = nullptr;
+  if (need_a) {
+    if (!(dA = get_desc(A, Am, An, LDA, es, NB, &err))) return rt_error(err);
+    if ((err = make_valid(dA, 0, Am, 0, An))) return rt_error(err);
+  }
+  Desc* dC = get_desc(C, N, N, LDC, es, NB, &err);
+  if (!dC) return rt_error(err);
+  if ((err = make_valid(dC, 0, N, 0, N))) return rt_error(err);
+  const int tr = herm ? XKB_OP_C : XKB_OP_T;
+  const int opA = trans == CblasNoTrans ? XKB_OP_N : tr;
+  const int opB = trans == CblasNoTrans ? tr : XKB_OP_N;
+  xkb_gemm_args a = base_args<T>(opA, opB, N, N, need_a ? K : 0, &alpha, &beta);
+  a.A = dA ? dev_ptr(dA, 0, 0) : nullptr;
+  a.lda = dA ? (long)dA->dld : 1;
+  a.B = a.A;
+  a.ldb = a.lda;
+  a.C = dev_ptr(dC, 0, 0);
+  a.ldc = (long)dC->dld;
+  a.uplo = maskcode(uplo);
+  a.herm_diag = herm;
+  if ((err = run_gemm(a))) return rt_error(err);
+  mark_written(dC, 0, N, 0, N, uplo);
+  return 0;
+}
+
+// syr2k / her2k: C = alpha op(A) op(B)^T + alpha' op(B) op(A)^T + beta C
+template <class T>
+int r2k_async(int herm, int uplo, int trans, int N, int K, const T& alpha, const T* A, int LDA,
+              const T* B, int LDB, const T& beta, T* C, int LDC) {
+  if (uplo != CblasUpper && uplo != CblasLower) return -1;
+  // reference: syrk/syr2k accept N or T, herk/her2k N or C (all precisions)
+  if (herm) {
+    if (trans != CblasNoTrans && trans != CblasConjTrans) return -2;
+  } else {
+    if (trans != CblasNoTrans && trans != CblasTrans) return -2;
+  }
+  const int Am = trans == CblasNoTrans ? N : K, An = trans == CblasNoTrans ? K : N;
+  if (N < 0) return -3;
+  if (K < 0) return -4;
+  if (LDA < std::max(1, Am)) return -7;
+  if (LDB < std::max(1, Am)) return -9;
+  if (LDC < std::max(1, N)) return -12;
+  if (N == 0 || ((is_zero(alpha) || K == 0) && is_one(beta))) return 0;
+  Guard g;
+  if (int e = ensure_init()) return rt_error(e);
+  Runtime& R = rt();
+  R.stats.calls++;
+  R.stats.flops += (HT<T>::cplx ? 8.0 : 2.0) * N * (double)N * K;
+  const size_t NB = auto_tilesize(herm ? KERN_HER2K : KERN_SYR2K, N, N, K), es = sizeof(T);
+  int err;
+  const bool need_ab = !is_zero(alpha) && K > 0;
+  Desc *dA = nullptr, *dB = nullptr;
+  if (need_ab) {
+    if (!(dA = get_desc(A, Am, An, LDA, es, NB, &err))) return rt_error(err);
+    if ((err = make_valid(dA, 0, Am, 0, An))) return rt_error(err);
+    if (!(dB = get_desc(B, Am, An, LDB, es, NB, &err))) return rt_error(err);
+    if ((err = make_valid(dB, 0, Am, 0, An))) return rt_error(err);
+  }
+  Desc* dC = get_desc(C, N, N, LDC, es, NB, &err);
+  if (!dC) return rt_error(err);
+  if ((err = make_valid(dC, 0, N, 0, N))) return rt_error(err);
+  const int tr = herm ? XKB_OP_C : XKB_OP_T;
+  const int opA = trans == CblasNoTrans ? XKB_OP_N : tr;
+  const int opB = trans == CblasNoTrans ? tr : XKB_OP_N;
+  T alpha2 = alpha;
+  if constexpr (HT<T>::cplx)
+    if (herm) alpha2 = std::conj(alpha);
+  const T one = T(1);
+  xkb_gemm_args a = base_args<T>(opA, opB, N, N, need_ab ? K : 0, &alpha, &beta);
+  a.A = dA ? dev_ptr(dA, 0, 0) : nullptr;
+  a.lda = dA ? (long)dA->dld : 1;
+  a.B = dB ? dev_ptr(dB, 0, 0) : nullptr;
+  a.ldb = dB ? (long)dB->dld : 1;
+  a.C = dev_ptr(dC, 0, 0);
+  a.ldc = (long)dC->dld;
+  a.uplo = maskcode(uplo);
+  a.herm_diag = herm;
+  if ((err = run_gemm(a))) return rt_error(err);
+  if (need_ab) {
+    xkb_gemm_args b = a;
+    std::swap(b.A, b.B);
+    std::swap(b.lda, b.ldb);
+    sc(alpha2, b.alpha);
+    sc(one, b.beta);
+    if ((err = run_gemm(b))) return rt_error(err);
+  }
+  mark_written(dC, 0, N, 0, N, uplo);
+  return 0;
+}
+
+template <class T>
+int sm_async(int herm, int side, int uplo, int M, int N, const T* alpha, const T* A, int LDA,
+             const T* B, int LDB, const T* beta, T* C, int LDC) {
+  if (side != CblasLeft && side != CblasRight) return -1;
+  if (uplo != CblasUpper && uplo != CblasLower) return -2;
+  const int Am = side == CblasLeft ? M : N;
+  if (M < 0) return -3;
+  if (N < 0) return -4;
+  if (LDA < std::max(1, Am)) return -7;
+  if (LDB < std::max(1, M)) return -9;
+  if (LDC < std::max(1, M)) return -12;
+  if (M == 0 || N == 0 || (is_zero(*alpha) && is_one(*beta))) return 0;
+  Guard g;
+  if (int e = ensure_init()) return rt_error(e);
+  Runtime& R = rt();
+  R.stats.calls++;
+  R.stats.flops += (HT<T>::cplx ? 8.0 : 2.0) * (double)M * N * Am;
+  const size_t NB = auto_tilesize(herm ? KERN_HEMM : KERN_SYMM, M, N, 0), es = sizeof(T);
+  int err;
+  Desc* dA = get_desc(A, Am, Am, LDA, es, NB, &err);
+  if (!dA) return rt_error(err);
+  if ((err = make_valid(dA, 0, Am, 0, Am))) return rt_error(err);
+  Desc* dB = get_desc(B, M, N, LDB, es, NB, &err);
+  if (!dB) return rt_error(err);
+  if ((err = make_valid(dB, 0, M, 0, N))) return rt_error(err);
+  Desc* dC = get_desc(C, M, N, LDC, es, NB, &err);
+  if (!dC) return rt_error(err);
+  if (!is_zero(*beta))
+    if ((err = make_valid(dC, 0, M, 0, N))) return rt_error(err);
+  double al[2], be[2];
+  sc(*alpha, al);
+  sc(*beta, be);
+  if ((err = xkb_cuda_symm(HT<T>::dt, herm, side == CblasLeft ? 0 : 1,
+                           uplo == CblasLower ? XKB_LOWER : XKB_UPPER, M, N, al,
+                           dev_ptr(dA, 0, 0), (long)dA->dld, dev_ptr(dB, 0, 0), (long)dB->dld,
+                           be, dev_ptr(dC, 0, 0), (long)dC->dld, R.s_comp)))
+    return rt_error(err);
+  mark_full_overwrite(dC, 0, M, 0, N);
+  return 0;
+}
+
+template <class T>
+int tr_async(int is_trsm, int side, int uplo, int transA, int diag, int M, int N, const T* alpha,
+             const T* A, int LDA, T* B, int LDB) {
+  // reference blas/ztrsm.c:117-169, blas/ztrmm.c:109-170 (N = rows of B, NRHS = cols)
+  const int NA = side == CblasLeft ? M : N;
+  if (side != CblasLeft && side != CblasRight) return -1;
+  if (uplo != CblasUpper && uplo != CblasLower) return -2;
+  if (transA < CblasNoTrans || transA > CblasConjTrans) return -3;
+  if (diag != CblasUnit && diag != CblasNonUnit) return -4;
+  if (M < 0) return -5;
+  if (N < 0) return -6;
+  if (LDA < std::max(1, NA)) return -8;
+  if (LDB < std::max(1, M)) return -10;
+  if (std::min(M, N) == 0) return 0;
+  Guard g;
+  if (int e = ensure_init()) return rt_error(e);
+  Runtime& R = rt();
+  R.stats.calls++;
+  {
+    const double f = side == CblasLeft ? (double)N * M * (M + 1) : (double)M * N * (N + 1);
+    R.stats.flops += (HT<T>::cplx ? 4.0 : 1.0) * f;
+  }
+  const size_t NB = auto_tilesize(is_trsm ? KERN_TRSM : KERN_TRMM, M, N, NA), es = sizeof(T);
+  int err;
+  Desc* dB = get_desc(B, M, N, LDB, es, NB, &err);
+  if (!dB) return rt_error(err);
+  const bool zero = is_zero(*alpha);
+  Desc* dA = nullptr;
+  if (!zero) {
+    if (!(dA = get_desc(A, NA, NA, LDA, es, NB, &err))) return rt_error(err);
+    if ((err = make_valid(dA, 0, NA, 0, NA))) return rt_error(err);
+    if ((err = make_valid(dB, 0, M, 0, N))) return rt_error(err);
+  }
+  double al[2];
+  sc(*alpha, al);
+  const int sd = side == CblasLeft ? 0 : 1;
+  const int ul = uplo == CblasLower ? XKB_LOWER : XKB_UPPER;
+  const int dg = diag == CblasUnit ? 1 : 0;
+  if (zero) {
+    const double z[2] = {0, 0};
+    err = xkb_cuda_scale(HT<T>::dt, M, N, z, dev_ptr(dB, 0, 0), (long)dB->dld, XKB_FULL, 0, 0,
+                         R.s_comp);
+  } else if (is_trsm) {
+    const int oz = (R.math == XKBLAS_TENSOR_OP_MATH) && (HT<T>::dt == XKB_D || HT<T>::dt == XKB_Z);
+    err = xkb_cuda_trsm(HT<T>::dt, sd, ul, opcode(transA), dg, M, N, al, dev_ptr(dA, 0, 0),
+                        (long)dA->dld, dev_ptr(dB, 0, 0), (long)dB->dld, oz, R.s_comp);
+  } else {
+    err = xkb_cuda_trmm(HT<T>::dt, sd, ul, opcode(transA), dg, M, N, al, dev_ptr(dA, 0, 0),
+                        (long)dA->dld, dev_ptr(dB, 0, 0), (long)dB->dld, R.s_comp);
+  }
+  if (err) return rt_error(err);
+  mark_full_overwrite(dB, 0, M, 0, N);
+  return 0;
+}
+
+}  // namespace
+
+// ============================================================================
+// exported symbols
+// ============================================================================
+#define XKB_DEFINE_OPS(p, T, R)                                                                \
+  extern "C" int xkblas_##p##gemm_async(int tA, int tB, int M, int N, int K, const T* al,      \
+                                        const T* A, int lda, const T* B, int ldb, const T* be, \
+                                        T* C, int ldc) {                                       \
+    return gemm_async<T>(tA, tB, M, N, K, al, A, lda, B, ldb, be, C, ldc);                     \
+  }                                                                                            \
+  extern "C" int xkblas_##p##gemmt_async(int ul, int tA, int tB, int N, int K, const T* al,    \
+                                         const T* A, int lda, const T* B, int ldb,             \
+                                         const T* be, T* C, int ldc) {                         \
+    return gemmt_async<T>(ul, tA, tB, N, K, al, A, lda, B, ldb, be, C, ldc);                   \
+  }                                                                                            \
+  extern "C" int xkblas_##p##trsm_async(int sd, int ul, int tA, int dg, int M, int N,          \
+                                        const T* al, const T* A, int lda, T* B, int ldb) {     \
+    return tr_async<T>(1, sd, ul, tA, dg, M, N, al, A, lda, B, ldb);                           \
+  }                                                                                            \
+  extern "C" int xkblas_##p##trmm_async(int sd, int ul, int tA, int dg, int M, int N,          \
+                                        const T* al, const T* A, int lda, T* B, int ldb) {     \
+    return tr_async<T>(0, sd, ul, tA, dg, M, N, al, A, lda, B, ldb);                           \
+  }                                                                                            \
+  extern "C" int xkblas_##p##symm_async(int sd, int ul, int M, int N, const T* al, const T* A, \
+                                        int lda, const T* B, int ldb, const T* be, T* C,       \
+                                        int ldc) {                                             \
+    return sm_async<T>(0, sd, ul, M, N, al, A, lda, B, ldb, be, C, ldc);                       \
+  }                                                                                            \
+  extern "C" int xkblas_##p##syrk_async(int ul, int tr, int N, int K, const T* al, const T* A, \
+                                        int lda, const T* be, T* C, int ldc) {                 \
+    return rk_async<T>(0, ul, tr, N, K, *al, A, lda, *be, C, ldc);                             \
+  }                                                                                            \
+  extern "C" int xkblas_##p##syr2k_async(int ul, int tr, int N, int K, const T* al,            \
+                                         const T* A, int lda, const T* B, int ldb,             \
+                                         const T* be, T* C, int ldc) {                         \
+    return r2k_async<T>(0, ul, tr, N, K, *al, A, lda, B, ldb, *be, C, ldc);                    \
+  }
+
+#define XKB_DEFINE_HE_OPS(p, T, R)                                                             \
+  extern "C" int xkblas_##p##hemm_async(int sd, int ul, int M, int N, const T* al, const T* A, \
+                                        int lda, const T* B, int ldb, const T* be, T* C,       \
+                                        int ldc) {                                             \
+    return sm_async<T>(1, sd, ul, M, N, al, A, lda, B, ldb, be, C, ldc);                       \
+  }                                                                                            \
+  extern "C" int xkblas_##p##herk_async(int ul, int tr, int N, int K, const R* al, const T* A, \
+                                        int lda, const R* be, T* C, int ldc) {                 \
+    return rk_async<T>(1, ul, tr, N, K, T(*al), A, lda, T(*be), C, ldc);                       \
+  }                                                                                            \
+  extern "C" int xkblas_##p##her2k_async(int ul, int tr, int N, int K, const T* al,            \
+                                         const T* A, int lda, const T* B, int ldb,             \
+                                         const R* be, T* C, int ldc) {                         \
+    return r2k_async<T>(1, ul, tr, N, K, *al, A, lda, B, ldb, T(*be), C, ldc);                 \
+  }
+
+XKB_DEFINE_OPS(s, float, float)
+XKB_DEFINE_OPS(d, double, double)
+XKB_DEFINE_OPS(c, Complex32_t, float)
+XKB_DEFINE_OPS(z, Complex64_t, double)
+XKB_DEFINE_HE_OPS(c, Complex32_t, float)
+XKB_DEFINE_HE_OPS(z, Complex64_t, double)

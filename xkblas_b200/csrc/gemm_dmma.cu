@@ -1,0 +1,434 @@
+// gemm_dmma.cu -- the plain FP64 tile GEMM for sm_100a.
+//
+// Replaces the reference's per-tile cuBLAS bodies (blas/ztask_gemm.c:176-216,
+// cublasZgemm at :206; the triangle-masked variants used for gemmt / syrk /
+// herk / syr2k / her2k diagonal tiles, ztask_gemmt.c:213, ztask_syrk.c:130,
+// ztask_herk.c:130).  One launch covers the whole matrix instead of one
+// NB x NB tile per task.
+//
+// Design (B200):
+//   * TMA 2-D tile loads (cp.async.bulk.tensor) fill a 4-stage shared-memory
+//     ring guarded by mbarriers (full: transaction bytes, empty: one arrive
+//     per warp); eight warps run FP64 DMMA tensor-core MMAs (mma.sync
+//     m16n8k8 f64), thread 0 also refilling each stage once it is released;
+//   * operands of any storage type (s/d/c/z) are loaded as raw tiles and
+//     widened to double when fragments are read, so every precision computes
+//     in FP64 and rounds once on store; complex products are four real MMAs;
+//   * the k index inside each 8-wide MMA step is permuted (logical t+4v <->
+//     physical 2t+v) identically for A and B, so each lane's two k values
+//     are adjacent in shared memory;
+//   * alpha/beta, the triangle mask and the Hermitian real-diagonal rule are
+//     applied in the register epilogue; tiles wholly outside the triangle
+//     exit before touching memory;
+//   * every barrier wait is bounded (xkb_dev.cuh) and records an error word.
+#include <cstdio>
+
+#include "xkb_dev.cuh"
+
+namespace xkb {
+
+template <class T>
+struct St;
+template <>
+struct St<float> {
+  using S = float;
+  static constexpr int W = 1;
+  static constexpr bool CPLX = false;
+  static constexpr CUtensorMapDataType DT = CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+};
+template <>
+struct St<double> {
+  using S = double;
+  static constexpr int W = 1;
+  static constexpr bool CPLX = false;
+  static constexpr CUtensorMapDataType DT = CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+};
+template <>
+struct St<float2> {
+  using S = float;
+  static constexpr int W = 2;
+  static constexpr bool CPLX = true;
+  static constexpr CUtensorMapDataType DT = CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+};
+template <>
+struct St<double2> {
+  using S = double;
+  static constexpr int W = 2;
+  static constexpr bool CPLX = true;
+  static constexpr CUtensorMapDataType DT = CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+};
+
+struct GemmParams {
+  int M, N, K;
+  void* C;
+  long ldc;
+  double ar, ai, br, bi;
+  int uplo, herm_diag;
+  long diag;
+  int conjA, conjB;
+  int tiles_m, tiles_n, ktiles;
+};
+
+constexpr int kBK = 16;      // k extent of one pipeline stage
+constexpr int kStages = 4;
+constexpr int kConsumerWarps = 8;
+constexpr int kThreads = kConsumerWarps * 32;
+
+__device__ __forceinline__ void dmma_k8(double (&d)[4], const double (&a)[4],
+                                        const double (&b)[2]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 "
+      "{%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+      : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+      : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
+}
+
+template <class T>
+__device__ __forceinline__ void ld_elem(const typename St<T>::S* s, int e, double& re,
+                                        double& im) {
+  if constexpr (St<T>::CPLX) {
+    re = static_cast<double>(s[2 * e]);
+    im = static_cast<double>(s[2 * e + 1]);
+  } else {
+    re = static_cast<double>(s[e]);
+    im = 0.0;
+  }
+}
+
+__device__ __forceinline__ bool in_mask(int uplo, long diag, int row, int col) {
+  if (uplo == XKB_LOWER) return (long)row + diag >= (long)col;
+  if (uplo == XKB_UPPER) return (long)row + diag <= (long)col;
+  return true;
+}
+
+// A_KC: op(A) != N, A tile stored [BM][BK] (k contiguous), else [BK][BM].
+// B_KC: op(B) == N, B tile stored [BN][BK], else [BK][BN].
+template <class T, int BM, int BN, bool A_KC, bool B_KC>
+__global__ void __launch_bounds__(kThreads, 1)
+    k_gemm_dmma(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                const GemmParams p) {
+  using S = typename St<T>::S;
+  constexpr int W = St<T>::W;
+  constexpr bool CPLX = St<T>::CPLX;
+  constexpr int WTM = BM / 2, WTN = BN / 4;   // 2 x 4 consumer warps
+  constexpr int MF = WTM / 16, NF = WTN / 8;
+  constexpr uint32_t A_BYTES = BM * kBK * sizeof(T);
+  constexpr uint32_t B_BYTES = BN * kBK * sizeof(T);
+  constexpr uint32_t STAGE_BYTES = A_BYTES + B_BYTES;
+  constexpr int NACC = CPLX ? 8 : 4;
+
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* base =
+      reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
+  uint64_t* full = reinterpret_cast<uint64_t*>(base + kStages * STAGE_BYTES);
+  uint64_t* empty = full + kStages;
+
+  // grouped rasterisation: 8 tile rows share a band of B columns in L2
+  const int GROUP = 8;
+  const int span = GROUP * p.tiles_n;
+  const int bid = blockIdx.x;
+  const int first_m = (bid / span) * GROUP;
+  const int gsz = min(p.tiles_m - first_m, GROUP);
+  const int tm = first_m + (bid % span) % gsz;
+  const int tn = (bid % span) / gsz;
+  const int m0 = tm * BM, n0 = tn * BN;
+
+  if (p.uplo == XKB_LOWER && (long)(m0 + BM - 1) + p.diag < (long)n0) return;
+  if (p.uplo == XKB_UPPER && (long)m0 + p.diag > (long)(n0 + BN - 1)) return;
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kStages; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], kConsumerWarps);
+    }
+    fence_barrier_init();
+  }
+  __syncthreads();
+
+  const int KT = p.ktiles;
+  // Thread 0 also drives the TMA ring: it fills every stage up front and
+  // refills stage s once all eight warps have released it.
+  auto issue = [&](int it) {
+    const int s = it % kStages;
+    uint8_t* sa = base + s * STAGE_BYTES;
+    uint8_t* sb = sa + A_BYTES;
+    mbar_expect_tx(&full[s], STAGE_BYTES);
+    const int k0 = it * kBK;
+    if (A_KC) tma_load_2d(sa, &tmA, k0 * W, m0, &full[s]);
+    else tma_load_2d(sa, &tmA, m0 * W, k0, &full[s]);
+    if (B_KC) tma_load_2d(sb, &tmB, k0 * W, n0, &full[s]);
+    else tma_load_2d(sb, &tmB, n0 * W, k0, &full[s]);
+  };
+  if (threadIdx.x == 0) {
+    tma_prefetch(&tmA);
+    tma_prefetch(&tmB);
+    for (int it = 0; it < kStages && it < KT; ++it) issue(it);
+  }
+
+  // ---------------- consumers: DMMA over the stage ring --------------------
+  const int wm = warp >> 2, wn = warp & 3;
+  const int g = lane >> 2, t = lane & 3;
+  double acc[MF][NF][NACC];
+#pragma unroll
+  for (int i = 0; i < MF; ++i)
+#pragma unroll
+    for (int j = 0; j < NF; ++j)
+#pragma unroll
+      for (int v = 0; v < NACC; ++v) acc[i][j][v] = 0.0;
+
+  const double sgnA = p.conjA ? -1.0 : 1.0;
+  const double sgnB = p.conjB ? -1.0 : 1.0;
+  bool ok = true;
+  for (int it = 0; it < KT; ++it) {
+    const int s = it % kStages;
+    const uint32_t ph = (it / kStages) & 1;
+    if (!mbar_wait(&full[s], ph, kErrFullWait)) {
+      ok = false;
+      break;
+    }
+    const S* sa = reinterpret_cast<const S*>(base + s * STAGE_BYTES);
+    const S* sb = reinterpret_cast<const S*>(base + s * STAGE_BYTES + A_BYTES);
+#pragma unroll
+    for (int kc = 0; kc < kBK / 8; ++kc) {
+      const int k0 = kc * 8 + 2 * t, k1 = k0 + 1;
+      double br[NF][2], bi[NF][2];
+#pragma unroll
+      for (int nf = 0; nf < NF; ++nf) {
+        const int n = wn * WTN + nf * 8 + g;
+        const int o0 = B_KC ? n * kBK + k0 : k0 * BN + n;
+        const int o1 = B_KC ? n * kBK + k1 : k1 * BN + n;
+        ld_elem<T>(sb, o0, br[nf][0], bi[nf][0]);
+        ld_elem<T>(sb, o1, br[nf][1], bi[nf][1]);
+        if (CPLX) {
+          bi[nf][0] *= sgnB;
+          bi[nf][1] *= sgnB;
+        }
+      }
+#pragma unroll
+      for (int mf = 0; mf < MF; ++mf) {
+        const int r0 = wm * WTM + mf * 16 + g, r1 = r0 + 8;
+        double ar[4], ai[4];
+        ld_elem<T>(sa, A_KC ? r0 * kBK + k0 : k0 * BM + r0, ar[0], ai[0]);
+        ld_elem<T>(sa, A_KC ? r1 * kBK + k0 : k0 * BM + r1, ar[1], ai[1]);
+        ld_elem<T>(sa, A_KC ? r0 * kBK + k1 : k1 * BM + r0, ar[2], ai[2]);
+        ld_elem<T>(sa, A_KC ? r1 * kBK + k1 : k1 * BM + r1, ar[3], ai[3]);
+        if constexpr (CPLX) {
+          double nai[4];
+#pragma unroll
+          for (int v = 0; v < 4; ++v) {
+            ai[v] *= sgnA;
+            nai[v] = -ai[v];
+          }
+#pragma unroll
+          for (int nf = 0; nf < NF; ++nf) {
+            double* a = acc[mf][nf];
+            double (&re)[4] = *reinterpret_cast<double(*)[4]>(a);
+            double (&im)[4] = *reinterpret_cast<double(*)[4]>(a + 4);
+            dmma_k8(re, ar, br[nf]);
+            dmma_k8(re, nai, bi[nf]);
+            dmma_k8(im, ar, bi[nf]);
+            dmma_k8(im, ai, br[nf]);
+          }
+        } else {
+#pragma unroll
+          for (int nf = 0; nf < NF; ++nf) {
+            double (&d)[4] = *reinterpret_cast<double(*)[4]>(acc[mf][nf]);
+            dmma_k8(d, ar, br[nf]);
+          }
+        }
+      }
+    }
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&empty[s]);
+    if (threadIdx.x == 0 && it + kStages < KT) {
+      if (!mbar_wait(&empty[s], ph, kErrEmptyWait)) {
+        ok = false;
+        break;
+      }
+      issue(it + kStages);
+    }
+  }
+  if (!ok) return;
+
+  // ---------------- epilogue: alpha/beta, mask, store ----------------------
+  S* C = reinterpret_cast<S*>(p.C);
+  const bool use_beta = (p.br != 0.0) || (p.bi != 0.0);
+#pragma unroll
+  for (int mf = 0; mf < MF; ++mf)
+#pragma unroll
+    for (int nf = 0; nf < NF; ++nf)
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int row = m0 + wm * WTM + mf * 16 + g + ((i >> 1) << 3);
+        const int col = n0 + wn * WTN + nf * 8 + 2 * t + (i & 1);
+        if (row >= p.M || col >= p.N || !in_mask(p.uplo, p.diag, row, col)) continue;
+        const size_t idx = (size_t)row + (size_t)col * (size_t)p.ldc;
+        if constexpr (CPLX) {
+          const double xr = acc[mf][nf][i], xi = acc[mf][nf][4 + i];
+          double vr = p.ar * xr - p.ai * xi;
+          double vi = p.ar * xi + p.ai * xr;
+          if (use_beta) {
+            const double cr = (double)C[2 * idx], ci = (double)C[2 * idx + 1];
+            vr += p.br * cr - p.bi * ci;
+            vi += p.br * ci + p.bi * cr;
+          }
+          if (p.herm_diag && (long)row + p.diag == (long)col) vi = 0.0;
+          C[2 * idx] = static_cast<S>(vr);
+          C[2 * idx + 1] = static_cast<S>(vi);
+        } else {
+          double v = p.ar * acc[mf][nf][i];
+          if (use_beta) v = fma(p.br, (double)C[idx], v);
+          C[idx] = static_cast<S>(v);
+        }
+      }
+}
+
+// C <- beta*C on the masked part (beta == 0 writes zeros without reading).
+template <class T>
+__global__ void k_scale(int M, int N, double br, double bi, T* Cv, long ldc, int uplo,
+                        int herm_diag, long diag) {
+  using S = typename St<T>::S;
+  S* C = reinterpret_cast<S*>(Cv);
+  const size_t total = (size_t)M * (size_t)N;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total;
+       e += (size_t)gridDim.x * blockDim.x) {
+    const int row = (int)(e % (size_t)M), col = (int)(e / (size_t)M);
+    if (!in_mask(uplo, diag, row, col)) continue;
+    const size_t idx = (size_t)row + (size_t)col * (size_t)ldc;
+    if constexpr (St<T>::CPLX) {
+      double cr = 0, ci = 0;
+      if (br != 0.0 || bi != 0.0) {
+        const double xr = (double)C[2 * idx], xi = (double)C[2 * idx + 1];
+        cr = br * xr - bi * xi;
+        ci = br * xi + bi * xr;
+      }
+      if (herm_diag && (long)row + diag == (long)col) ci = 0.0;
+      C[2 * idx] = (S)cr;
+      C[2 * idx + 1] = (S)ci;
+    } else {
+      C[idx] = (br != 0.0) ? (S)(br * (double)C[idx]) : (S)0;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// host side
+template <class T, int BM, int BN, bool A_KC, bool B_KC>
+static int launch_dmma(const xkb_gemm_args* a, cudaStream_t st) {
+  using S = typename St<T>::S;
+  constexpr int W = St<T>::W;
+  const int es = (int)sizeof(S);
+  CUtensorMap tA, tB;
+  // A stored (A_KC ? K x M : M x K), B stored (B_KC ? K x N : N x K)
+  const uint64_t a_rows = A_KC ? a->K : a->M, a_cols = A_KC ? a->M : a->K;
+  const uint64_t b_rows = B_KC ? a->K : a->N, b_cols = B_KC ? a->N : a->K;
+  if (!encode_tmap_2d(&tA, St<T>::DT, es, a->A, a_rows * W, a_cols, (uint64_t)a->lda * W,
+                      A_KC ? kBK * W : BM * W, A_KC ? BM : kBK, CU_TENSOR_MAP_SWIZZLE_NONE))
+    return XKB_EINVAL;
+  if (!encode_tmap_2d(&tB, St<T>::DT, es, a->B, b_rows * W, b_cols, (uint64_t)a->ldb * W,
+                      B_KC ? kBK * W : BN * W, B_KC ? BN : kBK, CU_TENSOR_MAP_SWIZZLE_NONE))
+    return XKB_EINVAL;
+  GemmParams p;
+  p.M = a->M;
+  p.N = a->N;
+  p.K = a->K;
+  p.C = a->C;
+  p.ldc = a->ldc;
+  p.ar = a->alpha[0];
+  p.ai = St<T>::CPLX ? a->alpha[1] : 0.0;
+  p.br = a->beta[0];
+  p.bi = St<T>::CPLX ? a->beta[1] : 0.0;
+  p.uplo = a->uplo;
+  p.herm_diag = a->herm_diag;
+  p.diag = a->diag;
+  p.conjA = (a->opA == XKB_OP_C);
+  p.conjB = (a->opB == XKB_OP_C);
+  p.tiles_m = (a->M + BM - 1) / BM;
+  p.tiles_n = (a->N + BN - 1) / BN;
+  p.ktiles = (a->K + kBK - 1) / kBK;
+  const size_t smem = kStages * (size_t)(BM + BN) * kBK * sizeof(T) + 2 * kStages * 8 + 128;
+  auto kern = k_gemm_dmma<T, BM, BN, A_KC, B_KC>;
+  static bool attr_done = false;  // one per instantiation
+  if (!attr_done) {
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+        cudaSuccess)
+      return XKB_ECUDA;
+    attr_done = true;
+  }
+  const long grid = (long)p.tiles_m * p.tiles_n;
+  kern<<<(unsigned)grid, kThreads, smem, st>>>(tA, tB, p);
+  count_launch();
+  return cudaPeekAtLastError() == cudaSuccess ? XKB_OK : XKB_ECUDA;
+}
+
+template <class T, int BM, int BN>
+static int dispatch_ops(const xkb_gemm_args* a, cudaStream_t st) {
+  const bool akc = a->opA != XKB_OP_N, bkc = a->opB == XKB_OP_N;
+  if (akc && bkc) return launch_dmma<T, BM, BN, true, true>(a, st);
+  if (akc && !bkc) return launch_dmma<T, BM, BN, true, false>(a, st);
+  if (!akc && bkc) return launch_dmma<T, BM, BN, false, true>(a, st);
+  return launch_dmma<T, BM, BN, false, false>(a, st);
+}
+
+template <class T>
+static int dispatch_type(const xkb_gemm_args* a, cudaStream_t st) {
+  constexpr bool CPLX = St<T>::CPLX;
+  constexpr int BMb = CPLX ? 64 : 128, BNb = 128;
+  const long tiles_big = (long)((a->M + BMb - 1) / BMb) * ((a->N + BNb - 1) / BNb);
+  if (tiles_big >= sm_count()) return dispatch_ops<T, BMb, BNb>(a, st);
+  return dispatch_ops<T, BMb / 2, BNb / 2>(a, st);
+}
+
+template <class T>
+static int launch_scale(int M, int N, const double* beta, void* C, long ldc, int uplo,
+                        int herm_diag, long diag, cudaStream_t st) {
+  const size_t total = (size_t)M * (size_t)N;
+  if (total == 0) return XKB_OK;
+  long blocks = (long)((total + 255) / 256);
+  if (blocks > 4L * sm_count() * 8) blocks = 4L * sm_count() * 8;
+  k_scale<T><<<(unsigned)blocks, 256, 0, st>>>(M, N, beta[0], St<T>::CPLX ? beta[1] : 0.0,
+                                               reinterpret_cast<T*>(C), ldc, uplo, herm_diag,
+                                               diag);
+  count_launch();
+  return cudaPeekAtLastError() == cudaSuccess ? XKB_OK : XKB_ECUDA;
+}
+
+}  // namespace xkb
+
+using namespace xkb;
+
+extern "C" int xkb_cuda_scale(int dtype, int M, int N, const double* beta, void* C, long ldc,
+                              int uplo, int herm_diag, long diag, void* stream) {
+  if (M < 0 || N < 0 || !beta) return XKB_EINVAL;
+  if (M == 0 || N == 0) return XKB_OK;
+  cudaStream_t st = resolve_stream(stream);
+  switch (dtype) {
+    case XKB_S: return launch_scale<float>(M, N, beta, C, ldc, uplo, herm_diag, diag, st);
+    case XKB_D: return launch_scale<double>(M, N, beta, C, ldc, uplo, herm_diag, diag, st);
+    case XKB_C: return launch_scale<float2>(M, N, beta, C, ldc, uplo, herm_diag, diag, st);
+    case XKB_Z: return launch_scale<double2>(M, N, beta, C, ldc, uplo, herm_diag, diag, st);
+  }
+  return XKB_EINVAL;
+}
+
+extern "C" int xkb_cuda_gemm(const xkb_gemm_args* a, void* stream) {
+  if (!a || a->M < 0 || a->N < 0 || a->K < 0) return XKB_EINVAL;
+  if (a->dtype < XKB_S || a->dtype > XKB_Z) return XKB_EINVAL;
+  if (a->opA < XKB_OP_N || a->opA > XKB_OP_C || a->opB < XKB_OP_N || a->opB > XKB_OP_C)
+    return XKB_EINVAL;
+  if (a->M == 0 || a->N == 0) return XKB_OK;
+  cudaStream_t st = resolve_stream(stream);
+  const bool cplx = (a->dtype == XKB_C || a->dtype == XKB_Z);
+  const bool alpha_zero = a->alpha[0] == 0.0 && (!cplx || a->alpha[1] == 0.0);
+  if (a->K == 0 || alpha_zero)
+    return xkb_cuda_scale(a->dtype, a->M, a->N, a->beta, a->C, a->ldc, a->uplo, a->herm_diag,
+                          a->diag, stream);
+  switch (a->dtype) {
+    case XKB_S: return dispatch_type<float>(a, st);
+    case XKB_D: return dispatch_type<double>(a, st);
+    case XKB_C: return dispatch_type<float2>(a, st);
+    case XKB_Z: return dispatch_type<double2>(a, st);
+  }
+  return XKB_EINVAL;
+}

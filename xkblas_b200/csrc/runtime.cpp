@@ -1,0 +1,751 @@
+// runtime.cpp -- lifecycle, device-resident tile directory, coherence and the
+// host-memory part of the xkblas.h API.
+//
+// The reference runs an XKaapi data-flow runtime with one host thread per
+// GPU and an MSI-like software DSM (kaapi/kaapi_memory.c).  On one B200 the
+// same contract is kept with much less machinery:
+//   * every matrix has one device buffer (allocated stream-ordered from the
+//     CUDA memory pool) and a tile directory of valid / dirty bits;
+//   * missing tiles are fetched by pinned asynchronous 2-D copies on a copy
+//     stream, coalesced into column panels; the compute stream waits on an
+//     event, so transfers of later calls overlap earlier compute;
+//   * xkblas_memory_coherent_async() queues device->host copies of the dirty
+//     tiles on a second copy stream after the producing kernels;
+//   * xkblas_sync() drains the three streams and reports device errors.
+#include "runtime.hpp"
+
+#include <algorithm>
+#include <cerrno>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <ctime>
+
+namespace xkb {
+void set_library_stream(cudaStream_t s);
+}
+
+namespace xkbrt {
+
+Runtime& rt() {
+  static Runtime* r = new Runtime();  // never destroyed: safe at exit
+  return *r;
+}
+
+static int cuda_ok(cudaError_t e) { return e == cudaSuccess ? XKB_OK : XKB_ECUDA; }
+
+int ensure_init() {
+  Runtime& R = rt();
+  if (R.ready) return XKB_OK;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n <= 0) {
+    cudaGetLastError();
+    return XKB_ENODEV;
+  }
+  int dev = 0;
+  if (const char* g = getenv("XKBLAS_GPUSET")) dev = atoi(g);
+  if (dev < 0 || dev >= n) dev = 0;
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) return XKB_ENODEV;
+  if (prop.major != 10) return XKB_ENODEV;  // kernels are built for sm_100a only
+  if (cudaSetDevice(dev) != cudaSuccess) return XKB_ENODEV;
+  R.device = dev;
+  if (cudaStreamCreateWithFlags(&R.s_comp, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&R.s_h2d, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&R.s_d2h, cudaStreamNonBlocking) != cudaSuccess)
+    return XKB_ECUDA;
+  for (auto& e : R.ev_pool)
+    if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return XKB_ECUDA;
+  // keep freed pool memory cached: the directory allocates and frees often
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+    uint64_t thr = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+  }
+  xkb::set_library_stream(R.s_comp);
+  if (const char* t = getenv("XKBLAS_TILE_SIZE")) R.nb_param = (size_t)atol(t);
+  else if (const char* b = getenv("XKBLAS_BLOC_SIZE")) R.nb_param = (size_t)atol(b);
+  if (const char* m = getenv("XKBLAS_DEFAULT_MATH")) {
+    if (!strcmp(m, "TC") || !strcmp(m, "tensorcore")) R.math = XKBLAS_TENSOR_OP_MATH;
+    else R.math = XKBLAS_DEFAULT_MATH;
+  }
+  if (const char* s = getenv("XKBLAS_OZAKI_SLICES")) R.ozaki_moduli = atoi(s);
+  if (const char* s = getenv("XKBLAS_OZAKI_MIN_DIM")) R.ozaki_min_dim = atol(s);
+  R.ready = true;
+  return XKB_OK;
+}
+
+// Events are recycled round-robin; 64 in flight is far more than any call
+// sequence keeps outstanding between two stream waits.
+cudaEvent_t next_event() {
+  Runtime& R = rt();
+  cudaEvent_t e = R.ev_pool[R.ev_next];
+  R.ev_next = (R.ev_next + 1) % 64;
+  return e;
+}
+
+static size_t round_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+void* dev_ptr(const Desc* d, size_t r, size_t c) {
+  return static_cast<char*>(d->dev) + (r + c * d->dld) * d->esz;
+}
+
+void* scratch_alloc(size_t bytes) {
+  void* p = nullptr;
+  if (cudaMallocAsync(&p, std::max<size_t>(bytes, 256), rt().s_comp) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  return p;
+}
+void scratch_free(void* p) {
+  if (p) cudaFreeAsync(p, rt().s_comp);
+}
+
+static void free_desc_memory(Desc* d) {
+  Runtime& R = rt();
+  if (d->dev) {
+    // D2H copies and kernels may still read the buffer: order the free
+    // after both streams.
+    cudaEvent_t e = next_event();
+    cudaEventRecord(e, R.s_d2h);
+    cudaStreamWaitEvent(R.s_comp, e, 0);
+    cudaEvent_t e2 = next_event();
+    cudaEventRecord(e2, R.s_h2d);
+    cudaStreamWaitEvent(R.s_comp, e2, 0);
+    cudaFreeAsync(d->dev, R.s_comp);
+    d->dev = nullptr;
+  }
+}
+
+void drop_desc(Desc* d) {
+  Runtime& R = rt();
+  free_desc_memory(d);
+  R.descs.erase(d->host);
+  delete d;
+}
+
+// Copy back every dirty tile of d synchronously (used before a descriptor
+// must be rebuilt because a call reuses its pointer with another shape).
+static int flush_sync(Desc* d) {
+  int e = coherent(d, 0, 0);
+  if (e) return e;
+  return cuda_ok(cudaStreamSynchronize(rt().s_d2h));
+}
+
+static int alloc_desc(Desc* d) {
+  Runtime& R = rt();
+  const size_t align = std::max<size_t>(1, 128 / d->esz);  // 128-byte columns
+  d->dld = round_up(std::max<size_t>(d->M, 1), align);
+  const size_t bytes = d->dld * std::max<size_t>(d->N, 1) * d->esz;
+  void* p = nullptr;
+  if (cudaMallocAsync(&p, bytes, R.s_comp) != cudaSuccess) {
+    cudaGetLastError();
+    return XKB_ENOMEM;
+  }
+  d->dev = p;
+  // the copy stream must see the allocation
+  cudaEvent_t e = next_event();
+  cudaEventRecord(e, R.s_comp);
+  cudaStreamWaitEvent(R.s_h2d, e, 0);
+  return XKB_OK;
+}
+
+Desc* get_desc(const void* host, size_t M, size_t N, size_t ld, size_t esz, size_t NB,
+               int* err) {
+  Runtime& R = rt();
+  *err = XKB_OK;
+  auto it = R.descs.find(host);
+  if (it != R.descs.end()) {
+    Desc* d = it->second;
+    if (d->ld == ld && d->esz == esz && M <= d->M && N <= d->N) return d;
+    // Same pointer, different geometry: write back, rebuild.
+    if ((*err = flush_sync(d)) != XKB_OK) return nullptr;
+    drop_desc(d);
+  }
+  Desc* d = new Desc();
+  d->host = const_cast<void*>(host);
+  d->M = M;
+  d->N = N;
+  d->ld = ld;
+  d->esz = esz;
+  d->mb = d->nb = std::max<size_t>(NB, 1);
+  d->mt = std::max<size_t>(1, (M + d->mb - 1) / d->mb);
+  d->nt = std::max<size_t>(1, (N + d->nb - 1) / d->nb);
+  d->st.assign(d->mt * d->nt, 0);
+  d->registered_init = true;
+  if ((*err = alloc_desc(d)) != XKB_OK) {
+    delete d;
+    return nullptr;
+  }
+  R.descs[host] = d;
+  return d;
+}
+
+// H2D of rows [r0,r1) x cols [c0,c1) of the host view.
+static int copy_h2d(Desc* d, size_t r0, size_t r1, size_t c0, size_t c1) {
+  Runtime& R = rt();
+  if (r1 <= r0 || c1 <= c0) return XKB_OK;
+  const char* src = static_cast<const char*>(d->host) + (r0 + c0 * d->ld) * d->esz;
+  char* dst = static_cast<char*>(dev_ptr(d, r0, c0));
+  const size_t w = (r1 - r0) * d->esz;
+  cudaError_t e = cudaMemcpy2DAsync(dst, d->dld * d->esz, src, d->ld * d->esz, w, c1 - c0,
+                                    cudaMemcpyHostToDevice, R.s_h2d);
+  R.stats.h2d += w * (c1 - c0);
+  return cuda_ok(e);
+}
+
+static int copy_d2h(Desc* d, size_t r0, size_t r1, size_t c0, size_t c1) {
+  Runtime& R = rt();
+  if (r1 <= r0 || c1 <= c0) return XKB_OK;
+  char* dst = static_cast<char*>(d->host) + (r0 + c0 * d->ld) * d->esz;
+  const char* src = static_cast<const char*>(dev_ptr(d, r0, c0));
+  const size_t w = (r1 - r0) * d->esz;
+  cudaError_t e = cudaMemcpy2DAsync(dst, d->ld * d->esz, src, d->dld * d->esz, w, c1 - c0,
+                                    cudaMemcpyDeviceToHost, R.s_d2h);
+  R.stats.d2h += w * (c1 - c0);
+  return cuda_ok(e);
+}
+
+// For each tile column in [tc0, tc1) find runs of tiles whose state
+// satisfies `want`; whole-height runs of consecutive tile columns merge into
+// one 2-D copy.  `fn(r0, r1, c0, c1)` issues the copy.
+template <class Pred, class Fn>
+static int for_runs(Desc* d, size_t tr0, size_t tr1, size_t tc0, size_t tc1, Pred want,
+                    Fn fn) {
+  size_t pend_c0 = 0, pend_c1 = 0;  // pending full-height column range
+  bool pend = false;
+  auto flush = [&]() -> int {
+    if (!pend) return XKB_OK;
+    pend = false;
+    return fn(tr0 * d->mb, std::min(tr1 * d->mb, d->M), pend_c0 * d->nb,
+              std::min(pend_c1 * d->nb, d->N));
+  };
+  for (size_t j = tc0; j < tc1; ++j) {
+    bool all = true;
+    for (size_t i = tr0; i < tr1 && all; ++i) all = want(d->tile(i, j), i, j);
+    if (all) {
+      if (pend && pend_c1 == j) pend_c1 = j + 1;
+      else {
+        int e = flush();
+        if (e) return e;
+        pend = true;
+        pend_c0 = j;
+        pend_c1 = j + 1;
+      }
+      continue;
+    }
+    int e = flush();
+    if (e) return e;
+    size_t i = tr0;
+    while (i < tr1) {
+      if (!want(d->tile(i, j), i, j)) {
+        ++i;
+        continue;
+      }
+      size_t i1 = i;
+      while (i1 < tr1 && want(d->tile(i1, j), i1, j)) ++i1;
+      e = fn(i * d->mb, std::min(i1 * d->mb, d->M), j * d->nb, std::min((j + 1) * d->nb, d->N));
+      if (e) return e;
+      i = i1;
+    }
+  }
+  return flush();
+}
+
+int make_valid(Desc* d, size_t r0, size_t r1, size_t c0, size_t c1) {
+  Runtime& R = rt();
+  if (r1 <= r0 || c1 <= c0) return XKB_OK;
+  const size_t tr0 = r0 / d->mb, tr1 = (r1 + d->mb - 1) / d->mb;
+  const size_t tc0 = c0 / d->nb, tc1 = (c1 + d->nb - 1) / d->nb;
+  uint64_t miss = 0, hit = 0;
+  for (size_t j = tc0; j < tc1; ++j)
+    for (size_t i = tr0; i < tr1; ++i) (d->tile(i, j) & kDevValid) ? ++hit : ++miss;
+  R.stats.hits += hit;
+  R.stats.misses += miss;
+  if (miss == 0) return XKB_OK;
+  int e = for_runs(
+      d, tr0, tr1, tc0, tc1, [](uint8_t s, size_t, size_t) { return !(s & kDevValid); },
+      [&](size_t a, size_t b, size_t c, size_t dd) { return copy_h2d(d, a, b, c, dd); });
+  if (e) return e;
+  for (size_t j = tc0; j < tc1; ++j)
+    for (size_t i = tr0; i < tr1; ++i) d->tile(i, j) |= kDevValid;
+  cudaEvent_t ev = next_event();
+  cudaEventRecord(ev, R.s_h2d);
+  return cuda_ok(cudaStreamWaitEvent(R.s_comp, ev, 0));
+}
+
+static bool tile_in_uplo(const Desc* d, size_t i, size_t j, int uplo) {
+  // tile (i,j) intersects the uplo triangle of the matrix
+  const size_t r0 = i * d->mb, r1 = std::min((i + 1) * d->mb, d->M);
+  const size_t c0 = j * d->nb, c1 = std::min((j + 1) * d->nb, d->N);
+  if (uplo == CblasLower) return r1 > c0;   // some row >= some col
+  if (uplo == CblasUpper) return c1 > r0;
+  (void)r0;
+  return true;
+}
+
+void mark_written(Desc* d, size_t r0, size_t r1, size_t c0, size_t c1, int uplo) {
+  if (r1 <= r0 || c1 <= c0) return;
+  const size_t tr0 = r0 / d->mb, tr1 = (r1 + d->mb - 1) / d->mb;
+  const size_t tc0 = c0 / d->nb, tc1 = (c1 + d->nb - 1) / d->nb;
+  for (size_t j = tc0; j < tc1; ++j)
+    for (size_t i = tr0; i < tr1; ++i)
+      if (!uplo || tile_in_uplo(d, i, j, uplo)) d->tile(i, j) |= kDevValid | kHostStale;
+}
+
+void mark_full_overwrite(Desc* d, size_t r0, size_t r1, size_t c0, size_t c1) {
+  mark_written(d, r0, r1, c0, c1, 0);
+}
+
+int coherent(Desc* d, int uplo, int memflag) {
+  Runtime& R = rt();
+  // D2H after everything already queued on the compute stream
+  cudaEvent_t ev = next_event();
+  cudaEventRecord(ev, R.s_comp);
+  cudaStreamWaitEvent(R.s_d2h, ev, 0);
+  int e = for_runs(
+      d, 0, d->mt, 0, d->nt,
+      [&](uint8_t s, size_t i, size_t j) {
+        return (s & kHostStale) && (uplo == 0 || tile_in_uplo(d, i, j, uplo));
+      },
+      [&](size_t a, size_t b, size_t c, size_t dd) { return copy_d2h(d, a, b, c, dd); });
+  if (e) return e;
+  for (size_t j = 0; j < d->nt; ++j)
+    for (size_t i = 0; i < d->mt; ++i) {
+      uint8_t& s = d->tile(i, j);
+      const bool in = uplo == 0 || tile_in_uplo(d, i, j, uplo);
+      if (in) s &= (uint8_t)~kHostStale;
+      else if (memflag == 1) s = 0;  // strict mode: the other part is dropped
+    }
+  return XKB_OK;
+}
+
+size_t auto_tilesize(xkblas_kernel_t kernel, size_t M, size_t N, size_t K) {
+  // reference blas/xkblas.c:2239-2533 with one GPU; a preset NB wins.
+  (void)N;
+  (void)K;
+  Runtime& R = rt();
+  if (R.nb_param) return R.nb_param;
+  const size_t ng = 1;
+  size_t NB = 0, fact = 1;
+  switch (kernel) {
+    case KERN_GEMM:
+    case KERN_GEMMT:
+      NB = M / ng;
+      if (M > 16384 && NB < 2048) NB = 2048;
+      if (NB > 4096) NB = M / (2 * ng);
+      if (NB < 512) NB = 512;
+      NB = (NB + 63) & ~size_t(63);
+      break;
+    case KERN_HERK:
+    case KERN_SYRK:
+      fact = 2;
+      for (;;) {
+        NB = M / (fact * ng);
+        if (NB >= 2048) NB &= ~size_t(2047);
+        if (NB <= 1024 && fact == 2) {
+          fact = 1;
+          continue;
+        }
+        break;
+      }
+      if (NB > 4096) NB = M / (2 * fact * ng);
+      if (NB < 512) NB = 512;
+      break;
+    case KERN_HER2K:
+    case KERN_SYR2K:
+      fact = 4;
+      for (;;) {
+        NB = (M / (fact * ng) + 63) & ~size_t(63);
+        if (NB <= 2048 && fact > 2) {
+          --fact;
+          continue;
+        }
+        break;
+      }
+      if (NB > 4096) NB = M / (2 * fact * ng);
+      if (NB < 512) NB = 512;
+      break;
+    case KERN_HEMM:
+    case KERN_SYMM:
+      NB = (M / ng) & ~size_t(1023);
+      if (NB < 1024) NB = 1024;
+      if (NB < 4096) NB *= 2;
+      break;
+    case KERN_TRMM:
+    case KERN_TRSM:
+      NB = (M / (2 * ng) + 63) & ~size_t(63);
+      if (NB < 2048) NB = 2048;
+      break;
+    default:
+      NB = M / ng;
+      if (NB >= 4096) NB = M / (2 * ng);
+      if (NB < 1024) NB = 1024;
+      NB = (NB + 63) & ~size_t(63);
+      break;
+  }
+  return std::max<size_t>(NB, 64);
+}
+
+}  // namespace xkbrt
+
+using namespace xkbrt;
+
+// ============================================================================
+// C API: lifecycle, parameters, memory, coherence
+// ============================================================================
+extern "C" {
+
+int xkblas_get_devicecount(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
+
+int xkblas_init(void) {
+  Runtime& R = rt();
+  std::lock_guard<std::recursive_mutex> g(R.mu);
+  if (R.refcount++ != 0) return 0;
+  int e = ensure_init();
+  return e == XKB_OK ? 0 : e;
+}
+
+int xkblas_finalize(void) {
+  Runtime& R = rt();
+  std::lock_guard<std::recursive_mutex> g(R.mu);
+  if (R.refcount == 0) return 0;
+  if (--R.refcount != 0) return 0;
+  if (!R.ready) return 0;
+  cudaStreamSynchronize(R.s_comp);
+  cudaStreamSynchronize(R.s_h2d);
+  cudaStreamSynchronize(R.s_d2h);
+  std::vector<Desc*> all;
+  for (auto& kv : R.descs) all.push_back(kv.second);
+  for (Desc* d : all) drop_desc(d);
+  cudaStreamSynchronize(R.s_comp);
+  return 0;
+}
+
+int xkblas_get_device_count(int* count) {
+  if (!count) return EINVAL;
+  *count = xkblas_get_devicecount() > 0 ? 1 : 0;
+  return 0;
+}
+
+int xkblas_get_device_properties(struct xkblas_dev_prop_t* prop) {
+  if (!prop) return EINVAL;
+  prop->device_count = xkblas_get_devicecount() > 0 ? 1 : 0;
+  prop->has_unified = 0;
+  prop->arch = XKBLAS_ARCH_UNKNOWN;
+  if (prop->device_count) {
+    cudaDeviceProp p;
+    if (cudaGetDeviceProperties(&p, rt().device) == cudaSuccess && p.major == 10)
+      prop->arch = XKBLAS_ARCH_B200;
+  }
+  return 0;
+}
+
+int xkblas_force_set_unified(void) { return EINVAL; }
+
+const char* xkblas_get_configuration(void) {
+  return "xkblas-b200 0.6: sm_100a; FP64 DMMA (TMA+mbarrier) tile GEMM; Ozaki-II INT8 "
+         "tcgen05/TMEM; device tile directory; 1 GPU";
+}
+
+void xkblas_load_sym(void** ptr, const char* name);  // native.cpp
+
+int xkblas_sync(void) {
+  Runtime& R = rt();
+  std::lock_guard<std::recursive_mutex> g(R.mu);
+  if (!R.ready) return 0;
+  int e = XKB_OK;
+  if (cudaStreamSynchronize(R.s_comp) != cudaSuccess) e = XKB_ECUDA;
+  if (cudaStreamSynchronize(R.s_h2d) != cudaSuccess) e = XKB_ECUDA;
+  if (cudaStreamSynchronize(R.s_d2h) != cudaSuccess) e = XKB_ECUDA;
+  int de = xkb_cuda_take_device_error();
+  if (de) {
+    R.sticky_error = de;
+    e = XKB_ETIMEDOUT;
+  }
+  return e;
+}
+
+int xkblas_last_device_error(void) {
+  Runtime& R = rt();
+  std::lock_guard<std::recursive_mutex> g(R.mu);
+  int v = R.sticky_error;
+  R.sticky_error = 0;
+  return v;
+}
+
+xkblas_context_t* xkblas_context_get(void) {
+  // one runtime per process; the handle is an opaque non-null token
+  return reinterpret_cast<xkblas_context_t*>(&rt());
+}
+
+void xkblas_set_modemath(xkblas_mode_math_t mode) {
+  Runtime& R = rt();
+  std::lock_guard<std::recursive_mutex> g(R.mu);
+  R.math = (mode == XKBLAS_TENSOR_OP_MATH) ? XKBLAS_TENSOR_OP_MATH : XKBLAS_DEFAULT_MATH;
+}
+
+size_t xkblas_get_param(void) { return rt().nb_param; }
+void xkblas_set_param(size_t nb, size_t p) {
+  Runtime& R = rt();
+  std::lock_guard<std::recursive_mutex> g(R.mu);
+  R.nb_param = nb;
+  R.prec_param = p ? p : 8;
+}
+int xkblas_get_ngpus(void) { return xkblas_get_devicecount() > 0 ? 1 : 0; }
+int xkblas_set_ngpus(int ngpus) { return (ngpus == 1 || ngpus == 0) ? 0 : EINVAL; }
+
+uint64_t xkblas_elapsedns(void) {
+  return (uint64_t)std::chrono::duration_cast<std::chrono::nanoseconds>(
+             std::chrono::steady_clock::now().time_since_epoch())
+      .count();
+}
+double xkblas_elapsedtime(void) { return 1e-9 * (double)xkblas_elapsedns(); }
+
+size_t xkblas_auto_tilesize(xkblas_context_t* ctx, xkblas_kernel_t kernel, size_t M,
+                            size_t N, size_t K) {
+  (void)ctx;
+  return auto_tilesize(kernel, M, N, K);
+}
+
+// ---- descriptors -----------------------------------------------------------
+xkblas_matrix_descr_t* xkblas_find(const void* A) {
+  Runtime& R = rt();
+  std::lock_guard<std::recursive_mutex> g(R.mu);
+  auto it = R.descs.find(A);
+  return it == R.descs.end() ? nullptr : reinterpret_cast<xkblas_matrix_descr_t*>(it->second);
+}
+
+int xkblas_matrix_descr_isinit(xkblas_matrix_descr_t* Ah) {
+  return Ah && reinterpret_cast<Desc*>(Ah)->registered_init;
+}
+
+int xkblas_init_matrix_handle(xkblas_matrix_descr_t* Ah, void* A, size_t M, size_t N,
+                              size_t LD, size_t eltsize, size_t MB, size_t NB) {
+  // Descriptors are created by the library on first touch; this entry point
+  // (re)creates the one of A with the given geometry.
+  (void)Ah;
+  Runtime& R = rt();
+  std::lock_guard<std::recursive_mutex> g(R.mu);
+  if (!A || LD < std::max<size_t>(M, 1) || eltsize == 0) return EINVAL;
+  if (ensure_init() != XKB_OK) return ENODEV;
+  int err;
+  Desc* d = get_desc(A, M, N, LD, eltsize, std::max(MB, NB), &err);
+  return d ? 0 : EINVAL;
+}
+
+// ---- host memory -----------------------------------------------------------
+void* xkblas_malloc(size_t sz) {
+  void* p = nullptr;
+  if (cudaHostAlloc(&p, std::max<size_t>(sz, 1), cudaHostAllocPortable) != cudaSuccess) {
+    cudaGetLastError();
+    return malloc(std::max<size_t>(sz, 1));  // no driver: plain host memory
+  }
+  return p;
+}
+
+void xkblas_free(void* ptr, size_t sz) {
+  (void)sz;
+  if (!ptr) return;
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, ptr) == cudaSuccess && a.type == cudaMemoryTypeHost) {
+    cudaFreeHost(ptr);
+    return;
+  }
+  cudaGetLastError();
+  free(ptr);
+}
+
+int xkblas_malloc_unified(void** ptr, size_t size) {
+  if (!ptr) return EINVAL;
+  *ptr = malloc(std::max<size_t>(size, 1));  // no unified memory path on B200+x86
+  return *ptr ? 0 : EINVAL;
+}
+int xkblas_free_unified(void* ptr) {
+  free(ptr);
+  return 0;
+}
+void xkblas_activate_custom_alloc(void) {}
+void xkblas_deactivate_custom_alloc(void) {}
+
+// Host registration is synchronous here (cudaHostRegister is fast on this
+// platform); the async forms return a handle that is already complete.
+uint64_t xkblas_register_memory_async(void* ptr, size_t sz) {
+  return xkblas_register_memory(ptr, sz) == 0 ? (uint64_t)(uintptr_t)ptr : 0;
+}
+uint64_t xkblas_unregister_memory_async(void* ptr, size_t sz) {
+  return xkblas_unregister_memory(ptr, sz) == 0 ? (uint64_t)(uintptr_t)ptr : 0;
+}
+int xkblas_register_memory_test(uint64_t h) { return h != 0; }
+int xkblas_register_memory_wait(uint64_t h) { return h ? 0 : EINVAL; }
+int xkblas_register_memory_waitall(void) { return 0; }
+int xkblas_register_memory(void* ptr, size_t sz) {
+  if (!ptr || !sz) return EINVAL;
+  cudaError_t e = cudaHostRegister(ptr, sz, cudaHostRegisterPortable);
+  if (e == cudaErrorHostMemoryAlreadyRegistered || e == cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  cudaGetLastError();
+  return EINVAL;
+}
+int xkblas_unregister_memory(void* ptr, size_t sz) {
+  (void)sz;
+  if (!ptr) return EINVAL;
+  cudaError_t e = cudaHostUnregister(ptr);
+  cudaGetLastError();
+  return (e == cudaSuccess || e == cudaErrorHostMemoryNotRegistered) ? 0 : EINVAL;
+}
+void xkblas_memset(void* ptr, int v, size_t sz) {
+  if (ptr) memset(ptr, v, sz);
+}
+void xkblas_memcpy(void* dst, void* src, size_t sz) {
+  if (dst && src) memcpy(dst, src, sz);
+}
+void xkblas_register_work_buffer(void* ptr, size_t sz) { xkblas_register_memory(ptr, sz); }
+void xkblas_unregister_work_buffer(void* ptr) { xkblas_unregister_memory(ptr, 0); }
+void* xkblas_get_work_pos(size_t sz) { return xkblas_malloc(sz); }
+void xkblas_free_work_pos(void* ptr) { xkblas_free(ptr, 0); }
+void xkblas_bind_cpu(void* ptr, size_t sz) {
+  (void)ptr;
+  (void)sz;
+}
+void xkblas_host_register_direct(void* ptr, size_t sz) { xkblas_register_memory(ptr, sz); }
+void xkblas_host_unregister_direct(void* ptr) { xkblas_unregister_memory(ptr, 0); }
+
+// ---- debug / placement: one GPU ------------------------------------------
+int xkblas_dbg_setname(const char* name, xkblas_matrix_descr_t* Mh) {
+  return xkblas_dbg_setname_with_flags(name, Mh, 0);
+}
+int xkblas_dbg_setname_with_flags(const char* name, xkblas_matrix_descr_t* Mh,
+                                  uint32_t flags) {
+  (void)flags;
+  if (!Mh || !name) return EINVAL;
+  reinterpret_cast<Desc*>(Mh)->name = name;
+  return 0;
+}
+void xkblas_dbg_dump_graph(const char* name) { (void)name; }
+int xkblas_map_2Dblock_cyclic(xkblas_context_t* ctx, int hlevel, int storage, size_t m,
+                              size_t n, const void* A, size_t ld, size_t eltsize, size_t Bp,
+                              size_t Bq, size_t Gp, size_t Gq, int force) {
+  (void)ctx; (void)hlevel; (void)storage; (void)m; (void)n; (void)ld; (void)eltsize;
+  (void)Bp; (void)Bq; (void)force;
+  if (!A || Gp == 0 || Gq == 0) return EINVAL;
+  return 0;
+}
+int xkblas_map_1Dblock_cyclic(xkblas_context_t* ctx, int hlevel, int storage, int colrow,
+                              size_t m, size_t n, const void* A, size_t ld, size_t eltsize,
+                              size_t B, size_t G, int force) {
+  (void)ctx; (void)hlevel; (void)storage; (void)colrow; (void)m; (void)n; (void)ld;
+  (void)eltsize; (void)B; (void)force;
+  if (!A || G == 0) return EINVAL;
+  return 0;
+}
+int xkblas_distribute_2Dblock_cyclic_async(int hlevel, int storage, int uplo, size_t NB,
+                                           size_t m, size_t n, const void* A, size_t ld,
+                                           size_t eltsize, size_t Bp, size_t Bq, size_t Gp,
+                                           size_t Gq) {
+  (void)hlevel; (void)storage; (void)Bp; (void)Bq; (void)Gp; (void)Gq;
+  // one GPU: "distribute" = upload the tiles now
+  Runtime& R = rt();
+  std::lock_guard<std::recursive_mutex> g(R.mu);
+  if (!A || ld < m || eltsize == 0) return EINVAL;
+  if (ensure_init() != XKB_OK) return ENODEV;
+  int err;
+  Desc* d = get_desc(A, m, n, ld, eltsize, NB ? NB : auto_tilesize(KERN_GEMM, m, n, 0), &err);
+  if (!d) return EINVAL;
+  (void)uplo;
+  return make_valid(d, 0, m, 0, n) ? EINVAL : 0;
+}
+int xkblas_distribute_1Dblock_cyclic_async(int hlevel, int storage, int uplo, int colrow,
+                                           size_t NB, size_t m, size_t n, const void* A,
+                                           size_t ld, size_t eltsize, size_t B, size_t G) {
+  (void)colrow; (void)B; (void)G;
+  return xkblas_distribute_2Dblock_cyclic_async(hlevel, storage, uplo, NB, m, n, A, ld, eltsize,
+                                                1, 1, 1, 1);
+}
+
+// ---- coherence ---------------------------------------------------------------
+int xkblas_memory_coherent_async(int uplo, int memflag, size_t M, size_t N, void* A, size_t ld,
+                                 size_t elsize) {
+  Runtime& R = rt();
+  std::lock_guard<std::recursive_mutex> g(R.mu);
+  if (!R.ready) return 0;
+  if (uplo != 0 && uplo != CblasUpper && uplo != CblasLower) return EINVAL;
+  auto it = R.descs.find(A);
+  if (it == R.descs.end()) return 0;  // never used on the device: host is current
+  Desc* d = it->second;
+  (void)M; (void)N; (void)ld; (void)elsize;
+  return coherent(d, uplo, memflag) ? EINVAL : 0;
+}
+
+int xkblas_memory_syncall(void) {
+  Runtime& R = rt();
+  std::lock_guard<std::recursive_mutex> g(R.mu);
+  if (!R.ready) return 0;
+  for (auto& kv : R.descs)
+    if (coherent(kv.second, 0, 0)) return EINVAL;
+  return xkblas_sync() ? EINVAL : 0;
+}
+
+int xkblas_memory_invalidate(const void* A) {
+  Runtime& R = rt();
+  std::lock_guard<std::recursive_mutex> g(R.mu);
+  auto it = R.descs.find(A);
+  if (it == R.descs.end()) return 0;
+  drop_desc(it->second);
+  return 0;
+}
+
+int xkblas_memory_invalidate_caches(void) {
+  Runtime& R = rt();
+  std::lock_guard<std::recursive_mutex> g(R.mu);
+  std::vector<Desc*> all;
+  for (auto& kv : R.descs) all.push_back(kv.second);
+  for (Desc* d : all) drop_desc(d);
+  return 0;
+}
+
+int xkblas_memory_free(void) {
+  Runtime& R = rt();
+  std::lock_guard<std::recursive_mutex> g(R.mu);
+  xkblas_memory_invalidate_caches();
+  if (!R.ready) return 0;
+  cudaStreamSynchronize(R.s_comp);
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, R.device) == cudaSuccess) cudaMemPoolTrimTo(pool, 0);
+  return 0;
+}
+
+int xkblas_get_stats(xkblas_stats_t* st) {
+  if (!st) return EINVAL;
+  Runtime& R = rt();
+  std::lock_guard<std::recursive_mutex> g(R.mu);
+  st->calls = R.stats.calls;
+  st->kernels = xkb_cuda_kernel_count();
+  st->h2d_bytes = R.stats.h2d;
+  st->d2h_bytes = R.stats.d2h;
+  st->tile_hits = R.stats.hits;
+  st->tile_misses = R.stats.misses;
+  st->ozaki_calls = R.stats.ozaki_calls;
+  st->ozaki_moduli = R.stats.ozaki_moduli;
+  st->flops = R.stats.flops;
+  return 0;
+}
+
+void xkblas_reset_stats(void) {
+  Runtime& R = rt();
+  std::lock_guard<std::recursive_mutex> g(R.mu);
+  R.stats = Stats();
+}
+
+}  // extern "C"

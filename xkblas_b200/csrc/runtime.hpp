@@ -1,0 +1,90 @@
+// runtime.hpp -- host runtime of libxkblas.so: the device-resident tile
+// directory (replacing the reference's XKaapi software DSM,
+// kaapi/kaapi_memory.c:2553-2778), streams, and the per-call statistics.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+#include <mutex>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "xkb_cuda.h"
+#include "xkblas.h"
+
+namespace xkbrt {
+
+// Per-tile state bits of the directory.
+enum : uint8_t {
+  kDevValid = 1,   // device copy holds the current value
+  kHostStale = 2,  // device copy is newer than the host copy
+};
+
+// One user matrix known to the library (reference: xkblas_matrix_descr,
+// blas/common.gen:167-187; created on first touch like
+// xkblas_init_matrix_handle, blas/xkblas.c:458-510).  Unlike the reference,
+// the device copy is ONE column-major buffer for the whole matrix; tiles are
+// the unit of coherence (valid / dirty bits) and of host<->device copies.
+struct Desc {
+  void* host = nullptr;
+  size_t M = 0, N = 0, ld = 0, esz = 0;   // host view
+  void* dev = nullptr;
+  size_t dld = 0;                         // device leading dimension (elements)
+  size_t mb = 0, nb = 0, mt = 0, nt = 0;  // tile grid
+  std::vector<uint8_t> st;                // mt*nt tile states, column major
+  bool registered_init = false;           // handle initialised (isinit)
+  std::string name;
+  uint8_t& tile(size_t i, size_t j) { return st[i + j * mt]; }
+};
+
+struct Stats {
+  uint64_t calls = 0, h2d = 0, d2h = 0, hits = 0, misses = 0;
+  uint64_t ozaki_calls = 0, ozaki_moduli = 0;
+  double flops = 0;
+};
+
+struct Runtime {
+  std::recursive_mutex mu;
+  int refcount = 0;
+  bool ready = false;
+  int device = 0;
+  cudaStream_t s_comp = nullptr, s_h2d = nullptr, s_d2h = nullptr;
+  cudaEvent_t ev_pool[64];
+  int ev_next = 0;
+  std::unordered_map<const void*, Desc*> descs;
+  size_t nb_param = 0;        // preset tile size (0 = automatic)
+  size_t prec_param = 8;
+  int math = XKBLAS_DEFAULT_MATH;
+  int ozaki_moduli = 0;       // 0 = automatic
+  long ozaki_min_dim = 1024;  // contractions smaller than this stay plain
+  Stats stats;
+  int sticky_error = 0;
+};
+
+Runtime& rt();
+int ensure_init();  // lazily initialises (returns XKB_* code)
+cudaEvent_t next_event();
+
+// Directory operations (caller holds rt().mu).
+Desc* get_desc(const void* host, size_t M, size_t N, size_t ld, size_t esz, size_t NB,
+               int* err);
+// Make the tiles covering rows [r0,r1) x cols [c0,c1) valid on the device
+// (H2D on the copy stream; the compute stream then waits).
+int make_valid(Desc* d, size_t r0, size_t r1, size_t c0, size_t c1);
+// Mark a region as written by the compute stream (device newer than host).
+void mark_written(Desc* d, size_t r0, size_t r1, size_t c0, size_t c1, int uplo);
+// Mark a region as produced on the device without reading the host copy.
+void mark_full_overwrite(Desc* d, size_t r0, size_t r1, size_t c0, size_t c1);
+int coherent(Desc* d, int uplo, int memflag);
+void drop_desc(Desc* d);
+void* dev_ptr(const Desc* d, size_t r, size_t c);
+
+size_t auto_tilesize(xkblas_kernel_t kernel, size_t M, size_t N, size_t K);
+
+// Scratch device memory for a call, stream-ordered on the compute stream.
+void* scratch_alloc(size_t bytes);
+void scratch_free(void* p);
+
+}  // namespace xkbrt

@@ -1,0 +1,130 @@
+// xkb_dev.cuh -- device-side primitives shared by the sm_100a kernels:
+// mbarrier pipeline, TMA (cp.async.bulk.tensor), bounded waits, launch
+// accounting and the device error word.
+#pragma once
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "xkb_cuda.h"
+
+namespace xkb {
+
+// A bounded wait gives up after this many nanoseconds of %globaltimer
+// (no correct launch of this library waits that long on one barrier).
+constexpr uint64_t kWaitLimitNs = 4000000000ull;  // 4 s
+
+// Device error word, one per translation unit (no relocatable device code);
+// each unit registers a reader so xkb_cuda_take_device_error() sees all.
+static __device__ int g_dev_error;
+
+enum DevErr : int {
+  kErrNone = 0,
+  kErrFullWait = 1,    // consumer gave up waiting for a TMA stage
+  kErrEmptyWait = 2,   // producer gave up waiting for a free stage
+  kErrMmaWait = 3,     // tensor-core completion wait gave up
+  kErrAccWait = 4,     // epilogue gave up waiting for the accumulator
+  kErrBounds = 5,      // a bounds check refused an access
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ uint64_t globaltimer() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ void dev_error(int code) {
+  atomicCAS(&g_dev_error, 0, code);
+}
+
+__device__ __forceinline__ bool dev_error_set() {
+  return *reinterpret_cast<volatile int*>(&g_dev_error) != 0;
+}
+
+// ---- mbarrier ---------------------------------------------------------------
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+               : "memory");
+}
+__device__ __forceinline__ void fence_barrier_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait on phase `parity`.  Returns false (and records `code`) when
+// the time limit passes or another thread already recorded an error.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int code) {
+  if (mbar_try_wait(bar, parity)) return true;
+  uint64_t t0 = globaltimer();
+  for (uint32_t i = 1;; ++i) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if ((i & 63u) == 0) {
+      if (dev_error_set()) return false;
+      if (globaltimer() - t0 > kWaitLimitNs) {
+        dev_error(code);
+        return false;
+      }
+    }
+  }
+}
+
+// ---- TMA --------------------------------------------------------------------
+__device__ __forceinline__ void tma_prefetch(const CUtensorMap* m) {
+  asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(m)) : "memory");
+}
+// 2D tiled load into shared memory, completion counted on `bar` (bytes).
+// The caller guarantees x * element size is a multiple of 16 bytes.
+__device__ __forceinline__ void tma_load_2d(void* smem_dst, const CUtensorMap* m, int x, int y,
+                                            uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3}], [%4];" ::"r"(smem_u32(smem_dst)),
+      "l"(reinterpret_cast<uint64_t>(m)), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
+}
+
+}  // namespace xkb
+
+// Host-side helpers shared by the launch code (defined in runtime_cuda.cu).
+namespace xkb {
+typedef int (*ErrReader)();
+int register_error_reader(ErrReader r);
+// Reads and clears this unit's error word.
+static int take_unit_error() {
+  int v = 0, z = 0;
+  if (cudaMemcpyFromSymbol(&v, g_dev_error, sizeof v) != cudaSuccess) return 0;
+  if (v) cudaMemcpyToSymbol(g_dev_error, &z, sizeof z);
+  return v;
+}
+static int g_unit_reader_registered = register_error_reader(&take_unit_error);
+// Encode a 2-D tiled tensor map: rows x cols column-major with leading
+// dimension ld (elements of `elem_bytes`), box bx (along rows) x by.
+// Returns false if the driver entry point is missing or encoding fails.
+bool encode_tmap_2d(CUtensorMap* map, CUtensorMapDataType dtype, int elem_bytes,
+                    const void* base, uint64_t rows, uint64_t cols, uint64_t ld,
+                    uint32_t bx, uint32_t by, CUtensorMapSwizzle swz);
+cudaStream_t resolve_stream(void* s);
+void count_launch(int n = 1);
+int sm_count();
+}  // namespace xkb
