@@ -1,0 +1,402 @@
+"""Benchmark: FP64-accurate DGEMM TFLOP/s on one B200, Ozaki INT8 tensor-core
+form vs the plain FP64 DMMA kernel, on the workload
+"DGEMM NN M=N=K=16384 with wide exponent spread (a_ij = u*2^e, u ~ U[-1,1],
+e ~ U{-20..20} per row of A and per column of B)".
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+One JSON line on rank 0.  `value` = 2*M*N*K / device time of one Ozaki DGEMM
+call (C ABI xkb_cuda_ozaki_gemm, inputs resident in HBM, 2 GiB each, so every
+step streams from HBM rather than L2).  `e2e` = the same metric through the
+public XKBlas API (xkblas_dgemm_async + xkblas_memory_coherent_async +
+xkblas_sync with pinned host buffers; host->device copies of A and B and the
+device->host copy of C inside the timed region, caches dropped every step).
+Multi-GPU (torchrun): independent replicas, one per GPU, time = max over
+ranks (weak scaling; the path has no exchange step).
+Inputs are synthetic (seeded numpy generator); the CPU baseline and the
+accuracy check against the double-double oracle use bounded samples.
+"""
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+M = N = K = 16384
+EMAX = 20
+METRIC = "FP64-accurate TFLOP/s (DGEMM/DTRSM/DSYRK): Ozaki-TC vs plain DMMA, 1 B200"
+WORKLOAD = "dgemm_nn_16384_expspread20_ozaki"
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f), "measured"
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, \
+            "fallback"
+
+
+def gen_expspread(rows, cols, seed, by_col):
+    """u * 2^e, u ~ U[-1,1], e ~ U{-EMAX..EMAX} per row (or per column)."""
+    rng = np.random.default_rng(seed)
+    e = rng.integers(-EMAX, EMAX + 1, size=cols if by_col else rows)
+    A = np.asfortranarray(rng.uniform(-1.0, 1.0, size=(rows, cols)))
+    if by_col:
+        A *= np.ldexp(1.0, e)[None, :]
+    else:
+        A *= np.ldexp(1.0, e)[:, None]
+    return A
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, idx):
+        self.idx = idx
+        self.proc = None
+        self.out = []
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.idx), "--query-gpu=" + q, "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.out.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.out:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(budget_s=12.0):
+    """The reference's CPU path: OpenBLAS dgemm_ through the Fortran symbol
+    xkblas_dgemm_native loads (restated by the oracle), all host threads, on
+    a row sample of the workload sized to ~budget_s seconds."""
+    import oracle as O
+    path = O.blas_open(threads=os.cpu_count())
+    B = gen_expspread(K, N, 2, True)
+    rows = 64
+    A = gen_expspread(rows, K, 1, False)
+    C = np.zeros((rows, N), order="F")
+    t0 = time.perf_counter()
+    O.native_gemm(O.NOTRANS, O.NOTRANS, 1.0, A, B, 0.0, C)
+    t1 = time.perf_counter() - t0
+    rows = int(max(64, min(M, rows * budget_s / max(t1, 1e-3))))
+    rows = rows // 64 * 64
+    A = gen_expspread(rows, K, 1, False)
+    C = np.zeros((rows, N), order="F")
+    t0 = time.perf_counter()
+    O.native_gemm(O.NOTRANS, O.NOTRANS, 1.0, A, B, 0.0, C)
+    t = time.perf_counter() - t0
+    return {"value": 2.0 * rows * N * K / t / 1e12, "unit": "TFLOP/s", "cores": os.cpu_count(),
+            "kind": "port",
+            "sample": "OpenBLAS %s dgemm_ via the oracle's restatement of xkblas_dgemm_native; "
+                      "%d x %d x %d row block of the 16384^3 workload, %.1f s" % (
+                          os.path.basename(path), rows, N, K, t)}
+
+
+def dd_errors(A, B, Cs, nrow=16, ncol=256, seed=7):
+    """Componentwise error |C - C_dd| / (|A||B|) on sampled entries, against
+    the double-double oracle (checker only)."""
+    import oracle as O
+    rng = np.random.default_rng(seed)
+    rows = np.sort(rng.choice(M, nrow, replace=False))
+    cols = np.sort(rng.choice(N, ncol, replace=False))
+    dd = O.gemm_dd(O.NOTRANS, O.NOTRANS, 1.0, A, B, 0.0, None, rows, cols)
+    scale = np.abs(A[rows]) @ np.abs(B[:, cols])
+    out = {}
+    for name, C in Cs.items():
+        e = np.abs(C[np.ix_(rows, cols)] - dd) / scale
+        out[name] = {"max": float(e.max()), "mean": float(e.mean())}
+    return out
+
+
+class GemmArgs(ctypes.Structure):
+    _fields_ = [("dtype", ctypes.c_int), ("opA", ctypes.c_int), ("opB", ctypes.c_int),
+                ("M", ctypes.c_int), ("N", ctypes.c_int), ("K", ctypes.c_int),
+                ("A", ctypes.c_void_p), ("lda", ctypes.c_long),
+                ("B", ctypes.c_void_p), ("ldb", ctypes.c_long),
+                ("C", ctypes.c_void_p), ("ldc", ctypes.c_long),
+                ("alpha", ctypes.c_double * 2), ("beta", ctypes.c_double * 2),
+                ("uplo", ctypes.c_int), ("herm_diag", ctypes.c_int), ("diag", ctypes.c_long)]
+
+
+class TraceRec(ctypes.Structure):
+    _fields_ = [("op", ctypes.c_char * 16), ("dtype", ctypes.c_int), ("M", ctypes.c_int),
+                ("N", ctypes.c_int), ("K", ctypes.c_int), ("nmod", ctypes.c_int),
+                ("ms_total", ctypes.c_float), ("ms_convert", ctypes.c_float),
+                ("ms_gemm", ctypes.c_float), ("ms_crt", ctypes.c_float)]
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    import oracle as O
+    O.blas_open(threads=os.cpu_count())
+    B = gen_expspread(K, N, 2, True)
+    rows = 256
+    A = gen_expspread(rows, K, 1, False)
+    C = np.zeros((rows, N), order="F")
+    times = []
+    for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        O.native_gemm(O.NOTRANS, O.NOTRANS, 1.0, A, B, 0.0, C)
+        dt = time.perf_counter() - t0
+        if i >= args.warmup:
+            times.append(dt)
+    t = max(times)
+    v = 2.0 * rows * N * K / t / 1e12
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "TFLOP/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD, "M": M, "N": N, "K": K, "sample_rows": rows},
+            "cpu_baseline": {"value": v, "unit": "TFLOP/s", "cores": os.cpu_count(), "kind": "port",
+                             "sample": "OpenBLAS dgemm_ (xkblas_dgemm_native's call) on a "
+                                       "%d-row block of the workload per step" % rows},
+            "e2e": {"value": v, "unit": "TFLOP/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="skip the CPU baseline and the double-double accuracy sample")
+    ap.add_argument("--size", type=int, default=16384,
+                    help="M = N = K (the benchmark workload is 16384; smaller sizes for profiling)")
+    args = ap.parse_args()
+    global M, N, K, WORKLOAD
+    if args.size != M:
+        M = N = K = args.size
+        WORKLOAD = "dgemm_nn_%d_expspread20_ozaki" % args.size
+    args.warmup = max(args.warmup, 3)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    os.environ["XKBLAS_GPUSET"] = str(local)
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    import xkblas_b200 as X
+    lib = X.lib()
+    X.init()
+    lib.xkb_trace_take.argtypes = [ctypes.POINTER(TraceRec), ctypes.c_int]
+
+    stream = torch.cuda.Stream()
+    sp = ctypes.c_void_p(stream.cuda_stream)
+    A = gen_expspread(M, K, 1 + 10 * rank, False)
+    B = gen_expspread(K, N, 2 + 10 * rank, True)
+    # column-major A (M x K) == row-major torch (K, M)
+    dA = torch.from_numpy(A.T).to(f"cuda:{local}")
+    dB = torch.from_numpy(B.T).to(f"cuda:{local}")
+    dC = torch.zeros(N, M, dtype=torch.float64, device=f"cuda:{local}")
+    dP = torch.zeros_like(dC)
+    torch.cuda.synchronize()
+
+    def args_for(C):
+        g = GemmArgs(1, 0, 0, M, N, K, dA.data_ptr(), M, dB.data_ptr(), K, C.data_ptr(), M)
+        g.alpha[0] = 1.0
+        return g
+
+    g_oz = args_for(dC)
+    g_pl = args_for(dP)
+    nmod = lib.xkb_ozaki_default_moduli(K)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+
+    def maxreduce(v):
+        if not dist:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- device-resident Ozaki steps --------------------------------------
+    k0 = lib.xkb_cuda_kernel_count()
+    for _ in range(args.warmup):
+        assert lib.xkb_cuda_ozaki_gemm(ctypes.byref(g_oz), 0, sp) == 0
+    barrier()
+    lib.xkb_trace_enable(1)
+    lib.xkb_trace_take(None, 0)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    k1 = lib.xkb_cuda_kernel_count()
+    with Clocks(local) as clk:
+        barrier()
+        ev0.record(stream)
+        for _ in range(args.steps):
+            assert lib.xkb_cuda_ozaki_gemm(ctypes.byref(g_oz), 0, sp) == 0
+        ev1.record(stream)
+        barrier()
+    launches = lib.xkb_cuda_kernel_count() - k1
+    ms = maxreduce(ev0.elapsed_time(ev1) / args.steps)
+    recs = (TraceRec * 256)()
+    n = lib.xkb_trace_take(recs, 256)
+    lib.xkb_trace_enable(0)
+    gemm_ms = [recs[i].ms_gemm for i in range(n) if recs[i].op == b"ozaki_gemm"]
+    conv_ms = [recs[i].ms_convert for i in range(n) if recs[i].op == b"ozaki_gemm"]
+    crt_ms = [recs[i].ms_crt for i in range(n) if recs[i].op == b"ozaki_gemm"]
+    flops = 2.0 * M * N * K
+    value = world * flops / (ms * 1e-3) / 1e12
+    deverr = lib.xkb_cuda_take_device_error()
+
+    # ---- roofline of the dominant kernel (INT8 tensor-core GEMM, all moduli)
+    pk, pk_src = peaks()
+    int8_peak = 2.0 * pk["bf16_tflops"]  # dense INT8 rate = 2x dense BF16 on B200
+    gm = statistics.mean(gemm_ms) if gemm_ms else float("nan")
+    int8_ops = 2.0 * M * N * K * nmod  # algorithmic INT8 ops per launch (one launch, all moduli)
+    achieved = int8_ops / (gm * 1e-3) / 1e12
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tp):
+        try:
+            traffic = json.load(open(tp)).get("k_oz_gemm_bytes_per_launch_16384")
+        except Exception:
+            traffic = None
+
+    # ---- plain DMMA reference point on the same inputs ---------------------
+    lib.xkb_cuda_gemm(ctypes.byref(g_pl), sp)
+    barrier()
+    ev0.record(stream)
+    steps_plain = 2
+    for _ in range(steps_plain):
+        lib.xkb_cuda_gemm(ctypes.byref(g_pl), sp)
+    ev1.record(stream)
+    barrier()
+    ms_plain = maxreduce(ev0.elapsed_time(ev1) / steps_plain)
+    plain_tflops = world * flops / (ms_plain * 1e-3) / 1e12
+    fp64_nominal = 148 * 128 * 1.965e9 / 1e12  # DMMA: 64 FMA/clk/SM at max clock
+
+    # ---- end to end through the public API ---------------------------------
+    hA = X.pinned_empty((M, K), np.float64)
+    hB = X.pinned_empty((K, N), np.float64)
+    hC = X.pinned_empty((M, N), np.float64)
+    hA[...] = A
+    hB[...] = B
+    X.set_modemath(X.XKBLAS_TENSOR_OP_MATH)
+    one = np.array([1.0])
+    zero = np.array([0.0])
+    P = ctypes.c_void_p
+
+    def e2e_step():
+        r = lib.xkblas_dgemm_async(111, 111, M, N, K, P(one.ctypes.data), P(hA.ctypes.data), M,
+                                   P(hB.ctypes.data), K, P(zero.ctypes.data), P(hC.ctypes.data),
+                                   M)
+        assert r == 0
+        lib.xkblas_memory_coherent_async(0, 0, M, N, P(hC.ctypes.data), M, 8)
+        assert lib.xkblas_sync() == 0
+        lib.xkblas_memory_invalidate_caches()
+
+    e2e_steps = max(2, min(args.steps, 3))
+    for _ in range(2):
+        e2e_step()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        e2e_step()
+    t_e2e = maxreduce((time.perf_counter() - t0) / e2e_steps)
+    X.set_modemath(X.XKBLAS_DEFAULT_MATH)
+    e2e_value = world * flops / t_e2e / 1e12
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD, "M": M, "N": N, "K": K, "exp_spread": EMAX,
+                   "moduli": nmod, "parallelism": "replicas" if world > 1 else "single",
+                   "l2": "inputs 2 GiB each > 126 MB L2 (no flush needed)"},
+        "e2e": {"value": e2e_value, "unit": "TFLOP/s",
+                "h2d_bytes_per_step": 2 * M * K * 8, "d2h_bytes_per_step": M * N * 8,
+                "ms_per_step": t_e2e * 1e3},
+        "gpu_launches": int(launches),
+        "clocks": clk.summary(),
+        "roofline": {"bound": "tensor", "kernel": "k_oz_gemm (INT8 tcgen05, all moduli)",
+                     "achieved": achieved, "peak": int8_peak, "unit": "TFLOP/s",
+                     "frac": achieved / int8_peak, "traffic": traffic,
+                     "peak_source": "%s bf16 dense x2 (INT8:BF16 dense rate 2:1)" % pk_src,
+                     "ms_per_launch": gm},
+        "plain_dmma": {"value": plain_tflops, "unit": "TFLOP/s", "ms_per_step": ms_plain,
+                       "frac_of_fp64_nominal": plain_tflops / fp64_nominal,
+                       "fp64_nominal_tflops": fp64_nominal},
+        "ozaki_speedup_vs_plain": ms_plain / ms,
+        "ozaki_phases_ms": {"convert": statistics.mean(conv_ms) if conv_ms else None,
+                            "int8_gemm": gm, "crt": statistics.mean(crt_ms) if crt_ms else None},
+        "device_error": deverr,
+    }
+    if rank == 0 and not args.no_extra:
+        # accuracy against the double-double oracle and the CPU baseline
+        # (bounded samples; checker / baseline only)
+        Co = np.asfortranarray(dC.cpu().numpy().T)
+        Cp = np.asfortranarray(dP.cpu().numpy().T)
+        line["error_vs_dd"] = dd_errors(A, B, {"ozaki": Co, "plain": Cp})
+        line["cpu_baseline"] = cpu_baseline()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -12,7 +12,7 @@
  *   xkb_cuda_trsm       <- blas/ztask_trsm.c:162-180   (cublasZtrsm, :172)
  *   xkb_cuda_trmm       <- blas/ztask_trmm.c:156       (cublasZtrmm)
  *   xkb_cuda_symm       <- blas/ztask_symm.c:133, ztask_hemm.c:132
- *   xkb_cuda_ozaki_dgemm / xkb_cuda_ozaki_zgemm: no counterpart in the
+ *   xkb_cuda_ozaki_gemm: no counterpart in the
  *                          reference (FP64 contraction on INT8 tensor cores).
  * Every function returns 0 or a negative XKB_E* code; nothing aborts.
  */
@@ -68,8 +68,9 @@ int xkb_cuda_gemm(const xkb_gemm_args* a, void* stream);
 /* Triangular solve, all side/uplo/trans/diag cases:
  *   side L: B <- alpha * op(A)^-1 * B   (A is M x M)
  *   side R: B <- alpha * B * op(A)^-1   (A is N x N)
- * FP64 diagonal-block substitution + DMMA GEMM updates (or Ozaki updates
- * when ozaki != 0 and dtype is XKB_D/XKB_Z). */
+ * FP64 diagonal-block substitution + DMMA GEMM updates; when ozaki > 0 and
+ * dtype is XKB_D/XKB_Z, updates whose three dimensions are all >= ozaki run
+ * in the Ozaki INT8 form. */
 int xkb_cuda_trsm(int dtype, int side, int uplo, int trans, int diag, int M,
                   int N, const double* alpha, const void* A, long lda, void* B,
                   long ldb, int ozaki, void* stream);
@@ -100,6 +101,23 @@ int xkb_cuda_ozaki_gemm(const xkb_gemm_args* a, int nmod, void* stream);
 /* Number of moduli the Ozaki path uses for contraction length K (0 if K is
  * beyond the exact-INT32 limit). */
 int xkb_ozaki_default_moduli(long K);
+
+/* Per-call trace (off by default): when enabled, contractions record CUDA
+ * events around their phases on their own stream; xkb_trace_take() waits for
+ * the recorded events and returns up to `max` completed records, oldest
+ * first (a fixed ring of 256 records; older ones are overwritten). */
+typedef struct xkb_trace_rec {
+  char op[16];        /* "dmma_gemm", "ozaki_gemm"                         */
+  int dtype, M, N, K; /* shape of the contraction                          */
+  int nmod;           /* Ozaki moduli (0 for the plain path)               */
+  float ms_total;     /* whole call on the device                          */
+  float ms_convert;   /* Ozaki: scaling + residue planes of A and B        */
+  float ms_gemm;      /* Ozaki: INT8 tensor-core products (all moduli);
+                         plain: the DMMA kernel                            */
+  float ms_crt;       /* Ozaki: CRT reconstruction + alpha/beta            */
+} xkb_trace_rec;
+int xkb_trace_enable(int on);
+int xkb_trace_take(xkb_trace_rec* out, int max);
 
 /* Device error word written by bounded waits (0 = none); clears it. */
 int xkb_cuda_take_device_error(void);

@@ -4,6 +4,9 @@ import sys
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+# tensor-op (Ozaki) tests use small matrices: lower the size floor below which
+# contractions stay on the plain FP64 path (read at library initialisation)
+os.environ.setdefault("XKBLAS_OZAKI_MIN_DIM", "64")
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 

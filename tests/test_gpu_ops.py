@@ -214,7 +214,7 @@ def test_syrk_herk(xk, dt, uplo):
             sel = np.tril if uplo == LO else np.triu
             other = np.triu if uplo == LO else np.tril
             assert checks.rk_ratio(sel(C), sel(R), A, C0, N) <= 10
-            k = -1 if uplo == LO else 1
+            k = 1 if uplo == LO else -1  # strictly the other triangle
             np.testing.assert_array_equal(other(C, k), other(C0, k))  # untouched
             if herm:
                 assert np.all(np.diag(C).imag == 0)
@@ -344,3 +344,19 @@ def test_async_chain_without_host_round_trip(xk):
     assert np.all(C1 == 0)  # never requested
     np.testing.assert_allclose(C2, (A @ B) @ B, rtol=1e-12, atol=1e-11)
     xk.invalidate_caches()
+
+
+@pytest.mark.parametrize("mnk", [(1024, 1024, 128), (1024, 1024, 1024), (1536, 1024, 777),
+                                 (640, 2048, 1000)])
+def test_gemm_many_ctas_per_sm(xk, mnk):
+    """Mid sizes run the 64x64 tile with several CTAs per SM: stage reuse
+    under co-residency must stay exact (repeated to catch ordering races)."""
+    M, N, K = mnk
+    A, B = O.plrnt(M, K, 41), O.plrnt(K, N, 42)
+    ref = 1.5 * (A @ B)
+    for _ in range(3):
+        C = np.zeros((M, N), order="F")
+        xk.gemm(N_, N_, 1.5, A, B, 0.0, C)
+        xk.invalidate_caches()
+        err = np.abs(C - ref).max() / (1.5 * np.abs(A).max() * np.abs(B).max() * K)
+        assert err < 1e-15, err

@@ -1,0 +1,160 @@
+"""GPU parity of the Ozaki-II INT8 tensor-core form (XKBLAS_TENSOR_OP_MATH):
+same reference bounds as the plain path, and never worse than the plain FP64
+DMMA result against the double-double oracle.  Requires a B200."""
+import ctypes
+
+import numpy as np
+import pytest
+
+import oracle as O
+from tests import checks
+
+pytestmark = pytest.mark.gpu
+
+N_, T_, C_ = 111, 112, 113
+UP, LO = 121, 122
+LEFT = 141
+NONUNIT = 131
+
+
+@pytest.fixture
+def tc(xk):
+    xk.set_modemath(xk.XKBLAS_TENSOR_OP_MATH)
+    yield xk
+    xk.set_modemath(xk.XKBLAS_DEFAULT_MATH)
+
+
+def _dd_err(C, A, B, alpha, ta=N_, tb=N_, nrow=24, ncol=24, seed=0):
+    rng = np.random.default_rng(seed)
+    M, N = C.shape
+    rows = np.sort(rng.choice(M, min(M, nrow), replace=False))
+    cols = np.sort(rng.choice(N, min(N, ncol), replace=False))
+    dd = O.gemm_dd(ta, tb, alpha, A, B, 0.0, None, rows, cols)
+    opA = A if ta == N_ else A.T
+    opB = B if tb == N_ else B.T
+    scale = np.abs(opA[rows]) @ np.abs(opB[:, cols]) * abs(alpha)
+    return float(np.max(np.abs(C[np.ix_(rows, cols)] - dd) / scale))
+
+
+@pytest.mark.parametrize("mnk", [(300, 200, 513), (129, 257, 1000), (1024, 1024, 1024)])
+def test_ozaki_dgemm_bounds(tc, mnk):
+    M, N, K = mnk
+    s0 = tc.stats()["ozaki_calls"]
+    for ta in (N_, T_):
+        for tb in (N_, T_):
+            A = O.plrnt(M, K, 5) if ta == N_ else O.plrnt(K, M, 5)
+            B = O.plrnt(K, N, 6) if tb == N_ else O.plrnt(N, K, 6)
+            C0 = O.plrnt(M, N, 7)
+            C = C0.copy(order="F")
+            tc.gemm(ta, tb, 1.5, A, B, -0.5, C)
+            tc.invalidate_caches()
+            R = O.gemm(ta, tb, 1.5, A, B, -0.5, C0.copy(order="F"))
+            assert checks.gemm_ratio(C, R, A, B, C0, 1.5, -0.5, K) <= 3.0
+            assert checks.plasma_ratio(C, R, A, B, 1.5, K) < 10
+    assert tc.stats()["ozaki_calls"] >= s0 + 4
+
+
+def test_ozaki_no_worse_than_plain_exponent_spread(xk):
+    """Config-4 distribution (per-row / per-column exponents in [-20, 20]) at
+    a size the oracle handles: Ozaki error vs double-double <= plain error."""
+    M = N = K = 768
+    A = O.expspread(M, K, 101, emax=20, by_col=False)
+    B = O.expspread(K, N, 102, emax=20, by_col=True)
+    Cp = np.zeros((M, N), order="F")
+    xk.gemm(N_, N_, 1.0, A, B, 0.0, Cp)
+    xk.invalidate_caches()
+    xk.set_modemath(xk.XKBLAS_TENSOR_OP_MATH)
+    try:
+        Co = np.zeros((M, N), order="F")
+        xk.gemm(N_, N_, 1.0, A, B, 0.0, Co)
+        xk.invalidate_caches()
+    finally:
+        xk.set_modemath(xk.XKBLAS_DEFAULT_MATH)
+    ep = _dd_err(Cp, A, B, 1.0, nrow=48, ncol=48)
+    eo = _dd_err(Co, A, B, 1.0, nrow=48, ncol=48)
+    assert eo <= max(ep, 2.0 ** -52), (eo, ep)
+    assert eo < 2.0 ** -50
+
+
+def test_ozaki_zgemm_all_trans(tc):
+    M, N, K = 150, 170, 333
+    for ta in (N_, T_, C_):
+        for tb in (N_, T_, C_):
+            A = O.plrnt(M, K, 8, True) if ta == N_ else O.plrnt(K, M, 8, True)
+            B = O.plrnt(K, N, 9, True) if tb == N_ else O.plrnt(N, K, 9, True)
+            C0 = O.plrnt(M, N, 10, True)
+            al, be = 1.5 - 0.25j, -0.5 + 0.125j
+            C = C0.copy(order="F")
+            tc.gemm(ta, tb, al, A, B, be, C)
+            tc.invalidate_caches()
+            R = O.gemm(ta, tb, al, A, B, be, C0.copy(order="F"))
+            assert checks.gemm_ratio(C, R, A, B, C0, al, be, K) <= 3.0, (ta, tb)
+
+
+@pytest.mark.parametrize("uplo", [UP, LO])
+def test_ozaki_syrk_herk(tc, uplo):
+    N, K = 300, 280
+    A = O.plrnt(N, K, 11)
+    C0 = O.plgsy(N, 12)
+    C = C0.copy(order="F")
+    tc.syrk(uplo, N_, 1.0, A, 1.0, C)
+    tc.invalidate_caches()
+    R = O.syrk(uplo, N_, 1.0, A, 1.0, C0.copy(order="F"))
+    sel = np.tril if uplo == LO else np.triu
+    assert checks.rk_ratio(sel(C), sel(R), A, C0, N) <= 10
+    Az = O.plrnt(K, N, 13, True)
+    Cz0 = O.plgsy(N, 14, cplx=True)
+    Cz = Cz0.copy(order="F")
+    tc.syrk(uplo, C_, 1.0, Az, 1.0, Cz, herm=True)
+    tc.invalidate_caches()
+    Rz = O.syrk(uplo, C_, 1.0, Az, 1.0, Cz0.copy(order="F"), herm=True)
+    assert checks.rk_ratio(sel(Cz), sel(Rz), Az, Cz0, N) <= 10
+    assert np.all(np.diag(Cz).imag == 0)
+
+
+def test_ozaki_trsm_updates(tc):
+    M = N = 640
+    A = np.asfortranarray(np.tril(O.plrnt(M, M, 15)) + M * np.eye(M))
+    B0 = O.plrnt(M, N, 16)
+    B = B0.copy(order="F")
+    s0 = tc.stats()["ozaki_calls"]
+    tc.trsm(LEFT, LO, N_, NONUNIT, 2.0, A, B)
+    tc.invalidate_caches()
+    R = O.trsm(LEFT, LO, N_, NONUNIT, 2.0, A, B0.copy(order="F"), nb=128)
+    assert checks.trsm_ratio(B, R, A, M, N) <= 10
+
+
+class GemmArgs(ctypes.Structure):
+    _fields_ = [("dtype", ctypes.c_int), ("opA", ctypes.c_int), ("opB", ctypes.c_int),
+                ("M", ctypes.c_int), ("N", ctypes.c_int), ("K", ctypes.c_int),
+                ("A", ctypes.c_void_p), ("lda", ctypes.c_long),
+                ("B", ctypes.c_void_p), ("ldb", ctypes.c_long),
+                ("C", ctypes.c_void_p), ("ldc", ctypes.c_long),
+                ("alpha", ctypes.c_double * 2), ("beta", ctypes.c_double * 2),
+                ("uplo", ctypes.c_int), ("herm_diag", ctypes.c_int), ("diag", ctypes.c_long)]
+
+
+def test_ozaki_moduli_count_controls_accuracy(xk):
+    """Through the thin C ABI on device memory: fewer moduli -> larger error;
+    the default count reaches FP64 accuracy."""
+    import torch
+    M = N = K = 512
+    A = O.plrnt(M, K, 21)
+    B = O.plrnt(K, N, 22)
+    dA = torch.from_numpy(A.T.copy()).cuda()  # row-major (K,M) = column-major A
+    dB = torch.from_numpy(B.T.copy()).cuda()
+    torch.cuda.synchronize()
+    lib = xk.lib()
+    errs = {}
+    for nm in (8, 10, 12, 0):
+        dC = torch.zeros(N, M, dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        g = GemmArgs(1, 0, 0, M, N, K, dA.data_ptr(), M, dB.data_ptr(), K, dC.data_ptr(), M)
+        g.alpha[0] = 1.0
+        assert lib.xkb_cuda_ozaki_gemm(ctypes.byref(g), nm, None) == 0
+        xk.sync()
+        C = np.asfortranarray(dC.cpu().numpy().T)
+        errs[nm] = _dd_err(C, A, B, 1.0, nrow=32, ncol=32)
+    assert errs[8] > errs[12] > 0 or errs[12] < 1e-15
+    assert errs[0] < 2.0 ** -50
+    assert lib.xkb_cuda_take_device_error() == 0

@@ -429,7 +429,9 @@ int tr_async(int is_trsm, int side, int uplo, int transA, int diag, int M, int N
     err = xkb_cuda_scale(HT<T>::dt, M, N, z, dev_ptr(dB, 0, 0), (long)dB->dld, XKB_FULL, 0, 0,
                          R.s_comp);
   } else if (is_trsm) {
-    const int oz = (R.math == XKBLAS_TENSOR_OP_MATH) && (HT<T>::dt == XKB_D || HT<T>::dt == XKB_Z);
+    const int oz = ((R.math == XKBLAS_TENSOR_OP_MATH) && (HT<T>::dt == XKB_D || HT<T>::dt == XKB_Z))
+                       ? (int)std::max<long>(R.ozaki_min_dim, 1)
+                       : 0;
     err = xkb_cuda_trsm(HT<T>::dt, sd, ul, opcode(transA), dg, M, N, al, dev_ptr(dA, 0, 0),
                         (long)dA->dld, dev_ptr(dB, 0, 0), (long)dB->dld, oz, R.s_comp);
   } else {

@@ -22,6 +22,7 @@
 //     exit before touching memory;
 //   * every barrier wait is bounded (xkb_dev.cuh) and records an error word.
 #include <cstdio>
+#include <cstdlib>
 
 #include "xkb_dev.cuh"
 
@@ -183,7 +184,10 @@ __global__ void __launch_bounds__(kThreads, 1)
   for (int it = 0; it < KT; ++it) {
     const int s = it % kStages;
     const uint32_t ph = (it / kStages) & 1;
-    if (!mbar_wait(&full[s], ph, kErrFullWait)) {
+    // every lane observes the phase itself (acquire of the TMA bytes); the
+    // vote reconverges the warp before the .aligned MMAs
+    const bool got = mbar_wait(&full[s], ph, kErrFullWait);
+    if (!__all_sync(0xffffffffu, got)) {
       ok = false;
       break;
     }
@@ -239,14 +243,23 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
       }
     }
+    // the stage was read through the generic proxy and will be rewritten by
+    // TMA (async proxy): order the reads before the release of the stage
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncwarp();
     if (lane == 0) mbar_arrive(&empty[s]);
-    if (threadIdx.x == 0 && it + kStages < KT) {
-      if (!mbar_wait(&empty[s], ph, kErrEmptyWait)) {
+    if (warp == 0) {
+      // lane 0 refills the stage; the vote keeps warp 0 converged for the
+      // next iteration's .aligned MMAs
+      bool refill_ok = true;
+      if (lane == 0 && it + kStages < KT) {
+        refill_ok = mbar_wait(&empty[s], ph, kErrEmptyWait);
+        if (refill_ok) issue(it + kStages);
+      }
+      if (!__all_sync(0xffffffffu, refill_ok)) {
         ok = false;
         break;
       }
-      issue(it + kStages);
     }
   }
   if (!ok) return;
@@ -376,7 +389,10 @@ static int dispatch_type(const xkb_gemm_args* a, cudaStream_t st) {
   constexpr bool CPLX = St<T>::CPLX;
   constexpr int BMb = CPLX ? 64 : 128, BNb = 128;
   const long tiles_big = (long)((a->M + BMb - 1) / BMb) * ((a->N + BNb - 1) / BNb);
-  if (tiles_big >= sm_count()) return dispatch_ops<T, BMb, BNb>(a, st);
+  // XKBLAS_GEMM_TILE=big|small overrides the size rule (tuning sweeps)
+  static const char* force = getenv("XKBLAS_GEMM_TILE");
+  const bool big = force ? (force[0] == 'b') : (tiles_big >= sm_count());
+  if (big) return dispatch_ops<T, BMb, BNb>(a, st);
   return dispatch_ops<T, BMb / 2, BNb / 2>(a, st);
 }
 
@@ -424,11 +440,16 @@ extern "C" int xkb_cuda_gemm(const xkb_gemm_args* a, void* stream) {
   if (a->K == 0 || alpha_zero)
     return xkb_cuda_scale(a->dtype, a->M, a->N, a->beta, a->C, a->ldc, a->uplo, a->herm_diag,
                           a->diag, stream);
+  const int slot = trace_begin("dmma_gemm", a->dtype, a->M, a->N, a->K, 0, st);
+  trace_mark(slot, 1, st);
+  int r = XKB_EINVAL;
   switch (a->dtype) {
-    case XKB_S: return dispatch_type<float>(a, st);
-    case XKB_D: return dispatch_type<double>(a, st);
-    case XKB_C: return dispatch_type<float2>(a, st);
-    case XKB_Z: return dispatch_type<double2>(a, st);
+    case XKB_S: r = dispatch_type<float>(a, st); break;
+    case XKB_D: r = dispatch_type<double>(a, st); break;
+    case XKB_C: r = dispatch_type<float2>(a, st); break;
+    case XKB_Z: r = dispatch_type<double2>(a, st); break;
   }
-  return XKB_EINVAL;
+  trace_mark(slot, 2, st);
+  trace_mark(slot, 3, st);
+  return r;
 }

@@ -53,6 +53,23 @@ bool encode_tmap_2d(CUtensorMap* map, CUtensorMapDataType dtype, int elem_bytes,
   return r == CUDA_SUCCESS;
 }
 
+bool encode_tmap_3d_u8(CUtensorMap* map, const void* base, uint64_t inner, uint64_t rows,
+                       uint64_t planes, uint32_t box_inner, uint32_t box_rows) {
+  PFN_encodeTiled enc = get_encode();
+  if (!enc || !base || inner == 0 || rows == 0 || planes == 0) return false;
+  if ((reinterpret_cast<uintptr_t>(base) & 15u) != 0 || (inner & 15u) != 0) return false;
+  if (box_inner > 128 || box_rows > 256 || (box_inner & 15u) != 0) return false;
+  cuuint64_t dims[3] = {inner, rows, planes};
+  cuuint64_t strides[2] = {inner, inner * rows};
+  cuuint32_t box[3] = {box_inner, box_rows, 1};
+  cuuint32_t estr[3] = {1, 1, 1};
+  std::memset(map, 0, sizeof(*map));
+  CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<void*>(base), dims, strides,
+                   box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
 static cudaStream_t g_lib_stream = nullptr;
 static std::atomic<uint64_t> g_launches{0};
 
@@ -84,6 +101,86 @@ int register_error_reader(ErrReader r) {
 }
 
 void set_library_stream(cudaStream_t s) { g_lib_stream = s; }
+
+// ---- trace ring ---------------------------------------------------------------
+struct TraceSlot {
+  xkb_trace_rec rec;
+  cudaEvent_t ev[4];
+  bool created = false, pending = false;
+};
+static std::mutex g_trace_mu;
+static bool g_trace_on = false;
+static TraceSlot g_trace[256];
+static int g_trace_head = 0;  // next slot to write
+static int g_trace_count = 0;
+
+bool trace_on() { return g_trace_on; }
+
+int trace_begin(const char* op, int dtype, int M, int N, int K, int nmod, cudaStream_t st) {
+  if (!g_trace_on) return -1;
+  std::lock_guard<std::mutex> g(g_trace_mu);
+  const int i = g_trace_head;
+  TraceSlot& t = g_trace[i];
+  if (!t.created) {
+    for (auto& e : t.ev)
+      if (cudaEventCreate(&e) != cudaSuccess) return -1;
+    t.created = true;
+  }
+  std::memset(&t.rec, 0, sizeof(t.rec));
+  std::strncpy(t.rec.op, op, sizeof(t.rec.op) - 1);
+  t.rec.dtype = dtype;
+  t.rec.M = M;
+  t.rec.N = N;
+  t.rec.K = K;
+  t.rec.nmod = nmod;
+  t.pending = true;
+  g_trace_head = (g_trace_head + 1) % 256;
+  if (g_trace_count < 256) ++g_trace_count;
+  cudaEventRecord(t.ev[0], st);
+  return i;
+}
+
+void trace_mark(int slot, int k, cudaStream_t st) {
+  if (slot < 0 || k < 1 || k > 3) return;
+  cudaEventRecord(g_trace[slot].ev[k], st);
+}
+
+}  // namespace xkb
+
+extern "C" int xkb_trace_enable(int on) {
+  std::lock_guard<std::mutex> g(xkb::g_trace_mu);
+  const int prev = xkb::g_trace_on;
+  xkb::g_trace_on = on != 0;
+  return prev;
+}
+
+extern "C" int xkb_trace_take(xkb_trace_rec* out, int max) {
+  using namespace xkb;
+  std::lock_guard<std::mutex> g(g_trace_mu);
+  int n = 0;
+  const int first = (g_trace_head - g_trace_count + 256) % 256;
+  for (int c = 0; c < g_trace_count && n < max; ++c) {
+    TraceSlot& t = g_trace[(first + c) % 256];
+    if (!t.pending) continue;
+    if (cudaEventSynchronize(t.ev[3]) != cudaSuccess) continue;
+    float a = 0, b = 0, d = 0, tot = 0;
+    cudaEventElapsedTime(&tot, t.ev[0], t.ev[3]);
+    cudaEventElapsedTime(&a, t.ev[0], t.ev[1]);
+    cudaEventElapsedTime(&b, t.ev[1], t.ev[2]);
+    cudaEventElapsedTime(&d, t.ev[2], t.ev[3]);
+    t.rec.ms_total = tot;
+    t.rec.ms_convert = a;
+    t.rec.ms_gemm = b;
+    t.rec.ms_crt = d;
+    t.pending = false;
+    if (out) out[n] = t.rec;
+    ++n;
+  }
+  g_trace_count = 0;
+  return n;
+}
+
+namespace xkb {
 
 }  // namespace xkb
 

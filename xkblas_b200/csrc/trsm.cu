@@ -306,7 +306,7 @@ static int update(const TrsmCtx& c, long p0, long p1, long q0, long q1, const do
     g.C = c.B + p0 * c.ldb * (long)c.es;
     g.ldc = c.ldb;
   }
-  if (c.ozaki && std::min<long>(std::min<long>(g.M, g.N), g.K) >= 1024) {
+  if (c.ozaki > 0 && std::min<long>(std::min<long>(g.M, g.N), g.K) >= c.ozaki) {
     int e = xkb_cuda_ozaki_gemm(&g, 0, c.st);
     if (e != XKB_ERANGE) return e;
   }
@@ -353,7 +353,7 @@ extern "C" int xkb_cuda_trsm(int dtype, int side, int uplo, int trans, int diag,
   c.left = side == 0;
   c.trans = (!cplx && trans == XKB_OP_C) ? XKB_OP_T : trans;
   c.unit = diag != 0;
-  c.ozaki = ozaki && (dtype == XKB_D || dtype == XKB_Z);
+  c.ozaki = (dtype == XKB_D || dtype == XKB_Z) ? ozaki : 0;
   c.A = static_cast<const char*>(A);
   c.lda = lda;
   c.B = static_cast<char*>(B);

@@ -124,7 +124,15 @@ static int g_unit_reader_registered = register_error_reader(&take_unit_error);
 bool encode_tmap_2d(CUtensorMap* map, CUtensorMapDataType dtype, int elem_bytes,
                     const void* base, uint64_t rows, uint64_t cols, uint64_t ld,
                     uint32_t bx, uint32_t by, CUtensorMapSwizzle swz);
+// 3-D byte tensor (planes of rows x inner bytes), 128-byte swizzle, box
+// (box_inner x box_rows x 1): the layout tcgen05 K-major operands use.
+bool encode_tmap_3d_u8(CUtensorMap* map, const void* base, uint64_t inner, uint64_t rows,
+                       uint64_t planes, uint32_t box_inner, uint32_t box_rows);
 cudaStream_t resolve_stream(void* s);
+// trace: begin a record (returns a slot or -1 when tracing is off) and mark
+// phase boundaries 1..3 (3 = end) on the launching stream.
+int trace_begin(const char* op, int dtype, int M, int N, int K, int nmod, cudaStream_t st);
+void trace_mark(int slot, int k, cudaStream_t st);
 void count_launch(int n = 1);
 int sm_count();
 }  // namespace xkb
