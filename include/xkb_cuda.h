@@ -98,6 +98,18 @@ int xkb_cuda_scale(int dtype, int M, int N, const double* beta, void* C,
  * uplo/herm_diag/diag mask C as in xkb_gemm_args.  dtype XKB_D or XKB_Z. */
 int xkb_cuda_ozaki_gemm(const xkb_gemm_args* a, int nmod, void* stream);
 
+/* The same real (XKB_D) Ozaki contraction as xkb_cuda_ozaki_gemm, for
+ * callers that cannot allocate device memory at call time (a process whose
+ * free GPU memory is held by its own caching allocator, a loop that must not
+ * risk an allocation stalling or failing mid-step).  No counterpart in the
+ * reference.  Allocates nothing: its scratch is one fixed device array
+ * inside the library (about 12.6 MiB per GPU that loads it, held until the
+ * process exits).  M, N, K <= 512, otherwise XKB_ERANGE; nmod as above.
+ * Every call uses the same array, so calls that overlap on the GPU race:
+ * serialise them.  The first call on a device looks the array up (once per
+ * device); make it before any stream capture. */
+int xkb_cuda_ozaki_gemm_noalloc(const xkb_gemm_args* a, int nmod, void* stream);
+
 /* Number of moduli the Ozaki path uses for contraction length K (0 if K is
  * beyond the exact-INT32 limit). */
 int xkb_ozaki_default_moduli(long K);

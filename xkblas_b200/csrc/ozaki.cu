@@ -987,3 +987,132 @@ extern "C" int xkb_cuda_ozaki_gemm(const xkb_gemm_args* a, int nmod, void* strea
   if (re) cudaFreeAsync(re, st);
   return err;
 }
+
+// ===========================================================================
+// Scratch-free variant of the real Ozaki contraction.
+//
+// Who needs it: callers that cannot ask the CUDA allocator for memory at call
+// time -- for example a program that has already handed all free device
+// memory to its own caching allocator (cudaMallocAsync would then fail), or a
+// latency-bound loop that must not risk an allocation stalling or failing in
+// the middle of a step.  xkb_cuda_ozaki_gemm takes its scratch (residue
+// planes, shifts, norm partials) from the stream-ordered pool on every call;
+// this entry point takes it from one fixed device array compiled into the
+// library instead, and allocates nothing.
+//
+// Limits and rules:
+//   * real double (XKB_D) only, M, N, K <= kNoAllocMaxDim (512); larger sizes
+//     are refused with XKB_ERANGE before anything is launched;
+//   * the array (kNoAllocBytes, about 12.6 MiB) lives in every GPU that
+//     loads this library, for the life of the process;
+//   * all calls share it: two calls whose kernels overlap on the GPU (other
+//     streams, other host threads) race on it and corrupt each other --
+//     serialise them;
+//   * the first call on a device looks the array's device address up with
+//     cudaGetSymbolAddress (once per device, with that device current); make
+//     that first call before capturing a stream.
+// Nothing in the array has to start at zero: every byte a call reads is
+// written earlier in the same call (planes padded by the residue kernel and a
+// 2-D memset, shifts and partials fully rewritten).
+namespace xkb {
+namespace oz {
+constexpr int kNoAllocMaxDim = 512;
+// per-plane rows and k extent at the limit: max(rup(512,128), rup(512,256))
+constexpr size_t kNoAllocRows = 512, kNoAllocK = 512;
+constexpr size_t kNoAllocPlane = kNoAllocRows * kNoAllocK;              // bytes
+constexpr size_t kNoAllocA = kMaxMod * kNoAllocPlane;                  // A planes
+constexpr size_t kNoAllocB = kMaxMod * kNoAllocPlane;                  // B planes
+constexpr size_t kNoAllocR = kMaxMod * kNoAllocRows * kNoAllocRows;    // C residues
+constexpr size_t kNoAllocShift = 2 * 4 * kNoAllocRows;                 // mu, nu
+constexpr size_t kNoAllocPart = sizeof(double2) * 2 * kNoAllocRows;    // 1 k-chunk
+constexpr size_t kNoAllocBytes =
+    kNoAllocA + kNoAllocB + kNoAllocR + kNoAllocShift + kNoAllocPart + 4096;
+
+static __device__ __align__(256) unsigned char g_oz_noalloc_scratch[kNoAllocBytes];
+
+// Device address of the array, looked up once per device.
+static int noalloc_base(unsigned char** out) {
+  static std::mutex mu;
+  static unsigned char* ptr[64] = {nullptr};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return XKB_ECUDA;
+  std::lock_guard<std::mutex> g(mu);
+  if (!ptr[dev]) {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_oz_noalloc_scratch) != cudaSuccess || !p) {
+      cudaGetLastError();
+      return XKB_ECUDA;
+    }
+    ptr[dev] = static_cast<unsigned char*>(p);
+  }
+  *out = ptr[dev];
+  return XKB_OK;
+}
+}  // namespace oz
+}  // namespace xkb
+
+extern "C" int xkb_cuda_ozaki_gemm_noalloc(const xkb_gemm_args* a, int nmod, void* stream) {
+  if (!a || a->dtype != XKB_D) return XKB_EINVAL;
+  if (a->M < 0 || a->N < 0 || a->K < 0) return XKB_EINVAL;
+  if (a->M > kNoAllocMaxDim || a->N > kNoAllocMaxDim || a->K > kNoAllocMaxDim) return XKB_ERANGE;
+  if (a->M == 0 || a->N == 0) return XKB_OK;
+  if (a->K == 0 || a->alpha[0] == 0.0) return xkb_cuda_gemm(a, stream);  // beta*C only
+  if (nmod == 0) nmod = default_moduli(a->K);
+  const Consts* c = consts_for(nmod);
+  if (!c) return XKB_ERANGE;
+  unsigned char* base = nullptr;
+  int err = noalloc_base(&base);
+  if (err) return err;
+  cudaStream_t st = resolve_stream(stream);
+  const int M = a->M, N = a->N, K = a->K;
+  const long Kpad = (long)rup(K, BKB), Mpad = (long)rup(M, BM), Npad = (long)rup(N, BN);
+  const bool akc = a->opA != XKB_OP_N, bkc = a->opB == XKB_OP_N;
+  const bool same = (a->A == a->B) && (a->lda == a->ldb) && (akc == bkc) && M == N;
+  const long Arows = same ? std::max(Mpad, Npad) : Mpad;
+  // carve the fixed array (all offsets 256-byte aligned)
+  int8_t* Ap = reinterpret_cast<int8_t*>(base);
+  int8_t* Bp = reinterpret_cast<int8_t*>(base + kNoAllocA);
+  uint8_t* R = base + kNoAllocA + kNoAllocB;
+  int* mu = reinterpret_cast<int*>(base + kNoAllocA + kNoAllocB + kNoAllocR);
+  int* nu = mu + kNoAllocRows;
+  double2* part = reinterpret_cast<double2*>(base + kNoAllocA + kNoAllocB + kNoAllocR + kNoAllocShift);
+  const double* Ad = static_cast<const double*>(a->A);
+  const double* Bd = static_cast<const double*>(a->B);
+  View va{Ad, a->lda, akc, 1, 0, 1.0}, vb{Bd, a->ldb, bkc, 1, 0, 1.0};
+  err = launch_norm(va, M, K, 0, c, part, mu, st);
+  if (!err) err = launch_norm(vb, N, K, 0, c, part + kNoAllocRows, nu, st);
+  if (!err) err = launch_res(va, M, K, mu, c, Ap, Arows, Kpad, 0, st);
+  if (!err && !same) err = launch_res(vb, N, K, nu, c, Bp, Npad, Kpad, 0, st);
+  if (!err && Kpad > (long)rup(K, 64)) {
+    const size_t kz = rup(K, 64);
+    if (cudaMemset2DAsync(Ap + kz, Kpad, 0, Kpad - kz, (size_t)nmod * Arows, st) != cudaSuccess ||
+        (!same &&
+         cudaMemset2DAsync(Bp + kz, Kpad, 0, Kpad - kz, (size_t)nmod * Npad, st) != cudaSuccess))
+      err = XKB_ECUDA;
+  }
+  if (!err)
+    err = same ? launch_gemm(Ap, Arows, Ap, Arows, Mpad, Npad, Kpad, c, R, a->uplo, a->diag, st)
+               : launch_gemm(Ap, Mpad, Bp, Npad, Mpad, Npad, Kpad, c, R, a->uplo, a->diag, st);
+  if (!err) {
+    CrtP cp;
+    std::memset(&cp, 0, sizeof(cp));
+    cp.M = M;
+    cp.N = N;
+    cp.R = R;
+    cp.Mpad = Mpad;
+    cp.Npad = Npad;
+    cp.mu = mu;
+    cp.nu = nu;
+    cp.C = static_cast<double*>(a->C);
+    cp.ldc = a->ldc;
+    cp.ar = a->alpha[0];
+    cp.br = a->beta[0];
+    cp.uplo = a->uplo;
+    cp.diag = a->diag;
+    const dim3 cg((unsigned)((M / 4 + 1 + 255) / 256), (unsigned)N);
+    k_oz_crt<<<cg, 256, 0, st>>>(cp, *c);
+    count_launch();
+    if (cudaPeekAtLastError() != cudaSuccess) err = XKB_ECUDA;
+  }
+  return err;
+}
