@@ -171,6 +171,93 @@ class TraceRec(ctypes.Structure):
                 ("ms_gemm", ctypes.c_float), ("ms_crt", ctypes.c_float)]
 
 
+def other_configs(lib, torch, dev, sp, stream):
+    """The remaining BASELINE configurations, device resident, plain FP64
+    DMMA vs Ozaki: DGEMM 1024^3 (alpha 1.5, beta -0.5), DTRSM L/L/N/N 4096
+    (alpha 2, A lower + 4096 on the diagonal), DSYRK and ZHERK L/N
+    N = K = 8192 (alpha = beta = 1).  Flops: reference blas/flops.h."""
+    g = torch.Generator(device=dev).manual_seed(1234)
+    out = {}
+
+    def u(*shape, cplx=False):
+        if cplx:
+            return torch.complex(torch.rand(*shape, generator=g, device=dev, dtype=torch.float64) - 0.5,
+                                 torch.rand(*shape, generator=g, device=dev, dtype=torch.float64) - 0.5)
+        return torch.rand(*shape, generator=g, device=dev, dtype=torch.float64) - 0.5
+
+    def timed(fn, reps, reset=None):
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        if reset:
+            reset()
+        assert fn() == 0
+        torch.cuda.synchronize()
+        tot = 0.0
+        for _ in range(reps):
+            if reset:
+                reset()
+            ev0.record(stream)
+            assert fn() == 0
+            ev1.record(stream)
+            torch.cuda.synchronize()
+            tot += ev0.elapsed_time(ev1)
+        return tot / reps
+
+    # config 1: DGEMM NN 1024^3
+    n = 1024
+    A, B, C0 = u(n, n), u(n, n), u(n, n)
+    C = C0.clone()
+    ga = GemmArgs(1, 0, 0, n, n, n, A.data_ptr(), n, B.data_ptr(), n, C.data_ptr(), n)
+    ga.alpha[0], ga.beta[0] = 1.5, -0.5
+    fl = 2.0 * n ** 3
+    with torch.cuda.stream(stream):
+        rs = lambda: C.copy_(C0)
+        tp = timed(lambda: lib.xkb_cuda_gemm(ctypes.byref(ga), sp), 10, rs)
+        to = timed(lambda: lib.xkb_cuda_ozaki_gemm(ctypes.byref(ga), 0, sp), 10, rs)
+    out["dgemm_nn_1024_nb256"] = {"plain_tflops": fl / tp / 1e9, "ozaki_tflops": fl / to / 1e9,
+                                  "plain_ms": tp, "ozaki_ms": to}
+    del A, B, C, C0
+    # config 2: DTRSM L/L/N/N 4096, alpha 2
+    n = 4096
+    A = torch.tril(u(n, n)) + n * torch.eye(n, device=dev, dtype=torch.float64)
+    Acm = A.t().contiguous()  # row-major storage of the column-major lower matrix
+    B0 = u(n, n)
+    B = B0.clone()
+    al = (ctypes.c_double * 2)(2.0, 0.0)
+    al = ctypes.cast(al, ctypes.POINTER(ctypes.c_double))
+    fl = float(n) * n * (n + 1)
+    with torch.cuda.stream(stream):
+        rs = lambda: B.copy_(B0)
+        tp = timed(lambda: lib.xkb_cuda_trsm(1, 0, 1, 0, 0, n, n, al, Acm.data_ptr(), n,
+                                             B.data_ptr(), n, 0, sp), 5, rs)
+        to = timed(lambda: lib.xkb_cuda_trsm(1, 0, 1, 0, 0, n, n, al, Acm.data_ptr(), n,
+                                             B.data_ptr(), n, 1024, sp), 5, rs)
+    out["dtrsm_llnn_4096"] = {"plain_tflops": fl / tp / 1e9, "ozaki_tflops": fl / to / 1e9,
+                              "plain_ms": tp, "ozaki_ms": to}
+    del A, Acm, B, B0
+    # config 3: DSYRK / ZHERK lower, no-trans, N = K = 8192
+    n = 8192
+    for name, cplx, code, mult in (("dsyrk_ln_8192", False, 1, 1.0), ("zherk_ln_8192", True, 3, 4.0)):
+        A = u(n, n, cplx=cplx)
+        C0 = u(n, n, cplx=cplx)
+        C = C0.clone()
+        gs = GemmArgs(code, 0, 2 if cplx else 1, n, n, n, A.data_ptr(), n, A.data_ptr(), n,
+                      C.data_ptr(), n)
+        gs.alpha[0], gs.beta[0] = 1.0, 1.0
+        gs.uplo = 1  # lower
+        gs.herm_diag = 1 if cplx else 0
+        fl = mult * n * (n + 1.0) * n
+        with torch.cuda.stream(stream):
+            rs = lambda: C.copy_(C0)
+            tp = timed(lambda: lib.xkb_cuda_gemm(ctypes.byref(gs), sp), 2, rs)
+            to = timed(lambda: lib.xkb_cuda_ozaki_gemm(ctypes.byref(gs), 0, sp), 3, rs)
+        out[name] = {"plain_tflops": fl / tp / 1e9, "ozaki_tflops": fl / to / 1e9,
+                     "plain_ms": tp, "ozaki_ms": to}
+        del A, C, C0
+    torch.cuda.empty_cache()
+    return out
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -385,6 +472,7 @@ def main():
         "device_error": deverr,
     }
     if rank == 0 and not args.no_extra:
+        line["other_configs"] = other_configs(lib, torch, f"cuda:{local}", sp, stream)
         # accuracy against the double-double oracle and the CPU baseline
         # (bounded samples; checker / baseline only)
         Co = np.asfortranarray(dC.cpu().numpy().T)

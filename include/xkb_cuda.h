@@ -131,6 +131,34 @@ typedef struct xkb_trace_rec {
 int xkb_trace_enable(int on);
 int xkb_trace_take(xkb_trace_rec* out, int max);
 
+/* Batched execution: a list of independent GEMM / left-TRSM calls on device
+ * operands run as ONE persistent launch of tile tasks (a DAG with device
+ * dependency counters; replaces the reference's task runtime,
+ * kaapi/kaapi_task.c:1277-1327 and kaapi/kaapi_offload_device.c:463-683).
+ * dtype XKB_D or XKB_Z; leading dimensions x element size multiples of 16
+ * bytes, 16-byte aligned bases.  Calls of one batch must not write memory
+ * another call of the batch reads or writes. */
+#define XKB_BATCH_GEMM 0
+#define XKB_BATCH_TRSM 1
+typedef struct xkb_batch_op {
+  int kind;                    /* XKB_BATCH_GEMM / XKB_BATCH_TRSM            */
+  int dtype;                   /* XKB_D / XKB_Z                              */
+  int opA, opB;                /* gemm: XKB_OP_N/T/C                         */
+  int side, uplo, trans, diag; /* trsm: side 0 (left) only; uplo XKB_LOWER/
+                                  XKB_UPPER; trans XKB_OP_*; diag 1 = unit   */
+  int M, N, K;                 /* gemm: C is M x N, K inner; trsm: B is M x N */
+  const void* A; long lda;
+  const void* B; long ldb;     /* gemm only                                  */
+  void* C; long ldc;           /* gemm: C; trsm: B (solved in place)         */
+  double alpha[2], beta[2];
+} xkb_batch_op;
+/* schedule: 0 = gemm tiles first, 1 = solve steps interleaved with gemm
+ * tiles (dependent steps far apart in the claim order). */
+int xkb_cuda_batch(const xkb_batch_op* ops, int nops, int schedule, void* stream);
+/* After a batch: ms[i] = completion time of call i after the batch's first
+ * task started (synchronises the device). */
+int xkb_cuda_batch_latency(double* ms, int n);
+
 /* Device error word written by bounded waits (0 = none); clears it. */
 int xkb_cuda_take_device_error(void);
 

@@ -29,6 +29,18 @@ _REAL = {"s": np.float32, "d": np.float64, "c": np.float32, "z": np.float64}
 _lib = None
 
 
+class BatchOp(ctypes.Structure):
+    """xkb_batch_op of include/xkb_cuda.h."""
+    _fields_ = [("kind", ctypes.c_int), ("dtype", ctypes.c_int), ("opA", ctypes.c_int),
+                ("opB", ctypes.c_int), ("side", ctypes.c_int), ("uplo", ctypes.c_int),
+                ("trans", ctypes.c_int), ("diag", ctypes.c_int), ("M", ctypes.c_int),
+                ("N", ctypes.c_int), ("K", ctypes.c_int),
+                ("A", ctypes.c_void_p), ("lda", ctypes.c_long),
+                ("B", ctypes.c_void_p), ("ldb", ctypes.c_long),
+                ("C", ctypes.c_void_p), ("ldc", ctypes.c_long),
+                ("alpha", ctypes.c_double * 2), ("beta", ctypes.c_double * 2)]
+
+
 class XkblasError(RuntimeError):
     pass
 
@@ -67,6 +79,19 @@ def lib():
             ctypes.c_size_t, ctypes.c_size_t]
         _lib.xkblas_memory_invalidate.argtypes = [ctypes.c_void_p]
         _lib.xkb_cuda_kernel_count.restype = ctypes.c_uint64
+        c_int, c_long, c_vp = ctypes.c_int, ctypes.c_long, ctypes.c_void_p
+        dptr = ctypes.POINTER(ctypes.c_double)
+        _lib.xkb_cuda_trsm.argtypes = [c_int, c_int, c_int, c_int, c_int, c_int, c_int, dptr,
+                                       c_vp, c_long, c_vp, c_long, c_int, c_vp]
+        _lib.xkb_cuda_trmm.argtypes = [c_int, c_int, c_int, c_int, c_int, c_int, c_int, dptr,
+                                       c_vp, c_long, c_vp, c_long, c_vp]
+        _lib.xkb_cuda_symm.argtypes = [c_int, c_int, c_int, c_int, c_int, c_int, dptr, c_vp,
+                                       c_long, c_vp, c_long, dptr, c_vp, c_long, c_vp]
+        _lib.xkb_cuda_scale.argtypes = [c_int, c_int, c_int, dptr, c_vp, c_long, c_int, c_int,
+                                        c_long, c_vp]
+        _lib.xkb_ozaki_default_moduli.argtypes = [c_long]
+        _lib.xkb_cuda_batch.argtypes = [ctypes.POINTER(BatchOp), c_int, c_int, c_vp]
+        _lib.xkb_cuda_batch_latency.argtypes = [ctypes.POINTER(ctypes.c_double), c_int]
         _lib.xkblas_get_stats.argtypes = [ctypes.POINTER(Stats)]
     return _lib
 

@@ -24,40 +24,10 @@
 #include <cstdio>
 #include <cstdlib>
 
+#include "dmma_common.cuh"
 #include "xkb_dev.cuh"
 
 namespace xkb {
-
-template <class T>
-struct St;
-template <>
-struct St<float> {
-  using S = float;
-  static constexpr int W = 1;
-  static constexpr bool CPLX = false;
-  static constexpr CUtensorMapDataType DT = CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
-};
-template <>
-struct St<double> {
-  using S = double;
-  static constexpr int W = 1;
-  static constexpr bool CPLX = false;
-  static constexpr CUtensorMapDataType DT = CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
-};
-template <>
-struct St<float2> {
-  using S = float;
-  static constexpr int W = 2;
-  static constexpr bool CPLX = true;
-  static constexpr CUtensorMapDataType DT = CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
-};
-template <>
-struct St<double2> {
-  using S = double;
-  static constexpr int W = 2;
-  static constexpr bool CPLX = true;
-  static constexpr CUtensorMapDataType DT = CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
-};
 
 struct GemmParams {
   int M, N, K;
@@ -74,33 +44,6 @@ constexpr int kBK = 16;      // k extent of one pipeline stage
 constexpr int kStages = 4;
 constexpr int kConsumerWarps = 8;
 constexpr int kThreads = kConsumerWarps * 32;
-
-__device__ __forceinline__ void dmma_k8(double (&d)[4], const double (&a)[4],
-                                        const double (&b)[2]) {
-  asm volatile(
-      "mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 "
-      "{%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
-      : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
-      : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
-}
-
-template <class T>
-__device__ __forceinline__ void ld_elem(const typename St<T>::S* s, int e, double& re,
-                                        double& im) {
-  if constexpr (St<T>::CPLX) {
-    re = static_cast<double>(s[2 * e]);
-    im = static_cast<double>(s[2 * e + 1]);
-  } else {
-    re = static_cast<double>(s[e]);
-    im = 0.0;
-  }
-}
-
-__device__ __forceinline__ bool in_mask(int uplo, long diag, int row, int col) {
-  if (uplo == XKB_LOWER) return (long)row + diag >= (long)col;
-  if (uplo == XKB_UPPER) return (long)row + diag <= (long)col;
-  return true;
-}
 
 // A_KC: op(A) != N, A tile stored [BM][BK] (k contiguous), else [BK][BM].
 // B_KC: op(B) == N, B tile stored [BN][BK], else [BK][BN].

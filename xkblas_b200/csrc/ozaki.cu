@@ -48,6 +48,7 @@ struct Consts {
   float invp_f[kMaxMod];
   double invp_d[kMaxMod];
   uint32_t wlo[kMaxMod], whi[kMaxMod];  // bytes of 2^(8t) mod p, t = 0..3, 4..7
+  uint32_t off[kMaxMod];                // p - (2^62 mod p): undoes the +2^62 offset
   uint32_t crt[kMaxMod][4];             // (P/p)((P/p)^-1 mod p) mod P, 32-bit limbs
   uint32_t P[4], Ph[4];                 // P and floor(P/2)
   double Pd, invPd;
@@ -125,7 +126,7 @@ static bool make_consts(int n, Consts* c) {
   for (int i = 0; i < n; ++i) {
     const int p = m[i];
     c->p[i] = p;
-    c->invp_f[i] = 1.0f / (float)p;
+    c->invp_f[i] = std::nextafter(1.0f / (float)p, 0.0f);  // <= 1/p (see k_oz_residues)
     c->invp_d[i] = 1.0 / (double)p;
     uint32_t lo = 0, hi = 0;
     for (int t = 0; t < 8; ++t) {
@@ -136,6 +137,9 @@ static bool make_consts(int n, Consts* c) {
     }
     c->wlo[i] = lo;
     c->whi[i] = hi;
+    uint64_t t62 = 1;
+    for (int s2 = 0; s2 < 62; ++s2) t62 = (t62 * 2) % (uint64_t)p;
+    c->off[i] = (uint32_t)((uint64_t)p - t62);
     const u128 Mi = P / (u128)p;
     const int inv = inv_mod((int)(Mi % (u128)p), p);
     const u128 w = mulmod(Mi, (u128)inv, P);
@@ -221,6 +225,11 @@ __global__ void __launch_bounds__(256) k_oz_norm(int L, int K, const double* X, 
   }
 }
 
+// 2^e as a double for -1022 <= e <= 1023 (exact, no libm call)
+__device__ __forceinline__ double pow2(int e) {
+  return __longlong_as_double((long long)(1023 + e) << 52);
+}
+
 // Sentinel shift: the row holds Inf/NaN; the result entries become NaN.
 constexpr int kShiftNonFinite = -100000;
 
@@ -256,7 +265,7 @@ __global__ void k_oz_shift(int L, int K, int nchunks, const double2* part, int H
 // 2. residues: planes[m][l][k] (int8, row stride Kpad) for l < Lpad, k < Kpad
 //    (zero padding), from X (L x K view, KC: k contiguous).  Complex operands
 //    (cplx = 1) are handled by the caller through the concatenated views.
-template <bool KC>
+template <bool KC, int NM>
 __global__ void __launch_bounds__(256) k_oz_residues(int L, int K, const double* X, long ld,
                                                       long estride, long eoff, double esign,
                                                       const int* mu, const Consts c,
@@ -288,40 +297,39 @@ __global__ void __launch_bounds__(256) k_oz_residues(int L, int K, const double*
     const int ll = it >> 4, kq = (it & 15) * 4;
     const int l = l0 + ll;
     const int s = (l < L) ? mu[l] : 0;
+    // a' = a + 2^62 >= 0 (|a| < 2^62); residues of a' are shifted back by the
+    // per-modulus constant folded into c.off (no sign handling per modulus)
+    const double sc = (s == kShiftNonFinite) ? 0.0 : pow2(s / 2) * pow2(s - s / 2);
     long long a[4];
-#pragma unroll
-    for (int v = 0; v < 4; ++v) {
-      const double x = tile[ll][kq + v];
-      a[v] = (s == kShiftNonFinite) ? 0LL : llrint(ldexp(x, s));
-    }
     uint32_t lo[4], hi[4];
-    bool neg[4];
 #pragma unroll
     for (int v = 0; v < 4; ++v) {
-      neg[v] = a[v] < 0;
-      const unsigned long long u = neg[v] ? (unsigned long long)(-a[v]) : (unsigned long long)a[v];
+      const double x = tile[ll][kq + v] * sc;  // exact power-of-two scaling
+      a[v] = llrint(x);
+      const unsigned long long u = (unsigned long long)a[v] + (1ull << 62);
       lo[v] = (uint32_t)u;
       hi[v] = (uint32_t)(u >> 32);
     }
     int8_t* dst = planes + (size_t)l * Kpad + kofs + k0 + kq;
-    for (int m = 0; m < c.nmod; ++m) {
+#pragma unroll
+    for (int m = 0; m < NM; ++m) {
       uint32_t packed = 0;
       const int p = c.p[m];
 #pragma unroll
       for (int v = 0; v < 4; ++v) {
         int r;
-        if (p == 256) {
-          r = (int)(int8_t)(uint8_t)(uint32_t)(unsigned long long)a[v];  // two's complement
+        if (m == 0) {  // p_0 = 256: the two's complement low byte
+          r = (int)(int8_t)(uint8_t)(unsigned long long)a[v];  // offset 2^62 = 0 mod 256
         } else {
-          unsigned int sacc = __dp4a(lo[v], c.wlo[m], 0u);
+          // a' mod p from its bytes: off + sum_t byte_t (2^(8t) mod p), where
+          // off = p - (2^62 mod p) removes the offset (total < 2^20)
+          unsigned int sacc = __dp4a(lo[v], c.wlo[m], c.off[m]);
           sacc = __dp4a(hi[v], c.whi[m], sacc);
-          const unsigned int q = (unsigned int)((float)sacc * c.invp_f[m]);
-          int rr = (int)sacc - (int)(q * (unsigned int)p);
-          if (rr < 0) rr += p;
-          else if (rr >= p) rr -= p;
-          if (neg[v] && rr) rr = p - rr;
-          if (rr > (p >> 1)) rr -= p;
-          r = rr;
+          // invp_f <= 1/p, round toward zero: q in {floor(s/p) - 1, floor(s/p)}
+          const unsigned int q = __float2uint_rz(__fmul_rz(__uint2float_rn(sacc), c.invp_f[m]));
+          int rr = (int)(sacc - q * (unsigned int)p);
+          if (rr >= p) rr -= p;
+          r = rr > (p >> 1) ? rr - p : rr;  // symmetric residue
         }
         packed |= ((uint32_t)(uint8_t)(int8_t)r) << (8 * v);
       }
@@ -331,15 +339,21 @@ __global__ void __launch_bounds__(256) k_oz_residues(int L, int K, const double*
 }
 
 // ---------------------------------------------------------------------------
-// 3. INT8 tensor-core GEMM, one CTA per (128 x 256 C tile, modulus).
+// 3. INT8 tensor-core GEMM: persistent CTAs (one per SM) walking the
+//    (modulus, 128 x 256 C tile) list.  Warp 0: TMA producer into a 4-stage
+//    ring; warp 1: TMEM allocator (512 columns = two 256-column accumulators)
+//    and single-thread MMA issuer; warps 2-5: epilogue.  The accumulator is
+//    double buffered, so the epilogue of tile i (TMEM -> registers -> mod p ->
+//    uint8 plane) runs while the MMAs of tile i+1 fill the other buffer.
 constexpr int BM = 128, BN = 256, BKB = 128;  // BKB: k bytes per stage
 constexpr int S = 4;
 constexpr uint32_t A_STAGE = BM * BKB, B_STAGE = BN * BKB;
 constexpr int kGemmThreads = 192;
-constexpr uint32_t kTmemCols = 256;
+constexpr uint32_t kTmemCols = 512;  // two accumulators of BN columns
+constexpr int kEpiWarps = 4;
 
 struct GemmP {
-  int tiles_m, tiles_n, kblocks;
+  int tiles_m, tiles_n, kblocks, nmod;
   uint8_t* R;
   long Mpad, Npad;
   int uplo;
@@ -387,6 +401,25 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* m, int
       : "memory");
 }
 
+// tile t of the (modulus-major, grouped raster) list; false if the tile lies
+// wholly outside the written triangle
+__device__ __forceinline__ bool oz_tile(const GemmP& p, int t, int& mod, int& m0, int& n0) {
+  const int tiles_mn = p.tiles_m * p.tiles_n;
+  mod = t / tiles_mn;
+  const int r = t - mod * tiles_mn;
+  const int GROUP = 8;
+  const int span = GROUP * p.tiles_n;
+  const int first_m = (r / span) * GROUP;
+  const int gsz = min(p.tiles_m - first_m, GROUP);
+  const int tm = first_m + (r % span) % gsz;
+  const int tn = (r % span) / gsz;
+  m0 = tm * BM;
+  n0 = tn * BN;
+  if (p.uplo == XKB_LOWER && (long)(m0 + BM - 1) + p.diag < (long)n0) return false;
+  if (p.uplo == XKB_UPPER && (long)m0 + p.diag > (long)(n0 + BN - 1)) return false;
+  return true;
+}
+
 __global__ void __launch_bounds__(kGemmThreads, 1)
     k_oz_gemm(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUtensorMap tB,
               const GemmP p) {
@@ -397,28 +430,21 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
   uint8_t* sB = sm + S * A_STAGE;
   uint64_t* full = reinterpret_cast<uint64_t*>(sB + S * B_STAGE);
   uint64_t* empty = full + S;
-  uint64_t* accf = empty + S;
-  uint32_t* tslot = reinterpret_cast<uint32_t*>(accf + 1);
+  uint64_t* accf = empty + S;  // [2] accumulator ready
+  uint64_t* acce = accf + 2;   // [2] accumulator drained
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(acce + 2);
 
-  const int mod = blockIdx.y;
-  const int GROUP = 8;
-  const int span = GROUP * p.tiles_n;
-  const int bid = blockIdx.x;
-  const int first_m = (bid / span) * GROUP;
-  const int gsz = min(p.tiles_m - first_m, GROUP);
-  const int tm = first_m + (bid % span) % gsz;
-  const int tn = (bid % span) / gsz;
-  const int m0 = tm * BM, n0 = tn * BN;
-  if (p.uplo == XKB_LOWER && (long)(m0 + BM - 1) + p.diag < (long)n0) return;
-  if (p.uplo == XKB_UPPER && (long)m0 + p.diag > (long)(n0 + BN - 1)) return;
-
+  const int total = p.tiles_m * p.tiles_n * p.nmod;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
     for (int s = 0; s < S; ++s) {
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
     }
-    mbar_init(accf, 1);
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&accf[b], 1);
+      mbar_init(&acce[b], kEpiWarps);
+    }
     fence_barrier_init();
   }
   if (warp == 1) {
@@ -438,13 +464,22 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
     if (lane == 0) {  // ---- TMA producer
       tma_prefetch(&tA);
       tma_prefetch(&tB);
-      for (int kb = 0; kb < KB; ++kb) {
-        const int s = kb % S;
-        const uint32_t ph = (kb / S) & 1;
-        if (!mbar_wait(&empty[s], ph ^ 1, kErrEmptyWait)) break;
-        mbar_expect_tx(&full[s], A_STAGE + B_STAGE);
-        tma_load_3d(sA + s * A_STAGE, &tA, kb * BKB, m0, mod, &full[s]);
-        tma_load_3d(sB + s * B_STAGE, &tB, kb * BKB, n0, mod, &full[s]);
+      uint32_t it = 0;
+      bool ok = true;
+      for (int t = blockIdx.x; t < total && ok; t += gridDim.x) {
+        int mod, m0, n0;
+        if (!oz_tile(p, t, mod, m0, n0)) continue;
+        for (int kb = 0; kb < KB; ++kb, ++it) {
+          const int s = it % S;
+          const uint32_t ph = (it / S) & 1;
+          if (!mbar_wait(&empty[s], ph ^ 1, kErrEmptyWait)) {
+            ok = false;
+            break;
+          }
+          mbar_expect_tx(&full[s], A_STAGE + B_STAGE);
+          tma_load_3d(sA + s * A_STAGE, &tA, kb * BKB, m0, mod, &full[s]);
+          tma_load_3d(sB + s * B_STAGE, &tB, kb * BKB, n0, mod, &full[s]);
+        }
       }
     }
   } else if (warp == 1) {
@@ -453,28 +488,49 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
       // N >> 3 at bit 17, M >> 4 at bit 24
       const uint32_t idesc = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
                              ((uint32_t)(BM >> 4) << 24);
-      for (int kb = 0; kb < KB; ++kb) {
-        const int s = kb % S;
-        const uint32_t ph = (kb / S) & 1;
-        if (!mbar_wait(&full[s], ph, kErrFullWait)) break;
+      uint32_t it = 0, tl = 0;
+      bool ok = true;
+      for (int t = blockIdx.x; t < total && ok; t += gridDim.x) {
+        int mod, m0, n0;
+        if (!oz_tile(p, t, mod, m0, n0)) continue;
+        const int b = tl & 1;
+        const uint32_t aph = (tl >> 1) & 1;
+        if (!mbar_wait(&acce[b], aph ^ 1, kErrAccWait)) break;  // buffer drained
         tc_fence_after();
-        const uint32_t a0 = smem_u32(sA + s * A_STAGE), b0 = smem_u32(sB + s * B_STAGE);
+        const uint32_t d = tmem + (uint32_t)(b * BN);
+        for (int kb = 0; kb < KB; ++kb, ++it) {
+          const int s = it % S;
+          const uint32_t ph = (it / S) & 1;
+          if (!mbar_wait(&full[s], ph, kErrFullWait)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t a0 = smem_u32(sA + s * A_STAGE), b0 = smem_u32(sB + s * B_STAGE);
 #pragma unroll
-        for (int k = 0; k < BKB / 32; ++k)
-          tc_mma_i8(tmem, desc_sw128(a0 + 32 * k), desc_sw128(b0 + 32 * k), idesc,
-                    (kb | k) != 0 ? 1u : 0u);
-        tc_commit(&empty[s]);  // stage s free once these MMAs have read it
+          for (int k = 0; k < BKB / 32; ++k)
+            tc_mma_i8(d, desc_sw128(a0 + 32 * k), desc_sw128(b0 + 32 * k), idesc,
+                      (kb | k) != 0 ? 1u : 0u);
+          tc_commit(&empty[s]);  // stage s free once these MMAs have read it
+        }
+        tc_commit(&accf[b]);  // accumulator b complete (also drains an aborted loop)
+        ++tl;
       }
-      tc_commit(accf);  // accumulator complete (also drains an aborted loop)
     }
   } else {
     // ---- epilogue: warps 2..5, TMEM lanes 32*(warp%4) .. +31
-    const bool got = mbar_wait(accf, 0, kErrAccWait);
-    if (__all_sync(0xffffffffu, got)) {  // uniform and converged for tcgen05.ld
+    const int q = warp & 3;
+    uint32_t tl = 0;
+    for (int t = blockIdx.x; t < total; t += gridDim.x) {
+      int mod, m0, n0;
+      if (!oz_tile(p, t, mod, m0, n0)) continue;
+      const int b = tl & 1;
+      const uint32_t aph = (tl >> 1) & 1;
+      const bool got = mbar_wait(&accf[b], aph, kErrAccWait);
+      if (!__all_sync(0xffffffffu, got)) break;  // uniform and converged for tcgen05.ld
       tc_fence_after();
-      const int q = warp & 3;
       const int row = m0 + q * 32 + lane;
-      const uint32_t tbase = tmem + ((uint32_t)(q * 32) << 16);
+      const uint32_t tbase = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * BN);
       const int pm = p.p[mod];
       const double ip = p.invp[mod];
       uint8_t* plane = p.R + (size_t)mod * (size_t)p.Mpad * (size_t)p.Npad;
@@ -488,6 +544,12 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
               "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
             : "r"(tbase + (uint32_t)(c * 16)));
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        if (c == BN / 16 - 1) {
+          // every column of buffer b is in registers: hand it back to the MMA warp
+          tc_fence_before();
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&acce[b]);
+        }
 #pragma unroll
         for (int e = 0; e < 16; ++e) {
           const int acc = (int)v[e];
@@ -499,6 +561,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
           plane[col * (size_t)p.Mpad + (size_t)row] = (uint8_t)r;
         }
       }
+      ++tl;
     }
   }
   tc_fence_before();
@@ -529,125 +592,64 @@ struct CrtP {
   long diag;
 };
 
-__device__ __forceinline__ double crt_value(const uint32_t (&r)[kMaxMod], const Consts& c) {
-  // S = sum_l r_l * w_l   (< 2^138), 32-bit limbs accumulated in 64 bits
+// Exact recombination.  S = sum_l r_l w_l (< 2^12 P, 160 bits as 32-bit
+// limbs).  The shifts keep |C'| <= P/8, so the wanted value is S - qP with
+// q = round(S / P): a double estimate of S/P is within 2^-38 of the truth and
+// S/P lies within 1/8 of an integer, so q is exact and no correction or
+// range mapping is needed.  |S - qP| < 2^124: it is computed modulo 2^128 and
+// read as a signed 128-bit integer, then converted to double (two roundings).
+template <int NM>
+__device__ __forceinline__ double crt_value(const uint32_t (&r)[NM], const Consts& c) {
   unsigned long long a0 = 0, a1 = 0, a2 = 0, a3 = 0;
-  for (int m = 0; m < c.nmod; ++m) {
+#pragma unroll
+  for (int m = 0; m < NM; ++m) {
     const unsigned long long rv = r[m];
     a0 += rv * c.crt[m][0];
     a1 += rv * c.crt[m][1];
     a2 += rv * c.crt[m][2];
     a3 += rv * c.crt[m][3];
   }
-  uint32_t L0, L1, L2, L3, L4;
-  L0 = (uint32_t)a0;
   a1 += a0 >> 32;
-  L1 = (uint32_t)a1;
   a2 += a1 >> 32;
-  L2 = (uint32_t)a2;
   a3 += a2 >> 32;
-  L3 = (uint32_t)a3;
-  L4 = (uint32_t)(a3 >> 32);
-  // q ~ floor(S / P)
-  const double Sd = ((double)L4 * 4294967296.0 + (double)L3) * 79228162514264337593543950336.0 +
-                    (double)L2 * 18446744073709551616.0;
-  long long qq = (long long)floor(Sd * c.invPd);
-  if (qq < 0) qq = 0;
-  const unsigned long long q = (unsigned long long)qq;
-  // R = S - q*P  (5 limbs, signed via borrow)
-  unsigned long long t;
-  long long borrow;
-  t = q * c.P[0];
-  long long d0 = (long long)L0 - (long long)(t & 0xffffffffull);
-  unsigned long long carry = t >> 32;
-  borrow = d0 < 0 ? 1 : 0;
-  uint32_t R0 = (uint32_t)(d0 + (borrow << 32));
-  t = q * c.P[1] + carry;
-  carry = t >> 32;
-  long long d1 = (long long)L1 - (long long)(t & 0xffffffffull) - borrow;
-  borrow = d1 < 0 ? 1 : 0;
-  uint32_t R1 = (uint32_t)(d1 + (borrow << 32));
-  t = q * c.P[2] + carry;
-  carry = t >> 32;
-  long long d2 = (long long)L2 - (long long)(t & 0xffffffffull) - borrow;
-  borrow = d2 < 0 ? 1 : 0;
-  uint32_t R2 = (uint32_t)(d2 + (borrow << 32));
-  t = q * c.P[3] + carry;
-  carry = t >> 32;
-  long long d3 = (long long)L3 - (long long)(t & 0xffffffffull) - borrow;
-  borrow = d3 < 0 ? 1 : 0;
-  uint32_t R3 = (uint32_t)(d3 + (borrow << 32));
-  long long d4 = (long long)L4 - (long long)carry - borrow;  // top limb (small, signed)
-  // bring R into [0, P): at most a couple of corrections either way
-  for (int it = 0; it < 3; ++it) {
-    if (d4 < 0) {  // add P
-      unsigned long long s0 = (unsigned long long)R0 + c.P[0];
-      R0 = (uint32_t)s0;
-      unsigned long long s1 = (unsigned long long)R1 + c.P[1] + (s0 >> 32);
-      R1 = (uint32_t)s1;
-      unsigned long long s2 = (unsigned long long)R2 + c.P[2] + (s1 >> 32);
-      R2 = (uint32_t)s2;
-      unsigned long long s3 = (unsigned long long)R3 + c.P[3] + (s2 >> 32);
-      R3 = (uint32_t)s3;
-      d4 += (long long)(s3 >> 32);
-    } else {
-      // R >= P ?
-      bool ge = d4 > 0;
-      if (!ge) {
-        ge = R3 > c.P[3] ||
-             (R3 == c.P[3] && (R2 > c.P[2] || (R2 == c.P[2] && (R1 > c.P[1] ||
-                                                              (R1 == c.P[1] && R0 >= c.P[0])))));
-      }
-      if (!ge) break;
-      long long e0 = (long long)R0 - c.P[0];
-      long long b = e0 < 0;
-      R0 = (uint32_t)(e0 + (b << 32));
-      long long e1 = (long long)R1 - c.P[1] - b;
-      b = e1 < 0;
-      R1 = (uint32_t)(e1 + (b << 32));
-      long long e2 = (long long)R2 - c.P[2] - b;
-      b = e2 < 0;
-      R2 = (uint32_t)(e2 + (b << 32));
-      long long e3 = (long long)R3 - c.P[3] - b;
-      b = e3 < 0;
-      R3 = (uint32_t)(e3 + (b << 32));
-      d4 -= b;
-    }
+  const unsigned long long lo = (a0 & 0xffffffffull) | (a1 << 32);
+  const unsigned long long hi = (a2 & 0xffffffffull) | (a3 << 32);  // S mod 2^128
+  const double Sd = (double)(a3 >> 32) * 340282366920938463463374607431768211456.0 +
+                    (double)(a3 & 0xffffffffull) * 79228162514264337593543950336.0 +
+                    (double)(a2 & 0xffffffffull) * 18446744073709551616.0;
+  const unsigned long long q = (unsigned long long)rint(Sd * c.invPd);
+  const unsigned long long Plo = ((unsigned long long)c.P[1] << 32) | c.P[0];
+  const unsigned long long Phi = ((unsigned long long)c.P[3] << 32) | c.P[2];
+  const unsigned long long qlo = q * Plo;
+  const unsigned long long qhi = q * Phi + __umul64hi(q, Plo);
+  unsigned long long rlo = lo - qlo;
+  unsigned long long rhi = hi - qhi - (lo < qlo ? 1ull : 0ull);
+  const bool neg = (long long)rhi < 0;
+  if (neg) {
+    rlo = ~rlo + 1ull;
+    rhi = ~rhi + (rlo == 0 ? 1ull : 0ull);
   }
-  // symmetric range: R > P/2 -> R - P (negative)
-  bool gt = R3 > c.Ph[3] ||
-            (R3 == c.Ph[3] && (R2 > c.Ph[2] || (R2 == c.Ph[2] && (R1 > c.Ph[1] ||
-                                                                (R1 == c.Ph[1] && R0 > c.Ph[0])))));
-  bool negv = false;
-  if (gt) {  // value = -(P - R)
-    long long e0 = (long long)c.P[0] - R0;
-    long long b = e0 < 0;
-    R0 = (uint32_t)(e0 + (b << 32));
-    long long e1 = (long long)c.P[1] - R1 - b;
-    b = e1 < 0;
-    R1 = (uint32_t)(e1 + (b << 32));
-    long long e2 = (long long)c.P[2] - R2 - b;
-    b = e2 < 0;
-    R2 = (uint32_t)(e2 + (b << 32));
-    long long e3 = (long long)c.P[3] - R3 - b;
-    b = e3 < 0;
-    R3 = (uint32_t)(e3 + (b << 32));
-    negv = true;
-  }
-  const unsigned long long hi = ((unsigned long long)R3 << 32) | R2;
-  const unsigned long long lo = ((unsigned long long)R1 << 32) | R0;
-  const double v = fma((double)hi, 18446744073709551616.0, (double)lo);
-  return negv ? -v : v;
+  const double v = fma((double)rhi, 18446744073709551616.0, (double)rlo);
+  return neg ? -v : v;
 }
 
+// x * 2^e for the shift range used here (|e| <= 2000), exact unless the
+// result under/overflows
+__device__ __forceinline__ double scale2(double x, int e) {
+  const int e1 = e / 2, e2 = e - e1;
+  return x * pow2(e1) * pow2(e2);
+}
+
+template <int NM>
 __global__ void __launch_bounds__(256) k_oz_crt(const CrtP p, const Consts c) {
   const long iq = (long)blockIdx.x * blockDim.x + threadIdx.x;  // row quad
   const long i0 = iq * 4;
   if (i0 >= p.M) return;
   for (int j = blockIdx.y; j < p.N; j += gridDim.y) {
   const size_t plane = (size_t)p.Mpad * (size_t)p.Npad;
-  uint32_t words[kMaxMod];
-  for (int m = 0; m < c.nmod; ++m)
+  uint32_t words[NM];
+#pragma unroll
+  for (int m = 0; m < NM; ++m)
     words[m] = *reinterpret_cast<const uint32_t*>(p.R + (size_t)m * plane + (size_t)j * p.Mpad + i0);
   const int nuj = p.nu[j];
 #pragma unroll
@@ -656,12 +658,13 @@ __global__ void __launch_bounds__(256) k_oz_crt(const CrtP p, const Consts c) {
     if (i >= p.M) break;
     if (p.uplo == XKB_LOWER && i + p.diag < j) continue;
     if (p.uplo == XKB_UPPER && i + p.diag > j) continue;
-    uint32_t r[kMaxMod];
-    for (int m = 0; m < c.nmod; ++m) r[m] = (words[m] >> (8 * v)) & 0xffu;
+    uint32_t r[NM];
+#pragma unroll
+    for (int m = 0; m < NM; ++m) r[m] = (words[m] >> (8 * v)) & 0xffu;
     const int mui = p.mu[i];
     double y;
     if (mui == kShiftNonFinite || nuj == kShiftNonFinite) y = __longlong_as_double(0x7ff8000000000000ll);
-    else y = ldexp(crt_value(r, c), -(mui + nuj));
+    else y = scale2(crt_value<NM>(r, c), -(mui + nuj));
     const size_t idx = (size_t)i + (size_t)j * p.ldc;
     if (!p.cplx) {
       double out = p.ar * y;
@@ -688,14 +691,16 @@ __global__ void __launch_bounds__(256) k_oz_crt(const CrtP p, const Consts c) {
 }
 
 // Complex first pass: Re(op(A)op(B)) (unscaled by alpha) into a scratch M x N.
+template <int NM>
 __global__ void __launch_bounds__(256) k_oz_crt_store(const CrtP p, const Consts c, double* out) {
   const long iq = (long)blockIdx.x * blockDim.x + threadIdx.x;
   const long i0 = iq * 4;
   if (i0 >= p.M) return;
   for (int j = blockIdx.y; j < p.N; j += gridDim.y) {
   const size_t plane = (size_t)p.Mpad * (size_t)p.Npad;
-  uint32_t words[kMaxMod];
-  for (int m = 0; m < c.nmod; ++m)
+  uint32_t words[NM];
+#pragma unroll
+  for (int m = 0; m < NM; ++m)
     words[m] = *reinterpret_cast<const uint32_t*>(p.R + (size_t)m * plane + (size_t)j * p.Mpad + i0);
   const int nuj = p.nu[j];
 #pragma unroll
@@ -704,15 +709,37 @@ __global__ void __launch_bounds__(256) k_oz_crt_store(const CrtP p, const Consts
     if (i >= p.M) break;
     if (p.uplo == XKB_LOWER && i + p.diag < j) continue;
     if (p.uplo == XKB_UPPER && i + p.diag > j) continue;
-    uint32_t r[kMaxMod];
-    for (int m = 0; m < c.nmod; ++m) r[m] = (words[m] >> (8 * v)) & 0xffu;
+    uint32_t r[NM];
+#pragma unroll
+    for (int m = 0; m < NM; ++m) r[m] = (words[m] >> (8 * v)) & 0xffu;
     const int mui = p.mu[i];
     double y;
     if (mui == kShiftNonFinite || nuj == kShiftNonFinite) y = __longlong_as_double(0x7ff8000000000000ll);
-    else y = ldexp(crt_value(r, c), -(mui + nuj));
+    else y = scale2(crt_value<NM>(r, c), -(mui + nuj));
     out[(size_t)i + (size_t)j * p.M] = y;
   }
   }
+}
+
+// CRT launches, dispatched on the moduli count
+template <int NM>
+static void crt_launch(dim3 g, cudaStream_t st, const CrtP& cp, const Consts& c, double* store) {
+  if (store) k_oz_crt_store<NM><<<g, 256, 0, st>>>(cp, c, store);
+  else k_oz_crt<NM><<<g, 256, 0, st>>>(cp, c);
+}
+static int launch_crt(dim3 g, cudaStream_t st, const CrtP& cp, const Consts& c, double* store) {
+  switch (c.nmod) {
+#define XKB_CRT_CASE(NM) \
+  case NM:               \
+    crt_launch<NM>(g, st, cp, c, store); break;
+    XKB_CRT_CASE(2) XKB_CRT_CASE(3) XKB_CRT_CASE(4) XKB_CRT_CASE(5) XKB_CRT_CASE(6)
+    XKB_CRT_CASE(7) XKB_CRT_CASE(8) XKB_CRT_CASE(9) XKB_CRT_CASE(10) XKB_CRT_CASE(11)
+    XKB_CRT_CASE(12) XKB_CRT_CASE(13) XKB_CRT_CASE(14) XKB_CRT_CASE(15) XKB_CRT_CASE(16)
+#undef XKB_CRT_CASE
+    default: return XKB_EINVAL;
+  }
+  count_launch();
+  return cudaPeekAtLastError() == cudaSuccess ? XKB_OK : XKB_ECUDA;
 }
 
 // ---------------------------------------------------------------------------
@@ -762,12 +789,22 @@ static int launch_res(const View& v, int L, int K, const int* mu, const Consts* 
                       long Lpad, long Kpad, long kofs, cudaStream_t st) {
   // grid covers Lpad x (K rounded to 64); kofs places the block at column kofs
   dim3 g((unsigned)(Lpad / 64), (unsigned)(rup((size_t)K, 64) / 64));
-  if (v.kc)
-    k_oz_residues<true><<<g, 256, 0, st>>>(L, K, v.X, v.ld, v.estride, v.eoff, v.sign, mu, *c,
-                                           planes, Lpad, Kpad, kofs);
-  else
-    k_oz_residues<false><<<g, 256, 0, st>>>(L, K, v.X, v.ld, v.estride, v.eoff, v.sign, mu, *c,
-                                            planes, Lpad, Kpad, kofs);
+#define XKB_RES_CASE(NM)                                                                     \
+  case NM:                                                                                   \
+    if (v.kc)                                                                                \
+      k_oz_residues<true, NM><<<g, 256, 0, st>>>(L, K, v.X, v.ld, v.estride, v.eoff, v.sign, \
+                                                 mu, *c, planes, Lpad, Kpad, kofs);          \
+    else                                                                                     \
+      k_oz_residues<false, NM><<<g, 256, 0, st>>>(L, K, v.X, v.ld, v.estride, v.eoff,       \
+                                                  v.sign, mu, *c, planes, Lpad, Kpad, kofs); \
+    break;
+  switch (c->nmod) {
+    XKB_RES_CASE(2) XKB_RES_CASE(3) XKB_RES_CASE(4) XKB_RES_CASE(5) XKB_RES_CASE(6)
+    XKB_RES_CASE(7) XKB_RES_CASE(8) XKB_RES_CASE(9) XKB_RES_CASE(10) XKB_RES_CASE(11)
+    XKB_RES_CASE(12) XKB_RES_CASE(13) XKB_RES_CASE(14) XKB_RES_CASE(15) XKB_RES_CASE(16)
+    default: return XKB_EINVAL;
+  }
+#undef XKB_RES_CASE
   count_launch();
   return cudaPeekAtLastError() == cudaSuccess ? XKB_OK : XKB_ECUDA;
 }
@@ -792,6 +829,7 @@ static int launch_gemm(const int8_t* Ap, long a_rows, const int8_t* Bp, long b_r
   p.tiles_m = (int)(Mpad / BM);
   p.tiles_n = (int)(Npad / BN);
   p.kblocks = (int)(Kpad / BKB);
+  p.nmod = c->nmod;
   p.R = R;
   p.Mpad = Mpad;
   p.Npad = Npad;
@@ -801,7 +839,7 @@ static int launch_gemm(const int8_t* Ap, long a_rows, const int8_t* Bp, long b_r
     p.p[m] = c->p[m];
     p.invp[m] = c->invp_d[m];
   }
-  const size_t smem = 1024 + S * (size_t)(A_STAGE + B_STAGE) + (2 * S + 1) * 8 + 16;
+  const size_t smem = 1024 + S * (size_t)(A_STAGE + B_STAGE) + (2 * S + 4) * 8 + 16;
   static bool attr = false;
   if (!attr) {
     if (cudaFuncSetAttribute(k_oz_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
@@ -809,8 +847,9 @@ static int launch_gemm(const int8_t* Ap, long a_rows, const int8_t* Bp, long b_r
       return XKB_ECUDA;
     attr = true;
   }
-  dim3 g((unsigned)(p.tiles_m * p.tiles_n), (unsigned)c->nmod);
-  k_oz_gemm<<<g, kGemmThreads, smem, st>>>(tA, tB, p);
+  const long total = (long)p.tiles_m * p.tiles_n * c->nmod;
+  const unsigned grid = (unsigned)std::min<long>(total, sm_count());  // persistent
+  k_oz_gemm<<<grid, kGemmThreads, smem, st>>>(tA, tB, p);
   count_launch();
   return cudaPeekAtLastError() == cudaSuccess ? XKB_OK : XKB_ECUDA;
 }
@@ -960,18 +999,15 @@ extern "C" int xkb_cuda_ozaki_gemm(const xkb_gemm_args* a, int nmod, void* strea
     if (!err) {
       if (!cplx) {
         trace_mark(slot, 2, st);
-        k_oz_crt<<<cg, 256, 0, st>>>(cp, *c);
-        count_launch();
+        err = launch_crt(cg, st, cp, *c, nullptr);
       } else {
-        k_oz_crt_store<<<cg, 256, 0, st>>>(cp, *c, re);
-        count_launch();
+        err = launch_crt(cg, st, cp, *c, re);
         err = launch_gemm(Ap, Mpad, Bp + szB, Npad, Mpad, Npad, Kpad, c, R, a->uplo, a->diag,
                           st);
         trace_mark(slot, 2, st);
         if (!err) {
           cp.other = re;
-          k_oz_crt<<<cg, 256, 0, st>>>(cp, *c);
-          count_launch();
+          err = launch_crt(cg, st, cp, *c, nullptr);
         }
       }
       if (!err && cudaPeekAtLastError() != cudaSuccess) err = XKB_ECUDA;
@@ -1110,9 +1146,7 @@ extern "C" int xkb_cuda_ozaki_gemm_noalloc(const xkb_gemm_args* a, int nmod, voi
     cp.uplo = a->uplo;
     cp.diag = a->diag;
     const dim3 cg((unsigned)((M / 4 + 1 + 255) / 256), (unsigned)N);
-    k_oz_crt<<<cg, 256, 0, st>>>(cp, *c);
-    count_launch();
-    if (cudaPeekAtLastError() != cudaSuccess) err = XKB_ECUDA;
+    err = launch_crt(cg, st, cp, *c, nullptr);
   }
   return err;
 }
