@@ -16,11 +16,6 @@ N_, T_, C_ = 0, 1, 2
 LO, UP = 1, 2
 
 
-def _cm(t):
-    """column-major view: a torch (cols, rows) row-major tensor."""
-    return t
-
-
 def _op(M, opc):
     return M if opc == N_ else (M.transpose(0, 1) if opc == T_ else M.transpose(0, 1).conj())
 
@@ -30,7 +25,7 @@ def test_mixed_batch(xk, schedule):
     import torch
     rng = np.random.default_rng(7)
     gen = torch.Generator(device="cuda").manual_seed(11)
-    ops, refs, keep = [], [], []
+    ops, refs, keep, hold = [], [], [], []
 
     def rnd(r, c, cplx):
         if cplx:
@@ -62,6 +57,7 @@ def test_mixed_batch(xk, schedule):
             o.alpha[0], o.alpha[1] = (al.real, al.imag) if cplx else (al, 0.0)
             o.beta[0], o.beta[1] = (be.real, be.imag) if cplx else (be, 0.0)
             out = C
+            hold.append(B)  # every operand must outlive the batch (allocator reuse)
         else:
             uplo = int(rng.choice([LO, UP]))
             trans = int(rng.integers(0, 3 if cplx else 2))
@@ -107,8 +103,9 @@ def test_batch_trsm_large_chain(xk):
     import torch
     M, N = 1000, 700
     g = torch.Generator(device="cuda").manual_seed(3)
-    A = torch.tril(torch.rand(M, M, generator=g, device="cuda", dtype=torch.float64) - 0.5).t() \
-        + M * torch.eye(M, device="cuda", dtype=torch.float64)  # column-major lower
+    L = torch.tril(torch.rand(M, M, generator=g, device="cuda", dtype=torch.float64) - 0.5) \
+        + M * torch.eye(M, device="cuda", dtype=torch.float64)
+    A = L.t().contiguous()  # column-major storage of the lower triangular L
     B0 = torch.rand(N, M, generator=g, device="cuda", dtype=torch.float64) - 0.5
     B = B0.clone()
     o = X.BatchOp()
@@ -118,6 +115,37 @@ def test_batch_trsm_large_chain(xk):
     torch.cuda.synchronize()
     assert xk.lib().xkb_cuda_batch(ctypes.byref(o), 1, 0, None) == 0
     xk.sync()
-    L = A.t()
+    assert xk.lib().xkb_cuda_take_device_error() == 0
     res = (L @ B.t() - 2.0 * B0.t()).abs().max().item()
     assert res < 1e-10
+
+
+def test_batch_ztrsm_multiblock(xk):
+    """Complex solves span several 64-row blocks: their trailing updates are
+    split into 32-row tasks (the complex tile height)."""
+    import torch
+    g = torch.Generator(device="cuda").manual_seed(5)
+    ops, keep = [], []
+    for (M, N, uplo, trans) in ((253, 182, UP, T_), (130, 70, LO, C_), (200, 65, LO, N_)):
+        L = torch.complex(torch.rand(M, M, generator=g, device="cuda", dtype=torch.float64),
+                          torch.rand(M, M, generator=g, device="cuda", dtype=torch.float64)) / M
+        L = L + torch.eye(M, device="cuda", dtype=torch.complex128)
+        A = L.t().contiguous()  # column-major storage of L
+        B0 = torch.complex(torch.rand(N, M, generator=g, device="cuda", dtype=torch.float64),
+                           torch.rand(N, M, generator=g, device="cuda", dtype=torch.float64))
+        B = B0.clone()
+        o = X.BatchOp()
+        o.kind, o.dtype, o.side, o.uplo, o.trans, o.diag, o.M, o.N = 1, 3, 0, uplo, trans, 0, M, N
+        o.A, o.lda, o.C, o.ldc = A.data_ptr(), M, B.data_ptr(), M
+        o.alpha[0], o.alpha[1] = 1.0, -1.0
+        ops.append(o)
+        tri = torch.tril(L) if uplo == LO else torch.triu(L)
+        keep.append((A, B, B0, _op(tri, trans)))
+    arr = (X.BatchOp * len(ops))(*ops)
+    torch.cuda.synchronize()
+    assert xk.lib().xkb_cuda_batch(arr, len(ops), 1, None) == 0
+    xk.sync()
+    assert xk.lib().xkb_cuda_take_device_error() == 0
+    for A, B, B0, opT in keep:
+        res = (opT @ B.t() - complex(1.0, -1.0) * B0.t()).abs().max().item()
+        assert res < 1e-12

@@ -5,27 +5,33 @@
 // (blas/ztask_gemm.c:107-158, ztask_trsm.c), their data-flow dependencies
 // (kaapi/kaapi_task.c:1277-1327) and the device threads that pop ready tasks
 // and launch one cuBLAS call each (kaapi/kaapi_offload_device.c:463-683,
-// 852-1210).  Here the host builds the task list once, in a topological
-// order; persistent CTAs claim tasks in that order with an atomic counter,
-// wait (bounded) on per-tile dependency counters, run the tile body on the
-// FP64 tensor cores, and bump the counters of the tiles they produced.  A
-// batch of small, uneven calls thus costs one launch instead of one launch
-// (or thousands of tile tasks with host round trips) per call.
+// 852-1210).  The host builds the task graph once; persistent CTAs (as many
+// as fit, two per SM) take dependency-free tasks from a bulk list and the
+// others from a device-side ready queue that completing tasks append their
+// successors to.  A batch of small, uneven calls thus costs one launch
+// instead of one launch (or thousands of tile tasks with host round trips)
+// per call.
 //
-// Tile bodies (256 threads):
-//   gemm   C[<=BM x <=BN] = alpha op(A) op(B) + beta C over the full K,
-//          cp.async 3-stage shared-memory ring (16-byte copies, or 8-byte
-//          ones when a leading dimension is odd; zero fill at ragged
-//          edges), DMMA m16n8k8; BM x BN = 64 x 64 (real), 32 x 64 (complex,
-//          four real MMAs per product);
-//   trsm   one 64-row diagonal block of a left triangular solve against up
-//          to 64 right-hand sides (the reference's tile body ztask_trsm.c);
-//          the trailing updates of the tile algorithm (blas/ztrsm.c:241-372)
-//          are gemm tasks.
+// Task bodies (256 threads):
+//   gemm     C[<=BM x <=BN] = alpha op(A) op(B) + beta C over the full K,
+//            cp.async 3-stage shared-memory ring (16-byte copies, or 8-byte
+//            L2 loads when a leading dimension is odd; zero fill at ragged
+//            edges), DMMA m16n8k8; BM x BN = 64 x 64 (real), 32 x 64
+//            (complex, four real MMAs per product);
+//   trsm     one 64-row block X_i of a left triangular solve against up to
+//            64 right-hand sides, left-looking: X_i = alpha B_i - sum_k
+//            op(A)[i,k] X_k over the blocks already solved (one gemm tile
+//            with the whole k range), then the diagonal solve with op(A)[i,i]
+//            in the same CTA.  The reference runs the same block algorithm
+//            right-looking (blas/ztrsm.c:241-372: diagonal trsm tasks, then
+//            gemm updates of the trailing blocks); here each right-hand-side
+//            block is one chain of mt tasks, and the sums are formed in
+//            registers once instead of read-modified-written per step.
 // Ordering rules: a producer stores, then __syncthreads, then thread 0
-// issues __threadfence and increments the counter; a consumer's thread 0
-// observes the counter, issues __threadfence, and the CTA reads through L2
-// (cp.async.cg / ld.global.cg) -- no stale L1 lines, no async-proxy reads.
+// issues __threadfence and decrements its successors' dependency counts;
+// the consumer's thread 0 takes the queued task, issues __threadfence, and
+// the CTA reads through L2 (cp.async.cg / ld.global.cg) -- no stale L1
+// lines, no async-proxy reads.
 #include <algorithm>
 #include <cstring>
 #include <mutex>
@@ -37,21 +43,43 @@
 namespace xkb {
 namespace sched {
 
-enum : int { kTaskGemm = 0, kTaskTrsmDiag = 1 };
+enum : int { kTaskGemm = 0, kTaskTrsm = 1 };
 // kFlagNarrow: an operand base or leading dimension is not 16-byte aligned,
-// so the gemm tile stages it with 8-byte copies instead of 16-byte ones
+// so the gemm tile stages it with 8-byte L2 loads instead of 16-byte copies
 enum : int { kFlagSwap = 1, kFlagConj = 2, kFlagLower = 4, kFlagUnit = 8, kFlagNarrow = 16 };
 
+// One task.  succ0 / nsucc: its successors in the batch's successor array
+// (tasks whose dependency count it decrements when it completes).
+//   gemm:  C = (ar,ai) op(A) op(B) + (br,bi) C, C is M x N, inner K.
+//   trsm:  C = X_i (M rows, N right-hand sides); A, B = the op(A) panel and
+//          the solved X rows it multiplies (K = their inner length, 0 for
+//          the first block); D = the diagonal block; (ar,ai) = alpha.
 struct alignas(16) Task {
   int kind, dtype, opA, opB;
   int M, N, K, call;
   const void* A;
   const void* B;
   void* C;
+  const void* D;
   long lda, ldb, ldc;
   double ar, ai, br, bi;
-  int wait0, target0, wait1, target1;
-  int signal, flags, pad0, pad1;
+  int succ0, nsucc, flags, pad;
+};
+static_assert(sizeof(Task) == 144, "task record");
+
+// Device-side queues of one batch (ints in global memory):
+//   bulk[nbulk]   tasks without dependencies (gemm tiles of gemm calls), in
+//                 call order; claimed with an atomic head;
+//   urq[nurg]     the solve tasks: a ready queue.  The first block of every
+//                 chain is queued at launch; a task is appended (atomic
+//                 tail, then the slot is written) when its last dependency
+//                 completes; slots not yet written hold -1.  A CTA takes a
+//                 ticket (atomic head) only while the queue shows a task it
+//                 could get, then waits for its slot: one atomic per claim,
+//                 no retry storms, and no deadlock (slots fill in order and
+//                 every queued task's producers were queued before it).
+struct Ctl {
+  int head_bulk, head_urg, tail_urg, pad;
 };
 
 constexpr int kThreads = 256;
@@ -77,74 +105,140 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
-// Bounded wait: *c >= target.  Returns false (error recorded) after the
-// time limit or when another CTA already recorded an error.
-__device__ __forceinline__ bool wait_ge(const int* c, int target) {
-  const volatile int* v = c;
-  if (*v >= target) return true;
-  const uint64_t t0 = globaltimer();
-  for (uint32_t i = 1;; ++i) {
-    if (*v >= target) return true;
-    __nanosleep(64);
-    if ((i & 63u) == 0) {
-      if (dev_error_set()) return false;
-      if (globaltimer() - t0 > kWaitLimitNs) {
+__device__ __forceinline__ int ld_volatile(const int* p) { return *(const volatile int*)p; }
+
+// Claim the next task for this CTA (thread 0 only): from the ready queue of
+// the solves or from the bulk list, in the order `urgent_first` asks.  Spins
+// (bounded) while every remaining task still waits for a dependency.
+// Returns the task id, -1 when every task has been claimed, -2 on timeout or
+// when another CTA recorded an error.
+__device__ __forceinline__ int claim_task(Ctl* ctl, const int* bulk, int nbulk, const int* urq,
+                                          int nurg, bool urgent_first) {
+  uint64_t t0 = 0;
+  for (uint32_t spin = 0;; ++spin) {
+    for (int pass = 0; pass < 2; ++pass) {
+      if ((pass == 0) == urgent_first) {
+        const int h = ld_volatile(&ctl->head_urg);
+        if (h < nurg && ld_volatile(&ctl->tail_urg) > h) {
+          const int tk = atomicAdd(&ctl->head_urg, 1);
+          if (tk < nurg) {  // the slot fills once its task is queued
+            uint64_t w0 = 0;
+            for (uint32_t k = 0;; ++k) {
+              const int t = ld_volatile(urq + tk);
+              if (t >= 0) return t;
+              __nanosleep(64);
+              if ((k & 63u) == 0) {
+                if (dev_error_set()) return -2;
+                const uint64_t now = globaltimer();
+                if (w0 == 0) w0 = now;
+                else if (now - w0 > kWaitLimitNs) {
+                  dev_error(kErrFullWait);
+                  return -2;
+                }
+              }
+            }
+          }
+        }
+      } else if (ld_volatile(&ctl->head_bulk) < nbulk) {
+        const int b = atomicAdd(&ctl->head_bulk, 1);
+        if (b < nbulk) return bulk[b];
+      }
+    }
+    if (ld_volatile(&ctl->head_bulk) >= nbulk && ld_volatile(&ctl->head_urg) >= nurg) return -1;
+    __nanosleep(256);
+    if ((spin & 31u) == 0) {
+      if (dev_error_set()) return -2;
+      const uint64_t now = globaltimer();
+      if (t0 == 0) t0 = now;
+      else if (now - t0 > kWaitLimitNs) {
         dev_error(kErrFullWait);
-        return false;
+        return -2;
       }
     }
   }
 }
 
 // ---- gemm tile ---------------------------------------------------------------
-template <class T, bool A_KC, bool B_KC>
-__device__ __forceinline__ void gemm_tile(const Task& t, uint8_t* smem) {
+// Shared layout of a stage: op(A) as BM x kBK, op(B) as kBK x BN, each in the
+// orientation of its global storage so that 16-byte copies run along the
+// contiguous dimension.  "KC" = k contiguous (row m of op(A) / column n of
+// op(B) holds kBK consecutive k).  Real tiles are padded: KC rows by 8
+// doubles (a lane's k-pair is one 16-byte load, conflict-free across the
+// eight lanes of a phase), the other orientation by 2 (the 16 lanes of a
+// phase hit 16 distinct 8-byte bank pairs).  Warp grid: real 64 x 64 tiles
+// 2 x 4 warps (32 x 16 each), real 128 x 64 tiles 4 x 2 (32 x 32), complex
+// 32 x 64 tiles 2 x 4 (16 x 16).
+template <class T, bool A_KC, bool B_KC, int BM>
+struct TileShape {
+  static constexpr bool CPLX = St<T>::CPLX;
+  static constexpr int BN = 64;
+  static constexpr int WM = BM == 128 ? 4 : 2, WN = kThreads / 32 / WM;
+  static constexpr int WTM = BM / WM, WTN = BN / WN;
+  static constexpr int MF = WTM / 16, NF = WTN / 8;
+  static constexpr int PKC = CPLX ? 0 : 8, PMN = CPLX ? 0 : 2;
+  static constexpr int LDA = A_KC ? kBK + PKC : BM + PMN;  // smem stride (elements)
+  static constexpr int LDB = B_KC ? kBK + PKC : BN + PMN;
+  static constexpr int A_S = A_KC ? BM * LDA : kBK * LDA;  // smem elements per stage
+  static constexpr int B_S = B_KC ? BN * LDB : kBK * LDB;
+  static constexpr int ES = (int)sizeof(T);
+  static constexpr int STAGE_BYTES = (A_S + B_S) * ES;
+};
+
+// Staging modes: kCopy16 16-byte cp.async.cg copies (aligned operands);
+// kCopy8 8-byte cp.async.ca copies (an operand not 16-byte aligned, operands
+// not written while the batch runs: L1 may keep them); kLoad8 8-byte L2 loads
+// through registers, one stage ahead (not 16-byte aligned, and B holds rows
+// other CTAs solved during this launch).
+enum : int { kCopy16 = 0, kCopy8 = 1, kLoad8 = 2 };
+
+// not inlined: each instantiation keeps its own register allocation
+template <class T, bool A_KC, bool B_KC, int BM, int MODE>
+__device__ __noinline__ void gemm_tile(const Task& t, uint8_t* smem) {
+  using Sh = TileShape<T, A_KC, B_KC, BM>;
   using S = typename St<T>::S;
-  constexpr bool CPLX = St<T>::CPLX;
-  constexpr int BM = CPLX ? 32 : 64, BN = 64;
-  constexpr int WTM = BM / 2, WTN = BN / 4;
-  constexpr int MF = WTM / 16, NF = WTN / 8;
-  constexpr int ES = (int)sizeof(T);
+  constexpr bool CPLX = Sh::CPLX;
+  constexpr int BN = Sh::BN, WTM = Sh::WTM, WTN = Sh::WTN, MF = Sh::MF, NF = Sh::NF;
+  constexpr int LDA = Sh::LDA, LDB = Sh::LDB, ES = Sh::ES;
   constexpr int EPC = 16 / ES;  // elements per 16-byte chunk
   constexpr int A_ELEMS = BM * kBK, B_ELEMS = BN * kBK;
-  constexpr int STAGE_BYTES = (A_ELEMS + B_ELEMS) * ES;
+  constexpr int STAGE_BYTES = Sh::STAGE_BYTES;
   constexpr int NACC = CPLX ? 8 : 4;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const char* Ag = static_cast<const char*>(t.A);
   const char* Bg = static_cast<const char*>(t.B);
   const int M = t.M, N = t.N, K = t.K;
   const int KT = (K + kBK - 1) / kBK;
+  // shared offset (elements) of op(A)(m, k) / op(B)(k, n)
+  auto a_off = [](int m, int k) { return A_KC ? m * LDA + k : k * LDA + m; };
+  auto b_off = [](int k, int n) { return B_KC ? n * LDB + k : k * LDB + n; };
 
-  const bool narrow = t.flags & kFlagNarrow;
+  // cp.async paths: 16-byte chunks (kCopy16) or 8-byte words (kCopy8)
   auto load_stage = [&](int it, int buf) {
     uint8_t* sa = smem + buf * STAGE_BYTES;
-    uint8_t* sb = sa + A_ELEMS * ES;
+    uint8_t* sb = sa + Sh::A_S * ES;
     const int k0 = it * kBK;
-    if (narrow) {  // same shared layout, one 8-byte word per copy
-      constexpr int WPE = ES / 8;
-      for (int w = tid; w < A_ELEMS * WPE; w += kThreads) {
-        const int e = w / WPE, h = w % WPE;
+    if constexpr (MODE == kCopy8) {
+      constexpr int W = ES / 8;  // words per element
+      for (int w = tid; w < A_ELEMS * W; w += kThreads) {
+        const int e = w / W, h = w % W;
         const int mm = A_KC ? e / kBK : e % BM, kk = A_KC ? e % kBK : e / BM;
         const int gk = k0 + kk;
         const bool v = mm < M && gk < K;
         const size_t gi =
             A_KC ? (size_t)gk + (size_t)mm * t.lda : (size_t)mm + (size_t)gk * t.lda;
-        const int soff = A_KC ? (mm * kBK + kk) : (kk * BM + mm);
-        cp_async8(sa + soff * ES + h * 8, v ? Ag + gi * ES + h * 8 : Ag, v ? 8 : 0);
+        cp_async8(sa + a_off(mm, kk) * ES + h * 8, v ? Ag + gi * ES + h * 8 : Ag, v ? 8 : 0);
       }
-      for (int w = tid; w < B_ELEMS * WPE; w += kThreads) {
-        const int e = w / WPE, h = w % WPE;
+      for (int w = tid; w < B_ELEMS * W; w += kThreads) {
+        const int e = w / W, h = w % W;
         const int nn = B_KC ? e / kBK : e % BN, kk = B_KC ? e % kBK : e / BN;
         const int gk = k0 + kk;
         const bool v = nn < N && gk < K;
         const size_t gi =
             B_KC ? (size_t)gk + (size_t)nn * t.ldb : (size_t)nn + (size_t)gk * t.ldb;
-        const int soff = B_KC ? (nn * kBK + kk) : (kk * BN + nn);
-        cp_async8(sb + soff * ES + h * 8, v ? Bg + gi * ES + h * 8 : Bg, v ? 8 : 0);
+        cp_async8(sb + b_off(kk, nn) * ES + h * 8, v ? Bg + gi * ES + h * 8 : Bg, v ? 8 : 0);
       }
       return;
     }
-    // A chunks
     constexpr int A_CH = A_ELEMS / EPC;
     for (int c = tid; c < A_CH; c += kThreads) {
       int mm, kk;  // first element of the chunk
@@ -155,18 +249,17 @@ __device__ __forceinline__ void gemm_tile(const Task& t, uint8_t* smem) {
         kk = c / (BM / EPC);
         mm = (c % (BM / EPC)) * EPC;
       }
-      const int gm = mm, gk = k0 + kk;
+      const int gk = k0 + kk;
       int valid;
       const char* src;
       if (A_KC) {  // element (m,k) at A[k + m*lda]; chunk runs along k
-        valid = (gm < M) ? max(0, min(EPC, K - gk)) : 0;
-        src = Ag + ((size_t)gk + (size_t)gm * t.lda) * ES;
+        valid = (mm < M) ? max(0, min(EPC, K - gk)) : 0;
+        src = Ag + ((size_t)gk + (size_t)mm * t.lda) * ES;
       } else {     // element (m,k) at A[m + k*lda]; chunk runs along m
-        valid = (gk < K) ? max(0, min(EPC, M - gm)) : 0;
-        src = Ag + ((size_t)gm + (size_t)gk * t.lda) * ES;
+        valid = (gk < K) ? max(0, min(EPC, M - mm)) : 0;
+        src = Ag + ((size_t)mm + (size_t)gk * t.lda) * ES;
       }
-      const int soff = A_KC ? (mm * kBK + kk) : (kk * BM + mm);
-      cp_async16(sa + soff * ES, valid ? src : Ag, valid * ES);
+      cp_async16(sa + a_off(mm, kk) * ES, valid ? src : Ag, valid * ES);
     }
     constexpr int B_CH = B_ELEMS / EPC;
     for (int c = tid; c < B_CH; c += kThreads) {
@@ -178,22 +271,75 @@ __device__ __forceinline__ void gemm_tile(const Task& t, uint8_t* smem) {
         kk = c / (BN / EPC);
         nn = (c % (BN / EPC)) * EPC;
       }
-      const int gn = nn, gk = k0 + kk;
+      const int gk = k0 + kk;
       int valid;
       const char* src;
       if (B_KC) {  // element (k,n) at B[k + n*ldb]
-        valid = (gn < N) ? max(0, min(EPC, K - gk)) : 0;
-        src = Bg + ((size_t)gk + (size_t)gn * t.ldb) * ES;
+        valid = (nn < N) ? max(0, min(EPC, K - gk)) : 0;
+        src = Bg + ((size_t)gk + (size_t)nn * t.ldb) * ES;
       } else {     // element (k,n) at B[n + k*ldb]
-        valid = (gk < K) ? max(0, min(EPC, N - gn)) : 0;
-        src = Bg + ((size_t)gn + (size_t)gk * t.ldb) * ES;
+        valid = (gk < K) ? max(0, min(EPC, N - nn)) : 0;
+        src = Bg + ((size_t)nn + (size_t)gk * t.ldb) * ES;
       }
-      const int soff = B_KC ? (nn * kBK + kk) : (kk * BN + nn);
-      cp_async16(sb + soff * ES, valid ? src : Bg, valid * ES);
+      cp_async16(sb + b_off(kk, nn) * ES, valid ? src : Bg, valid * ES);
     }
   };
 
-  const int wm = warp >> 2, wn = warp & 3;
+  // 8-byte register-staged path (an operand not 16-byte aligned): word w of
+  // a stage is 8-byte word w % WPE of element w / WPE
+  constexpr int WPE = ES / 8;
+  constexpr int NWA = A_ELEMS * WPE / kThreads, NWB = B_ELEMS * WPE / kThreads;
+  static_assert(NWA * kThreads == A_ELEMS * WPE && NWB * kThreads == B_ELEMS * WPE, "stage split");
+  double ra[MODE == kLoad8 ? NWA : 1], rb[MODE == kLoad8 ? NWB : 1];
+  auto a_elem = [](int e, int& mm, int& kk) {
+    if (A_KC) { mm = e / kBK; kk = e % kBK; } else { kk = e / BM; mm = e % BM; }
+  };
+  auto b_elem = [](int e, int& nn, int& kk) {
+    if (B_KC) { nn = e / kBK; kk = e % kBK; } else { kk = e / BN; nn = e % BN; }
+  };
+  auto fetch = [&](int it) {
+    const int k0 = it * kBK;
+    const double* Ad = reinterpret_cast<const double*>(Ag);
+    const double* Bd = reinterpret_cast<const double*>(Bg);
+#pragma unroll
+    for (int q = 0; q < NWA; ++q) {
+      const int w = tid + q * kThreads, e = w / WPE, h = w % WPE;
+      int mm, kk;
+      a_elem(e, mm, kk);
+      const int gk = k0 + kk;
+      const size_t gi = A_KC ? (size_t)gk + (size_t)mm * t.lda : (size_t)mm + (size_t)gk * t.lda;
+      ra[q] = (mm < M && gk < K) ? __ldcg(Ad + gi * WPE + h) : 0.0;
+    }
+#pragma unroll
+    for (int q = 0; q < NWB; ++q) {
+      const int w = tid + q * kThreads, e = w / WPE, h = w % WPE;
+      int nn, kk;
+      b_elem(e, nn, kk);
+      const int gk = k0 + kk;
+      const size_t gi = B_KC ? (size_t)gk + (size_t)nn * t.ldb : (size_t)nn + (size_t)gk * t.ldb;
+      rb[q] = (nn < N && gk < K) ? __ldcg(Bd + gi * WPE + h) : 0.0;
+    }
+  };
+  auto put = [&](int buf) {
+    double* sa = reinterpret_cast<double*>(smem + buf * STAGE_BYTES);
+    double* sb = sa + Sh::A_S * WPE;
+#pragma unroll
+    for (int q = 0; q < NWA; ++q) {
+      const int w = tid + q * kThreads, e = w / WPE, h = w % WPE;
+      int mm, kk;
+      a_elem(e, mm, kk);
+      sa[a_off(mm, kk) * WPE + h] = ra[q];
+    }
+#pragma unroll
+    for (int q = 0; q < NWB; ++q) {
+      const int w = tid + q * kThreads, e = w / WPE, h = w % WPE;
+      int nn, kk;
+      b_elem(e, nn, kk);
+      sb[b_off(kk, nn) * WPE + h] = rb[q];
+    }
+  };
+
+  const int wm = warp / Sh::WN, wn = warp % Sh::WN;
   const int g = lane >> 2, tq = lane & 3;
   double acc[MF][NF][NACC];
 #pragma unroll
@@ -205,40 +351,48 @@ __device__ __forceinline__ void gemm_tile(const Task& t, uint8_t* smem) {
   const double sgnA = (t.opA == XKB_OP_C) ? -1.0 : 1.0;
   const double sgnB = (t.opB == XKB_OP_C) ? -1.0 : 1.0;
 
-  for (int s = 0; s < kSt - 1; ++s) {
-    if (s < KT) load_stage(s, s);
-    cp_async_commit();
-  }
-  for (int it = 0; it < KT; ++it) {
-    cp_async_wait<kSt - 2>();
-    __syncthreads();  // stage `it` landed for everyone; stage it-1 no longer read
-    if (it + kSt - 1 < KT) load_stage(it + kSt - 1, (it + kSt - 1) % kSt);
-    cp_async_commit();
-    const uint8_t* sbase = smem + (it % kSt) * STAGE_BYTES;
+  auto compute = [&](int buf) {
+    const uint8_t* sbase = smem + buf * STAGE_BYTES;
     const S* sa = reinterpret_cast<const S*>(sbase);
-    const S* sb = reinterpret_cast<const S*>(sbase + A_ELEMS * ES);
+    const S* sb = reinterpret_cast<const S*>(sbase + Sh::A_S * ES);
 #pragma unroll
     for (int kc = 0; kc < kBK / 8; ++kc) {
+      // logical k = tq and tq + 4 of the MMA are physical k0 = 2 tq, k1 = k0 + 1
       const int k0 = kc * 8 + 2 * tq, k1 = k0 + 1;
       double br[NF][2], bi[NF][2];
 #pragma unroll
       for (int nf = 0; nf < NF; ++nf) {
         const int n = wn * WTN + nf * 8 + g;
-        ld_elem<T>(sb, B_KC ? n * kBK + k0 : k0 * BN + n, br[nf][0], bi[nf][0]);
-        ld_elem<T>(sb, B_KC ? n * kBK + k1 : k1 * BN + n, br[nf][1], bi[nf][1]);
-        if (CPLX) {
-          bi[nf][0] *= sgnB;
-          bi[nf][1] *= sgnB;
+        if constexpr (B_KC && !CPLX) {
+          const double2 v = *reinterpret_cast<const double2*>(sb + b_off(k0, n));
+          br[nf][0] = v.x;
+          br[nf][1] = v.y;
+        } else {
+          ld_elem<T>(sb, b_off(k0, n), br[nf][0], bi[nf][0]);
+          ld_elem<T>(sb, b_off(k1, n), br[nf][1], bi[nf][1]);
+          if (CPLX) {
+            bi[nf][0] *= sgnB;
+            bi[nf][1] *= sgnB;
+          }
         }
       }
 #pragma unroll
       for (int mf = 0; mf < MF; ++mf) {
         const int r0 = wm * WTM + mf * 16 + g, r1 = r0 + 8;
         double ar[4], ai[4];
-        ld_elem<T>(sa, A_KC ? r0 * kBK + k0 : k0 * BM + r0, ar[0], ai[0]);
-        ld_elem<T>(sa, A_KC ? r1 * kBK + k0 : k0 * BM + r1, ar[1], ai[1]);
-        ld_elem<T>(sa, A_KC ? r0 * kBK + k1 : k1 * BM + r0, ar[2], ai[2]);
-        ld_elem<T>(sa, A_KC ? r1 * kBK + k1 : k1 * BM + r1, ar[3], ai[3]);
+        if constexpr (A_KC && !CPLX) {
+          const double2 v0 = *reinterpret_cast<const double2*>(sa + a_off(r0, k0));
+          const double2 v1 = *reinterpret_cast<const double2*>(sa + a_off(r1, k0));
+          ar[0] = v0.x;
+          ar[1] = v1.x;
+          ar[2] = v0.y;
+          ar[3] = v1.y;
+        } else {
+          ld_elem<T>(sa, a_off(r0, k0), ar[0], ai[0]);
+          ld_elem<T>(sa, a_off(r1, k0), ar[1], ai[1]);
+          ld_elem<T>(sa, a_off(r0, k1), ar[2], ai[2]);
+          ld_elem<T>(sa, a_off(r1, k1), ar[3], ai[3]);
+        }
         if constexpr (CPLX) {
           double nai[4];
 #pragma unroll
@@ -265,8 +419,35 @@ __device__ __forceinline__ void gemm_tile(const Task& t, uint8_t* smem) {
         }
       }
     }
+  };
+
+  if constexpr (MODE != kLoad8) {
+    for (int s = 0; s < kSt - 1; ++s) {
+      if (s < KT) load_stage(s, s);
+      cp_async_commit();
+    }
+    for (int it = 0; it < KT; ++it) {
+      cp_async_wait<kSt - 2>();
+      __syncthreads();  // stage `it` landed for everyone; stage it-1 no longer read
+      if (it + kSt - 1 < KT) load_stage(it + kSt - 1, (it + kSt - 1) % kSt);
+      cp_async_commit();
+      compute(it % kSt);
+    }
+    cp_async_wait<0>();
+  } else {
+    // registers carry stage it+1 while stage it is computed (two buffers)
+    if (KT > 0) {
+      fetch(0);
+      put(0);
+      if (KT > 1) fetch(1);
+    }
+    for (int it = 0; it < KT; ++it) {
+      __syncthreads();  // buffer it%2 written; buffer (it+1)%2 no longer read
+      if (it + 1 < KT) put((it + 1) & 1);
+      if (it + 2 < KT) fetch(it + 2);
+      compute(it & 1);
+    }
   }
-  cp_async_wait<0>();
   __syncthreads();  // smem free for the next task
   S* C = reinterpret_cast<S*>(t.C);
   const bool use_beta = (t.br != 0.0) || (t.bi != 0.0);
@@ -299,167 +480,328 @@ __device__ __forceinline__ void gemm_tile(const Task& t, uint8_t* smem) {
       }
 }
 
+template <class T, int BM, int MODE>
+__device__ __forceinline__ void gemm_dispatch2(const Task& t, uint8_t* smem) {
+  const bool akc = t.opA != XKB_OP_N, bkc = t.opB == XKB_OP_N;
+  if (akc && bkc) gemm_tile<T, true, true, BM, MODE>(t, smem);
+  else if (akc) gemm_tile<T, true, false, BM, MODE>(t, smem);
+  else if (bkc) gemm_tile<T, false, true, BM, MODE>(t, smem);
+  else gemm_tile<T, false, false, BM, MODE>(t, smem);
+}
+
 // ---- trsm diagonal block ------------------------------------------------------
+// X = alpha * op(T)^-1 B for one 64-row diagonal block T and up to 64
+// right-hand sides, by substitution.  A column is held by G lanes of one
+// warp, lane g keeping rows RPL*g .. RPL*g + RPL-1 in registers (real: RPL
+// 16, G 4, 64 columns per pass; complex: RPL 8, G 8, 32 columns per pass).
+// At step i the owner of row i scales it by the reciprocal of T(i,i) (the
+// packed-reciprocal form CPU BLAS kernels use), the G lanes share it by
+// shuffle, and each lane updates its rows below (lower) or above (upper) i.
+// op(T) is staged column by column in shared memory, row groups GS = RPL + 2
+// doubles apart so that the G lanes' vector loads fall in distinct banks.
 template <class T>
-__device__ __forceinline__ void trsm_tile(const Task& t, uint8_t* smem) {
+struct TrsmShape {
+  static constexpr int RPL = St<T>::CPLX ? 8 : 16;  // rows per lane
+  static constexpr int G = kLeafS / RPL;            // lanes per column
+  static constexpr int GS = RPL + 2;                // staged row-group stride
+  static constexpr int COL = G * GS;                // staged column stride
+  static constexpr int CPP = kThreads / G;          // columns per pass
+};
+constexpr size_t kTrsmSmem =
+    2 * sizeof(double) * (kLeafS * TrsmShape<double2>::COL + kLeafS);  // complex, the larger
+
+template <class T, bool LOWER>
+__device__ __forceinline__ void trsm_solve(const Task& t, const double* Tr, const double* Ti,
+                                           const double* Dr, const double* Di, double ar,
+                                           double ai) {
+  using Sh = TrsmShape<T>;
+  constexpr int RPL = Sh::RPL, G = Sh::G, GS = Sh::GS, COL = Sh::COL;
   constexpr bool CP = St<T>::CPLX;
   using S = typename St<T>::S;
-  double (*Tr)[kLeafS + 1] = reinterpret_cast<double (*)[kLeafS + 1]>(smem);
-  double (*Ti)[kLeafS + 1] =
-      reinterpret_cast<double (*)[kLeafS + 1]>(smem + sizeof(double) * kLeafS * (kLeafS + 1));
+  const int tid = threadIdx.x, lane = tid & 31;
+  const int q = tid % G, gbase = lane & ~(G - 1);
   const int n = t.M, nrhs = t.N;
-  const bool swap = t.flags & kFlagSwap, conj = t.flags & kFlagConj;
-  const bool lower = t.flags & kFlagLower, unit = t.flags & kFlagUnit;
-  const S* A = static_cast<const S*>(t.A);
   S* B = static_cast<S*>(t.C);
-  for (int e = threadIdx.x; e < n * n; e += kThreads) {
-    const int i = e % n, j = e / n;
-    double re = 0, im = 0;
-    if (lower ? (j <= i) : (j >= i)) {
-      const size_t idx = swap ? (size_t)j + (size_t)i * t.lda : (size_t)i + (size_t)j * t.lda;
-      if (CP) {
-        re = __ldcg(A + 2 * idx);
-        im = __ldcg(A + 2 * idx + 1);
-        if (conj) im = -im;
-      } else {
-        re = __ldcg(A + idx);
-      }
-      if (i == j && unit) {
-        re = 1.0;
-        im = 0.0;
-      }
-    }
-    Tr[i][j] = re;
-    if (CP) Ti[i][j] = im;
-  }
-  __syncthreads();
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (int c = warp; c < nrhs; c += kThreads / 32) {
-    double xr[2], xi[2];
+  for (int c = tid / G; c < kLeafS; c += Sh::CPP) {  // uniform trip count per warp
+    double xr[RPL], xi[RPL];
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const int r = lane + 32 * h;
-      xr[h] = xi[h] = 0.0;
-      if (r < n) {
-        const size_t idx = (size_t)r + (size_t)c * t.ldc;
+    for (int r = 0; r < RPL; ++r) {
+      const int row = q * RPL + r;
+      xr[r] = xi[r] = 0.0;
+      if (row < n && c < nrhs) {
+        const size_t idx = (size_t)row + (size_t)c * t.ldc;
         const double br = CP ? __ldcg(B + 2 * idx) : __ldcg(B + idx);
         const double bi = CP ? __ldcg(B + 2 * idx + 1) : 0.0;
-        xr[h] = t.ar * br - t.ai * bi;
-        xi[h] = CP ? (t.ar * bi + t.ai * br) : 0.0;
+        xr[r] = ar * br - ai * bi;
+        if (CP) xi[r] = ar * bi + ai * br;
       }
     }
-    for (int s = 0; s < n; ++s) {
-      const int i = lower ? s : n - 1 - s;
-      const int h = i >> 5, src = i & 31;
-      double vr = __shfl_sync(0xffffffffu, h ? xr[1] : xr[0], src);
-      double vi = CP ? __shfl_sync(0xffffffffu, h ? xi[1] : xi[0], src) : 0.0;
-      const double dr = Tr[i][i], di = CP ? Ti[i][i] : 0.0;
-      if (CP) {
-        const double den = dr * dr + di * di;
-        const double qr = (vr * dr + vi * di) / den, qi = (vi * dr - vr * di) / den;
-        vr = qr;
-        vi = qi;
-      } else {
-        vr = vr / dr;
-      }
+    // steps in G rounds of RPL: the register index is a compile-time constant
+    // within a round, the owning lane a run-time one
+#pragma unroll 1
+    for (int og = 0; og < G; ++og) {
 #pragma unroll
-      for (int hh = 0; hh < 2; ++hh) {
-        const int r = lane + 32 * hh;
-        if (r == i) {
-          xr[hh] = vr;
-          xi[hh] = vi;
-        } else if (r < n && (lower ? r > i : r < i)) {
-          const double tr = Tr[r][i];
-          if (CP) {
-            const double ti = Ti[r][i];
-            xr[hh] -= tr * vr - ti * vi;
-            xi[hh] -= tr * vi + ti * vr;
-          } else {
-            xr[hh] -= tr * vr;
+    for (int ss = 0; ss < RPL; ++ss) {
+      const int oq = LOWER ? og : G - 1 - og, oi = LOWER ? ss : RPL - 1 - ss;
+      const int i = oq * RPL + oi;
+      double vr = __shfl_sync(0xffffffffu, xr[oi], gbase | oq);
+      double vi = CP ? __shfl_sync(0xffffffffu, xi[oi], gbase | oq) : 0.0;
+      if (CP) {
+        const double dr = Dr[i], di = Di[i];
+        const double wr = vr * dr - vi * di;
+        vi = vr * di + vi * dr;
+        vr = wr;
+      } else {
+        vr *= Dr[i];
+      }
+      if (q == oq) {
+        xr[oi] = vr;
+        if (CP) xi[oi] = vi;
+      }
+      // update row > i (lower) / row < i (upper): the staged column holds
+      // zeros outside the triangle, but the predicate keeps final rows
+      // untouched even when v is not finite
+      const double2* colr = reinterpret_cast<const double2*>(Tr + i * COL + q * GS);
+      const double2* coli = reinterpret_cast<const double2*>(Ti + i * COL + q * GS);
+#pragma unroll
+      for (int h = 0; h < RPL / 2; ++h) {
+        const double2 tr = colr[h];
+        double2 ti = make_double2(0.0, 0.0);
+        if (CP) ti = coli[h];
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+          const int r = 2 * h + u;
+          const int row = q * RPL + r;
+          const double a = u ? tr.y : tr.x;
+          if (LOWER ? row > i : row < i) {
+            if (CP) {
+              const double b = u ? ti.y : ti.x;
+              xr[r] -= a * vr - b * vi;
+              xi[r] -= a * vi + b * vr;
+            } else {
+              xr[r] -= a * vr;
+            }
           }
         }
       }
     }
+    }
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const int r = lane + 32 * h;
-      if (r < n) {
-        const size_t idx = (size_t)r + (size_t)c * t.ldc;
+    for (int r = 0; r < RPL; ++r) {
+      const int row = q * RPL + r;
+      if (row < n && c < nrhs) {
+        const size_t idx = (size_t)row + (size_t)c * t.ldc;
         if (CP) {
-          B[2 * idx] = xr[h];
-          B[2 * idx + 1] = xi[h];
+          B[2 * idx] = xr[r];
+          B[2 * idx + 1] = xi[r];
         } else {
-          B[idx] = xr[h];
+          B[idx] = xr[r];
         }
       }
     }
   }
+}
+
+// not inlined: its register allocation stays apart from the gemm tile's
+template <class T>
+__device__ __noinline__ void trsm_tile(const Task& t, uint8_t* smem, double ar, double ai) {
+  using Sh = TrsmShape<T>;
+  constexpr bool CP = St<T>::CPLX;
+  using S = typename St<T>::S;
+  double* Tr = reinterpret_cast<double*>(smem);
+  double* Ti = Tr + kLeafS * Sh::COL;
+  double* Dr = Ti + (CP ? kLeafS * Sh::COL : 0);
+  double* Di = Dr + kLeafS;
+  const int n = t.M;
+  const bool swap = t.flags & kFlagSwap, conj = t.flags & kFlagConj;
+  const bool lower = t.flags & kFlagLower, unit = t.flags & kFlagUnit;
+  const S* A = static_cast<const S*>(t.D);
+  // stage op(T): column j, row i at j * COL + (i / RPL) * GS + i % RPL; zero
+  // outside the triangle, on the diagonal and beyond n.  Element e maps to
+  // (a0, a1) = (e % 64, e / 64) at A[a0 + a1 * lda], so consecutive threads
+  // read consecutive addresses whether op(T) is A's triangle or its
+  // transpose; all loads are issued before the first shared store.
+  constexpr int PER = kLeafS * kLeafS / kThreads;
+  double vr[PER], vi[PER];
+#pragma unroll
+  for (int k = 0; k < PER; ++k) {
+    const int e = threadIdx.x + k * kThreads;
+    const int a0 = e & (kLeafS - 1), a1 = e / kLeafS;
+    const int i = swap ? a1 : a0, j = swap ? a0 : a1;
+    vr[k] = vi[k] = 0.0;
+    if (i < n && j < n && (lower ? (j < i) : (j > i))) {
+      const size_t idx = (size_t)a0 + (size_t)a1 * t.lda;
+      if (CP) {
+        vr[k] = __ldcg(A + 2 * idx);
+        vi[k] = __ldcg(A + 2 * idx + 1);
+      } else {
+        vr[k] = __ldcg(A + idx);
+      }
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < PER; ++k) {
+    const int e = threadIdx.x + k * kThreads;
+    const int a0 = e & (kLeafS - 1), a1 = e / kLeafS;
+    const int i = swap ? a1 : a0, j = swap ? a0 : a1;
+    const int o = j * Sh::COL + (i / Sh::RPL) * Sh::GS + (i % Sh::RPL);
+    Tr[o] = vr[k];
+    if (CP) Ti[o] = conj ? -vi[k] : vi[k];
+  }
+  // reciprocal diagonal; 1 beyond n (those rows hold zeros)
+  for (int i = threadIdx.x; i < kLeafS; i += kThreads) {
+    double dr = 1.0, di = 0.0;
+    if (i < n && !unit) {
+      const size_t idx = (size_t)i + (size_t)i * t.lda;
+      if (CP) {
+        dr = __ldcg(A + 2 * idx);
+        di = __ldcg(A + 2 * idx + 1);
+        if (conj) di = -di;
+      } else {
+        dr = __ldcg(A + idx);
+      }
+    }
+    if (CP) {
+      const double den = dr * dr + di * di;
+      Dr[i] = dr / den;
+      Di[i] = -di / den;
+    } else {
+      Dr[i] = 1.0 / dr;
+    }
+  }
+  __syncthreads();
+  if (lower) trsm_solve<T, true>(t, Tr, Ti, Dr, Di, ar, ai);
+  else trsm_solve<T, false>(t, Tr, Ti, Dr, Di, ar, ai);
   __syncthreads();
 }
 
-// smem: max(complex gemm 3 x 24 KB, complex trsm 2 x 33 KB) + alignment
-constexpr size_t kSmemBytes = 3 * (32 + 64) * kBK * 16 + 128 > 2 * 8 * kLeafS * (kLeafS + 1) + 128
-                                  ? 3 * (32 + 64) * kBK * 16 + 128
-                                  : 2 * 8 * kLeafS * (kLeafS + 1) + 128;
+// dynamic shared memory: the largest task body (the complex solve's staging,
+// 81 KB; gemm stages: real 128 x 64 3 x 26 KB, complex 3 x 24 KB) + alignment
+constexpr size_t kSmemMax(size_t a, size_t b) { return a > b ? a : b; }
+constexpr size_t kSmemBytes =
+    kSmemMax(kTrsmSmem,
+             kSmemMax((size_t)kSt * TileShape<double, true, true, 128>::STAGE_BYTES,
+                      kSmemMax((size_t)kSt * TileShape<double, false, false, 128>::STAGE_BYTES,
+                               (size_t)kSt * TileShape<double2, false, false, 32>::STAGE_BYTES))) +
+    128;
 
-__global__ void __launch_bounds__(kThreads) k_sched(const Task* __restrict__ tasks, int ntasks,
-                                                    int* counters, int* next, int* call_left,
-                                                    unsigned long long* call_end,
-                                                    unsigned long long* t_start) {
+__global__ void __launch_bounds__(kThreads, 2)
+    k_sched(const Task* __restrict__ tasks, int* ndep, const int* __restrict__ succ,
+            const int* __restrict__ bulk, int nbulk, int* urq, int nurg, Ctl* ctl,
+            int urgent_first, int* call_left, unsigned long long* call_end,
+            unsigned long long* t_start) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem =
       reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
-  __shared__ int s_idx, s_ok;
+  __shared__ int s_idx;
+  __shared__ Task s_task;  // the claimed task, read by every thread from here
+  __shared__ Task s_sub;   // a gemm step of a solve task
   if (threadIdx.x == 0) atomicMin(t_start, (unsigned long long)globaltimer());
   for (;;) {
     if (threadIdx.x == 0) {
-      const int i = atomicAdd(next, 1);
-      int ok = 1;
-      if (i < ntasks) {
-        const Task* tp = tasks + i;
-        if (tp->wait0 >= 0 && !wait_ge(counters + tp->wait0, tp->target0)) ok = 0;
-        if (ok && tp->wait1 >= 0 && !wait_ge(counters + tp->wait1, tp->target1)) ok = 0;
-        __threadfence();
+      const int i = claim_task(ctl, bulk, nbulk, urq, nurg, urgent_first != 0);
+      if (i >= 0) {
+        __threadfence();  // acquire: the producers' outputs before the reads
+        s_task = tasks[i];
       }
       s_idx = i;
-      s_ok = ok;
     }
     __syncthreads();
-    const int i = s_idx;
-    if (i >= ntasks || !s_ok) break;
-    const Task t = tasks[i];
-    if (t.kind == kTaskGemm) {
-      const bool akc = t.opA != XKB_OP_N, bkc = t.opB == XKB_OP_N;
-      if (t.dtype == XKB_D) {
-        if (akc && bkc) gemm_tile<double, true, true>(t, smem);
-        else if (akc) gemm_tile<double, true, false>(t, smem);
-        else if (bkc) gemm_tile<double, false, true>(t, smem);
-        else gemm_tile<double, false, false>(t, smem);
+    if (s_idx < 0) break;
+    // only thread 0 rewrites s_task, after every thread is past the barrier
+    // that ends this task
+    const Task& t = s_task;
+    if (t.kind == kTaskGemm) {  // a gemm call's tile: operands read-only here
+      const bool nar = t.flags & kFlagNarrow;
+      if (t.dtype == XKB_Z) {
+        if (nar) gemm_dispatch2<double2, 32, kCopy8>(t, smem);
+        else gemm_dispatch2<double2, 32, kCopy16>(t, smem);
+      } else if (t.M > 64) {
+        if (nar) gemm_dispatch2<double, 128, kCopy8>(t, smem);
+        else gemm_dispatch2<double, 128, kCopy16>(t, smem);
       } else {
-        if (akc && bkc) gemm_tile<double2, true, true>(t, smem);
-        else if (akc) gemm_tile<double2, true, false>(t, smem);
-        else if (bkc) gemm_tile<double2, false, true>(t, smem);
-        else gemm_tile<double2, false, false>(t, smem);
+        if (nar) gemm_dispatch2<double, 64, kCopy8>(t, smem);
+        else gemm_dispatch2<double, 64, kCopy16>(t, smem);
       }
     } else {
-      if (t.dtype == XKB_D) trsm_tile<double>(t, smem);
-      else trsm_tile<double2>(t, smem);
+      // X_i = alpha B_i - op(A)[i, solved] X_solved in gemm tiles of BM rows,
+      // then the diagonal solve of X_i (same CTA: the tiles' stores are
+      // ordered before its loads by the barrier, both go through L2)
+      const bool cplx = t.dtype == XKB_Z;
+      double sar = t.ar, sai = t.ai;
+      if (t.K > 0) {
+        const int bm = cplx ? 32 : 64;
+        const int es = cplx ? 16 : 8;
+        for (int r0 = 0; r0 < t.M; r0 += bm) {
+          if (threadIdx.x == 0) {
+            s_sub = t;
+            s_sub.M = min(bm, t.M - r0);
+            s_sub.A = static_cast<const char*>(t.A) +
+                      (size_t)r0 * (t.opA == XKB_OP_N ? 1 : t.lda) * es;
+            s_sub.C = static_cast<char*>(t.C) + (size_t)r0 * es;
+            s_sub.ar = -1.0;
+            s_sub.ai = 0.0;
+            s_sub.br = t.ar;
+            s_sub.bi = t.ai;
+          }
+          __syncthreads();
+          // op(B) = X rows solved by other CTAs of this launch: L2 only
+          const bool nar = t.flags & kFlagNarrow;
+          if (!cplx) {
+            if (t.opA == XKB_OP_N) {
+              if (nar) gemm_tile<double, false, true, 64, kLoad8>(s_sub, smem);
+              else gemm_tile<double, false, true, 64, kCopy16>(s_sub, smem);
+            } else {
+              if (nar) gemm_tile<double, true, true, 64, kLoad8>(s_sub, smem);
+              else gemm_tile<double, true, true, 64, kCopy16>(s_sub, smem);
+            }
+          } else {
+            if (t.opA == XKB_OP_N) {
+              if (nar) gemm_tile<double2, false, true, 32, kLoad8>(s_sub, smem);
+              else gemm_tile<double2, false, true, 32, kCopy16>(s_sub, smem);
+            } else {
+              if (nar) gemm_tile<double2, true, true, 32, kLoad8>(s_sub, smem);
+              else gemm_tile<double2, true, true, 32, kCopy16>(s_sub, smem);
+            }
+          }
+          __syncthreads();  // s_sub is rewritten by the next row part
+        }
+        sar = 1.0;
+        sai = 0.0;
+      }
+      if (!cplx) trsm_tile<double>(t, smem, sar, sai);
+      else trsm_tile<double2>(t, smem, sar, sai);
     }
     __syncthreads();  // every output of the task is stored
     if (threadIdx.x == 0) {
-      __threadfence();
-      if (t.signal >= 0) atomicAdd(counters + t.signal, 1);
+      __threadfence();  // release the outputs before any successor is queued
+      for (int k = 0; k < t.nsucc; ++k) {
+        const int sidx = succ[t.succ0 + k];
+        if (atomicSub(ndep + sidx, 1) == 1) {
+          const int pos = atomicAdd(&ctl->tail_urg, 1);
+          atomicExch(urq + pos, sidx);
+        }
+      }
       if (atomicSub(call_left + t.call, 1) == 1) call_end[t.call] = globaltimer();
     }
   }
 }
 
 // ---------------------------------------------------------------------------
-// host: task list construction
+// host: task graph construction
 struct Built {
-  std::vector<Task> tasks;
+  std::vector<Task> tasks;                 // indexed by task id
+  std::vector<int> ndep;                   // initial dependency count
+  std::vector<std::pair<int, int>> edges;  // (producer, consumer)
+  std::vector<int> bulk;                   // dependency-free gemm tiles
+  std::vector<int> urg_ready;              // solve tasks ready at launch
+  int nurg = 0;                            // solve tasks in total
   std::vector<int> call_tasks;
-  int ncounters = 0;
+  int add(const Task& t, int ndep0) {
+    tasks.push_back(t);
+    ndep.push_back(ndep0);
+    return (int)tasks.size() - 1;
+  }
 };
 
 static int esz(int dt) { return dt == XKB_Z ? 16 : 8; }
@@ -470,9 +812,40 @@ static bool aligned_ok(const void* p, long ld, int es) {
 
 static bool ptr8(const void* p) { return reinterpret_cast<uintptr_t>(p) % 8 == 0; }
 
+static Task gemm_task(int dtype, int opA, int opB, int M, int N, int K, int call, const void* A,
+                      long lda, const void* B, long ldb, void* C, long ldc, double ar, double ai,
+                      double br, double bi, int flags) {
+  Task t;
+  std::memset(&t, 0, sizeof(t));
+  t.kind = kTaskGemm;
+  t.dtype = dtype;
+  t.opA = opA;
+  t.opB = opB;
+  t.M = M;
+  t.N = N;
+  t.K = K;
+  t.call = call;
+  t.A = A;
+  t.lda = lda;
+  t.B = B;
+  t.ldb = ldb;
+  t.C = C;
+  t.ldc = ldc;
+  t.ar = ar;
+  t.ai = ai;
+  t.br = br;
+  t.bi = bi;
+  t.flags = flags;
+  return t;
+}
+
+// A gemm call: independent C tiles (the reference's tile loop,
+// blas/zgemm.c:279-367, with the whole K range in one task).
 static int add_gemm(Built& b, const xkb_batch_op& o, int call) {
   const int es = esz(o.dtype);
-  const int BM = o.dtype == XKB_Z ? 32 : 64, BN = 64;
+  // real calls taller than 96 rows use 128-row tiles (the kernel picks the
+  // 128 x 64 body for any real task taller than 64 rows)
+  const int BM = o.dtype == XKB_Z ? 32 : (o.M >= 96 ? 128 : 64), BN = 64;
   if (!ptr8(o.A) || !ptr8(o.B) || !ptr8(o.C)) return XKB_EINVAL;
   const int narrow =
       (aligned_ok(o.A, o.lda, es) && aligned_ok(o.B, o.ldb, es)) ? 0 : kFlagNarrow;
@@ -482,39 +855,29 @@ static int add_gemm(Built& b, const xkb_batch_op& o, int call) {
   int n = 0;
   for (int n0 = 0; n0 < o.N; n0 += BN)
     for (int m0 = 0; m0 < o.M; m0 += BM) {
-      Task t;
-      std::memset(&t, 0, sizeof(t));
-      t.kind = kTaskGemm;
-      t.dtype = o.dtype;
-      t.opA = o.opA;
-      t.opB = o.opB;
-      t.M = std::min(BM, o.M - m0);
-      t.N = std::min(BN, o.N - n0);
-      t.K = o.K;
-      t.call = call;
-      t.A = o.opA == XKB_OP_N ? A + (size_t)m0 * es : A + (size_t)m0 * o.lda * es;
-      t.B = o.opB == XKB_OP_N ? B + (size_t)n0 * o.ldb * es : B + (size_t)n0 * es;
-      t.C = C + ((size_t)m0 + (size_t)n0 * o.ldc) * es;
-      t.lda = o.lda;
-      t.ldb = o.ldb;
-      t.ldc = o.ldc;
-      t.ar = o.alpha[0];
-      t.ai = o.alpha[1];
-      t.br = o.beta[0];
-      t.bi = o.beta[1];
-      t.flags = narrow;
-      t.wait0 = t.wait1 = -1;
-      t.signal = -1;
-      b.tasks.push_back(t);
+      const char* Ap = o.opA == XKB_OP_N ? A + (size_t)m0 * es : A + (size_t)m0 * o.lda * es;
+      const char* Bp = o.opB == XKB_OP_N ? B + (size_t)n0 * o.ldb * es : B + (size_t)n0 * es;
+      char* Cp = C + ((size_t)m0 + (size_t)n0 * o.ldc) * es;
+      b.bulk.push_back(b.add(gemm_task(o.dtype, o.opA, o.opB, std::min(BM, o.M - m0),
+                                       std::min(BN, o.N - n0), o.K, call, Ap, o.lda, Bp, o.ldb,
+                                       Cp, o.ldc, o.alpha[0], o.alpha[1], o.beta[0],
+                                       o.beta[1], narrow),
+                             0));
       ++n;
     }
   return n;
 }
 
-// Left triangular solve as the reference's tile algorithm (blas/ztrsm.c):
-// diagonal solves + trailing gemm updates with lalpha on the first step.
-static int add_trsm(Built& b, const xkb_batch_op& o, int call,
-                    std::vector<std::vector<Task>>& steps) {
+// Left triangular solve: the reference's block algorithm (blas/ztrsm.c:
+// 241-372; alpha applied once, its lalpha), left-looking.  Blocks are taken
+// in solve order s = 0 .. mt-1 (bk = order(s): forward for an effectively
+// lower op(A), backward otherwise); task (s, j) forms
+//   X_bk,j = alpha B_bk,j - op(A)[bk, done] X_done,j,   done = order(0..s-1)
+// and solves with op(A)[bk,bk].  The blocks already solved are contiguous
+// (rows [0, bk*64) forward, [(bk+1)*64, M) backward), so the sum is one gemm
+// with K = 64 s (64 (mt-1-s) backward, the last block possibly shorter).
+// Task (s, j) depends on task (s-1, j) only: one chain per j.
+static int add_trsm(Built& b, const xkb_batch_op& o, int call) {
   const int es = esz(o.dtype);
   if (o.side != 0) return XKB_EINVAL;  // right side: not a batch task
   if (!ptr8(o.A) || !ptr8(o.C)) return XKB_EINVAL;
@@ -522,94 +885,65 @@ static int add_trsm(Built& b, const xkb_batch_op& o, int call,
       (aligned_ok(o.A, o.lda, es) && aligned_ok(o.C, o.ldc, es)) ? 0 : kFlagNarrow;
   const bool cplx = o.dtype == XKB_Z;
   const int trans = (!cplx && o.trans == XKB_OP_C) ? XKB_OP_T : o.trans;
-  const bool lower_eff = (o.uplo == XKB_LOWER) ^ (trans != XKB_OP_N);
+  const bool fwd = (o.uplo == XKB_LOWER) ^ (trans != XKB_OP_N);
   const int mt = (o.M + kLeafS - 1) / kLeafS, nt = (o.N + kLeafS - 1) / kLeafS;
-  const int cb = b.ncounters;
-  b.ncounters += mt * nt;
-  auto cnt = [&](int blk, int j) { return cb + blk + j * mt; };
-  auto order = [&](int s) { return lower_eff ? s : mt - 1 - s; };
-  auto rows = [&](int blk) { return std::min(kLeafS, o.M - blk * kLeafS); };
   const char* A = static_cast<const char*>(o.A);
   char* X = static_cast<char*>(o.C);
+  const int dflags = (trans != XKB_OP_N ? kFlagSwap : 0) | (trans == XKB_OP_C ? kFlagConj : 0) |
+                     (fwd ? kFlagLower : 0) | (o.diag ? kFlagUnit : 0);
+  // element (r, c) of op(A) lives at A[r + c lda] (trans N) or A[c + r lda]
+  auto opA_at = [&](size_t r, size_t c) {
+    return trans == XKB_OP_N ? A + (r + c * o.lda) * es : A + (c + r * o.lda) * es;
+  };
   int n = 0;
-  for (int s = 0; s < mt; ++s) {
-    const int bk = order(s);
-    steps.emplace_back();
-    std::vector<Task>& out = steps.back();
-    for (int j = 0; j < nt; ++j) {
+  for (int j = 0; j < nt; ++j) {
+    const size_t c0 = (size_t)j * kLeafS;
+    int prev = -1;
+    for (int s = 0; s < mt; ++s) {
+      const int bk = fwd ? s : mt - 1 - s;
+      const size_t r0 = (size_t)bk * kLeafS;
+      const int rows = std::min(kLeafS, o.M - bk * kLeafS);
+      const size_t k0 = fwd ? 0 : r0 + rows;             // first solved row
+      const int K = fwd ? (int)r0 : o.M - (int)(r0 + rows);  // solved rows
       Task t;
       std::memset(&t, 0, sizeof(t));
-      t.kind = kTaskTrsmDiag;
+      t.kind = kTaskTrsm;
       t.dtype = o.dtype;
-      t.M = rows(bk);
+      t.opA = trans;
+      t.opB = XKB_OP_N;
+      t.M = rows;
       t.N = std::min(kLeafS, o.N - j * kLeafS);
+      t.K = K;
       t.call = call;
-      t.A = A + ((size_t)bk * kLeafS + (size_t)bk * kLeafS * o.lda) * es;
-      t.C = X + ((size_t)bk * kLeafS + (size_t)j * kLeafS * o.ldc) * es;
+      t.A = K > 0 ? opA_at(r0, k0) : A;
       t.lda = o.lda;
+      t.B = X + (k0 + c0 * o.ldc) * es;
+      t.ldb = o.ldc;
+      t.C = X + (r0 + c0 * o.ldc) * es;
       t.ldc = o.ldc;
-      t.ar = s == 0 ? o.alpha[0] : 1.0;
-      t.ai = s == 0 ? o.alpha[1] : 0.0;
-      t.flags = (trans != XKB_OP_N ? kFlagSwap : 0) | (trans == XKB_OP_C ? kFlagConj : 0) |
-                (lower_eff ? kFlagLower : 0) | (o.diag ? kFlagUnit : 0);
-      t.wait0 = cnt(bk, j);
-      t.target0 = s;  // the s updates from earlier steps are in
-      t.wait1 = -1;
-      t.signal = cnt(bk, j);
-      out.push_back(t);
+      t.D = A + (r0 + r0 * o.lda) * es;
+      t.ar = o.alpha[0];
+      t.ai = cplx ? o.alpha[1] : 0.0;
+      t.flags = dflags | narrow;
+      const int id = b.add(t, prev >= 0 ? 1 : 0);
+      ++b.nurg;
       ++n;
-    }
-    for (int p = s + 1; p < mt; ++p) {  // next diagonal block first (look-ahead)
-      const int bi = order(p);
-      for (int j = 0; j < nt; ++j) {
-        Task t;
-        std::memset(&t, 0, sizeof(t));
-        t.kind = kTaskGemm;
-        t.dtype = o.dtype;
-        t.M = rows(bi);
-        t.N = std::min(kLeafS, o.N - j * kLeafS);
-        t.K = rows(bk);
-        t.call = call;
-        // op(A)[bi rows, bk cols] = trans N: A[bi, bk]; else op(A[bk, bi])
-        if (trans == XKB_OP_N) {
-          t.opA = XKB_OP_N;
-          t.A = A + ((size_t)bi * kLeafS + (size_t)bk * kLeafS * o.lda) * es;
-        } else {
-          t.opA = trans;
-          t.A = A + ((size_t)bk * kLeafS + (size_t)bi * kLeafS * o.lda) * es;
-        }
-        t.opB = XKB_OP_N;
-        t.B = X + ((size_t)bk * kLeafS + (size_t)j * kLeafS * o.ldc) * es;
-        t.C = X + ((size_t)bi * kLeafS + (size_t)j * kLeafS * o.ldc) * es;
-        t.lda = o.lda;
-        t.ldb = o.ldc;
-        t.ldc = o.ldc;
-        t.ar = -1.0;
-        t.ai = 0.0;
-        t.br = s == 0 ? o.alpha[0] : 1.0;
-        t.bi = s == 0 ? o.alpha[1] : 0.0;
-        t.wait0 = cnt(bk, j);
-        t.target0 = s + 1;  // X_bk solved
-        t.wait1 = cnt(bi, j);
-        t.target1 = s;      // earlier updates of this block applied
-        t.signal = cnt(bi, j);
-        t.flags = narrow;
-        out.push_back(t);
-        ++n;
-      }
+      if (prev >= 0) b.edges.emplace_back(prev, id);
+      else b.urg_ready.push_back(id);
+      prev = id;
     }
   }
   return n;
 }
 
 struct Batch {
-  Task* h_tasks = nullptr;  // pinned
-  size_t cap = 0;
-  Task* d_tasks = nullptr;
-  int* d_counters = nullptr;  // counters, next, call_left (contiguous)
+  uint8_t* h_stage = nullptr;  // pinned: tasks then ints
+  size_t h_cap = 0;
+  uint8_t* d_buf = nullptr;    // device: tasks then ints
+  size_t d_cap = 0;
   unsigned long long* d_times = nullptr;  // call_end[ncalls], t_start
-  size_t d_cap_tasks = 0, d_cap_ints = 0, d_cap_times = 0;
-  int ntasks = 0, ncalls = 0, nctr = 0;
+  size_t d_cap_times = 0;
+  int ncalls = 0;
   std::vector<int> call_tasks;
 };
 
@@ -639,85 +973,76 @@ extern "C" int xkb_cuda_batch(const xkb_batch_op* ops, int nops, int schedule, v
   cudaStream_t st = resolve_stream(stream);
   Built b;
   b.call_tasks.assign(nops, 0);
-  std::vector<std::vector<std::vector<Task>>> solves;  // per solve: its steps
   for (int c = 0; c < nops; ++c) {
     const xkb_batch_op& o = ops[c];
     if ((o.dtype != XKB_D && o.dtype != XKB_Z) || o.M < 0 || o.N < 0 || o.K < 0) return XKB_EINVAL;
     if (o.M == 0 || o.N == 0) continue;
+    int n;
     if (o.kind == XKB_BATCH_GEMM) {
       if (o.K == 0) return XKB_EINVAL;  // beta-only calls are not batch tasks
-      const int n = add_gemm(b, o, c);
-      if (n < 0) return n;
-      b.call_tasks[c] = n;
+      n = add_gemm(b, o, c);
     } else if (o.kind == XKB_BATCH_TRSM) {
-      std::vector<std::vector<Task>> st_steps;
-      const int n = add_trsm(b, o, c, st_steps);
-      if (n < 0) return n;
-      b.call_tasks[c] = n;
-      solves.push_back(std::move(st_steps));
+      n = add_trsm(b, o, c);
     } else {
       return XKB_EINVAL;
     }
-  }
-  // schedule 0: gemm tiles in call order, then the solves step by step;
-  // schedule 1: interleave -- step s of every solve, then an equal share of
-  // the gemm tiles, so dependent steps sit far apart in the claim order
-  std::vector<Task> gemms;
-  gemms.swap(b.tasks);
-  std::vector<Task>& out = b.tasks;
-  size_t longest = 0;
-  for (auto& sv : solves) longest = std::max(longest, sv.size());
-  if (schedule == 0 || solves.empty()) {
-    out = gemms;
-    for (size_t st2 = 0; st2 < longest; ++st2)
-      for (auto& sv : solves)
-        if (st2 < sv.size()) out.insert(out.end(), sv[st2].begin(), sv[st2].end());
-  } else {
-    const size_t chunk = (gemms.size() + longest) / (longest + 1);
-    size_t gi = 0;
-    for (size_t st2 = 0; st2 < longest; ++st2) {
-      for (auto& sv : solves)
-        if (st2 < sv.size()) out.insert(out.end(), sv[st2].begin(), sv[st2].end());
-      const size_t ge = std::min(gemms.size(), gi + chunk);
-      out.insert(out.end(), gemms.begin() + gi, gemms.begin() + ge);
-      gi = ge;
-    }
-    out.insert(out.end(), gemms.begin() + gi, gemms.end());
+    if (n < 0) return n;
+    b.call_tasks[c] = n;
   }
   Batch& B = batch();
-  const int ntasks = (int)out.size();
-  B.ntasks = ntasks;
   B.ncalls = nops;
   B.call_tasks = b.call_tasks;
+  const int ntasks = (int)b.tasks.size();
   if (ntasks == 0) return XKB_OK;
+  // successor lists (CSR over producers)
+  std::vector<int> succ0((size_t)ntasks + 1, 0);
+  for (auto& e : b.edges) ++succ0[(size_t)e.first + 1];
+  for (int i = 0; i < ntasks; ++i) succ0[(size_t)i + 1] += succ0[(size_t)i];
+  std::vector<int> succ(b.edges.size());
+  {
+    std::vector<int> fill(succ0.begin(), succ0.end() - 1);
+    for (auto& e : b.edges) succ[(size_t)fill[(size_t)e.first]++] = e.second;
+  }
+  for (int i = 0; i < ntasks; ++i) {
+    b.tasks[(size_t)i].succ0 = succ0[(size_t)i];
+    b.tasks[(size_t)i].nsucc = succ0[(size_t)i + 1] - succ0[(size_t)i];
+  }
+  // staging layout: tasks | ndep | succ | bulk | urq | call_left | ctl
+  const size_t nbulk = b.bulk.size(), nurg = (size_t)b.nurg;
+  const size_t o_ndep = (size_t)ntasks * sizeof(Task);
+  const size_t o_succ = o_ndep + (size_t)ntasks * 4;
+  const size_t o_bulk = o_succ + succ.size() * 4;
+  const size_t o_urq = o_bulk + nbulk * 4;
+  const size_t o_left = o_urq + nurg * 4;
+  const size_t o_ctl = (o_left + (size_t)nops * 4 + 15) & ~size_t(15);
+  const size_t bytes = o_ctl + sizeof(Ctl);
   // the previous batch may still read the pinned staging buffer
-  if (B.h_tasks) cudaStreamSynchronize(st);
-  if ((size_t)ntasks > B.cap) {
-    if (B.h_tasks) cudaFreeHost(B.h_tasks);
-    B.cap = (size_t)ntasks * 2;
-    if (cudaHostAlloc(&B.h_tasks, B.cap * sizeof(Task), cudaHostAllocDefault) != cudaSuccess) {
-      B.h_tasks = nullptr;
-      B.cap = 0;
+  if (B.h_stage) cudaStreamSynchronize(st);
+  if (bytes > B.h_cap) {
+    if (B.h_stage) cudaFreeHost(B.h_stage);
+    B.h_cap = bytes * 2;
+    if (cudaHostAlloc(&B.h_stage, B.h_cap, cudaHostAllocDefault) != cudaSuccess) {
+      B.h_stage = nullptr;
+      B.h_cap = 0;
       return XKB_ENOMEM;
     }
   }
-  std::memcpy(B.h_tasks, out.data(), (size_t)ntasks * sizeof(Task));
-  const size_t nints = (size_t)b.ncounters + 1 + (size_t)nops;
-  if ((size_t)ntasks > B.d_cap_tasks) {
-    if (B.d_tasks) cudaFreeAsync(B.d_tasks, st);
-    B.d_cap_tasks = (size_t)ntasks * 2;
-    if (cudaMallocAsync(&B.d_tasks, B.d_cap_tasks * sizeof(Task), st) != cudaSuccess) {
-      B.d_tasks = nullptr;
-      B.d_cap_tasks = 0;
-      return XKB_ENOMEM;
-    }
-  }
-  if (nints > B.d_cap_ints) {
-    if (B.d_counters) cudaFreeAsync(B.d_counters, st);
-    B.d_cap_ints = nints * 2;
-    if (cudaMallocAsync(&B.d_counters, B.d_cap_ints * sizeof(int), st) != cudaSuccess) {
-      B.d_counters = nullptr;
-      B.d_cap_ints = 0;
+  uint8_t* h = B.h_stage;
+  std::memcpy(h, b.tasks.data(), o_ndep);
+  std::memcpy(h + o_ndep, b.ndep.data(), (size_t)ntasks * 4);
+  if (!succ.empty()) std::memcpy(h + o_succ, succ.data(), succ.size() * 4);
+  if (nbulk) std::memcpy(h + o_bulk, b.bulk.data(), nbulk * 4);
+  int* urq = reinterpret_cast<int*>(h + o_urq);
+  for (size_t i = 0; i < nurg; ++i) urq[i] = i < b.urg_ready.size() ? b.urg_ready[i] : -1;
+  std::memcpy(h + o_left, b.call_tasks.data(), (size_t)nops * 4);
+  Ctl ctl{0, 0, (int)b.urg_ready.size(), 0};
+  std::memcpy(h + o_ctl, &ctl, sizeof(ctl));
+  if (bytes > B.d_cap) {
+    if (B.d_buf) cudaFreeAsync(B.d_buf, st);
+    B.d_cap = bytes * 2;
+    if (cudaMallocAsync(&B.d_buf, B.d_cap, st) != cudaSuccess) {
+      B.d_buf = nullptr;
+      B.d_cap = 0;
       return XKB_ENOMEM;
     }
   }
@@ -731,12 +1056,8 @@ extern "C" int xkb_cuda_batch(const xkb_batch_op* ops, int nops, int schedule, v
       return XKB_ENOMEM;
     }
   }
-  int* d_next = B.d_counters + b.ncounters;
-  int* d_left = d_next + 1;
-  cudaMemcpyAsync(B.d_tasks, B.h_tasks, (size_t)ntasks * sizeof(Task), cudaMemcpyHostToDevice, st);
-  cudaMemsetAsync(B.d_counters, 0, (size_t)(b.ncounters + 1) * sizeof(int), st);
-  cudaMemcpyAsync(d_left, b.call_tasks.data(), (size_t)nops * sizeof(int), cudaMemcpyHostToDevice,
-                  st);
+  uint8_t* d = B.d_buf;
+  cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, st);
   cudaMemsetAsync(B.d_times, 0, (size_t)nops * sizeof(unsigned long long), st);
   cudaMemsetAsync(B.d_times + nops, 0xff, sizeof(unsigned long long), st);
   static bool attr = false;
@@ -747,8 +1068,11 @@ extern "C" int xkb_cuda_batch(const xkb_batch_op* ops, int nops, int schedule, v
     attr = true;
   }
   const int grid = std::min(grid_size(), std::max(1, ntasks));
-  k_sched<<<grid, kThreads, kSmemBytes, st>>>(B.d_tasks, ntasks, B.d_counters, d_next, d_left,
-                                              B.d_times, B.d_times + nops);
+  k_sched<<<grid, kThreads, kSmemBytes, st>>>(
+      reinterpret_cast<const Task*>(d), reinterpret_cast<int*>(d + o_ndep),
+      reinterpret_cast<const int*>(d + o_succ), reinterpret_cast<const int*>(d + o_bulk),
+      (int)nbulk, reinterpret_cast<int*>(d + o_urq), (int)nurg, reinterpret_cast<Ctl*>(d + o_ctl),
+      schedule == 0 ? 1 : 0, reinterpret_cast<int*>(d + o_left), B.d_times, B.d_times + nops);
   count_launch();
   // the pinned staging buffer must outlive the copy: the copy is ordered
   // before the kernel, and the next batch synchronises before reusing it
