@@ -258,6 +258,135 @@ def other_configs(lib, torch, dev, sp, stream):
     return out
 
 
+class BatchOp(ctypes.Structure):
+    """xkb_batch_op of include/xkb_cuda.h."""
+    _fields_ = [("kind", ctypes.c_int), ("dtype", ctypes.c_int), ("opA", ctypes.c_int),
+                ("opB", ctypes.c_int), ("side", ctypes.c_int), ("uplo", ctypes.c_int),
+                ("trans", ctypes.c_int), ("diag", ctypes.c_int), ("M", ctypes.c_int),
+                ("N", ctypes.c_int), ("K", ctypes.c_int),
+                ("A", ctypes.c_void_p), ("lda", ctypes.c_long),
+                ("B", ctypes.c_void_p), ("ldb", ctypes.c_long),
+                ("C", ctypes.c_void_p), ("ldc", ctypes.c_long),
+                ("alpha", ctypes.c_double * 2), ("beta", ctypes.c_double * 2)]
+
+
+def batch_config(lib, torch, dev, sp, stream, ncalls=2000, seed=2024, reps=5):
+    """The mixed-call workload: `ncalls` independent calls, 70% DGEMM NN,
+    20% DTRSM left/lower/no-trans/non-unit with a diagonally dominant A, 10%
+    ZGEMM NN; M, N, K log-uniform in [64, 2048] (one seeded generator),
+    leading dimensions = row counts (mostly odd, so most operands are not
+    16-byte aligned), alpha = beta = 1.  Run as ONE persistent launch of the
+    tile-task executor (xkb_cuda_batch), device resident; reported: aggregate
+    TFLOP/s (sum of flops, reference blas/flops.h, / launch time), per-call
+    completion latency p50/p99 from the launch start (device timestamps), and
+    the same calls issued one launch per call (xkb_cuda_gemm / xkb_cuda_trsm)
+    on the same stream for comparison."""
+    rng = np.random.default_rng(seed)
+    g = torch.Generator(device=dev).manual_seed(seed)
+    f64, c128 = torch.float64, torch.complex128
+
+    def lu():
+        return int(np.exp(rng.uniform(np.log(64), np.log(2048))))
+
+    def u(r, c):  # column-major r x c (a row-major c x r tensor)
+        return torch.rand(c, r, generator=g, device=dev, dtype=f64) - 0.5
+
+    ops, keep, flops = [], [], 0.0
+    kinds = {"dgemm": 0, "dtrsm": 0, "zgemm": 0}
+    for _ in range(ncalls):
+        r = rng.random()
+        o = BatchOp()
+        if r < 0.7 or r >= 0.9:
+            cplx = r >= 0.9
+            m, n, k = lu(), lu(), lu()
+            A, B, C = u(m, k), u(k, n), u(m, n)
+            if cplx:
+                A = torch.complex(A, u(m, k))
+                B = torch.complex(B, u(k, n))
+                C = torch.complex(C, u(m, n))
+            o.kind, o.dtype, o.opA, o.opB, o.M, o.N, o.K = 0, 3 if cplx else 1, 0, 0, m, n, k
+            o.A, o.lda, o.B, o.ldb, o.C, o.ldc = A.data_ptr(), m, B.data_ptr(), k, C.data_ptr(), m
+            o.alpha[0] = 1.0
+            o.beta[0] = 1.0
+            flops += (8.0 if cplx else 2.0) * m * n * k
+            kinds["zgemm" if cplx else "dgemm"] += 1
+            keep.append((A, B, C))
+        else:
+            m, n = lu(), lu()
+            L = torch.tril(u(m, m).t()) + m * torch.eye(m, device=dev, dtype=f64)
+            A = L.t().contiguous()  # column-major storage of the lower L
+            B = u(m, n)
+            o.kind, o.dtype, o.side, o.uplo, o.trans, o.diag, o.M, o.N = 1, 1, 0, 1, 0, 0, m, n
+            o.A, o.lda, o.C, o.ldc = A.data_ptr(), m, B.data_ptr(), m
+            o.alpha[0] = 1.0
+            flops += float(n) * m * (m + 1)
+            kinds["dtrsm"] += 1
+            keep.append((A, B))
+        ops.append(o)
+    arr = (BatchOp * len(ops))(*ops)
+    lib.xkb_cuda_batch.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
+    lib.xkb_cuda_batch_latency.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    k0 = lib.xkb_cuda_kernel_count()
+    for _ in range(3):  # warm-up
+        assert lib.xkb_cuda_batch(ctypes.addressof(arr), len(ops), 0, sp) == 0
+    torch.cuda.synchronize()
+    times = []
+    for _ in range(reps):
+        ev0.record(stream)
+        assert lib.xkb_cuda_batch(ctypes.addressof(arr), len(ops), 0, sp) == 0
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        times.append(ev0.elapsed_time(ev1))
+    launches = (lib.xkb_cuda_kernel_count() - k0) // (reps + 3)
+    lat = (ctypes.c_double * len(ops))()
+    assert lib.xkb_cuda_batch_latency(ctypes.addressof(lat), len(ops)) == 0
+    lat = np.array(list(lat))
+    ms = statistics.median(times)
+    # one launch per call, same calls and stream
+    al = (ctypes.c_double * 2)(1.0, 0.0)
+    alp = ctypes.cast(al, ctypes.POINTER(ctypes.c_double))
+    gas = []
+    for o in ops:
+        if o.kind == 0:
+            ga = GemmArgs(o.dtype, 0, 0, o.M, o.N, o.K, o.A, o.lda, o.B, o.ldb, o.C, o.ldc)
+            ga.alpha[0] = 1.0
+            ga.beta[0] = 1.0
+            gas.append(ga)
+        else:
+            gas.append(None)
+
+    def per_call():
+        bad = 0
+        for o, ga in zip(ops, gas):
+            if ga is not None:
+                bad += lib.xkb_cuda_gemm(ctypes.byref(ga), sp) != 0
+            else:
+                bad += lib.xkb_cuda_trsm(1, 0, 1, 0, 0, o.M, o.N, alp, o.A, o.lda, o.C, o.ldc, 0,
+                                         sp) != 0
+        return bad
+
+    per_call()
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    rejected = per_call()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    ms_seq = ev0.elapsed_time(ev1)
+    del keep
+    torch.cuda.empty_cache()
+    return {"workload": "batch_%d_calls_70dgemm_20dtrsm_10zgemm_loguniform_64_2048" % ncalls,
+            "calls": kinds, "gflop": flops / 1e9,
+            "tflops": flops / ms / 1e9, "ms_per_batch": ms, "launches_per_batch": int(launches),
+            "latency_ms_p50": float(np.percentile(lat, 50)),
+            "latency_ms_p99": float(np.percentile(lat, 99)),
+            "per_call_launches": {"tflops": flops / ms_seq / 1e9, "ms": ms_seq,
+                                  "launches": len(ops), "rejected_calls": int(rejected)},
+            "speedup_vs_per_call": ms_seq / ms}
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -473,6 +602,8 @@ def main():
     }
     if rank == 0 and not args.no_extra:
         line["other_configs"] = other_configs(lib, torch, f"cuda:{local}", sp, stream)
+        line["other_configs"]["batch_2000_mixed"] = batch_config(lib, torch, f"cuda:{local}", sp,
+                                                                 stream)
         # accuracy against the double-double oracle and the CPU baseline
         # (bounded samples; checker / baseline only)
         Co = np.asfortranarray(dC.cpu().numpy().T)

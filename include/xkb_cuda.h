@@ -135,9 +135,10 @@ int xkb_trace_take(xkb_trace_rec* out, int max);
  * operands run as ONE persistent launch of tile tasks (a DAG with device
  * dependency counters; replaces the reference's task runtime,
  * kaapi/kaapi_task.c:1277-1327 and kaapi/kaapi_offload_device.c:463-683).
- * dtype XKB_D or XKB_Z; leading dimensions x element size multiples of 16
- * bytes, 16-byte aligned bases.  Calls of one batch must not write memory
- * another call of the batch reads or writes. */
+ * dtype XKB_D or XKB_Z; any leading dimension >= the row count, 8-byte
+ * aligned bases (operands not 16-byte aligned are staged with 8-byte
+ * copies).  Calls of one batch must not write memory another call of the
+ * batch reads or writes. */
 #define XKB_BATCH_GEMM 0
 #define XKB_BATCH_TRSM 1
 typedef struct xkb_batch_op {

@@ -24,6 +24,8 @@
 #include <cstdio>
 #include <cstdlib>
 
+#include <algorithm>
+
 #include "dmma_common.cuh"
 #include "xkb_dev.cuh"
 
@@ -339,6 +341,47 @@ static int dispatch_type(const xkb_gemm_args* a, cudaStream_t st) {
   return dispatch_ops<T, BMb / 2, BNb / 2>(a, st);
 }
 
+// Copy a rows x cols column-major array (element size es) into a packed
+// array with leading dimension ldd.  Used to give TMA a 16-byte aligned view
+// of an operand whose base or leading dimension is not 16-byte aligned.
+template <class W>
+__global__ void k_repack(int rows_w, int cols, const W* __restrict__ src, long lds_w,
+                         W* __restrict__ dst, long ldd_w) {
+  const size_t total = (size_t)rows_w * (size_t)cols;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total;
+       e += (size_t)gridDim.x * blockDim.x) {
+    const size_t i = e % (size_t)rows_w, j = e / (size_t)rows_w;
+    dst[i + j * (size_t)ldd_w] = src[i + j * (size_t)lds_w];
+  }
+}
+
+static bool tma_ok(const void* p, long ld, int es) {
+  return reinterpret_cast<uintptr_t>(p) % 16 == 0 && ((size_t)ld * es) % 16 == 0;
+}
+
+// Packed copy of a stored operand (rows x cols, element size es); *out is a
+// stream-ordered allocation the caller frees on the same stream.
+static int repack(const void* src, long ld, int rows, int cols, int es, void** out, long* ldo,
+                  cudaStream_t st) {
+  const long ldp = (long)(((size_t)rows * es + 15) / 16 * 16 / es);
+  if (cudaMallocAsync(out, std::max<size_t>((size_t)ldp * cols * es, 16), st) != cudaSuccess)
+    return XKB_ENOMEM;
+  *ldo = ldp;
+  const size_t total = (size_t)rows * cols;
+  const unsigned grid = (unsigned)std::max<size_t>(
+      1, std::min<size_t>((total + 255) / 256, (size_t)sm_count() * 16));
+  if (es % 8 == 0 && reinterpret_cast<uintptr_t>(src) % 8 == 0)
+    k_repack<double><<<grid, 256, 0, st>>>(rows * (es / 8), cols,
+                                           static_cast<const double*>(src), ld * (es / 8),
+                                           static_cast<double*>(*out), ldp * (es / 8));
+  else
+    k_repack<float><<<grid, 256, 0, st>>>(rows * (es / 4), cols, static_cast<const float*>(src),
+                                          ld * (es / 4), static_cast<float*>(*out),
+                                          ldp * (es / 4));
+  count_launch();
+  return cudaPeekAtLastError() == cudaSuccess ? XKB_OK : XKB_ECUDA;
+}
+
 template <class T>
 static int launch_scale(int M, int N, const double* beta, void* C, long ldc, int uplo,
                         int herm_diag, long diag, cudaStream_t st) {
@@ -385,13 +428,36 @@ extern "C" int xkb_cuda_gemm(const xkb_gemm_args* a, void* stream) {
                           a->diag, stream);
   const int slot = trace_begin("dmma_gemm", a->dtype, a->M, a->N, a->K, 0, st);
   trace_mark(slot, 1, st);
-  int r = XKB_EINVAL;
-  switch (a->dtype) {
-    case XKB_S: r = dispatch_type<float>(a, st); break;
-    case XKB_D: r = dispatch_type<double>(a, st); break;
-    case XKB_C: r = dispatch_type<float2>(a, st); break;
-    case XKB_Z: r = dispatch_type<double2>(a, st); break;
+  // the tensor-map loads need 16-byte aligned bases and leading dimensions:
+  // other operands are first copied to packed, aligned arrays (C is read and
+  // written with plain loads and stores, any alignment)
+  const int es = (a->dtype == XKB_S) ? 4 : (a->dtype == XKB_Z ? 16 : 8);
+  if (reinterpret_cast<uintptr_t>(a->A) % 4 || reinterpret_cast<uintptr_t>(a->B) % 4 ||
+      reinterpret_cast<uintptr_t>(a->C) % 4)
+    return XKB_EINVAL;
+  xkb_gemm_args pa = *a;
+  void* packA = nullptr;
+  void* packB = nullptr;
+  int r = XKB_OK;
+  if (!tma_ok(a->A, a->lda, es))
+    r = repack(a->A, a->lda, a->opA == XKB_OP_N ? a->M : a->K,
+               a->opA == XKB_OP_N ? a->K : a->M, es, &packA, &pa.lda, st);
+  if (r == XKB_OK && !tma_ok(a->B, a->ldb, es))
+    r = repack(a->B, a->ldb, a->opB == XKB_OP_N ? a->K : a->N,
+               a->opB == XKB_OP_N ? a->N : a->K, es, &packB, &pa.ldb, st);
+  if (packA) pa.A = packA;
+  if (packB) pa.B = packB;
+  if (r == XKB_OK) {
+    r = XKB_EINVAL;
+    switch (a->dtype) {
+      case XKB_S: r = dispatch_type<float>(&pa, st); break;
+      case XKB_D: r = dispatch_type<double>(&pa, st); break;
+      case XKB_C: r = dispatch_type<float2>(&pa, st); break;
+      case XKB_Z: r = dispatch_type<double2>(&pa, st); break;
+    }
   }
+  if (packA) cudaFreeAsync(packA, st);
+  if (packB) cudaFreeAsync(packB, st);
   trace_mark(slot, 2, st);
   trace_mark(slot, 3, st);
   return r;
