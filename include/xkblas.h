@@ -248,6 +248,8 @@ typedef struct xkblas_stats_t {
   uint64_t ozaki_calls;    /* contractions run in the Ozaki INT8 form */
   uint64_t ozaki_moduli;   /* sum over those calls of the moduli used */
   double   flops;          /* algorithmic flops (reference blas/flops.h) */
+  uint64_t batches;        /* deferred-call batches run as one executor launch */
+  uint64_t batched_calls;  /* calls those batches held */
 } xkblas_stats_t;
 int  xkblas_get_stats(xkblas_stats_t* st);
 void xkblas_reset_stats(void);

@@ -50,7 +50,8 @@ class Stats(ctypes.Structure):
                 ("h2d_bytes", ctypes.c_uint64), ("d2h_bytes", ctypes.c_uint64),
                 ("tile_hits", ctypes.c_uint64), ("tile_misses", ctypes.c_uint64),
                 ("ozaki_calls", ctypes.c_uint64), ("ozaki_moduli", ctypes.c_uint64),
-                ("flops", ctypes.c_double)]
+                ("flops", ctypes.c_double), ("batches", ctypes.c_uint64),
+                ("batched_calls", ctypes.c_uint64)]
 
 
 def lib():
@@ -124,6 +125,10 @@ def stats():
     s = Stats()
     lib().xkblas_get_stats(ctypes.byref(s))
     return {k: getattr(s, k) for k, _ in Stats._fields_}
+
+
+def reset_stats():
+    lib().xkblas_reset_stats()
 
 
 def invalidate_caches():

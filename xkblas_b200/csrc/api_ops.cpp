@@ -101,6 +101,7 @@ bool use_ozaki(int dt, long m, long n, long k) {
 // One contraction on device operands: plain DMMA or Ozaki.
 int run_gemm(xkb_gemm_args& a) {
   Runtime& R = rt();
+  if (int e = flush_pending()) return e;  // queued calls first, in call order
   if (use_ozaki(a.dtype, a.M, a.N, a.K)) {
     int nm = R.ozaki_moduli ? R.ozaki_moduli : xkb_ozaki_default_moduli(a.K);
     int e = xkb_cuda_ozaki_gemm(&a, nm, R.s_comp);
@@ -176,7 +177,31 @@ int gemm_async(int transA, int transB, int M, int N, int K, const T* alpha, cons
   a.C = dev_ptr(dC, 0, 0);
   a.ldc = (long)dC->dld;
   if (!need_ab) a.K = 0;
-  if ((err = run_gemm(a))) return rt_error(err);
+  if (R.batch_on && need_ab && (a.dtype == XKB_D || a.dtype == XKB_Z) &&
+      !use_ozaki(a.dtype, M, N, K)) {
+    // queued for the tile-task executor (launched at the next coherence point)
+    xkb_batch_op o{};
+    o.kind = XKB_BATCH_GEMM;
+    o.dtype = a.dtype;
+    o.opA = a.opA;
+    o.opB = a.opB;
+    o.M = M;
+    o.N = N;
+    o.K = K;
+    o.A = a.A;
+    o.lda = a.lda;
+    o.B = a.B;
+    o.ldb = a.ldb;
+    o.C = a.C;
+    o.ldc = a.ldc;
+    o.alpha[0] = a.alpha[0];
+    o.alpha[1] = a.alpha[1];
+    o.beta[0] = a.beta[0];
+    o.beta[1] = a.beta[1];
+    if ((err = defer_op(o, dA, dB, is_zero(*beta) ? nullptr : dC, dC))) return rt_error(err);
+  } else if ((err = run_gemm(a))) {
+    return rt_error(err);
+  }
   mark_full_overwrite(dC, 0, M, 0, N);
   return 0;
 }
@@ -377,6 +402,7 @@ int sm_async(int herm, int side, int uplo, int M, int N, const T* alpha, const T
   double al[2], be[2];
   sc(*alpha, al);
   sc(*beta, be);
+  if ((err = flush_pending())) return rt_error(err);
   if ((err = xkb_cuda_symm(HT<T>::dt, herm, side == CblasLeft ? 0 : 1,
                            uplo == CblasLower ? XKB_LOWER : XKB_UPPER, M, N, al,
                            dev_ptr(dA, 0, 0), (long)dA->dld, dev_ptr(dB, 0, 0), (long)dB->dld,
@@ -424,14 +450,36 @@ int tr_async(int is_trsm, int side, int uplo, int transA, int diag, int M, int N
   const int sd = side == CblasLeft ? 0 : 1;
   const int ul = uplo == CblasLower ? XKB_LOWER : XKB_UPPER;
   const int dg = diag == CblasUnit ? 1 : 0;
+  const bool tc = (R.math == XKBLAS_TENSOR_OP_MATH) && (HT<T>::dt == XKB_D || HT<T>::dt == XKB_Z);
+  if (!zero && is_trsm && sd == 0 && R.batch_on && !tc &&
+      (HT<T>::dt == XKB_D || HT<T>::dt == XKB_Z)) {
+    // left solve queued for the tile-task executor
+    xkb_batch_op o{};
+    o.kind = XKB_BATCH_TRSM;
+    o.dtype = HT<T>::dt;
+    o.side = 0;
+    o.uplo = ul;
+    o.trans = opcode(transA);
+    o.diag = dg;
+    o.M = M;
+    o.N = N;
+    o.A = dev_ptr(dA, 0, 0);
+    o.lda = (long)dA->dld;
+    o.C = dev_ptr(dB, 0, 0);
+    o.ldc = (long)dB->dld;
+    o.alpha[0] = al[0];
+    o.alpha[1] = al[1];
+    if ((err = defer_op(o, dA, dB, nullptr, dB))) return rt_error(err);
+    mark_full_overwrite(dB, 0, M, 0, N);
+    return 0;
+  }
+  if ((err = flush_pending())) return rt_error(err);
   if (zero) {
     const double z[2] = {0, 0};
     err = xkb_cuda_scale(HT<T>::dt, M, N, z, dev_ptr(dB, 0, 0), (long)dB->dld, XKB_FULL, 0, 0,
                          R.s_comp);
   } else if (is_trsm) {
-    const int oz = ((R.math == XKBLAS_TENSOR_OP_MATH) && (HT<T>::dt == XKB_D || HT<T>::dt == XKB_Z))
-                       ? (int)std::max<long>(R.ozaki_min_dim, 1)
-                       : 0;
+    const int oz = tc ? (int)std::max<long>(R.ozaki_min_dim, 1) : 0;
     err = xkb_cuda_trsm(HT<T>::dt, sd, ul, opcode(transA), dg, M, N, al, dev_ptr(dA, 0, 0),
                         (long)dA->dld, dev_ptr(dB, 0, 0), (long)dB->dld, oz, R.s_comp);
   } else {

@@ -64,6 +64,7 @@ int ensure_init() {
     cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
   }
   xkb::set_library_stream(R.s_comp);
+  if (const char* b = getenv("XKBLAS_BATCH")) R.batch_on = atoi(b) != 0;
   if (const char* t = getenv("XKBLAS_TILE_SIZE")) R.nb_param = (size_t)atol(t);
   else if (const char* b = getenv("XKBLAS_BLOC_SIZE")) R.nb_param = (size_t)atol(b);
   if (const char* m = getenv("XKBLAS_DEFAULT_MATH")) {
@@ -106,6 +107,7 @@ void scratch_free(void* p) {
 static void free_desc_memory(Desc* d) {
   Runtime& R = rt();
   if (d->dev) {
+    flush_pending();  // queued calls may use the buffer
     // D2H copies and kernels may still read the buffer: order the free
     // after both streams.
     cudaEvent_t e = next_event();
@@ -299,8 +301,67 @@ void mark_full_overwrite(Desc* d, size_t r0, size_t r1, size_t c0, size_t c1) {
   mark_written(d, r0, r1, c0, c1, 0);
 }
 
+int flush_pending() {
+  Runtime& R = rt();
+  if (R.pending.empty()) return XKB_OK;
+  std::vector<xkb_batch_op> ops;
+  ops.swap(R.pending);
+  for (Desc* d : R.pend_descs) d->pend = 0;
+  R.pend_descs.clear();
+  if (ops.size() == 1) {  // a lone call: the whole-matrix kernels
+    const xkb_batch_op& o = ops[0];
+    if (o.kind == XKB_BATCH_TRSM)
+      return xkb_cuda_trsm(o.dtype, 0, o.uplo, o.trans, o.diag, o.M, o.N, o.alpha, o.A, o.lda,
+                           o.C, o.ldc, 0, R.s_comp);
+    xkb_gemm_args a{};
+    a.dtype = o.dtype;
+    a.opA = o.opA;
+    a.opB = o.opB;
+    a.M = o.M;
+    a.N = o.N;
+    a.K = o.K;
+    a.A = o.A;
+    a.lda = o.lda;
+    a.B = o.B;
+    a.ldb = o.ldb;
+    a.C = o.C;
+    a.ldc = o.ldc;
+    a.alpha[0] = o.alpha[0];
+    a.alpha[1] = o.alpha[1];
+    a.beta[0] = o.beta[0];
+    a.beta[1] = o.beta[1];
+    a.uplo = XKB_FULL;
+    return xkb_cuda_gemm(&a, R.s_comp);
+  }
+  R.batches++;
+  R.batched_calls += ops.size();
+  return xkb_cuda_batch(ops.data(), (int)ops.size(), 0, R.s_comp);
+}
+
+int defer_op(const xkb_batch_op& o, Desc* r0, Desc* r1, Desc* r2, Desc* w) {
+  Runtime& R = rt();
+  auto has = [](const Desc* d, uint8_t bits) { return d && (d->pend & bits); };
+  // read-after-write, write-after-read, write-after-write on a queued buffer
+  const bool conflict = has(r0, 2) || has(r1, 2) || has(r2, 2) || has(w, 3);
+  if (conflict || R.pending.size() >= R.batch_max) {
+    if (int e = flush_pending()) return e;
+  }
+  R.pending.push_back(o);
+  auto mark = [&](Desc* d, uint8_t bit) {
+    if (!d) return;
+    if (!d->pend) R.pend_descs.push_back(d);
+    d->pend |= bit;
+  };
+  mark(r0, 1);
+  mark(r1, 1);
+  mark(r2, 1);
+  mark(w, 2);
+  return XKB_OK;
+}
+
 int coherent(Desc* d, int uplo, int memflag) {
   Runtime& R = rt();
+  if (int e = flush_pending()) return e;
   // D2H after everything already queued on the compute stream
   cudaEvent_t ev = next_event();
   cudaEventRecord(ev, R.s_comp);
@@ -463,7 +524,7 @@ int xkblas_sync(void) {
   Runtime& R = rt();
   std::lock_guard<std::recursive_mutex> g(R.mu);
   if (!R.ready) return 0;
-  int e = XKB_OK;
+  int e = flush_pending();
   if (cudaStreamSynchronize(R.s_comp) != cudaSuccess) e = XKB_ECUDA;
   if (cudaStreamSynchronize(R.s_h2d) != cudaSuccess) e = XKB_ECUDA;
   if (cudaStreamSynchronize(R.s_d2h) != cudaSuccess) e = XKB_ECUDA;
@@ -739,6 +800,8 @@ int xkblas_get_stats(xkblas_stats_t* st) {
   st->ozaki_calls = R.stats.ozaki_calls;
   st->ozaki_moduli = R.stats.ozaki_moduli;
   st->flops = R.stats.flops;
+  st->batches = R.batches;
+  st->batched_calls = R.batched_calls;
   return 0;
 }
 
@@ -746,6 +809,8 @@ void xkblas_reset_stats(void) {
   Runtime& R = rt();
   std::lock_guard<std::recursive_mutex> g(R.mu);
   R.stats = Stats();
+  R.batches = 0;
+  R.batched_calls = 0;
 }
 
 }  // extern "C"

@@ -35,6 +35,7 @@ struct Desc {
   size_t mb = 0, nb = 0, mt = 0, nt = 0;  // tile grid
   std::vector<uint8_t> st;                // mt*nt tile states, column major
   bool registered_init = false;           // handle initialised (isinit)
+  uint8_t pend = 0;                       // deferred calls: 1 read, 2 written
   std::string name;
   uint8_t& tile(size_t i, size_t j) { return st[i + j * mt]; }
 };
@@ -61,6 +62,16 @@ struct Runtime {
   long ozaki_min_dim = 1024;  // contractions smaller than this stay plain
   Stats stats;
   int sticky_error = 0;
+  // Deferred calls: async GEMM / left-TRSM calls queued as one batch for the
+  // persistent tile-task executor (XKBLAS_BATCH=0 disables).  The queue is
+  // launched at the next coherence point (memory_coherent_async, sync, a
+  // buffer release), before any call that is not deferred, and before a call
+  // that touches what a queued call writes or writes what one reads.
+  bool batch_on = true;
+  size_t batch_max = 8192;
+  std::vector<xkb_batch_op> pending;
+  std::vector<Desc*> pend_descs;  // buffers the queued calls touch (Desc::pend set)
+  uint64_t batches = 0, batched_calls = 0;
 };
 
 Runtime& rt();
@@ -78,6 +89,11 @@ void mark_written(Desc* d, size_t r0, size_t r1, size_t c0, size_t c1, int uplo)
 // Mark a region as produced on the device without reading the host copy.
 void mark_full_overwrite(Desc* d, size_t r0, size_t r1, size_t c0, size_t c1);
 int coherent(Desc* d, int uplo, int memflag);
+// Launch the deferred calls (caller holds rt().mu); returns an XKB_* code.
+int flush_pending();
+// Queue a call for the executor; reads: the buffers it reads (nullptr
+// entries ignored), w: the buffer it writes.  Flushes first on a conflict.
+int defer_op(const xkb_batch_op& o, Desc* r0, Desc* r1, Desc* r2, Desc* w);
 void drop_desc(Desc* d);
 void* dev_ptr(const Desc* d, size_t r, size_t c);
 
