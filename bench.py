@@ -387,6 +387,108 @@ def batch_config(lib, torch, dev, sp, stream, ncalls=2000, seed=2024, reps=5):
             "speedup_vs_per_call": ms_seq / ms}
 
 
+def batch_config_e2e(lib, torch, ncalls=2000, seed=2024, reps=2):
+    """The mixed-call workload of batch_config (same sizes, same generator)
+    through the public XKBlas API with host-resident, user-owned matrices:
+    every call is xkblas_dgemm_async / xkblas_ztrsm... as the reference's
+    users issue them, then memory_coherent_async on every output and one
+    xkblas_sync, all inside the timed region (host->device copies of every
+    operand and device->host copies of every output included; the device
+    caches are dropped between repetitions).  The library queues the calls
+    and runs them as executor batches."""
+    rng = np.random.default_rng(seed)
+
+    def lu():
+        return int(np.exp(rng.uniform(np.log(64), np.log(2048))))
+
+    plan = []
+    for _ in range(ncalls):  # the same draw sequence as batch_config
+        r = rng.random()
+        if r < 0.7 or r >= 0.9:
+            plan.append(("zgemm" if r >= 0.9 else "dgemm", lu(), lu(), lu()))
+        else:
+            plan.append(("dtrsm", lu(), lu(), 0))
+    words = 0
+    for kind, m, n, k in plan:
+        w = 2 if kind == "zgemm" else 1
+        words += w * ((m * k + k * n + m * n) if kind != "dtrsm" else (m * m + m * n))
+    buf = torch.empty(words, dtype=torch.float64, pin_memory=True).numpy()
+    fill = np.random.default_rng(seed + 1)
+    for i in range(0, words, 1 << 26):
+        seg = buf[i:i + (1 << 26)]
+        fill.random(out=seg)
+        seg -= 0.5
+    mats, off, flops, h2d, d2h = [], 0, 0.0, 0, 0
+
+    def take(rows, cols, cplx):
+        nonlocal off
+        w = 2 if cplx else 1
+        a = buf[off:off + w * rows * cols]
+        off += w * rows * cols
+        a = a.view(np.complex128) if cplx else a
+        return a.reshape(cols, rows).T  # Fortran-ordered rows x cols view
+
+    for kind, m, n, k in plan:
+        if kind == "dtrsm":
+            A, B = take(m, m, False), take(m, n, False)
+            A[np.arange(m), np.arange(m)] += m  # diagonally dominant lower triangle
+            mats.append((kind, m, n, 0, A, None, B))
+            flops += float(n) * m * (m + 1)
+            h2d += 8 * (m * m + m * n)
+            d2h += 8 * m * n
+        else:
+            c = kind == "zgemm"
+            A, B, C = take(m, k, c), take(k, n, c), take(m, n, c)
+            mats.append((kind, m, n, k, A, B, C))
+            flops += (8.0 if c else 2.0) * m * n * k
+            es = 16 if c else 8
+            h2d += es * (m * k + k * n + m * n)
+            d2h += es * m * n
+    one_d = ctypes.c_double(1.0)
+    one_z = (ctypes.c_double * 2)(1.0, 0.0)
+    P = ctypes.c_void_p
+
+    def run():
+        for kind, m, n, k, A, B, C in mats:
+            if kind == "dgemm":
+                r = lib.xkblas_dgemm_async(111, 111, m, n, k, ctypes.byref(one_d),
+                                           P(A.ctypes.data), m, P(B.ctypes.data), k,
+                                           ctypes.byref(one_d), P(C.ctypes.data), m)
+            elif kind == "zgemm":
+                r = lib.xkblas_zgemm_async(111, 111, m, n, k, one_z, P(A.ctypes.data), m,
+                                           P(B.ctypes.data), k, one_z, P(C.ctypes.data), m)
+            else:
+                r = lib.xkblas_dtrsm_async(141, 122, 111, 131, m, n, ctypes.byref(one_d),
+                                           P(A.ctypes.data), m, P(C.ctypes.data), m)
+            assert r == 0, (kind, r)
+        for kind, m, n, k, A, B, C in mats:
+            es = 16 if kind == "zgemm" else 8
+            assert lib.xkblas_memory_coherent_async(0, 0, ctypes.c_size_t(m), ctypes.c_size_t(n),
+                                                    P(C.ctypes.data), ctypes.c_size_t(m),
+                                                    ctypes.c_size_t(es)) == 0
+        assert lib.xkblas_sync() == 0
+
+    import xkblas_b200 as X
+    st = X.Stats()
+    lib.xkblas_reset_stats()
+    run()  # warm-up (allocations, pinned staging)
+    lib.xkblas_memory_invalidate_caches()
+    times = []
+    for _ in range(reps):
+        lib.xkblas_reset_stats()
+        t0 = time.perf_counter()
+        run()
+        times.append(time.perf_counter() - t0)
+        lib.xkblas_get_stats(ctypes.byref(st))
+        lib.xkblas_memory_invalidate_caches()
+    sec = min(times)
+    out = {"value": flops / sec / 1e12, "unit": "TFLOP/s", "ms": sec * 1e3,
+           "h2d_bytes": h2d, "d2h_bytes": d2h, "batches": int(st.batches),
+           "batched_calls": int(st.batched_calls)}
+    del mats, buf
+    return out
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -604,6 +706,7 @@ def main():
         line["other_configs"] = other_configs(lib, torch, f"cuda:{local}", sp, stream)
         line["other_configs"]["batch_2000_mixed"] = batch_config(lib, torch, f"cuda:{local}", sp,
                                                                  stream)
+        line["other_configs"]["batch_2000_mixed"]["e2e_public_api"] = batch_config_e2e(lib, torch)
         # accuracy against the double-double oracle and the CPU baseline
         # (bounded samples; checker / baseline only)
         Co = np.asfortranarray(dC.cpu().numpy().T)

@@ -236,6 +236,46 @@ XKBLAS_DECL_OPS(z, Complex64_t, double)
 XKBLAS_DECL_HE_OPS(c, Complex32_t, float)
 XKBLAS_DECL_HE_OPS(z, Complex64_t, double)
 
+/* ---- synchronous forms: _async + memory_coherent_async on the output
+ * (its written triangle for gemmt/syrk/herk/syr2k/her2k) + xkblas_sync +
+ * xkblas_memory_invalidate_caches -- the sequence the reference's F77
+ * wrapper runs for every BLAS call (blas/zlibxkblas_wrapper.c:67-73), as C
+ * entry points with the _async argument lists.  Return 0, -i for the i-th
+ * bad argument, or a positive errno from the runtime. -------------------- */
+#define XKBLAS_DECL_SYNC_OPS(p, T, R)                                          \
+  int xkblas_##p##gemm_sync(int transA, int transB, int M, int N, int K,       \
+      const T* alpha, const T* A, int LDA, const T* B, int LDB,                \
+      const T* beta, T* C, int LDC);                                           \
+  int xkblas_##p##gemmt_sync(int uplo, int transA, int transB, int N, int K,   \
+      const T* alpha, const T* A, int LDA, const T* B, int LDB,                \
+      const T* beta, T* C, int LDC);                                           \
+  int xkblas_##p##trsm_sync(int side, int uplo, int transA, int diag, int N,   \
+      int NRHS, const T* alpha, const T* A, int LDA, T* B, int LDB);           \
+  int xkblas_##p##trmm_sync(int side, int uplo, int transA, int diag, int N,   \
+      int NRHS, const T* alpha, const T* A, int LDA, T* B, int LDB);           \
+  int xkblas_##p##symm_sync(int side, int uplo, int M, int N, const T* alpha,  \
+      const T* A, int LDA, const T* B, int LDB, const T* beta, T* C, int LDC); \
+  int xkblas_##p##syrk_sync(int uplo, int trans, int N, int K,                 \
+      const T* alpha, const T* A, int LDA, const T* beta, T* C, int LDC);      \
+  int xkblas_##p##syr2k_sync(int uplo, int trans, int N, int K,                \
+      const T* alpha, const T* A, int LDA, const T* B, int LDB,                \
+      const T* beta, T* C, int LDC);
+#define XKBLAS_DECL_HE_SYNC_OPS(p, T, R)                                       \
+  int xkblas_##p##hemm_sync(int side, int uplo, int M, int N, const T* alpha,  \
+      const T* A, int LDA, const T* B, int LDB, const T* beta, T* C, int LDC); \
+  int xkblas_##p##herk_sync(int uplo, int trans, int N, int K,                 \
+      const R* alpha, const T* A, int LDA, const R* beta, T* C, int LDC);      \
+  int xkblas_##p##her2k_sync(int uplo, int trans, int N, int K,                \
+      const T* alpha, const T* A, int LDA, const T* B, int LDB,                \
+      const R* beta, T* C, int LDC);
+
+XKBLAS_DECL_SYNC_OPS(s, float, float)
+XKBLAS_DECL_SYNC_OPS(d, double, double)
+XKBLAS_DECL_SYNC_OPS(c, Complex32_t, float)
+XKBLAS_DECL_SYNC_OPS(z, Complex64_t, double)
+XKBLAS_DECL_HE_SYNC_OPS(c, Complex32_t, float)
+XKBLAS_DECL_HE_SYNC_OPS(z, Complex64_t, double)
+
 /* ---- added: per-call counters (reference XKBLAS_VERBOSE statistics,
  * blas/xkblas.c:1635-1700, as a queryable record) ------------------------ */
 typedef struct xkblas_stats_t {

@@ -25,11 +25,11 @@ def _header_functions(name):
     if "XKBLAS_DECL_OPS" in src:
         for p in "sdcz":
             for op in ("gemm", "gemmt", "trsm", "trmm", "symm", "syrk", "syr2k"):
-                for kind in ("async", "native"):
+                for kind in ("async", "native", "sync"):
                     names.add("xkblas_%s%s_%s" % (p, op, kind))
         for p in "cz":
             for op in ("hemm", "herk", "her2k"):
-                for kind in ("async", "native"):
+                for kind in ("async", "native", "sync"):
                     names.add("xkblas_%s%s_%s" % (p, op, kind))
     names = {n for n in names if not n.startswith("xkblas_blas2cblas")}
     names.discard("xkblas_DECL_OPS")
@@ -41,6 +41,27 @@ def test_exports_every_declared_symbol(header):
     lib = X.lib()
     missing = [n for n in _header_functions(header) if not hasattr(lib, n)]
     assert not missing, missing
+
+
+def test_f77_library_exports_the_blas_names():
+    """libxkblas_blas.so (the drop-in BLAS) exports every Fortran name that
+    include/xkblas_f77.h declares, and libxkblas.so exports none of them (it
+    must not replace a process's BLAS just by being loaded)."""
+    src = open(os.path.join(ROOT, "include", "xkblas_f77.h")).read()
+    names = []
+    for p in "sdcz":
+        for op in ("gemm", "gemmt", "trsm", "trmm", "symm", "syrk", "syr2k"):
+            names.append("%s%s_" % (p, op))
+    for p in "cz":
+        for op in ("hemm", "herk", "her2k"):
+            names.append("%s%s_" % (p, op))
+    for op in ("gemm", "gemmt", "trsm", "trmm", "symm", "syrk", "syr2k", "hemm", "herk", "her2k"):
+        assert "p##%s_(" % op in src  # declared by the header's macros
+    f77 = ctypes.CDLL(X.F77_LIB_PATH)
+    missing = [n for n in names if not hasattr(f77, n)]
+    assert not missing, missing
+    lib = X.lib()
+    assert not [n for n in names if hasattr(lib, n)]
 
 
 def test_configuration_and_tilesize():

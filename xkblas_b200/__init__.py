@@ -14,6 +14,8 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libxkblas.so")
+# the Fortran-77 drop-in BLAS (dgemm_ ...), built on top of libxkblas.so
+F77_LIB_PATH = os.path.join(HERE, "libxkblas_blas.so")
 
 # CBLAS enum values of the reference header (blas/xkblas.h:114-118)
 CblasNoTrans, CblasTrans, CblasConjTrans = 111, 112, 113

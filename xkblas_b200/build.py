@@ -8,6 +8,10 @@ compiled by nvcc as well.  The CUDA runtime is linked statically and the
 driver is reached through cudaGetDriverEntryPoint, so the library loads on a
 machine without a GPU driver (entry points then report ENODEV).
 Objects go to xkblas_b200/_build/, the library to xkblas_b200/libxkblas.so.
+The Fortran-77 BLAS names (f77/xkblas_f77.cpp) are linked into a second
+library, xkblas_b200/libxkblas_blas.so, on top of libxkblas.so: loading it
+replaces the system BLAS level 3 for an unmodified application, so it is
+kept out of libxkblas.so itself.
 """
 import argparse
 import os
@@ -20,6 +24,9 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libxkblas.so")
+F77_SRC = os.path.join(HERE, "f77", "xkblas_f77.cpp")
+F77_LIB = os.path.join(HERE, "libxkblas_blas.so")
+CXX = os.environ.get("CXX", "g++")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -76,6 +83,15 @@ def build(force=False, jobs=None, verbose=False):
             raise RuntimeError("link failed:\n" + " ".join(cmd) + "\n" + r.stdout + r.stderr)
         if verbose:
             print("linked", LIB)
+    if force or not os.path.exists(F77_LIB) or max(
+            os.path.getmtime(LIB), _deps_mtime(F77_SRC)) > os.path.getmtime(F77_LIB):
+        cmd = [CXX, "-O2", "-std=c++17", "-fPIC", "-shared", "-I" + os.path.join(ROOT, "include"),
+               F77_SRC, "-o", F77_LIB, "-L" + HERE, "-lxkblas", "-Wl,-rpath,$ORIGIN"]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError("link failed:\n" + " ".join(cmd) + "\n" + r.stdout + r.stderr)
+        if verbose:
+            print("linked", F77_LIB)
     return LIB
 
 
