@@ -1,0 +1,106 @@
+"""Small, self-contained cases for profiling single kernels with ncu:
+
+    python -m xkblas_b200.profcases dmma|ozaki|repack|trsm|batch
+
+dmma    DGEMM NN 4096^3 through xkb_cuda_gemm (k_gemm_dmma), two calls
+ozaki   the same through xkb_cuda_ozaki_gemm, 16 moduli (k_oz_* kernels)
+repack  the DGEMM with lda = ldb = 4097 (k_repack, then k_gemm_dmma)
+trsm    DTRSM L/L/N/N 4096 x 4096, diagonally dominant (k_trsm_diag, GEMMs)
+batch   150 mixed calls (70% DGEMM, 20% DTRSM, 10% ZGEMM; M, N, K
+        log-uniform in [64, 2048]) as one xkb_cuda_batch launch (k_sched)
+
+Each case holds a few GB at most and finishes in seconds.  Inputs are seeded
+uniform [-0.5, 0.5] matrices on the device."""
+import ctypes
+import sys
+
+import numpy as np
+
+
+class _GemmArgs(ctypes.Structure):
+    _fields_ = [("dtype", ctypes.c_int), ("opA", ctypes.c_int), ("opB", ctypes.c_int),
+                ("M", ctypes.c_int), ("N", ctypes.c_int), ("K", ctypes.c_int),
+                ("A", ctypes.c_void_p), ("lda", ctypes.c_long),
+                ("B", ctypes.c_void_p), ("ldb", ctypes.c_long),
+                ("C", ctypes.c_void_p), ("ldc", ctypes.c_long),
+                ("alpha", ctypes.c_double * 2), ("beta", ctypes.c_double * 2),
+                ("uplo", ctypes.c_int), ("herm_diag", ctypes.c_int), ("diag", ctypes.c_long)]
+
+
+def main(case):
+    import torch
+    import xkblas_b200 as X
+    lib = X.lib()
+    X.init()
+    st = torch.cuda.Stream()
+    torch.cuda.set_stream(st)
+    sp = ctypes.c_void_p(st.cuda_stream)
+    g = torch.Generator(device="cuda").manual_seed(1)
+    f64 = torch.float64
+
+    def rnd(r, c):  # column-major r x c
+        return torch.rand(c, r, generator=g, device="cuda", dtype=f64) - 0.5
+
+    keep = []
+    if case in ("dmma", "ozaki", "repack"):
+        n = 4096
+        ld = n + 1 if case == "repack" else n
+        A, B, C = rnd(ld, n), rnd(ld, n), rnd(n, n)
+        keep += [A, B, C]
+        ga = _GemmArgs(1, 0, 0, n, n, n, A.data_ptr(), ld, B.data_ptr(), ld, C.data_ptr(), n)
+        ga.alpha[0] = ga.beta[0] = 1.0
+        for _ in range(2):
+            rc = (lib.xkb_cuda_ozaki_gemm(ctypes.byref(ga), 0, sp) if case == "ozaki"
+                  else lib.xkb_cuda_gemm(ctypes.byref(ga), sp))
+            assert rc == 0, rc
+    elif case == "trsm":
+        n = 4096
+        L = torch.tril(rnd(n, n).t()) + n * torch.eye(n, device="cuda", dtype=f64)
+        A, B = L.t().contiguous(), rnd(n, n)
+        keep += [A, B]
+        al = (ctypes.c_double * 2)(2.0, 0.0)
+        for _ in range(2):
+            assert lib.xkb_cuda_trsm(1, 0, 1, 0, 0, n, n,
+                                     ctypes.cast(al, ctypes.POINTER(ctypes.c_double)),
+                                     A.data_ptr(), n, B.data_ptr(), n, 0, sp) == 0
+    elif case == "batch":
+        rng = np.random.default_rng(2024)
+
+        def lu():
+            return int(np.exp(rng.uniform(np.log(64), np.log(2048))))
+
+        ops = []
+        for _ in range(150):
+            r = rng.random()
+            o = X.BatchOp()
+            if r < 0.7 or r >= 0.9:
+                cplx = r >= 0.9
+                m, n, k = lu(), lu(), lu()
+                A, B, C = rnd(m, k), rnd(k, n), rnd(m, n)
+                if cplx:
+                    A, B, C = torch.complex(A, A), torch.complex(B, B), torch.complex(C, C)
+                o.kind, o.dtype, o.M, o.N, o.K = 0, 3 if cplx else 1, m, n, k
+                o.A, o.lda, o.B, o.ldb, o.C, o.ldc = A.data_ptr(), m, B.data_ptr(), k, C.data_ptr(), m
+                o.alpha[0] = o.beta[0] = 1.0
+                keep += [A, B, C]
+            else:
+                m, n = lu(), lu()
+                L = torch.tril(rnd(m, m).t()) + m * torch.eye(m, device="cuda", dtype=f64)
+                A, B = L.t().contiguous(), rnd(m, n)
+                o.kind, o.dtype, o.side, o.uplo, o.trans, o.diag, o.M, o.N = 1, 1, 0, 1, 0, 0, m, n
+                o.A, o.lda, o.C, o.ldc = A.data_ptr(), m, B.data_ptr(), m
+                o.alpha[0] = 1.0
+                keep += [A, B]
+            ops.append(o)
+        arr = (X.BatchOp * len(ops))(*ops)
+        for _ in range(2):
+            assert lib.xkb_cuda_batch(arr, len(ops), 0, sp) == 0
+    else:
+        raise SystemExit("unknown case %r" % case)
+    torch.cuda.synchronize()
+    assert lib.xkb_cuda_take_device_error() == 0
+    print("ok", case)
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "dmma")
