@@ -280,7 +280,9 @@ def batch_config(lib, torch, dev, sp, stream, ncalls=2000, seed=2024, reps=5):
     TFLOP/s (sum of flops, reference blas/flops.h, / launch time), per-call
     completion latency p50/p99 from the launch start (device timestamps), and
     the same calls issued one launch per call (xkb_cuda_gemm / xkb_cuda_trsm)
-    on the same stream for comparison."""
+    on the same stream for comparison.  The timed submissions replay the
+    batch's CUDA graph (kept from the second submission); the first
+    submission, which builds and uploads the task list, is reported apart."""
     rng = np.random.default_rng(seed)
     g = torch.Generator(device=dev).manual_seed(seed)
     f64, c128 = torch.float64, torch.complex128
@@ -329,18 +331,32 @@ def batch_config(lib, torch, dev, sp, stream, ncalls=2000, seed=2024, reps=5):
     torch.cuda.synchronize()
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
+    # first submission: host task construction + task upload + launch; the
+    # second is kept as a CUDA graph, later ones replay it
+    lib.xkb_cuda_batch_release()
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    h0 = time.perf_counter()
+    assert lib.xkb_cuda_batch(ctypes.addressof(arr), len(ops), 0, sp) == 0
+    host_first = (time.perf_counter() - h0) * 1e3
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    ms_first = ev0.elapsed_time(ev1)
     k0 = lib.xkb_cuda_kernel_count()
     for _ in range(3):  # warm-up
         assert lib.xkb_cuda_batch(ctypes.addressof(arr), len(ops), 0, sp) == 0
     torch.cuda.synchronize()
-    times = []
+    times, host = [], []
     for _ in range(reps):
         ev0.record(stream)
+        h0 = time.perf_counter()
         assert lib.xkb_cuda_batch(ctypes.addressof(arr), len(ops), 0, sp) == 0
+        host.append((time.perf_counter() - h0) * 1e3)
         ev1.record(stream)
         torch.cuda.synchronize()
         times.append(ev0.elapsed_time(ev1))
     launches = (lib.xkb_cuda_kernel_count() - k0) // (reps + 3)
+    cached = lib.xkb_cuda_batch_cached()
     lat = (ctypes.c_double * len(ops))()
     assert lib.xkb_cuda_batch_latency(ctypes.addressof(lat), len(ops)) == 0
     lat = np.array(list(lat))
@@ -380,6 +396,9 @@ def batch_config(lib, torch, dev, sp, stream, ncalls=2000, seed=2024, reps=5):
     return {"workload": "batch_%d_calls_70dgemm_20dtrsm_10zgemm_loguniform_64_2048" % ncalls,
             "calls": kinds, "gflop": flops / 1e9,
             "tflops": flops / ms / 1e9, "ms_per_batch": ms, "launches_per_batch": int(launches),
+            "graph_replay": bool(cached), "host_ms_per_submission": statistics.median(host),
+            "first_submission": {"ms": ms_first, "tflops": flops / ms_first / 1e9,
+                                 "host_ms": host_first},
             "latency_ms_p50": float(np.percentile(lat, 50)),
             "latency_ms_p99": float(np.percentile(lat, 99)),
             "per_call_launches": {"tflops": flops / ms_seq / 1e9, "ms": ms_seq,

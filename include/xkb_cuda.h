@@ -159,6 +159,15 @@ int xkb_cuda_batch(const xkb_batch_op* ops, int nops, int schedule, void* stream
 /* After a batch: ms[i] = completion time of call i after the batch's first
  * task started (synchronises the device). */
 int xkb_cuda_batch_latency(double* ms, int n);
+/* Repeated batches: when an op list identical to one submitted recently
+ * (same calls, pointers, sizes, scalars and schedule) comes again, the
+ * batch is kept as a CUDA graph with its task list resident on the device,
+ * and later submissions replay the graph (no host-side task construction,
+ * no task upload).  At most 8 graphs / 2 GiB are kept (least recently used
+ * dropped); XKBLAS_BATCH_GRAPHS=0 disables.  xkb_cuda_batch_cached returns
+ * how many are held; xkb_cuda_batch_release drops them (synchronises). */
+int xkb_cuda_batch_cached(void);
+int xkb_cuda_batch_release(void);
 
 /* Device error word written by bounded waits (0 = none); clears it. */
 int xkb_cuda_take_device_error(void);

@@ -149,3 +149,57 @@ def test_batch_ztrsm_multiblock(xk):
     for A, B, B0, opT in keep:
         res = (opT @ B.t() - complex(1.0, -1.0) * B0.t()).abs().max().item()
         assert res < 1e-12
+
+
+def test_repeated_batch_replays_a_graph(xk):
+    """The same op list three times: the second submission is kept as a CUDA
+    graph and the third replays it; inputs changed between submissions are
+    read afresh (the graph holds the task list, not the data)."""
+    import torch
+    lib = xk.lib()
+    assert lib.xkb_cuda_batch_release() == 0
+    g = torch.Generator(device="cuda").manual_seed(9)
+    ops, mats = [], []
+    for (M, N, K) in ((200, 130, 77), (64, 300, 129), (513, 65, 40)):
+        A = torch.rand(K, M, generator=g, device="cuda", dtype=torch.float64) - 0.5
+        B = torch.rand(N, K, generator=g, device="cuda", dtype=torch.float64) - 0.5
+        C = torch.zeros(N, M, device="cuda", dtype=torch.float64)
+        o = X.BatchOp()
+        o.kind, o.dtype, o.opA, o.opB, o.M, o.N, o.K = 0, 1, N_, N_, M, N, K
+        o.A, o.lda, o.B, o.ldb, o.C, o.ldc = A.data_ptr(), M, B.data_ptr(), K, C.data_ptr(), M
+        o.alpha[0] = 1.0
+        ops.append(o)
+        mats.append((A, B, C))
+    M, N = 300, 150
+    L = torch.tril(torch.rand(M, M, generator=g, device="cuda", dtype=torch.float64)) / M \
+        + torch.eye(M, device="cuda", dtype=torch.float64)
+    A = L.t().contiguous()
+    Bt = torch.zeros(N, M, device="cuda", dtype=torch.float64)
+    o = X.BatchOp()
+    o.kind, o.dtype, o.side, o.uplo, o.trans, o.diag, o.M, o.N = 1, 1, 0, LO, N_, 0, M, N
+    o.A, o.lda, o.C, o.ldc = A.data_ptr(), M, Bt.data_ptr(), M
+    o.alpha[0] = 1.0
+    ops.append(o)
+    arr = (X.BatchOp * len(ops))(*ops)
+    for rep in range(3):
+        for (Am, Bm, Cm) in mats:
+            Bm.mul_(-1.0)  # new input values every submission
+            Cm.zero_()
+        B0 = torch.rand(N, M, generator=g, device="cuda", dtype=torch.float64)
+        Bt.copy_(B0)
+        torch.cuda.synchronize()
+        assert lib.xkb_cuda_batch(arr, len(ops), 0, None) == 0
+        torch.cuda.synchronize()
+        assert lib.xkb_cuda_take_device_error() == 0
+        for (Am, Bm, Cm) in mats:
+            ref = Am.t() @ Bm.t()
+            assert (Cm.t() - ref).abs().max().item() <= 1e-12 * max(ref.abs().max().item(), 1)
+        res = (L @ Bt.t() - B0.t()).abs().max().item()
+        assert res < 1e-12
+        if rep >= 1:
+            assert lib.xkb_cuda_batch_cached() >= 1
+    lat = (ctypes.c_double * len(ops))()
+    assert lib.xkb_cuda_batch_latency(lat, len(ops)) == 0
+    assert all(v > 0 for v in lat)
+    assert lib.xkb_cuda_batch_release() == 0
+    assert lib.xkb_cuda_batch_cached() == 0

@@ -489,6 +489,7 @@ int xkblas_finalize(void) {
   for (auto& kv : R.descs) all.push_back(kv.second);
   for (Desc* d : all) drop_desc(d);
   cudaStreamSynchronize(R.s_comp);
+  xkb_cuda_batch_release();
   return 0;
 }
 
@@ -782,6 +783,7 @@ int xkblas_memory_free(void) {
   xkblas_memory_invalidate_caches();
   if (!R.ready) return 0;
   cudaStreamSynchronize(R.s_comp);
+  xkb_cuda_batch_release();  // cached batch graphs hold device memory
   cudaMemPool_t pool;
   if (cudaDeviceGetDefaultMemPool(&pool, R.device) == cudaSuccess) cudaMemPoolTrimTo(pool, 0);
   return 0;

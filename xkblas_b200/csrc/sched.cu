@@ -936,15 +936,148 @@ static int add_trsm(Built& b, const xkb_batch_op& o, int call) {
   return n;
 }
 
+// Device image of one batch: tasks | ndep | succ | bulk | urq | call_left |
+// ctl.  tasks, succ and bulk are read-only during a launch; ndep, urq,
+// call_left and ctl are consumed by it.
+struct Layout {
+  int ntasks = 0, nops = 0;
+  size_t nbulk = 0, nurg = 0, nsucc = 0;
+  size_t o_ndep = 0, o_succ = 0, o_bulk = 0, o_urq = 0, o_left = 0, o_ctl = 0, bytes = 0;
+  void set(int nt, size_t ns, size_t nb, size_t nu, int no) {
+    ntasks = nt;
+    nsucc = ns;
+    nbulk = nb;
+    nurg = nu;
+    nops = no;
+    o_ndep = (size_t)nt * sizeof(Task);
+    o_succ = o_ndep + (size_t)nt * 4;
+    o_bulk = o_succ + ns * 4;
+    o_urq = o_bulk + nb * 4;
+    o_left = o_urq + nu * 4;
+    o_ctl = (o_left + (size_t)no * 4 + 15) & ~size_t(15);
+    bytes = o_ctl + sizeof(Ctl);
+  }
+};
+
+// A batch seen before, kept as a CUDA graph: reset the consumed state from
+// the pristine image (two device-to-device copies), clear the timestamps,
+// run k_sched.  Replaying skips the host-side task construction and the
+// upload of the task list.
+struct GraphEntry {
+  uint64_t key = 0;
+  int schedule = 0;
+  std::vector<xkb_batch_op> ops;  // the op list, compared on lookup
+  Layout L;
+  uint8_t* d_img = nullptr;       // pristine image
+  uint8_t* d_run = nullptr;       // image the launch consumes
+  unsigned long long* d_times = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  std::vector<int> call_tasks;
+  uint64_t last_use = 0;
+  size_t bytes() const { return 2 * L.bytes + ((size_t)L.nops + 1) * 8; }
+};
+
 struct Batch {
-  uint8_t* h_stage = nullptr;  // pinned: tasks then ints
+  uint8_t* h_stage = nullptr;  // pinned: the image of the batch being launched
   size_t h_cap = 0;
-  uint8_t* d_buf = nullptr;    // device: tasks then ints
+  uint8_t* d_buf = nullptr;    // device image of uncached batches
   size_t d_cap = 0;
   unsigned long long* d_times = nullptr;  // call_end[ncalls], t_start
   size_t d_cap_times = 0;
+  // the last launch (read by xkb_cuda_batch_latency)
   int ncalls = 0;
   std::vector<int> call_tasks;
+  unsigned long long* cur_times = nullptr;
+  // graph cache (XKBLAS_BATCH_GRAPHS=0 disables)
+  std::vector<GraphEntry*> graphs;
+  std::vector<uint64_t> seen;  // keys of recent uncached batches
+  uint64_t tick = 0;
+  size_t graph_bytes = 0;
+};
+
+constexpr size_t kGraphMaxEntries = 8;
+constexpr size_t kGraphMaxBytes = size_t(2) << 30;
+
+static void free_entry(GraphEntry* e, cudaStream_t st) {
+  if (e->exec) cudaGraphExecDestroy(e->exec);
+  if (e->graph) cudaGraphDestroy(e->graph);
+  if (e->d_img) cudaFreeAsync(e->d_img, st);
+  if (e->d_run) cudaFreeAsync(e->d_run, st);
+  if (e->d_times) cudaFreeAsync(e->d_times, st);
+  delete e;
+}
+
+// field-wise (the struct has padding bytes, which callers need not clear)
+static bool same_op(const xkb_batch_op& a, const xkb_batch_op& b) {
+  return a.kind == b.kind && a.dtype == b.dtype && a.opA == b.opA && a.opB == b.opB &&
+         a.side == b.side && a.uplo == b.uplo && a.trans == b.trans && a.diag == b.diag &&
+         a.M == b.M && a.N == b.N && a.K == b.K && a.A == b.A && a.lda == b.lda && a.B == b.B &&
+         a.ldb == b.ldb && a.C == b.C && a.ldc == b.ldc && a.alpha[0] == b.alpha[0] &&
+         a.alpha[1] == b.alpha[1] && a.beta[0] == b.beta[0] && a.beta[1] == b.beta[1];
+}
+
+static uint64_t op_key(const xkb_batch_op* ops, int nops, int schedule) {
+  uint64_t h = 1469598103934665603ull ^ (uint64_t)(unsigned)schedule;
+  auto mix = [&](uint64_t v) {
+    for (int i = 0; i < 8; ++i) h = (h ^ ((v >> (8 * i)) & 0xffu)) * 1099511628211ull;
+  };
+  auto bits = [](double d) {
+    uint64_t u;
+    std::memcpy(&u, &d, 8);
+    return u;
+  };
+  for (int c = 0; c < nops; ++c) {
+    const xkb_batch_op& o = ops[c];
+    mix(((uint64_t)(unsigned)o.kind << 32) ^ (uint64_t)(unsigned)o.dtype);
+    mix(((uint64_t)(unsigned)o.opA << 48) ^ ((uint64_t)(unsigned)o.opB << 32) ^
+        ((uint64_t)(unsigned)o.side << 16) ^ (uint64_t)(unsigned)o.uplo);
+    mix(((uint64_t)(unsigned)o.trans << 32) ^ (uint64_t)(unsigned)o.diag);
+    mix(((uint64_t)(unsigned)o.M << 32) ^ (uint64_t)(unsigned)o.N);
+    mix((uint64_t)(unsigned)o.K);
+    mix(reinterpret_cast<uintptr_t>(o.A));
+    mix((uint64_t)o.lda);
+    mix(reinterpret_cast<uintptr_t>(o.B));
+    mix((uint64_t)o.ldb);
+    mix(reinterpret_cast<uintptr_t>(o.C));
+    mix((uint64_t)o.ldc);
+    mix(bits(o.alpha[0]));
+    mix(bits(o.alpha[1]));
+    mix(bits(o.beta[0]));
+    mix(bits(o.beta[1]));
+  }
+  return h ^ (uint64_t)nops;
+}
+
+// kernel arguments of one launch on image d
+struct KArgs {
+  const Task* tasks;
+  int* ndep;
+  const int* succ;
+  const int* bulk;
+  int nbulk;
+  int* urq;
+  int nurg;
+  Ctl* ctl;
+  int urgent_first;
+  int* left;
+  unsigned long long* call_end;
+  unsigned long long* t_start;
+  KArgs(uint8_t* d, const Layout& L, int schedule, unsigned long long* times)
+      : tasks(reinterpret_cast<const Task*>(d)),
+        ndep(reinterpret_cast<int*>(d + L.o_ndep)),
+        succ(reinterpret_cast<const int*>(d + L.o_succ)),
+        bulk(reinterpret_cast<const int*>(d + L.o_bulk)),
+        nbulk((int)L.nbulk),
+        urq(reinterpret_cast<int*>(d + L.o_urq)),
+        nurg((int)L.nurg),
+        ctl(reinterpret_cast<Ctl*>(d + L.o_ctl)),
+        urgent_first(schedule == 0 ? 1 : 0),
+        left(reinterpret_cast<int*>(d + L.o_left)),
+        call_end(times),
+        t_start(times + L.nops) {}
+  void* params[12] = {&tasks, &ndep, &succ, &bulk, &nbulk, &urq,
+                      &nurg,  &ctl,  &urgent_first, &left, &call_end, &t_start};
 };
 
 static Batch& batch() {
@@ -960,6 +1093,61 @@ static int grid_size() {
   return per * sm_count();
 }
 
+static int set_smem_attr() {
+  static bool attr = false;
+  if (!attr) {
+    if (cudaFuncSetAttribute(k_sched, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)kSmemBytes) != cudaSuccess)
+      return XKB_ECUDA;
+    attr = true;
+  }
+  return XKB_OK;
+}
+
+static int launch_entry(Batch& B, GraphEntry* e, cudaStream_t st) {
+  e->last_use = ++B.tick;
+  B.ncalls = e->L.nops;
+  B.call_tasks = e->call_tasks;
+  B.cur_times = e->d_times;
+  if (cudaGraphLaunch(e->exec, st) != cudaSuccess) return XKB_ECUDA;
+  count_launch();
+  return XKB_OK;
+}
+
+// Build the graph of a cached batch whose image is in e->d_img.
+static int build_graph(GraphEntry* e) {
+  const Layout& L = e->L;
+  if (cudaGraphCreate(&e->graph, 0) != cudaSuccess) return XKB_ECUDA;
+  cudaGraphNode_t cp, m0, m1, kn;
+  if (cudaGraphAddMemcpyNode1D(&cp, e->graph, nullptr, 0, e->d_run, e->d_img, L.bytes,
+                               cudaMemcpyDeviceToDevice) != cudaSuccess)
+    return XKB_ECUDA;
+  cudaMemsetParams ms{};
+  ms.dst = e->d_times;
+  ms.value = 0;
+  ms.elementSize = 1;
+  ms.width = (size_t)L.nops * 8;
+  ms.height = 1;
+  ms.pitch = ms.width;
+  if (cudaGraphAddMemsetNode(&m0, e->graph, nullptr, 0, &ms) != cudaSuccess) return XKB_ECUDA;
+  ms.dst = e->d_times + L.nops;
+  ms.value = 0xff;
+  ms.width = 8;
+  ms.pitch = 8;
+  if (cudaGraphAddMemsetNode(&m1, e->graph, nullptr, 0, &ms) != cudaSuccess) return XKB_ECUDA;
+  KArgs a(e->d_run, L, e->schedule, e->d_times);
+  cudaKernelNodeParams kp{};
+  kp.func = reinterpret_cast<void*>(k_sched);
+  kp.gridDim = dim3((unsigned)std::min(grid_size(), std::max(1, L.ntasks)));
+  kp.blockDim = dim3(kThreads);
+  kp.sharedMemBytes = (unsigned)kSmemBytes;
+  kp.kernelParams = a.params;
+  const cudaGraphNode_t deps[3] = {cp, m0, m1};
+  if (cudaGraphAddKernelNode(&kn, e->graph, deps, 3, &kp) != cudaSuccess) return XKB_ECUDA;
+  if (cudaGraphInstantiate(&e->exec, e->graph, 0) != cudaSuccess) return XKB_ECUDA;
+  return XKB_OK;
+}
+
 }  // namespace sched
 }  // namespace xkb
 
@@ -971,6 +1159,21 @@ extern "C" int xkb_cuda_batch(const xkb_batch_op* ops, int nops, int schedule, v
   if (nops == 0) return XKB_OK;
   std::lock_guard<std::mutex> g(g_batch_mu);
   cudaStream_t st = resolve_stream(stream);
+  Batch& B = batch();
+  if (int e = set_smem_attr()) return e;
+  static const bool use_graphs = [] {
+    const char* v = getenv("XKBLAS_BATCH_GRAPHS");
+    return !(v && v[0] == '0');
+  }();
+  const uint64_t key = use_graphs ? op_key(ops, nops, schedule) : 0;
+  if (use_graphs) {
+    for (GraphEntry* e : B.graphs) {
+      if (e->key != key || e->schedule != schedule || (int)e->ops.size() != nops) continue;
+      bool same = true;
+      for (int c = 0; c < nops && same; ++c) same = same_op(e->ops[(size_t)c], ops[c]);
+      if (same) return launch_entry(B, e, st);
+    }
+  }
   Built b;
   b.call_tasks.assign(nops, 0);
   for (int c = 0; c < nops; ++c) {
@@ -989,10 +1192,9 @@ extern "C" int xkb_cuda_batch(const xkb_batch_op* ops, int nops, int schedule, v
     if (n < 0) return n;
     b.call_tasks[c] = n;
   }
-  Batch& B = batch();
+  const int ntasks = (int)b.tasks.size();
   B.ncalls = nops;
   B.call_tasks = b.call_tasks;
-  const int ntasks = (int)b.tasks.size();
   if (ntasks == 0) return XKB_OK;
   // successor lists (CSR over producers)
   std::vector<int> succ0((size_t)ntasks + 1, 0);
@@ -1007,20 +1209,13 @@ extern "C" int xkb_cuda_batch(const xkb_batch_op* ops, int nops, int schedule, v
     b.tasks[(size_t)i].succ0 = succ0[(size_t)i];
     b.tasks[(size_t)i].nsucc = succ0[(size_t)i + 1] - succ0[(size_t)i];
   }
-  // staging layout: tasks | ndep | succ | bulk | urq | call_left | ctl
-  const size_t nbulk = b.bulk.size(), nurg = (size_t)b.nurg;
-  const size_t o_ndep = (size_t)ntasks * sizeof(Task);
-  const size_t o_succ = o_ndep + (size_t)ntasks * 4;
-  const size_t o_bulk = o_succ + succ.size() * 4;
-  const size_t o_urq = o_bulk + nbulk * 4;
-  const size_t o_left = o_urq + nurg * 4;
-  const size_t o_ctl = (o_left + (size_t)nops * 4 + 15) & ~size_t(15);
-  const size_t bytes = o_ctl + sizeof(Ctl);
+  Layout L;
+  L.set(ntasks, succ.size(), b.bulk.size(), (size_t)b.nurg, nops);
   // the previous batch may still read the pinned staging buffer
   if (B.h_stage) cudaStreamSynchronize(st);
-  if (bytes > B.h_cap) {
+  if (L.bytes > B.h_cap) {
     if (B.h_stage) cudaFreeHost(B.h_stage);
-    B.h_cap = bytes * 2;
+    B.h_cap = L.bytes * 2;
     if (cudaHostAlloc(&B.h_stage, B.h_cap, cudaHostAllocDefault) != cudaSuccess) {
       B.h_stage = nullptr;
       B.h_cap = 0;
@@ -1028,18 +1223,64 @@ extern "C" int xkb_cuda_batch(const xkb_batch_op* ops, int nops, int schedule, v
     }
   }
   uint8_t* h = B.h_stage;
-  std::memcpy(h, b.tasks.data(), o_ndep);
-  std::memcpy(h + o_ndep, b.ndep.data(), (size_t)ntasks * 4);
-  if (!succ.empty()) std::memcpy(h + o_succ, succ.data(), succ.size() * 4);
-  if (nbulk) std::memcpy(h + o_bulk, b.bulk.data(), nbulk * 4);
-  int* urq = reinterpret_cast<int*>(h + o_urq);
-  for (size_t i = 0; i < nurg; ++i) urq[i] = i < b.urg_ready.size() ? b.urg_ready[i] : -1;
-  std::memcpy(h + o_left, b.call_tasks.data(), (size_t)nops * 4);
+  std::memcpy(h, b.tasks.data(), L.o_ndep);
+  std::memcpy(h + L.o_ndep, b.ndep.data(), (size_t)ntasks * 4);
+  if (!succ.empty()) std::memcpy(h + L.o_succ, succ.data(), succ.size() * 4);
+  if (L.nbulk) std::memcpy(h + L.o_bulk, b.bulk.data(), L.nbulk * 4);
+  int* urq = reinterpret_cast<int*>(h + L.o_urq);
+  for (size_t i = 0; i < L.nurg; ++i) urq[i] = i < b.urg_ready.size() ? b.urg_ready[i] : -1;
+  std::memcpy(h + L.o_left, b.call_tasks.data(), (size_t)nops * 4);
   Ctl ctl{0, 0, (int)b.urg_ready.size(), 0};
-  std::memcpy(h + o_ctl, &ctl, sizeof(ctl));
-  if (bytes > B.d_cap) {
+  std::memcpy(h + L.o_ctl, &ctl, sizeof(ctl));
+
+  // a batch seen before (recently, uncached) becomes a cached graph
+  bool cache = false;
+  if (use_graphs) {
+    auto it = std::find(B.seen.begin(), B.seen.end(), key);
+    if (it != B.seen.end()) {
+      B.seen.erase(it);
+      cache = 2 * L.bytes <= kGraphMaxBytes;
+    } else {
+      B.seen.push_back(key);
+      if (B.seen.size() > 32) B.seen.erase(B.seen.begin());
+    }
+  }
+  if (cache) {
+    GraphEntry* e = new GraphEntry;
+    e->key = key;
+    e->schedule = schedule;
+    e->ops.assign(ops, ops + nops);
+    e->L = L;
+    e->call_tasks = b.call_tasks;
+    if (cudaMallocAsync(&e->d_img, L.bytes, st) != cudaSuccess ||
+        cudaMallocAsync(&e->d_run, L.bytes, st) != cudaSuccess ||
+        cudaMallocAsync(&e->d_times, ((size_t)nops + 1) * 8, st) != cudaSuccess) {
+      cudaGetLastError();
+      free_entry(e, st);
+      return XKB_ENOMEM;
+    }
+    cudaMemcpyAsync(e->d_img, h, L.bytes, cudaMemcpyHostToDevice, st);
+    if (int r = build_graph(e)) {
+      free_entry(e, st);
+      return r;
+    }
+    // evict least recently used entries beyond the limits
+    while (!B.graphs.empty() && (B.graphs.size() >= kGraphMaxEntries ||
+                                 B.graph_bytes + e->bytes() > kGraphMaxBytes)) {
+      auto lru = std::min_element(B.graphs.begin(), B.graphs.end(),
+                                  [](GraphEntry* x, GraphEntry* y) { return x->last_use < y->last_use; });
+      B.graph_bytes -= (*lru)->bytes();
+      free_entry(*lru, st);
+      B.graphs.erase(lru);
+    }
+    B.graphs.push_back(e);
+    B.graph_bytes += e->bytes();
+    return launch_entry(B, e, st);
+  }
+
+  if (L.bytes > B.d_cap) {
     if (B.d_buf) cudaFreeAsync(B.d_buf, st);
-    B.d_cap = bytes * 2;
+    B.d_cap = L.bytes * 2;
     if (cudaMallocAsync(&B.d_buf, B.d_cap, st) != cudaSuccess) {
       B.d_buf = nullptr;
       B.d_cap = 0;
@@ -1057,22 +1298,15 @@ extern "C" int xkb_cuda_batch(const xkb_batch_op* ops, int nops, int schedule, v
     }
   }
   uint8_t* d = B.d_buf;
-  cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(d, h, L.bytes, cudaMemcpyHostToDevice, st);
   cudaMemsetAsync(B.d_times, 0, (size_t)nops * sizeof(unsigned long long), st);
   cudaMemsetAsync(B.d_times + nops, 0xff, sizeof(unsigned long long), st);
-  static bool attr = false;
-  if (!attr) {
-    if (cudaFuncSetAttribute(k_sched, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)kSmemBytes) != cudaSuccess)
-      return XKB_ECUDA;
-    attr = true;
-  }
+  B.cur_times = B.d_times;
+  KArgs a(d, L, schedule, B.d_times);
   const int grid = std::min(grid_size(), std::max(1, ntasks));
-  k_sched<<<grid, kThreads, kSmemBytes, st>>>(
-      reinterpret_cast<const Task*>(d), reinterpret_cast<int*>(d + o_ndep),
-      reinterpret_cast<const int*>(d + o_succ), reinterpret_cast<const int*>(d + o_bulk),
-      (int)nbulk, reinterpret_cast<int*>(d + o_urq), (int)nurg, reinterpret_cast<Ctl*>(d + o_ctl),
-      schedule == 0 ? 1 : 0, reinterpret_cast<int*>(d + o_left), B.d_times, B.d_times + nops);
+  k_sched<<<grid, kThreads, kSmemBytes, st>>>(a.tasks, a.ndep, a.succ, a.bulk, a.nbulk, a.urq,
+                                              a.nurg, a.ctl, a.urgent_first, a.left,
+                                              a.call_end, a.t_start);
   count_launch();
   // the pinned staging buffer must outlive the copy: the copy is ordered
   // before the kernel, and the next batch synchronises before reusing it
@@ -1082,14 +1316,32 @@ extern "C" int xkb_cuda_batch(const xkb_batch_op* ops, int nops, int schedule, v
 extern "C" int xkb_cuda_batch_latency(double* ms, int n) {
   Batch& B = batch();
   std::lock_guard<std::mutex> g(g_batch_mu);
-  if (!ms || n < 0 || n > B.ncalls || !B.d_times) return XKB_EINVAL;
+  if (!ms || n < 0 || n > B.ncalls || !B.cur_times) return XKB_EINVAL;
   if (cudaDeviceSynchronize() != cudaSuccess) return XKB_ECUDA;
   std::vector<unsigned long long> t((size_t)B.ncalls + 1);
-  if (cudaMemcpy(t.data(), B.d_times, t.size() * sizeof(unsigned long long),
+  if (cudaMemcpy(t.data(), B.cur_times, t.size() * sizeof(unsigned long long),
                  cudaMemcpyDeviceToHost) != cudaSuccess)
     return XKB_ECUDA;
   const unsigned long long t0 = t[B.ncalls];
   for (int i = 0; i < n; ++i)
     ms[i] = (B.call_tasks[i] && t[i] >= t0) ? (double)(t[i] - t0) * 1e-6 : 0.0;
   return XKB_OK;
+}
+
+extern "C" int xkb_cuda_batch_release(void) {
+  Batch& B = batch();
+  std::lock_guard<std::mutex> g(g_batch_mu);
+  if (cudaDeviceSynchronize() != cudaSuccess) return XKB_ECUDA;
+  for (GraphEntry* e : B.graphs) free_entry(e, nullptr);
+  B.graphs.clear();
+  B.seen.clear();
+  B.graph_bytes = 0;
+  if (B.cur_times && B.cur_times != B.d_times) B.cur_times = nullptr;
+  return XKB_OK;
+}
+
+extern "C" int xkb_cuda_batch_cached(void) {
+  Batch& B = batch();
+  std::lock_guard<std::mutex> g(g_batch_mu);
+  return (int)B.graphs.size();
 }
