@@ -726,11 +726,29 @@ def main():
         line["other_configs"]["batch_2000_mixed"] = batch_config(lib, torch, f"cuda:{local}", sp,
                                                                  stream)
         line["other_configs"]["batch_2000_mixed"]["e2e_public_api"] = batch_config_e2e(lib, torch)
+        # the autotuner's moduli choice for this K band (15 moduli, measured
+        # error at most half the plain kernel's): same workload, timed apart
+        d15 = torch.empty_like(dC)
+        g15 = args_for(d15)
+        for _ in range(2):
+            assert lib.xkb_cuda_ozaki_gemm(ctypes.byref(g15), 15, sp) == 0
+        torch.cuda.synchronize()
+        t15 = []
+        for _ in range(3):
+            ev0.record(stream)
+            assert lib.xkb_cuda_ozaki_gemm(ctypes.byref(g15), 15, sp) == 0
+            ev1.record(stream)
+            torch.cuda.synchronize()
+            t15.append(ev0.elapsed_time(ev1))
+        line["ozaki_15_moduli"] = {"value": flops / (min(t15) * 1e-3) / 1e12, "unit": "TFLOP/s",
+                                   "ms": min(t15)}
         # accuracy against the double-double oracle and the CPU baseline
         # (bounded samples; checker / baseline only)
         Co = np.asfortranarray(dC.cpu().numpy().T)
         Cp = np.asfortranarray(dP.cpu().numpy().T)
-        line["error_vs_dd"] = dd_errors(A, B, {"ozaki": Co, "plain": Cp})
+        C15 = np.asfortranarray(d15.cpu().numpy().T)
+        del d15
+        line["error_vs_dd"] = dd_errors(A, B, {"ozaki": Co, "plain": Cp, "ozaki_15_moduli": C15})
         line["cpu_baseline"] = cpu_baseline()
     if rank == 0:
         print(json.dumps(line), flush=True)

@@ -169,6 +169,23 @@ int xkb_cuda_batch_latency(double* ms, int n);
 int xkb_cuda_batch_cached(void);
 int xkb_cuda_batch_release(void);
 
+/* Tuning table: choices measured on the device by the autotuner
+ * (python -m xkblas_b200.autotune --out FILE; the runtime loads
+ * XKBLAS_TUNE_FILE at init).  Keys (built-in default):
+ *   gemm_big_min_tiles      whole-matrix GEMM uses 128-wide tiles when it has
+ *                           at least this many of them (SM count)
+ *   ozaki_min_dim           tensor-op mode uses Ozaki when min(M,N,K) >= (2048)
+ *   ozaki_moduli_k<=<K>     moduli count for contractions with inner size <= K
+ *                           (the smallest band covering K; else the K rule)
+ *   batch_schedule          executor claim order, 0 solves first / 1 gemms (0)
+ *   batch_tile128_min_rows  executor: real gemm calls this tall use 128-row
+ *                           tiles (96)
+ * xkb_tune_load returns the number of entries read or XKB_EINVAL. */
+int xkb_tune_set(const char* key, double value);
+double xkb_tune_get(const char* key, double dflt);
+int xkb_tune_load(const char* path);
+int xkb_tune_clear(void);
+
 /* Device error word written by bounded waits (0 = none); clears it. */
 int xkb_cuda_take_device_error(void);
 

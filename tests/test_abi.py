@@ -191,3 +191,29 @@ def test_cuda_abi_rejects_bad_arguments_without_device():
     assert lib.xkb_cuda_gemm(ctypes.byref(g), None) == -1
     g.M = 0
     assert lib.xkb_cuda_gemm(ctypes.byref(g), None) == 0
+
+
+def test_tuning_table_load_and_lookup(tmp_path):
+    """The autotuner's table: a file of "key value" lines is loaded, values
+    are read back, and the moduli-count bands drive xkb_ozaki_default_moduli
+    (host-only logic, no device needed)."""
+    lib = X.lib()
+    lib.xkb_tune_clear()
+    k16384 = lib.xkb_ozaki_default_moduli(16384)
+    assert k16384 == 16  # built-in rule: H - log2(K)/2 >= 53
+    f = tmp_path / "tune.txt"
+    f.write_text("# measured on a B200\n"
+                 "ozaki_moduli_k<=4096 13\n"
+                 "ozaki_moduli_k<=32768 15   # a comment\n"
+                 "batch_schedule 1\n"
+                 "not a number line\n")
+    assert lib.xkb_tune_load(str(f).encode()) == 3
+    assert lib.xkb_tune_get(b"batch_schedule", 0.0) == 1.0
+    assert lib.xkb_tune_get(b"missing_key", 7.5) == 7.5
+    assert lib.xkb_ozaki_default_moduli(1000) == 13
+    assert lib.xkb_ozaki_default_moduli(4096) == 13
+    assert lib.xkb_ozaki_default_moduli(16384) == 15
+    assert lib.xkb_ozaki_default_moduli(65536) == 16  # no band covers it: the K rule
+    lib.xkb_tune_clear()
+    assert lib.xkb_ozaki_default_moduli(16384) == k16384
+    assert lib.xkb_tune_load(b"/nonexistent/tune.txt") == -1

@@ -82,6 +82,10 @@ def lib():
             ctypes.c_size_t, ctypes.c_size_t]
         _lib.xkblas_memory_invalidate.argtypes = [ctypes.c_void_p]
         _lib.xkb_cuda_kernel_count.restype = ctypes.c_uint64
+        _lib.xkb_tune_get.restype = ctypes.c_double
+        _lib.xkb_tune_get.argtypes = [ctypes.c_char_p, ctypes.c_double]
+        _lib.xkb_tune_set.argtypes = [ctypes.c_char_p, ctypes.c_double]
+        _lib.xkb_tune_load.argtypes = [ctypes.c_char_p]
         c_int, c_long, c_vp = ctypes.c_int, ctypes.c_long, ctypes.c_void_p
         dptr = ctypes.POINTER(ctypes.c_double)
         _lib.xkb_cuda_trsm.argtypes = [c_int, c_int, c_int, c_int, c_int, c_int, c_int, dptr,

@@ -334,9 +334,12 @@ static int dispatch_type(const xkb_gemm_args* a, cudaStream_t st) {
   constexpr bool CPLX = St<T>::CPLX;
   constexpr int BMb = CPLX ? 64 : 128, BNb = 128;
   const long tiles_big = (long)((a->M + BMb - 1) / BMb) * ((a->N + BNb - 1) / BNb);
-  // XKBLAS_GEMM_TILE=big|small overrides the size rule (tuning sweeps)
+  // XKBLAS_GEMM_TILE=big|small overrides the size rule (tuning sweeps); the
+  // rule's threshold is the tuning table's gemm_big_min_tiles (default: one
+  // big tile per SM)
   static const char* force = getenv("XKBLAS_GEMM_TILE");
-  const bool big = force ? (force[0] == 'b') : (tiles_big >= sm_count());
+  const bool big = force ? (force[0] == 'b')
+                         : (tiles_big >= (long)tune("gemm_big_min_tiles", (double)sm_count()));
   if (big) return dispatch_ops<T, BMb, BNb>(a, st);
   return dispatch_ops<T, BMb / 2, BNb / 2>(a, st);
 }

@@ -856,6 +856,10 @@ static int launch_gemm(const int8_t* Ap, long a_rows, const int8_t* Bp, long b_r
 
 int default_moduli(long K) {
   if (K <= 0 || K > 131072) return 0;  // exact INT32 accumulation limit
+  // a count the autotuner measured for this K band (tuning table keys
+  // "ozaki_moduli_k<=<K>"), when one covers K
+  const int tuned = tune_band("ozaki_moduli_k<=", K);
+  if (tuned >= 2 && tuned <= kMaxMod) return tuned;
   // keep >= 53 bits for the largest entry of a row whose entries are all of
   // the same magnitude: H - log2(K)/2 >= 53
   for (int n = 8; n <= kMaxMod; ++n) {

@@ -71,6 +71,9 @@ int ensure_init() {
     if (!strcmp(m, "TC") || !strcmp(m, "tensorcore")) R.math = XKBLAS_TENSOR_OP_MATH;
     else R.math = XKBLAS_DEFAULT_MATH;
   }
+  // autotuner output (python -m xkblas_b200.autotune), then explicit settings
+  if (const char* f = getenv("XKBLAS_TUNE_FILE")) xkb_tune_load(f);
+  R.ozaki_min_dim = (long)xkb_tune_get("ozaki_min_dim", (double)R.ozaki_min_dim);
   if (const char* s = getenv("XKBLAS_OZAKI_SLICES")) R.ozaki_moduli = atoi(s);
   if (const char* s = getenv("XKBLAS_OZAKI_MIN_DIM")) R.ozaki_min_dim = atol(s);
   R.ready = true;
@@ -335,7 +338,8 @@ int flush_pending() {
   }
   R.batches++;
   R.batched_calls += ops.size();
-  return xkb_cuda_batch(ops.data(), (int)ops.size(), 0, R.s_comp);
+  return xkb_cuda_batch(ops.data(), (int)ops.size(), (int)xkb_tune_get("batch_schedule", 0.0),
+                        R.s_comp);
 }
 
 int defer_op(const xkb_batch_op& o, Desc* r0, Desc* r1, Desc* r2, Desc* w) {

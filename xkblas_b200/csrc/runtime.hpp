@@ -59,7 +59,8 @@ struct Runtime {
   size_t prec_param = 8;
   int math = XKBLAS_DEFAULT_MATH;
   int ozaki_moduli = 0;       // 0 = automatic
-  long ozaki_min_dim = 1024;  // contractions smaller than this stay plain
+  long ozaki_min_dim = 2048;  // contractions smaller than this stay plain
+                              // (measured crossover on a B200, autotune.py)
   Stats stats;
   int sticky_error = 0;
   // Deferred calls: async GEMM / left-TRSM calls queued as one batch for the

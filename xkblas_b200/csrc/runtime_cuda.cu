@@ -3,8 +3,12 @@
 // library loads on machines without a GPU driver), stream resolution,
 // launch accounting and the device error word readers.
 #include <atomic>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <map>
 #include <mutex>
+#include <string>
 #include <vector>
 
 #include "xkb_dev.cuh"
@@ -194,3 +198,77 @@ extern "C" int xkb_cuda_take_device_error(void) {
 }
 
 extern "C" uint64_t xkb_cuda_kernel_count(void) { return xkb::g_launches.load(); }
+
+// ---------------------------------------------------------------------------
+// Tuning table: the choices the autotuner (xkblas_b200/autotune.py) measures
+// on the device -- tile shapes, the Ozaki / plain crossover, moduli counts
+// per K band, the executor's schedule -- as key -> value pairs.  Every key
+// has a built-in default; xkb_tune_load reads "key value" lines ('#' starts
+// a comment) written by the autotuner.
+namespace xkb {
+static std::mutex g_tune_mu;
+static std::map<std::string, double>& tune_table() {
+  static std::map<std::string, double> t;
+  return t;
+}
+double tune(const char* key, double dflt) {
+  std::lock_guard<std::mutex> g(g_tune_mu);
+  auto& t = tune_table();
+  auto it = t.find(key);
+  return it == t.end() ? dflt : it->second;
+}
+// smallest band "<prefix><K_i>" with K <= K_i; 0 when none covers K
+int tune_band(const char* prefix, long K) {
+  std::lock_guard<std::mutex> g(g_tune_mu);
+  const size_t n = std::strlen(prefix);
+  long best_k = -1;
+  int best = 0;
+  for (auto& kv : tune_table()) {
+    if (kv.first.compare(0, n, prefix) != 0) continue;
+    const long ki = std::atol(kv.first.c_str() + n);
+    if (ki >= K && (best_k < 0 || ki < best_k)) {
+      best_k = ki;
+      best = (int)kv.second;
+    }
+  }
+  return best;
+}
+}  // namespace xkb
+
+extern "C" int xkb_tune_set(const char* key, double value) {
+  if (!key || !*key) return XKB_EINVAL;
+  std::lock_guard<std::mutex> g(xkb::g_tune_mu);
+  xkb::tune_table()[key] = value;
+  return XKB_OK;
+}
+
+extern "C" double xkb_tune_get(const char* key, double dflt) {
+  if (!key) return dflt;
+  return xkb::tune(key, dflt);
+}
+
+extern "C" int xkb_tune_load(const char* path) {
+  if (!path) return XKB_EINVAL;
+  FILE* f = std::fopen(path, "r");
+  if (!f) return XKB_EINVAL;
+  char line[512];
+  int n = 0;
+  while (std::fgets(line, sizeof line, f)) {
+    char* hash = std::strchr(line, '#');
+    if (hash) *hash = 0;
+    char key[256];
+    double v;
+    if (std::sscanf(line, "%255s %lf", key, &v) == 2) {
+      xkb_tune_set(key, v);
+      ++n;
+    }
+  }
+  std::fclose(f);
+  return n;
+}
+
+extern "C" int xkb_tune_clear(void) {
+  std::lock_guard<std::mutex> g(xkb::g_tune_mu);
+  xkb::tune_table().clear();
+  return XKB_OK;
+}

@@ -812,6 +812,8 @@ static bool aligned_ok(const void* p, long ld, int es) {
 
 static bool ptr8(const void* p) { return reinterpret_cast<uintptr_t>(p) % 8 == 0; }
 
+static int tile128_rows() { return (int)tune("batch_tile128_min_rows", 96.0); }
+
 static Task gemm_task(int dtype, int opA, int opB, int M, int N, int K, int call, const void* A,
                       long lda, const void* B, long ldb, void* C, long ldc, double ar, double ai,
                       double br, double bi, int flags) {
@@ -843,9 +845,10 @@ static Task gemm_task(int dtype, int opA, int opB, int M, int N, int K, int call
 // blas/zgemm.c:279-367, with the whole K range in one task).
 static int add_gemm(Built& b, const xkb_batch_op& o, int call) {
   const int es = esz(o.dtype);
-  // real calls taller than 96 rows use 128-row tiles (the kernel picks the
-  // 128 x 64 body for any real task taller than 64 rows)
-  const int BM = o.dtype == XKB_Z ? 32 : (o.M >= 96 ? 128 : 64), BN = 64;
+  // real calls of at least batch_tile128_min_rows rows (tuning table,
+  // default 96) use 128-row tiles (the kernel picks the 128 x 64 body for
+  // any real task taller than 64 rows)
+  const int BM = o.dtype == XKB_Z ? 32 : (o.M >= tile128_rows() ? 128 : 64), BN = 64;
   if (!ptr8(o.A) || !ptr8(o.B) || !ptr8(o.C)) return XKB_EINVAL;
   const int narrow =
       (aligned_ok(o.A, o.lda, es) && aligned_ok(o.B, o.ldb, es)) ? 0 : kFlagNarrow;
@@ -1176,6 +1179,27 @@ extern "C" int xkb_cuda_batch(const xkb_batch_op* ops, int nops, int schedule, v
   }
   Built b;
   b.call_tasks.assign(nops, 0);
+  {  // size every list once: the task build is a hot host path for big batches
+    size_t nt = 0, ne = 0, nb = 0;
+    for (int c = 0; c < nops; ++c) {
+      const xkb_batch_op& o = ops[c];
+      if (o.M <= 0 || o.N <= 0) continue;
+      if (o.kind == XKB_BATCH_GEMM) {
+        const size_t bm = o.dtype == XKB_Z ? 32 : (o.M >= tile128_rows() ? 128 : 64);
+        const size_t t = ((size_t)o.M + bm - 1) / bm * (((size_t)o.N + 63) / 64);
+        nt += t;
+        nb += t;
+      } else {
+        const size_t t = ((size_t)o.M + kLeafS - 1) / kLeafS * (((size_t)o.N + kLeafS - 1) / kLeafS);
+        nt += t;
+        ne += t;
+      }
+    }
+    b.tasks.reserve(nt);
+    b.ndep.reserve(nt);
+    b.bulk.reserve(nb);
+    b.edges.reserve(ne);
+  }
   for (int c = 0; c < nops; ++c) {
     const xkb_batch_op& o = ops[c];
     if ((o.dtype != XKB_D && o.dtype != XKB_Z) || o.M < 0 || o.N < 0 || o.K < 0) return XKB_EINVAL;

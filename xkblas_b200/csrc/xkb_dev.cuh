@@ -134,5 +134,7 @@ cudaStream_t resolve_stream(void* s);
 int trace_begin(const char* op, int dtype, int M, int N, int K, int nmod, cudaStream_t st);
 void trace_mark(int slot, int k, cudaStream_t st);
 void count_launch(int n = 1);
+double tune(const char* key, double dflt);   // tuning table (runtime_cuda.cu)
+int tune_band(const char* prefix, long K);
 int sm_count();
 }  // namespace xkb
