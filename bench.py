@@ -7,7 +7,10 @@ e ~ U{-20..20} per row of A and per column of B)".
 
 One JSON line on rank 0.  `value` = 2*M*N*K / device time of one Ozaki DGEMM
 call (C ABI xkb_cuda_ozaki_gemm, inputs resident in HBM, 2 GiB each, so every
-step streams from HBM rather than L2).  `e2e` = the same metric through the
+step streams from HBM rather than L2), with the moduli count the autotuner
+measures for this K band (config.moduli_choice); error_vs_dd checks that
+count against the double-double oracle in the same run, next to the plain
+kernel and the K rule's count (ozaki_rule_moduli).  `e2e` = the same metric through the
 public XKBlas API (xkblas_dgemm_async + xkblas_memory_coherent_async +
 xkblas_sync with pinned host buffers; host->device copies of A and B and the
 device->host copy of C inside the timed region, caches dropped every step).
@@ -594,7 +597,14 @@ def main():
 
     g_oz = args_for(dC)
     g_pl = args_for(dP)
-    nmod = lib.xkb_ozaki_default_moduli(K)
+    # moduli count: the autotuner's measured choice for this K band (the
+    # smallest count at most half as far from a 16-moduli product as the
+    # plain kernel, on a 1024 x 1024 x K sample of the same distribution);
+    # the K rule's count is timed beside it in the extras
+    from xkblas_b200.autotune import choose_moduli
+    nmod_rule = lib.xkb_ozaki_default_moduli(K)
+    nmod, tune_err_plain, tune_errs = choose_moduli(lib, K, 1024, 1024, sp)
+    torch.cuda.synchronize()
 
     def barrier():
         torch.cuda.synchronize()
@@ -611,7 +621,7 @@ def main():
     # ---- device-resident Ozaki steps --------------------------------------
     k0 = lib.xkb_cuda_kernel_count()
     for _ in range(args.warmup):
-        assert lib.xkb_cuda_ozaki_gemm(ctypes.byref(g_oz), 0, sp) == 0
+        assert lib.xkb_cuda_ozaki_gemm(ctypes.byref(g_oz), nmod, sp) == 0
     barrier()
     lib.xkb_trace_enable(1)
     lib.xkb_trace_take(None, 0)
@@ -622,7 +632,7 @@ def main():
         barrier()
         ev0.record(stream)
         for _ in range(args.steps):
-            assert lib.xkb_cuda_ozaki_gemm(ctypes.byref(g_oz), 0, sp) == 0
+            assert lib.xkb_cuda_ozaki_gemm(ctypes.byref(g_oz), nmod, sp) == 0
         ev1.record(stream)
         barrier()
     launches = lib.xkb_cuda_kernel_count() - k1
@@ -671,6 +681,9 @@ def main():
     hA[...] = A
     hB[...] = B
     X.set_modemath(X.XKBLAS_TENSOR_OP_MATH)
+    # the same moduli count through the runtime: the tuning-table entry for
+    # this K band (what XKBLAS_TUNE_FILE from the autotuner provides)
+    lib.xkb_tune_set(b"ozaki_moduli_k<=%d" % K, float(nmod))
     one = np.array([1.0])
     zero = np.array([0.0])
     P = ctypes.c_void_p
@@ -701,7 +714,11 @@ def main():
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
         "config": {"workload": WORKLOAD, "M": M, "N": N, "K": K, "exp_spread": EMAX,
-                   "moduli": nmod, "parallelism": "replicas" if world > 1 else "single",
+                   "moduli": nmod,
+                   "moduli_choice": "autotuned (xkblas_b200.autotune.choose_moduli on a 1024x1024x%d "
+                                    "sample: plain err %.2e, %s)" % (
+                                        K, tune_err_plain, ", ".join("%d: %.2e" % e for e in tune_errs)),
+                   "parallelism": "replicas" if world > 1 else "single",
                    "l2": "inputs 2 GiB each > 126 MB L2 (no flush needed)"},
         "e2e": {"value": e2e_value, "unit": "TFLOP/s",
                 "h2d_bytes_per_step": 2 * M * K * 8, "d2h_bytes_per_step": M * N * 8,
@@ -726,29 +743,30 @@ def main():
         line["other_configs"]["batch_2000_mixed"] = batch_config(lib, torch, f"cuda:{local}", sp,
                                                                  stream)
         line["other_configs"]["batch_2000_mixed"]["e2e_public_api"] = batch_config_e2e(lib, torch)
-        # the autotuner's moduli choice for this K band (15 moduli, measured
-        # error at most half the plain kernel's): same workload, timed apart
-        d15 = torch.empty_like(dC)
-        g15 = args_for(d15)
+        # the K rule's moduli count (worst-case bound, 16 at K = 16384): same
+        # workload, timed apart
+        d16 = torch.empty_like(dC)
+        g16 = args_for(d16)
         for _ in range(2):
-            assert lib.xkb_cuda_ozaki_gemm(ctypes.byref(g15), 15, sp) == 0
+            assert lib.xkb_cuda_ozaki_gemm(ctypes.byref(g16), nmod_rule, sp) == 0
         torch.cuda.synchronize()
-        t15 = []
+        t16 = []
         for _ in range(3):
             ev0.record(stream)
-            assert lib.xkb_cuda_ozaki_gemm(ctypes.byref(g15), 15, sp) == 0
+            assert lib.xkb_cuda_ozaki_gemm(ctypes.byref(g16), nmod_rule, sp) == 0
             ev1.record(stream)
             torch.cuda.synchronize()
-            t15.append(ev0.elapsed_time(ev1))
-        line["ozaki_15_moduli"] = {"value": flops / (min(t15) * 1e-3) / 1e12, "unit": "TFLOP/s",
-                                   "ms": min(t15)}
+            t16.append(ev0.elapsed_time(ev1))
+        line["ozaki_rule_moduli"] = {"moduli": nmod_rule,
+                                     "value": flops / (min(t16) * 1e-3) / 1e12,
+                                     "unit": "TFLOP/s", "ms": min(t16)}
         # accuracy against the double-double oracle and the CPU baseline
         # (bounded samples; checker / baseline only)
         Co = np.asfortranarray(dC.cpu().numpy().T)
         Cp = np.asfortranarray(dP.cpu().numpy().T)
-        C15 = np.asfortranarray(d15.cpu().numpy().T)
-        del d15
-        line["error_vs_dd"] = dd_errors(A, B, {"ozaki": Co, "plain": Cp, "ozaki_15_moduli": C15})
+        C16 = np.asfortranarray(d16.cpu().numpy().T)
+        del d16
+        line["error_vs_dd"] = dd_errors(A, B, {"ozaki": Co, "plain": Cp, "ozaki_rule_moduli": C16})
         line["cpu_baseline"] = cpu_baseline()
     if rank == 0:
         print(json.dumps(line), flush=True)

@@ -39,6 +39,49 @@ class _GemmArgs(ctypes.Structure):
                 ("uplo", ctypes.c_int), ("herm_diag", ctypes.c_int), ("diag", ctypes.c_long)]
 
 
+def choose_moduli(lib, K, M=1024, N=1024, stream=None, gen=None):
+    """The smallest moduli count whose Ozaki product, on M x K times K x N
+    inputs with exponents spread over [-20, 20] per row of A and per column
+    of B, is at most half as far from a 16-moduli product as the plain FP64
+    kernel is (errors normalised by |a_i| |b_j| K).  Returns (count, plain
+    error, [(count, error) tried]).  Runs on `stream` (a CUDA stream handle,
+    ctypes) and synchronises the device around every call."""
+    import torch as t
+    g = gen if gen is not None else t.Generator(device="cuda").manual_seed(77)
+    sp = stream if stream is not None else ctypes.c_void_p(0)
+
+    def spread(r, c, by_col):
+        u = 2 * t.rand(c, r, generator=g, device="cuda", dtype=t.float64) - 1
+        shape = (c, 1) if by_col else (1, r)
+        e = t.randint(-20, 21, shape, generator=g, device="cuda").double()
+        return u * t.pow(2.0, e)
+
+    A, B = spread(M, K, False), spread(K, N, True)
+    C = t.zeros(N, M, device="cuda", dtype=t.float64)
+    t.cuda.synchronize()
+    a = _GemmArgs(1, 0, 0, M, N, K, A.data_ptr(), M, B.data_ptr(), K, C.data_ptr(), M)
+    a.alpha[0] = 1.0
+    assert lib.xkb_cuda_ozaki_gemm(ctypes.byref(a), 16, sp) == 0
+    t.cuda.synchronize()
+    ref = C.clone()
+    assert lib.xkb_cuda_gemm(ctypes.byref(a), sp) == 0
+    t.cuda.synchronize()
+    scale = (A.abs().amax(dim=0)[None, :] * B.abs().amax(dim=1)[:, None]) * K  # |a_i||b_j| K
+    err_plain = ((C - ref).abs() / scale).max().item()
+    choice, errs = 16, []
+    for n in range(10, 16):
+        C.zero_()
+        t.cuda.synchronize()
+        assert lib.xkb_cuda_ozaki_gemm(ctypes.byref(a), n, sp) == 0
+        t.cuda.synchronize()
+        err = ((C - ref).abs() / scale).max().item()
+        errs.append((n, err))
+        if err <= 0.5 * err_plain:
+            choice = n
+            break
+    return choice, err_plain, errs
+
+
 class Tuner:
     def __init__(self, quick=False, log=print):
         import torch
@@ -134,29 +177,9 @@ class Tuner:
         self.table["ozaki_min_dim"] = (thr, "sizes: " + ", ".join("%d%s" % (n, "O" if w else "p") for n, w in wins))
 
     def moduli(self):
-        t, lib = self.torch, self.lib
         M = N = 512 if self.quick else 1024
         for K in ([1024, 16384] if self.quick else [256, 1024, 4096, 16384, 65536]):
-            A, B = self.spread(M, K, False), self.spread(K, N, True)
-            C = t.zeros(N, M, device="cuda", dtype=t.float64)
-            a = self.args(A, B, C, M, N, K)
-            assert lib.xkb_cuda_ozaki_gemm(ctypes.byref(a), 16, self.sp) == 0
-            t.cuda.synchronize()
-            ref = C.clone()
-            assert lib.xkb_cuda_gemm(ctypes.byref(a), self.sp) == 0
-            t.cuda.synchronize()
-            scale = (A.abs().amax(dim=0)[None, :] * B.abs().amax(dim=1)[:, None]) * K  # |a_i||b_j| K
-            err_plain = ((C - ref).abs() / scale).max().item()
-            choice, errs = 16, []
-            for n in range(10, 16):
-                C.zero_()
-                assert lib.xkb_cuda_ozaki_gemm(ctypes.byref(a), n, self.sp) == 0
-                t.cuda.synchronize()
-                err = ((C - ref).abs() / scale).max().item()
-                errs.append((n, err))
-                if err <= 0.5 * err_plain:
-                    choice = n
-                    break
+            choice, err_plain, errs = choose_moduli(self.lib, K, M, N, self.sp, self.g)
             self.log("moduli K=%6d: plain %.2e, " % (K, err_plain)
                      + ", ".join("%d: %.2e" % e for e in errs) + " -> %d" % choice)
             self.table["ozaki_moduli_k<=%d" % K] = (choice, "plain err %.2e; %s" % (

@@ -38,6 +38,7 @@
 #include <vector>
 
 #include "dmma_common.cuh"
+#include "trsm_leaf.cuh"
 #include "xkb_dev.cuh"
 
 namespace xkb {
@@ -85,7 +86,7 @@ struct Ctl {
 constexpr int kThreads = 256;
 constexpr int kBK = 16;
 constexpr int kSt = 3;      // cp.async stages
-constexpr int kLeafS = 64;  // trsm block
+constexpr int kLeafS = kLeafRows;  // trsm block (trsm_leaf.cuh)
 
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem, int src_bytes) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(smem)),
@@ -490,188 +491,21 @@ __device__ __forceinline__ void gemm_dispatch2(const Task& t, uint8_t* smem) {
 }
 
 // ---- trsm diagonal block ------------------------------------------------------
-// X = alpha * op(T)^-1 B for one 64-row diagonal block T and up to 64
-// right-hand sides, by substitution.  A column is held by G lanes of one
-// warp, lane g keeping rows RPL*g .. RPL*g + RPL-1 in registers (real: RPL
-// 16, G 4, 64 columns per pass; complex: RPL 8, G 8, 32 columns per pass).
-// At step i the owner of row i scales it by the reciprocal of T(i,i) (the
-// packed-reciprocal form CPU BLAS kernels use), the G lanes share it by
-// shuffle, and each lane updates its rows below (lower) or above (upper) i.
-// op(T) is staged column by column in shared memory, row groups GS = RPL + 2
-// doubles apart so that the G lanes' vector loads fall in distinct banks.
-template <class T>
-struct TrsmShape {
-  static constexpr int RPL = St<T>::CPLX ? 8 : 16;  // rows per lane
-  static constexpr int G = kLeafS / RPL;            // lanes per column
-  static constexpr int GS = RPL + 2;                // staged row-group stride
-  static constexpr int COL = G * GS;                // staged column stride
-  static constexpr int CPP = kThreads / G;          // columns per pass
-};
-constexpr size_t kTrsmSmem =
-    2 * sizeof(double) * (kLeafS * TrsmShape<double2>::COL + kLeafS);  // complex, the larger
+// One 64-row diagonal block against up to 64 right-hand sides: the shared
+// register-resident substitution of trsm_leaf.cuh.  Not inlined: its
+// register allocation stays apart from the gemm tile's.
+constexpr size_t kTrsmSmem = LeafShape<double2>::SMEM;  // complex, the larger
 
-template <class T, bool LOWER>
-__device__ __forceinline__ void trsm_solve(const Task& t, const double* Tr, const double* Ti,
-                                           const double* Dr, const double* Di, double ar,
-                                           double ai) {
-  using Sh = TrsmShape<T>;
-  constexpr int RPL = Sh::RPL, G = Sh::G, GS = Sh::GS, COL = Sh::COL;
-  constexpr bool CP = St<T>::CPLX;
-  using S = typename St<T>::S;
-  const int tid = threadIdx.x, lane = tid & 31;
-  const int q = tid % G, gbase = lane & ~(G - 1);
-  const int n = t.M, nrhs = t.N;
-  S* B = static_cast<S*>(t.C);
-  for (int c = tid / G; c < kLeafS; c += Sh::CPP) {  // uniform trip count per warp
-    double xr[RPL], xi[RPL];
-#pragma unroll
-    for (int r = 0; r < RPL; ++r) {
-      const int row = q * RPL + r;
-      xr[r] = xi[r] = 0.0;
-      if (row < n && c < nrhs) {
-        const size_t idx = (size_t)row + (size_t)c * t.ldc;
-        const double br = CP ? __ldcg(B + 2 * idx) : __ldcg(B + idx);
-        const double bi = CP ? __ldcg(B + 2 * idx + 1) : 0.0;
-        xr[r] = ar * br - ai * bi;
-        if (CP) xi[r] = ar * bi + ai * br;
-      }
-    }
-    // steps in G rounds of RPL: the register index is a compile-time constant
-    // within a round, the owning lane a run-time one
-#pragma unroll 1
-    for (int og = 0; og < G; ++og) {
-#pragma unroll
-    for (int ss = 0; ss < RPL; ++ss) {
-      const int oq = LOWER ? og : G - 1 - og, oi = LOWER ? ss : RPL - 1 - ss;
-      const int i = oq * RPL + oi;
-      double vr = __shfl_sync(0xffffffffu, xr[oi], gbase | oq);
-      double vi = CP ? __shfl_sync(0xffffffffu, xi[oi], gbase | oq) : 0.0;
-      if (CP) {
-        const double dr = Dr[i], di = Di[i];
-        const double wr = vr * dr - vi * di;
-        vi = vr * di + vi * dr;
-        vr = wr;
-      } else {
-        vr *= Dr[i];
-      }
-      if (q == oq) {
-        xr[oi] = vr;
-        if (CP) xi[oi] = vi;
-      }
-      // update row > i (lower) / row < i (upper): the staged column holds
-      // zeros outside the triangle, but the predicate keeps final rows
-      // untouched even when v is not finite
-      const double2* colr = reinterpret_cast<const double2*>(Tr + i * COL + q * GS);
-      const double2* coli = reinterpret_cast<const double2*>(Ti + i * COL + q * GS);
-#pragma unroll
-      for (int h = 0; h < RPL / 2; ++h) {
-        const double2 tr = colr[h];
-        double2 ti = make_double2(0.0, 0.0);
-        if (CP) ti = coli[h];
-#pragma unroll
-        for (int u = 0; u < 2; ++u) {
-          const int r = 2 * h + u;
-          const int row = q * RPL + r;
-          const double a = u ? tr.y : tr.x;
-          if (LOWER ? row > i : row < i) {
-            if (CP) {
-              const double b = u ? ti.y : ti.x;
-              xr[r] -= a * vr - b * vi;
-              xi[r] -= a * vi + b * vr;
-            } else {
-              xr[r] -= a * vr;
-            }
-          }
-        }
-      }
-    }
-    }
-#pragma unroll
-    for (int r = 0; r < RPL; ++r) {
-      const int row = q * RPL + r;
-      if (row < n && c < nrhs) {
-        const size_t idx = (size_t)row + (size_t)c * t.ldc;
-        if (CP) {
-          B[2 * idx] = xr[r];
-          B[2 * idx + 1] = xi[r];
-        } else {
-          B[idx] = xr[r];
-        }
-      }
-    }
-  }
-}
-
-// not inlined: its register allocation stays apart from the gemm tile's
 template <class T>
 __device__ __noinline__ void trsm_tile(const Task& t, uint8_t* smem, double ar, double ai) {
-  using Sh = TrsmShape<T>;
-  constexpr bool CP = St<T>::CPLX;
   using S = typename St<T>::S;
-  double* Tr = reinterpret_cast<double*>(smem);
-  double* Ti = Tr + kLeafS * Sh::COL;
-  double* Dr = Ti + (CP ? kLeafS * Sh::COL : 0);
-  double* Di = Dr + kLeafS;
-  const int n = t.M;
+  double* sm = reinterpret_cast<double*>(smem);
   const bool swap = t.flags & kFlagSwap, conj = t.flags & kFlagConj;
   const bool lower = t.flags & kFlagLower, unit = t.flags & kFlagUnit;
-  const S* A = static_cast<const S*>(t.D);
-  // stage op(T): column j, row i at j * COL + (i / RPL) * GS + i % RPL; zero
-  // outside the triangle, on the diagonal and beyond n.  Element e maps to
-  // (a0, a1) = (e % 64, e / 64) at A[a0 + a1 * lda], so consecutive threads
-  // read consecutive addresses whether op(T) is A's triangle or its
-  // transpose; all loads are issued before the first shared store.
-  constexpr int PER = kLeafS * kLeafS / kThreads;
-  double vr[PER], vi[PER];
-#pragma unroll
-  for (int k = 0; k < PER; ++k) {
-    const int e = threadIdx.x + k * kThreads;
-    const int a0 = e & (kLeafS - 1), a1 = e / kLeafS;
-    const int i = swap ? a1 : a0, j = swap ? a0 : a1;
-    vr[k] = vi[k] = 0.0;
-    if (i < n && j < n && (lower ? (j < i) : (j > i))) {
-      const size_t idx = (size_t)a0 + (size_t)a1 * t.lda;
-      if (CP) {
-        vr[k] = __ldcg(A + 2 * idx);
-        vi[k] = __ldcg(A + 2 * idx + 1);
-      } else {
-        vr[k] = __ldcg(A + idx);
-      }
-    }
-  }
-#pragma unroll
-  for (int k = 0; k < PER; ++k) {
-    const int e = threadIdx.x + k * kThreads;
-    const int a0 = e & (kLeafS - 1), a1 = e / kLeafS;
-    const int i = swap ? a1 : a0, j = swap ? a0 : a1;
-    const int o = j * Sh::COL + (i / Sh::RPL) * Sh::GS + (i % Sh::RPL);
-    Tr[o] = vr[k];
-    if (CP) Ti[o] = conj ? -vi[k] : vi[k];
-  }
-  // reciprocal diagonal; 1 beyond n (those rows hold zeros)
-  for (int i = threadIdx.x; i < kLeafS; i += kThreads) {
-    double dr = 1.0, di = 0.0;
-    if (i < n && !unit) {
-      const size_t idx = (size_t)i + (size_t)i * t.lda;
-      if (CP) {
-        dr = __ldcg(A + 2 * idx);
-        di = __ldcg(A + 2 * idx + 1);
-        if (conj) di = -di;
-      } else {
-        dr = __ldcg(A + idx);
-      }
-    }
-    if (CP) {
-      const double den = dr * dr + di * di;
-      Dr[i] = dr / den;
-      Di[i] = -di / den;
-    } else {
-      Dr[i] = 1.0 / dr;
-    }
-  }
-  __syncthreads();
-  if (lower) trsm_solve<T, true>(t, Tr, Ti, Dr, Di, ar, ai);
-  else trsm_solve<T, false>(t, Tr, Ti, Dr, Di, ar, ai);
+  leaf_stage<T, kThreads>(static_cast<const S*>(t.D), t.lda, t.M, swap, conj, lower, unit, sm);
+  S* X = static_cast<S*>(t.C);
+  if (lower) leaf_solve<T, kThreads, true>(X, t.ldc, false, t.M, 0, t.N, ar, ai, sm);
+  else leaf_solve<T, kThreads, false>(X, t.ldc, false, t.M, 0, t.N, ar, ai, sm);
   __syncthreads();
 }
 

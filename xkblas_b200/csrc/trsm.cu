@@ -9,11 +9,13 @@
 // two (split points multiple of 64), the leading half is solved, the coupling
 // block is applied to the trailing half as one GEMM (DMMA, or Ozaki when
 // requested and large), and the trailing half is solved.  Leaves of <= 64
-// unknowns are solved in FP64 by k_trsm_diag: one warp per right-hand side,
-// lane r holding unknowns r and r+32, the 64x64 triangle in shared memory.
+// unknowns are solved in FP64 by k_trsm_leaf (trsm_leaf.cuh): each
+// right-hand side held in the registers of a few lanes, the 64x64 triangle in
+// shared memory, about two CTAs per SM.
 // This keeps every flop except O(n * 64 * nrhs) inside large GEMMs.
 #include <algorithm>
 
+#include "trsm_leaf.cuh"
 #include "xkb_dev.cuh"
 
 namespace xkb {
@@ -67,98 +69,25 @@ __device__ __forceinline__ void stv(T* p, size_t i, double re, double im) {
   }
 }
 
-// Solve T x = alpha b for nrhs right-hand sides, T (n x n, n <= 64) the
-// effective triangle: T(i,j) = A[swap ? j + i*lda : i + j*lda] (conjugated
-// when conj), lower when `lower`.  RHS c, unknown i lives at
-// B[rhs_rows ? c + i*ldb : i + c*ldb] (rhs_rows: the right-side form).
-template <class T>
-__global__ void __launch_bounds__(256) k_trsm_diag(int n, int nrhs, const T* A, long lda,
-                                                    int swap, int conj, int lower, int unit,
-                                                    T* B, long ldb, int rhs_rows, double alr,
-                                                    double ali) {
-  constexpr bool CP = TT<T>::C;
-  extern __shared__ double smd[];
-  double (*Tr)[kLeaf + 1] = reinterpret_cast<double (*)[kLeaf + 1]>(smd);
-  double (*Ti)[kLeaf + 1] = reinterpret_cast<double (*)[kLeaf + 1]>(smd + kLeaf * (kLeaf + 1));
-  for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
-    const int i = e % n, j = e / n;
-    double re = 0, im = 0;
-    const bool in = lower ? (j <= i) : (j >= i);
-    if (in) {
-      const size_t idx = swap ? (size_t)j + (size_t)i * lda : (size_t)i + (size_t)j * lda;
-      ldv<T>(A, idx, re, im);
-      if (conj) im = -im;
-      if (i == j && unit) {
-        re = 1.0;
-        im = 0.0;
-      }
-    }
-    Tr[i][j] = re;
-    if constexpr (CP) Ti[i][j] = im;
-  }
-  __syncthreads();
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int nwarps = blockDim.x >> 5;
-  for (int c = blockIdx.x * nwarps + warp; c < nrhs; c += gridDim.x * nwarps) {
-    double xr[2], xi[2];
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const int r = lane + 32 * h;
-      xr[h] = xi[h] = 0.0;
-      if (r < n) {
-        const size_t idx = rhs_rows ? (size_t)c + (size_t)r * ldb : (size_t)r + (size_t)c * ldb;
-        double br, bi;
-        ldv<T>(B, idx, br, bi);
-        xr[h] = alr * br - ali * bi;
-        xi[h] = CP ? (alr * bi + ali * br) : 0.0;
-      }
-    }
-    for (int s = 0; s < n; ++s) {
-      const int i = lower ? s : n - 1 - s;
-      const int h = i >> 5, src = i & 31;
-      double vr = __shfl_sync(0xffffffffu, h ? xr[1] : xr[0], src);
-      double vi = CP ? __shfl_sync(0xffffffffu, h ? xi[1] : xi[0], src) : 0.0;
-      // x_i /= T(i,i)
-      const double dr = Tr[i][i], di = CP ? Ti[i][i] : 0.0;
-      if constexpr (CP) {
-        const double den = dr * dr + di * di;
-        const double qr = (vr * dr + vi * di) / den, qi = (vi * dr - vr * di) / den;
-        vr = qr;
-        vi = qi;
-      } else {
-        vr = vr / dr;
-      }
-#pragma unroll
-      for (int hh = 0; hh < 2; ++hh) {
-        const int r = lane + 32 * hh;
-        if (r == i) {
-          xr[hh] = vr;
-          xi[hh] = vi;
-        } else if (r < n && (lower ? r > i : r < i)) {
-          const double tr = Tr[r][i];
-          if constexpr (CP) {
-            const double ti = Ti[r][i];
-            xr[hh] -= tr * vr - ti * vi;
-            xi[hh] -= tr * vi + ti * vr;
-          } else {
-            xr[hh] -= tr * vr;
-          }
-        }
-      }
-    }
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const int r = lane + 32 * h;
-      if (r < n) {
-        const size_t idx = rhs_rows ? (size_t)c + (size_t)r * ldb : (size_t)r + (size_t)c * ldb;
-        stv<T>(B, idx, xr[h], xi[h]);
-      }
-    }
-  }
+// Leaf solve: T x = alpha b for the right-hand sides of this CTA's column
+// range, T (n x n, n <= 64) the effective triangle: T(i,j) = A[swap ? j + i*lda
+// : i + j*lda] (conjugated when conj), lower when LOWER.  RHS c, unknown i
+// lives at B[rhs_rows ? c + i*ldb : i + c*ldb] (rhs_rows: the right-side
+// form).  Body: trsm_leaf.cuh (register-resident substitution).
+constexpr int kLeafThreads = 128;
+
+template <class T, bool LOWER>
+__global__ void __launch_bounds__(kLeafThreads)
+    k_trsm_leaf(int n, int nrhs, int cols_per_cta, const typename St<T>::S* A, long lda, int swap,
+                int conj, int unit, typename St<T>::S* B, long ldb, int rhs_rows, double ar,
+                double ai) {
+  extern __shared__ double sm_leaf[];
+  leaf_stage<T, kLeafThreads>(A, lda, n, swap != 0, conj != 0, LOWER, unit != 0, sm_leaf);
+  const int c0 = blockIdx.x * cols_per_cta;
+  const int c1 = min(nrhs, c0 + cols_per_cta);
+  leaf_solve<T, kLeafThreads, LOWER>(B, ldb, rhs_rows != 0, n, c0, c1, ar, ai, sm_leaf);
 }
 
-// out = the stored uplo triangle of A (other triangle 0, unit diagonal if
-// unit).  n x n, column major.
 template <class T>
 __global__ void k_tri_fill(int n, const T* A, long lda, int lower, int unit, T* O, long ldo) {
   const size_t total = (size_t)n * n;
@@ -222,19 +151,25 @@ template <class T>
 static int launch_diag(int n, int nrhs, const void* A, long lda, int swap, int conj, int lower,
                        int unit, void* B, long ldb, int rhs_rows, const double* al,
                        cudaStream_t st) {
-  const int warps = 8;
-  const long need = (nrhs + warps - 1) / warps;
-  const unsigned grid = (unsigned)std::max<long>(1, std::min<long>(need, 8L * sm_count()));
-  const size_t smem = (TT<T>::C ? 2 : 1) * sizeof(double) * kLeaf * (kLeaf + 1);
-  static bool attr = false;
-  if (!attr) {
-    if (cudaFuncSetAttribute(k_trsm_diag<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem) != cudaSuccess)
+  using S = typename St<T>::S;
+  constexpr int cpp = kLeafThreads / LeafShape<T>::G;  // right-hand sides per pass
+  // about two CTAs per SM; each stages the block once for all its passes
+  const long want = 2L * sm_count();
+  long per = ((long)nrhs + want - 1) / want;
+  per = std::max<long>(cpp, (per + cpp - 1) / cpp * cpp);
+  const unsigned grid = (unsigned)std::max<long>(1, ((long)nrhs + per - 1) / per);
+  const size_t smem = LeafShape<T>::SMEM;
+  auto kl = lower ? k_trsm_leaf<T, true> : k_trsm_leaf<T, false>;
+  static bool attr[2] = {false, false};
+  if (!attr[lower ? 1 : 0]) {
+    if (cudaFuncSetAttribute(kl, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+        cudaSuccess)
       return XKB_ECUDA;
-    attr = true;
+    attr[lower ? 1 : 0] = true;
   }
-  k_trsm_diag<T><<<grid, warps * 32, smem, st>>>(n, nrhs, (const T*)A, lda, swap, conj, lower, unit,
-                                              (T*)B, ldb, rhs_rows, al[0], al[1]);
+  kl<<<grid, kLeafThreads, smem, st>>>(n, nrhs, (int)per, static_cast<const S*>(A), lda, swap,
+                                       conj, unit, static_cast<S*>(B), ldb, rhs_rows, al[0],
+                                       al[1]);
   count_launch();
   return cudaPeekAtLastError() == cudaSuccess ? XKB_OK : XKB_ECUDA;
 }
