@@ -568,11 +568,8 @@ def main():
     os.environ["XKBLAS_GPUSET"] = str(local)
     import torch
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    from xkblas_b200.replicas import Replicas
+    reps = Replicas(backend="nccl", timeout_s=300)  # one independent problem per GPU
 
     import xkblas_b200 as X
     lib = X.lib()
@@ -607,16 +604,9 @@ def main():
     torch.cuda.synchronize()
 
     def barrier():
-        torch.cuda.synchronize()
-        if dist:
-            dist.barrier()
+        reps.barrier(torch.cuda.synchronize)
 
-    def maxreduce(v):
-        if not dist:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    maxreduce = reps.max
 
     # ---- device-resident Ozaki steps --------------------------------------
     k0 = lib.xkb_cuda_kernel_count()
@@ -770,9 +760,7 @@ def main():
         line["cpu_baseline"] = cpu_baseline()
     if rank == 0:
         print(json.dumps(line), flush=True)
-    if dist:
-        dist.barrier()
-        dist.destroy_process_group()
+    reps.close()
 
 
 if __name__ == "__main__":
