@@ -188,16 +188,40 @@ Desc* get_desc(const void* host, size_t M, size_t N, size_t ld, size_t esz, size
   return d;
 }
 
-// H2D of rows [r0,r1) x cols [c0,c1) of the host view.
+// Host <-> device copies of rows [r0,r1) x cols [c0,c1).  The device copy
+// has a padded leading dimension; when the host block is contiguous (whole
+// columns of a matrix with ld == M) and its columns are short, the transfer
+// crosses the host link as one contiguous copy through a stream-ordered
+// staging buffer and is re-pitched on the device: pitched copies of short
+// rows move far below the link's bandwidth.
+constexpr size_t kStagedMaxRowBytes = 32768;
+
+static bool staged(const Desc* d, size_t r0, size_t r1) {
+  return r0 == 0 && r1 == d->M && d->ld == d->M && d->dld != d->ld &&
+         d->M * d->esz <= kStagedMaxRowBytes;
+}
+
 static int copy_h2d(Desc* d, size_t r0, size_t r1, size_t c0, size_t c1) {
   Runtime& R = rt();
   if (r1 <= r0 || c1 <= c0) return XKB_OK;
   const char* src = static_cast<const char*>(d->host) + (r0 + c0 * d->ld) * d->esz;
   char* dst = static_cast<char*>(dev_ptr(d, r0, c0));
   const size_t w = (r1 - r0) * d->esz;
+  R.stats.h2d += w * (c1 - c0);
+  if (staged(d, r0, r1)) {
+    void* tmp = nullptr;
+    if (cudaMallocAsync(&tmp, w * (c1 - c0), R.s_h2d) == cudaSuccess) {
+      cudaError_t e = cudaMemcpyAsync(tmp, src, w * (c1 - c0), cudaMemcpyHostToDevice, R.s_h2d);
+      if (e == cudaSuccess)
+        e = cudaMemcpy2DAsync(dst, d->dld * d->esz, tmp, w, w, c1 - c0,
+                              cudaMemcpyDeviceToDevice, R.s_h2d);
+      cudaFreeAsync(tmp, R.s_h2d);
+      return cuda_ok(e);
+    }
+    cudaGetLastError();  // no staging memory: pitched copy below
+  }
   cudaError_t e = cudaMemcpy2DAsync(dst, d->dld * d->esz, src, d->ld * d->esz, w, c1 - c0,
                                     cudaMemcpyHostToDevice, R.s_h2d);
-  R.stats.h2d += w * (c1 - c0);
   return cuda_ok(e);
 }
 
@@ -207,9 +231,21 @@ static int copy_d2h(Desc* d, size_t r0, size_t r1, size_t c0, size_t c1) {
   char* dst = static_cast<char*>(d->host) + (r0 + c0 * d->ld) * d->esz;
   const char* src = static_cast<const char*>(dev_ptr(d, r0, c0));
   const size_t w = (r1 - r0) * d->esz;
+  R.stats.d2h += w * (c1 - c0);
+  if (staged(d, r0, r1)) {
+    void* tmp = nullptr;
+    if (cudaMallocAsync(&tmp, w * (c1 - c0), R.s_d2h) == cudaSuccess) {
+      cudaError_t e = cudaMemcpy2DAsync(tmp, w, src, d->dld * d->esz, w, c1 - c0,
+                                        cudaMemcpyDeviceToDevice, R.s_d2h);
+      if (e == cudaSuccess)
+        e = cudaMemcpyAsync(dst, tmp, w * (c1 - c0), cudaMemcpyDeviceToHost, R.s_d2h);
+      cudaFreeAsync(tmp, R.s_d2h);
+      return cuda_ok(e);
+    }
+    cudaGetLastError();
+  }
   cudaError_t e = cudaMemcpy2DAsync(dst, d->ld * d->esz, src, d->dld * d->esz, w, c1 - c0,
                                     cudaMemcpyDeviceToHost, R.s_d2h);
-  R.stats.d2h += w * (c1 - c0);
   return cuda_ok(e);
 }
 
