@@ -8,6 +8,7 @@ import pytest
 
 import oracle as O
 from tests import checks
+from xkblas_b200 import GemmArgs  # xkb_gemm_args of include/xkb_cuda.h
 
 pytestmark = pytest.mark.gpu
 
@@ -122,16 +123,6 @@ def test_ozaki_trsm_updates(tc):
     tc.invalidate_caches()
     R = O.trsm(LEFT, LO, N_, NONUNIT, 2.0, A, B0.copy(order="F"), nb=128)
     assert checks.trsm_ratio(B, R, A, M, N) <= 10
-
-
-class GemmArgs(ctypes.Structure):
-    _fields_ = [("dtype", ctypes.c_int), ("opA", ctypes.c_int), ("opB", ctypes.c_int),
-                ("M", ctypes.c_int), ("N", ctypes.c_int), ("K", ctypes.c_int),
-                ("A", ctypes.c_void_p), ("lda", ctypes.c_long),
-                ("B", ctypes.c_void_p), ("ldb", ctypes.c_long),
-                ("C", ctypes.c_void_p), ("ldc", ctypes.c_long),
-                ("alpha", ctypes.c_double * 2), ("beta", ctypes.c_double * 2),
-                ("uplo", ctypes.c_int), ("herm_diag", ctypes.c_int), ("diag", ctypes.c_long)]
 
 
 def test_ozaki_moduli_count_controls_accuracy(xk):

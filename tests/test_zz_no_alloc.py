@@ -10,18 +10,9 @@ import numpy as np
 import pytest
 
 import oracle as O
+from xkblas_b200 import GemmArgs  # xkb_gemm_args of include/xkb_cuda.h
 
 pytestmark = pytest.mark.gpu
-
-
-class GemmArgs(ctypes.Structure):
-    _fields_ = [("dtype", ctypes.c_int), ("opA", ctypes.c_int), ("opB", ctypes.c_int),
-                ("M", ctypes.c_int), ("N", ctypes.c_int), ("K", ctypes.c_int),
-                ("A", ctypes.c_void_p), ("lda", ctypes.c_long),
-                ("B", ctypes.c_void_p), ("ldb", ctypes.c_long),
-                ("C", ctypes.c_void_p), ("ldc", ctypes.c_long),
-                ("alpha", ctypes.c_double * 2), ("beta", ctypes.c_double * 2),
-                ("uplo", ctypes.c_int), ("herm_diag", ctypes.c_int), ("diag", ctypes.c_long)]
 
 
 def _dev(X):

@@ -31,6 +31,17 @@ _REAL = {"s": np.float32, "d": np.float64, "c": np.float32, "z": np.float64}
 _lib = None
 
 
+class GemmArgs(ctypes.Structure):
+    """xkb_gemm_args of include/xkb_cuda.h."""
+    _fields_ = [("dtype", ctypes.c_int), ("opA", ctypes.c_int), ("opB", ctypes.c_int),
+                ("M", ctypes.c_int), ("N", ctypes.c_int), ("K", ctypes.c_int),
+                ("A", ctypes.c_void_p), ("lda", ctypes.c_long),
+                ("B", ctypes.c_void_p), ("ldb", ctypes.c_long),
+                ("C", ctypes.c_void_p), ("ldc", ctypes.c_long),
+                ("alpha", ctypes.c_double * 2), ("beta", ctypes.c_double * 2),
+                ("uplo", ctypes.c_int), ("herm_diag", ctypes.c_int), ("diag", ctypes.c_long)]
+
+
 class BatchOp(ctypes.Structure):
     """xkb_batch_op of include/xkb_cuda.h."""
     _fields_ = [("kind", ctypes.c_int), ("dtype", ctypes.c_int), ("opA", ctypes.c_int),

@@ -29,14 +29,7 @@ import sys
 import numpy as np
 
 
-class _GemmArgs(ctypes.Structure):
-    _fields_ = [("dtype", ctypes.c_int), ("opA", ctypes.c_int), ("opB", ctypes.c_int),
-                ("M", ctypes.c_int), ("N", ctypes.c_int), ("K", ctypes.c_int),
-                ("A", ctypes.c_void_p), ("lda", ctypes.c_long),
-                ("B", ctypes.c_void_p), ("ldb", ctypes.c_long),
-                ("C", ctypes.c_void_p), ("ldc", ctypes.c_long),
-                ("alpha", ctypes.c_double * 2), ("beta", ctypes.c_double * 2),
-                ("uplo", ctypes.c_int), ("herm_diag", ctypes.c_int), ("diag", ctypes.c_long)]
+from xkblas_b200 import GemmArgs as _GemmArgs  # xkb_gemm_args
 
 
 def choose_moduli(lib, K, M=1024, N=1024, stream=None, gen=None):

@@ -354,6 +354,7 @@ constexpr int kEpiWarps = 4;
 
 struct GemmP {
   int tiles_m, tiles_n, kblocks, nmod;
+  int group;  // raster: M tiles per group (tiles in flight share A / B panels in L2)
   uint8_t* R;
   long Mpad, Npad;
   int uplo;
@@ -407,7 +408,7 @@ __device__ __forceinline__ bool oz_tile(const GemmP& p, int t, int& mod, int& m0
   const int tiles_mn = p.tiles_m * p.tiles_n;
   mod = t / tiles_mn;
   const int r = t - mod * tiles_mn;
-  const int GROUP = 8;
+  const int GROUP = p.group;
   const int span = GROUP * p.tiles_n;
   const int first_m = (r / span) * GROUP;
   const int gsz = min(p.tiles_m - first_m, GROUP);
@@ -830,6 +831,8 @@ static int launch_gemm(const int8_t* Ap, long a_rows, const int8_t* Bp, long b_r
   p.tiles_n = (int)(Npad / BN);
   p.kblocks = (int)(Kpad / BKB);
   p.nmod = c->nmod;
+  // raster group (tuning table oz_group_m, default 8 M tiles)
+  p.group = std::max(1, std::min(p.tiles_m, (int)tune("oz_group_m", 8.0)));
   p.R = R;
   p.Mpad = Mpad;
   p.Npad = Npad;
