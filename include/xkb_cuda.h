@@ -180,6 +180,8 @@ int xkb_cuda_batch_release(void);
  *   batch_schedule          executor claim order, 0 solves first / 1 gemms (0)
  *   batch_tile128_min_rows  executor: real gemm calls this tall use 128-row
  *                           tiles (96)
+ *   oz_group_m              Ozaki INT8 GEMM raster: M tiles per group of the
+ *                           persistent tile walk (8)
  * xkb_tune_load returns the number of entries read or XKB_EINVAL. */
 int xkb_tune_set(const char* key, double value);
 double xkb_tune_get(const char* key, double dflt);
