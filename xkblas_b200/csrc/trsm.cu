@@ -75,6 +75,7 @@ __device__ __forceinline__ void stv(T* p, size_t i, double re, double im) {
 // lives at B[rhs_rows ? c + i*ldb : i + c*ldb] (rhs_rows: the right-side
 // form).  Body: trsm_leaf.cuh (register-resident substitution).
 constexpr int kLeafThreads = 128;
+constexpr int kLeafRplReal = 8;  // many right-hand sides: more lanes per column
 
 template <class T, bool LOWER>
 __global__ void __launch_bounds__(kLeafThreads)
@@ -82,10 +83,12 @@ __global__ void __launch_bounds__(kLeafThreads)
                 int conj, int unit, typename St<T>::S* B, long ldb, int rhs_rows, double ar,
                 double ai) {
   extern __shared__ double sm_leaf[];
-  leaf_stage<T, kLeafThreads>(A, lda, n, swap != 0, conj != 0, LOWER, unit != 0, sm_leaf);
+  leaf_stage<T, kLeafThreads, kLeafRplReal>(A, lda, n, swap != 0, conj != 0, LOWER, unit != 0,
+                                            sm_leaf);
   const int c0 = blockIdx.x * cols_per_cta;
   const int c1 = min(nrhs, c0 + cols_per_cta);
-  leaf_solve<T, kLeafThreads, LOWER>(B, ldb, rhs_rows != 0, n, c0, c1, ar, ai, sm_leaf);
+  leaf_solve<T, kLeafThreads, LOWER, kLeafRplReal>(B, ldb, rhs_rows != 0, n, c0, c1, ar, ai,
+                                                   sm_leaf);
 }
 
 template <class T>
@@ -152,13 +155,13 @@ static int launch_diag(int n, int nrhs, const void* A, long lda, int swap, int c
                        int unit, void* B, long ldb, int rhs_rows, const double* al,
                        cudaStream_t st) {
   using S = typename St<T>::S;
-  constexpr int cpp = kLeafThreads / LeafShape<T>::G;  // right-hand sides per pass
+  constexpr int cpp = kLeafThreads / LeafShape<T, kLeafRplReal>::G;  // right-hand sides per pass
   // about two CTAs per SM; each stages the block once for all its passes
   const long want = 2L * sm_count();
   long per = ((long)nrhs + want - 1) / want;
   per = std::max<long>(cpp, (per + cpp - 1) / cpp * cpp);
   const unsigned grid = (unsigned)std::max<long>(1, ((long)nrhs + per - 1) / per);
-  const size_t smem = LeafShape<T>::SMEM;
+  const size_t smem = LeafShape<T, kLeafRplReal>::SMEM;
   auto kl = lower ? k_trsm_leaf<T, true> : k_trsm_leaf<T, false>;
   static bool attr[2] = {false, false};
   if (!attr[lower ? 1 : 0]) {

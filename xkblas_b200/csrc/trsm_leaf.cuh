@@ -5,8 +5,9 @@
 // (blas/ztask_trsm.c:162-180).
 //
 // X = alpha op(T)^-1 B by substitution.  A right-hand side is held by G lanes
-// of one warp, lane g keeping rows RPL*g .. RPL*g + RPL-1 in registers (real:
-// RPL 16, G 4; complex: RPL 8, G 8).  At step i the owner of row i scales it
+// of one warp, lane g keeping rows RPL*g .. RPL*g + RPL-1 in registers (the
+// executor: real RPL 16, G 4, complex RPL 8, G 8; the recursive solver, with
+// thousands of right-hand sides: real 8 / 8, complex 4 / 16).  At step i the owner of row i scales it
 // by the reciprocal of T(i,i) (the packed-reciprocal form CPU BLAS kernels
 // use), the G lanes share it by shuffle, and each lane updates its rows below
 // (lower) or above (upper) i.  op(T) is staged column by column in shared
@@ -20,10 +21,14 @@ namespace xkb {
 
 constexpr int kLeafRows = 64;
 
-template <class T>
+// RPL_REAL: rows per lane for real types (complex: half of it).  Fewer rows
+// per lane mean more lanes per right-hand side: more warps to hide the
+// per-step shuffle latency when right-hand sides are many, more shuffles per
+// step when they are few.
+template <class T, int RPL_REAL = 16>
 struct LeafShape {
   static constexpr bool CPLX = St<T>::CPLX;
-  static constexpr int RPL = CPLX ? 8 : 16;     // rows per lane
+  static constexpr int RPL = CPLX ? RPL_REAL / 2 : RPL_REAL;  // rows per lane
   static constexpr int G = kLeafRows / RPL;     // lanes per right-hand side
   static constexpr int GS = RPL + 2;            // staged row-group stride
   static constexpr int COL = G * GS;            // staged column stride
@@ -41,10 +46,10 @@ __device__ __forceinline__ size_t leaf_at(int i, int c, long ldb, bool rhs_rows)
 // (conjugated when conj), zero outside the (lower / upper) triangle, on the
 // diagonal and beyond n; reciprocal diagonal (1 for unit and beyond n).
 // Ends with __syncthreads.
-template <class T, int NT>
+template <class T, int NT, int RPL_REAL = 16>
 __device__ __forceinline__ void leaf_stage(const typename St<T>::S* A, long lda, int n, bool swap,
                                            bool conj, bool lower, bool unit, double* sm) {
-  using Sh = LeafShape<T>;
+  using Sh = LeafShape<T, RPL_REAL>;
   constexpr bool CP = Sh::CPLX;
   double* Tr = sm;
   double* Ti = Tr + kLeafRows * Sh::COL;
@@ -110,11 +115,11 @@ __device__ __forceinline__ void leaf_stage(const typename St<T>::S* A, long lda,
 
 // Solve right-hand sides c0 .. c1-1 in place (alpha applied on load).  All
 // NT threads take part (every warp runs the same number of passes).
-template <class T, int NT, bool LOWER>
+template <class T, int NT, bool LOWER, int RPL_REAL = 16>
 __device__ __forceinline__ void leaf_solve(typename St<T>::S* B, long ldb, bool rhs_rows, int n,
                                            int c0, int c1, double ar, double ai,
                                            const double* sm) {
-  using Sh = LeafShape<T>;
+  using Sh = LeafShape<T, RPL_REAL>;
   constexpr int RPL = Sh::RPL, G = Sh::G, GS = Sh::GS, COL = Sh::COL;
   constexpr int CPP = NT / G;  // right-hand sides per pass
   constexpr bool CP = Sh::CPLX;
