@@ -250,6 +250,21 @@ def other_configs(lib, torch, dev, sp, stream):
         out[name] = {"plain_tflops": fl / tp / 1e9, "ozaki_tflops": fl / to / 1e9,
                      "plain_ms": tp, "ozaki_ms": to}
         del A, C, C0
+    # Cholesky (a next-row driver on the same kernels): DPOTRF lower 8192,
+    # A = B B^T / n + I; flops n^3/3 + n^2/2 + n/6 (reference flops.h)
+    n = 8192
+    Bm = u(n, n)
+    A0 = Bm @ Bm.t() / n + torch.eye(n, device=dev, dtype=torch.float64)
+    A = A0.clone()
+    info = torch.zeros(1, dtype=torch.int32, device=dev)
+    with torch.cuda.stream(stream):
+        rs = lambda: A.copy_(A0)
+        tp = timed(lambda: lib.xkb_cuda_potrf(1, 1, n, ctypes.c_void_p(A.data_ptr()), n,
+                                              ctypes.c_void_p(info.data_ptr()), sp), 3, rs)
+    fl = n ** 3 / 3.0 + n * n / 2.0 + n / 6.0
+    out["dpotrf_l_8192"] = {"plain_tflops": fl / tp / 1e9, "plain_ms": tp,
+                            "info": int(info.item())}
+    del Bm, A0, A, info
     torch.cuda.empty_cache()
     return out
 

@@ -188,6 +188,13 @@ double xkb_tune_get(const char* key, double dflt);
 int xkb_tune_load(const char* path);
 int xkb_tune_clear(void);
 
+/* Cholesky factorization in place: A = L L^H (XKB_LOWER) or U^H U
+ * (XKB_UPPER), s/d/c/z, only the stored triangle read and written
+ * (replaces the reference's tile driver blas/zpotrf.c:46-220).  d_info: a
+ * device int (may be NULL) that receives the first column, 1-based, whose
+ * pivot is not positive; it is not cleared here. */
+int xkb_cuda_potrf(int dtype, int uplo, int N, void* A, long lda, int* d_info, void* stream);
+
 /* Device error word written by bounded waits (0 = none); clears it. */
 int xkb_cuda_take_device_error(void);
 

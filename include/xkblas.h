@@ -236,6 +236,20 @@ XKBLAS_DECL_OPS(z, Complex64_t, double)
 XKBLAS_DECL_HE_OPS(c, Complex32_t, float)
 XKBLAS_DECL_HE_OPS(z, Complex64_t, double)
 
+/* ---- Cholesky factorization (reference blas/zpotrf.c:46, a tile driver
+ * outside the reference's public headers): A = L L^H (CblasLower) or U^H U
+ * (CblasUpper) in place on the host-resident matrix, asynchronous like the
+ * level-3 calls (memory_coherent_async + sync make A final on the host).
+ * Returns -2 (uplo), -5 (N), -8 (LDA) as the reference does.
+ * xkblas_potrf_info: after the factorization, the first column (1-based)
+ * whose pivot was not positive, 0 if A was positive definite (waits for the
+ * device). ------------------------------------------------------------- */
+int xkblas_spotrf_async(int uplo, int N, float* A, int LDA);
+int xkblas_dpotrf_async(int uplo, int N, double* A, int LDA);
+int xkblas_cpotrf_async(int uplo, int N, Complex32_t* A, int LDA);
+int xkblas_zpotrf_async(int uplo, int N, Complex64_t* A, int LDA);
+int xkblas_potrf_info(void);
+
 /* ---- synchronous forms: _async + memory_coherent_async on the output
  * (its written triangle for gemmt/syrk/herk/syr2k/her2k) + xkblas_sync +
  * xkblas_memory_invalidate_caches -- the sequence the reference's F77

@@ -1,0 +1,78 @@
+"""Cholesky factorization through the public API (xkblas_?potrf_async +
+memory_coherent_async on the stored triangle + sync; reference
+blas/zpotrf.c): the factor reproduces A (backward error bound), matches
+LAPACK's factor from numpy on the same matrix, leaves the other triangle of
+the host matrix untouched, and reports the first non-positive pivot of a
+matrix that is not positive definite.  Requires a B200."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+UP, LO = 121, 122
+EPS = {np.float64: 2.0 ** -53, np.complex128: 2.0 ** -53,
+       np.float32: 2.0 ** -24, np.complex64: 2.0 ** -24}
+
+
+def _spd(n, dt, seed):
+    rng = np.random.default_rng(seed)
+    B = rng.standard_normal((n, n))
+    if np.issubdtype(dt, np.complexfloating):
+        B = B + 1j * rng.standard_normal((n, n))
+    A = B @ B.conj().T / n + np.eye(n)
+    return np.asfortranarray(A.astype(dt))
+
+
+def _potrf(xk, A, uplo):
+    p = {np.dtype(np.float32): "s", np.dtype(np.float64): "d",
+         np.dtype(np.complex64): "c", np.dtype(np.complex128): "z"}[A.dtype]
+    lib = xk.lib()
+    r = getattr(lib, "xkblas_%spotrf_async" % p)(uplo, A.shape[0], xk._ptr(A), A.shape[0])
+    assert r == 0
+    xk.coherent(A, uplo)
+    xk.sync()
+    info = lib.xkblas_potrf_info()
+    xk.invalidate_caches()
+    return info
+
+
+@pytest.mark.parametrize("dt", [np.float64, np.complex128, np.float32, np.complex64])
+@pytest.mark.parametrize("uplo", [LO, UP])
+@pytest.mark.parametrize("n", [1, 64, 65, 200, 700])
+def test_potrf_factor(xk, dt, uplo, n):
+    A0 = _spd(n, dt, 10 + n)
+    A = A0.copy(order="F")
+    assert _potrf(xk, A, uplo) == 0
+    up = np.complex128 if np.issubdtype(dt, np.complexfloating) else np.float64
+    if uplo == LO:
+        L = np.tril(A).astype(up)
+        R = L @ L.conj().T
+        other = np.triu(A, 1) == np.triu(A0, 1)
+        ref = np.linalg.cholesky(A0.astype(up))
+        got = L
+    else:
+        U = np.triu(A).astype(up)
+        R = U.conj().T @ U
+        other = np.tril(A, -1) == np.tril(A0, -1)
+        ref = np.linalg.cholesky(A0.astype(up)).conj().T
+        got = U
+    assert other.all()  # the other triangle of the host matrix is untouched
+    scale = np.abs(A0).max() * n * EPS[dt]
+    assert np.abs(R - A0.astype(up)).max() <= 16 * scale
+    assert np.abs(got - ref).max() <= 64 * n * EPS[dt] * max(1.0, np.abs(ref).max())
+
+
+def test_potrf_reports_first_bad_pivot(xk):
+    n = 300
+    A = _spd(n, np.float64, 3)
+    A[150, 150] = -5.0  # leading 150x150 block stays positive definite
+    assert _potrf(xk, A, LO) == 151
+
+
+def test_potrf_argument_codes(xk):
+    lib = xk.lib()
+    A = np.zeros((4, 4), order="F")
+    assert lib.xkblas_dpotrf_async(120, 4, xk._ptr(A), 4) == -2
+    assert lib.xkblas_dpotrf_async(LO, -1, xk._ptr(A), 4) == -5
+    assert lib.xkblas_dpotrf_async(LO, 4, xk._ptr(A), 3) == -8
+    assert lib.xkblas_dpotrf_async(LO, 0, xk._ptr(A), 1) == 0

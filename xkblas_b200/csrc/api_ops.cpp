@@ -491,7 +491,65 @@ int tr_async(int is_trsm, int side, int uplo, int transA, int diag, int M, int N
   return 0;
 }
 
+// Cholesky factorization (reference blas/zpotrf.c:46-220; argument codes
+// :55-67).  Runs after the queued calls, on the stored triangle only.
+template <class T>
+int potrf_async(int uplo, int N, T* A, int LDA) {
+  if (uplo != CblasUpper && uplo != CblasLower) return -2;
+  if (N < 0) return -5;
+  if (LDA < std::max(1, N)) return -8;
+  if (N == 0) return 0;
+  Guard g;
+  if (int e = ensure_init()) return rt_error(e);
+  Runtime& R = rt();
+  R.stats.calls++;
+  {
+    const double n = N;
+    R.stats.flops += (HT<T>::cplx ? 4.0 : 1.0) * (n * n * n / 3.0 + n * n / 2.0 + n / 6.0);
+  }
+  int err;
+  if ((err = flush_pending())) return rt_error(err);
+  const size_t NB = auto_tilesize(KERN_GEMM, N, N, N), es = sizeof(T);
+  Desc* dA = get_desc(A, N, N, LDA, es, NB, &err);
+  if (!dA) return rt_error(err);
+  if ((err = make_valid(dA, 0, N, 0, N))) return rt_error(err);
+  if (!R.d_potrf_info) {
+    if (cudaMalloc(&R.d_potrf_info, sizeof(int)) != cudaSuccess) {
+      R.d_potrf_info = nullptr;
+      return rt_error(XKB_ENOMEM);
+    }
+  }
+  cudaMemsetAsync(R.d_potrf_info, 0, sizeof(int), R.s_comp);
+  err = xkb_cuda_potrf(HT<T>::dt, uplo == CblasLower ? XKB_LOWER : XKB_UPPER, N,
+                       dev_ptr(dA, 0, 0), (long)dA->dld, R.d_potrf_info, R.s_comp);
+  if (err) return rt_error(err);
+  mark_written(dA, 0, N, 0, N, uplo);
+  return 0;
+}
+
 }  // namespace
+
+extern "C" int xkblas_spotrf_async(int uplo, int N, float* A, int LDA) {
+  return potrf_async<float>(uplo, N, A, LDA);
+}
+extern "C" int xkblas_dpotrf_async(int uplo, int N, double* A, int LDA) {
+  return potrf_async<double>(uplo, N, A, LDA);
+}
+extern "C" int xkblas_cpotrf_async(int uplo, int N, Complex32_t* A, int LDA) {
+  return potrf_async<Complex32_t>(uplo, N, A, LDA);
+}
+extern "C" int xkblas_zpotrf_async(int uplo, int N, Complex64_t* A, int LDA) {
+  return potrf_async<Complex64_t>(uplo, N, A, LDA);
+}
+extern "C" int xkblas_potrf_info(void) {
+  Runtime& R = rt();
+  std::lock_guard<std::recursive_mutex> g(R.mu);
+  if (!R.ready || !R.d_potrf_info) return 0;
+  int v = 0;
+  cudaStreamSynchronize(R.s_comp);
+  if (cudaMemcpy(&v, R.d_potrf_info, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return 0;
+  return v;
+}
 
 // ============================================================================
 // exported symbols

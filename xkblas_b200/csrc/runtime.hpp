@@ -73,6 +73,7 @@ struct Runtime {
   std::vector<xkb_batch_op> pending;
   std::vector<Desc*> pend_descs;  // buffers the queued calls touch (Desc::pend set)
   uint64_t batches = 0, batched_calls = 0;
+  int* d_potrf_info = nullptr;  // device word for the last factorization
 };
 
 Runtime& rt();
