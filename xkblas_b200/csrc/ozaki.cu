@@ -559,7 +559,9 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
           if (r < 0) r += pm;
           else if (r >= pm) r -= pm;
           const size_t col = (size_t)(n0 + c * 16 + e);
-          plane[col * (size_t)p.Mpad + (size_t)row] = (uint8_t)r;
+          // streaming store: the residue planes are read once, by the CRT
+          // kernel; they should not evict the operand panels from L2
+          __stcs(plane + col * (size_t)p.Mpad + (size_t)row, (unsigned char)r);
         }
       }
       ++tl;
