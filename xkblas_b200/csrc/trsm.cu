@@ -300,7 +300,7 @@ extern "C" int xkb_cuda_trsm(int dtype, int side, int uplo, int trans, int diag,
   c.st = resolve_stream(stream);
   const bool lower = uplo == XKB_LOWER;
   const bool op_lower = lower ^ (c.trans != XKB_OP_N);  // op(A) lower?
-  // effective triangle element access, see k_trsm_diag
+  // effective triangle element access, as in k_trsm_leaf
   if (c.left) {
     c.swap = c.trans != XKB_OP_N;
     c.conj = c.trans == XKB_OP_C;

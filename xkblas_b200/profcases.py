@@ -1,11 +1,12 @@
 """Small, self-contained cases for profiling single kernels with ncu:
 
-    python -m xkblas_b200.profcases dmma|ozaki|repack|trsm|batch
+    python -m xkblas_b200.profcases dmma|ozaki|repack|trsm|potrf|batch
 
 dmma    DGEMM NN 4096^3 through xkb_cuda_gemm (k_gemm_dmma), two calls
 ozaki   the same through xkb_cuda_ozaki_gemm, 16 moduli (k_oz_* kernels)
 repack  the DGEMM with lda = ldb = 4097 (k_repack, then k_gemm_dmma)
-trsm    DTRSM L/L/N/N 4096 x 4096, diagonally dominant (k_trsm_diag, GEMMs)
+trsm    DTRSM L/L/N/N 4096 x 4096, diagonally dominant (k_trsm_leaf, GEMMs)
+potrf   DPOTRF lower 4096 (k_potrf_leaf, k_trsm_leaf, GEMMs)
 batch   150 mixed calls (70% DGEMM, 20% DTRSM, 10% ZGEMM; M, N, K
         log-uniform in [64, 2048]) as one xkb_cuda_batch launch (k_sched)
 
@@ -56,6 +57,16 @@ def main(case):
             assert lib.xkb_cuda_trsm(1, 0, 1, 0, 0, n, n,
                                      ctypes.cast(al, ctypes.POINTER(ctypes.c_double)),
                                      A.data_ptr(), n, B.data_ptr(), n, 0, sp) == 0
+    elif case == "potrf":
+        n = 4096
+        Bm = rnd(n, n)
+        A0 = Bm @ Bm.t() / n + torch.eye(n, device="cuda", dtype=f64)
+        A = A0.clone()
+        info = torch.zeros(1, dtype=torch.int32, device="cuda")
+        keep += [A0, A, info]
+        for _ in range(2):
+            A.copy_(A0)
+            assert lib.xkb_cuda_potrf(1, 1, n, A.data_ptr(), n, info.data_ptr(), sp) == 0
     elif case == "batch":
         rng = np.random.default_rng(2024)
 
