@@ -9,7 +9,8 @@
 // against it with xkb_cuda_trsm (FP64 leaves + DMMA GEMMs), update the
 // trailing block with one triangle-masked GEMM (the HERK/SYRK of the
 // reference: C = C - P P^H, only the stored triangle written), factor the
-// trailing block.  Blocks of <= 64 are factored in FP64 by k_potrf_leaf.
+// trailing block.  Blocks of <= 64 are factored in FP64 by k_potrf_leaf
+// (register-resident elements, one CTA).
 // A non-positive (or non-finite) pivot stops nothing on the device -- later
 // blocks become NaN as in LAPACK's unchecked use -- but the first failing
 // column (1-based, over the whole matrix) is recorded in *d_info (0 = none).
@@ -23,78 +24,118 @@ namespace xkb {
 constexpr int kPotrfLeaf = 64;
 
 // Factor the n x n (n <= 64) Hermitian block at A in place.  The block is
-// staged as its lower triangle L (upper: L = U^H, read transposed and
-// conjugated), factored right-looking column by column in shared memory,
-// and written back to the stored triangle only.
+// read as its lower triangle L (upper: L = U^H, read transposed and
+// conjugated) and factored right-looking column by column.  Element (i, k)
+// of the triangle lives in a register of thread ((i + k) mod 256) -- 8 or 9
+// elements per thread; per column j the pivot and the scaled column go
+// through shared memory (two barriers), and every thread updates its own
+// elements L(i,k) -= L(i,j) conj(L(k,j)), k > j.  Written back to the stored
+// triangle only.
+constexpr int kPotrfThreads = 256;
+constexpr int kPotrfPer = (kPotrfLeaf * (kPotrfLeaf + 1) / 2 + kPotrfThreads - 1) / kPotrfThreads;
+
 template <class T>
-__global__ void __launch_bounds__(256) k_potrf_leaf(int n, typename St<T>::S* A, long lda,
-                                                    int upper, int col0, int* info) {
+__global__ void __launch_bounds__(kPotrfThreads) k_potrf_leaf(int n, typename St<T>::S* A,
+                                                              long lda, int upper, int col0,
+                                                              int* info) {
   constexpr bool CP = St<T>::CPLX;
   using S = typename St<T>::S;
-  extern __shared__ double sm_potrf[];  // Lr (and Li): 64 x 65 doubles each
-  double (*Lr)[kPotrfLeaf + 1] = reinterpret_cast<double (*)[kPotrfLeaf + 1]>(sm_potrf);
-  double (*Li)[kPotrfLeaf + 1] =
-      reinterpret_cast<double (*)[kPotrfLeaf + 1]>(sm_potrf + kPotrfLeaf * (kPotrfLeaf + 1));
-  for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
-    const int i = e % n, j = e / n;  // L(i, j), i >= j
-    if (i < j) continue;
-    const size_t idx = upper ? (size_t)j + (size_t)i * lda : (size_t)i + (size_t)j * lda;
-    double re, im = 0.0;
-    if (CP) {
-      re = (double)A[2 * idx];
-      im = (double)A[2 * idx + 1];
-      if (upper) im = -im;  // L = U^H
-    } else {
-      re = (double)A[idx];
+  __shared__ double cr[kPotrfLeaf], ci[kPotrfLeaf];  // column j after scaling
+  __shared__ int s_bad;
+  // this thread's elements: the e-th element of the packed lower triangle
+  // (column-major, (i, k) with i >= k) for e = tid + 256 q
+  int ei[kPotrfPer], ek[kPotrfPer];
+  double vr[kPotrfPer], vi[kPotrfPer];
+#pragma unroll
+  for (int q = 0; q < kPotrfPer; ++q) {
+    const int e = threadIdx.x + q * kPotrfThreads;
+    // column k holds n - k elements: find k, i for packed index e
+    int k = 0, base = 0;
+    while (k < kPotrfLeaf && base + (kPotrfLeaf - k) <= e) {
+      base += kPotrfLeaf - k;
+      ++k;
     }
-    Lr[i][j] = re;
-    if (CP) Li[i][j] = (i == j) ? 0.0 : im;  // Hermitian: real diagonal
+    const int i = k + (e - base);
+    ei[q] = i;
+    ek[q] = k;
+    vr[q] = vi[q] = 0.0;
+    if (k < kPotrfLeaf && i < n && k < n) {
+      const size_t idx = upper ? (size_t)k + (size_t)i * lda : (size_t)i + (size_t)k * lda;
+      if (CP) {
+        vr[q] = (double)A[2 * idx];
+        vi[q] = (i == k) ? 0.0 : (upper ? -(double)A[2 * idx + 1] : (double)A[2 * idx + 1]);
+      } else {
+        vr[q] = (double)A[idx];
+      }
+    } else {
+      ei[q] = -1;  // padding slot
+    }
   }
-  __syncthreads();
-  for (int j = 0; j < n; ++j) {
-    const double d = Lr[j][j];
-    if (!(d > 0.0)) {  // non-positive or NaN pivot
+  if (threadIdx.x == 0) s_bad = 0;
+  int j = 0;
+  for (; j < n; ++j) {
+    // 1. the owner of (j, j) publishes the pivot; owners of column j publish it
+#pragma unroll
+    for (int q = 0; q < kPotrfPer; ++q)
+      if (ek[q] == j && ei[q] >= 0) {
+        cr[ei[q]] = vr[q];
+        if (CP) ci[ei[q]] = vi[q];
+      }
+    __syncthreads();
+    const double d = cr[j];
+    if (!(d > 0.0)) {  // non-positive or NaN pivot: uniform decision
       if (threadIdx.x == 0 && info) atomicCAS(info, 0, col0 + j + 1);
-      __syncthreads();
       break;
     }
-    const double ljj = sqrt(d);
-    const double inv = 1.0 / ljj;
-    __syncthreads();  // every thread has read the pivot
-    for (int i = j + 1 + threadIdx.x; i < n; i += blockDim.x) {
-      Lr[i][j] *= inv;
-      if (CP) Li[i][j] *= inv;
+    const double ljj = sqrt(d), inv = 1.0 / ljj;
+    // 2. scale column j in place (owners) and in the shared copy
+#pragma unroll
+    for (int q = 0; q < kPotrfPer; ++q)
+      if (ek[q] == j && ei[q] >= 0) {
+        if (ei[q] == j) {
+          vr[q] = ljj;
+        } else {
+          vr[q] *= inv;
+          if (CP) vi[q] *= inv;
+        }
+      }
+    __syncthreads();  // everyone read cr[j] before it is overwritten below
+    if (threadIdx.x < kPotrfLeaf && threadIdx.x > j && threadIdx.x < n) {
+      cr[threadIdx.x] *= inv;
+      if (CP) ci[threadIdx.x] *= inv;
     }
-    if (threadIdx.x == 0) Lr[j][j] = ljj;
     __syncthreads();
-    // trailing update: L(i,k) -= L(i,j) conj(L(k,j)), j < k <= i < n
-    const int m = n - j - 1;
-    for (int e = threadIdx.x; e < m * m; e += blockDim.x) {
-      const int i = j + 1 + e % m, k = j + 1 + e / m;
-      if (k > i) continue;
-      const double ar = Lr[i][j], br = Lr[k][j];
-      if (CP) {
-        const double ai = Li[i][j], bi = Li[k][j];
-        Lr[i][k] -= ar * br + ai * bi;  // (ar + i ai)(br - i bi)
-        if (i != k) Li[i][k] -= ai * br - ar * bi;
-      } else {
-        Lr[i][k] -= ar * br;
+    // 3. trailing update of this thread's elements, column k > j
+#pragma unroll
+    for (int q = 0; q < kPotrfPer; ++q) {
+      const int i = ei[q], k = ek[q];
+      if (i >= 0 && k > j && i < n) {
+        const double ar = cr[i], br = cr[k];
+        if (CP) {
+          const double ai = ci[i], bi = ci[k];
+          vr[q] -= ar * br + ai * bi;  // L(i,j) conj(L(k,j))
+          if (i != k) vi[q] -= ai * br - ar * bi;
+        } else {
+          vr[q] -= ar * br;
+        }
       }
     }
-    __syncthreads();
+    __syncthreads();  // column j + 1 is published next
   }
   // write back the stored triangle (columns past a failure hold partial values)
-  for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
-    const int i = e % n, j = e / n;
-    if (i < j) continue;
-    const size_t idx = upper ? (size_t)j + (size_t)i * lda : (size_t)i + (size_t)j * lda;
+#pragma unroll
+  for (int q = 0; q < kPotrfPer; ++q) {
+    const int i = ei[q], k = ek[q];
+    if (i < 0 || i >= n || k >= n) continue;
+    const size_t idx = upper ? (size_t)k + (size_t)i * lda : (size_t)i + (size_t)k * lda;
     if (CP) {
-      A[2 * idx] = static_cast<S>(Lr[i][j]);
-      A[2 * idx + 1] = static_cast<S>(upper ? -Li[i][j] : Li[i][j]);
+      A[2 * idx] = static_cast<S>(vr[q]);
+      A[2 * idx + 1] = static_cast<S>(upper ? -vi[q] : vi[q]);
     } else {
-      A[idx] = static_cast<S>(Lr[i][j]);
+      A[idx] = static_cast<S>(vr[q]);
     }
   }
+  (void)s_bad;
 }
 
 struct PotrfCtx {
@@ -107,16 +148,8 @@ struct PotrfCtx {
 
 template <class T>
 static int launch_leaf(const PotrfCtx& c, char* Ad, long n, long i0) {
-  constexpr size_t smem = (St<T>::CPLX ? 2 : 1) * sizeof(double) * kPotrfLeaf * (kPotrfLeaf + 1);
-  static bool attr = false;  // one per instantiation
-  if (!attr) {
-    if (cudaFuncSetAttribute(k_potrf_leaf<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem) != cudaSuccess)
-      return XKB_ECUDA;
-    attr = true;
-  }
-  k_potrf_leaf<T><<<1, 256, smem, c.st>>>((int)n, reinterpret_cast<typename St<T>::S*>(Ad),
-                                           c.lda, c.upper, (int)i0, c.info);
+  k_potrf_leaf<T><<<1, kPotrfThreads, 0, c.st>>>(
+      (int)n, reinterpret_cast<typename St<T>::S*>(Ad), c.lda, c.upper, (int)i0, c.info);
   count_launch();
   return cudaPeekAtLastError() == cudaSuccess ? XKB_OK : XKB_ECUDA;
 }
