@@ -98,6 +98,16 @@ int xkb_cuda_scale(int dtype, int M, int N, const double* beta, void* C,
  * uplo/herm_diag/diag mask C as in xkb_gemm_args.  dtype XKB_D or XKB_Z. */
 int xkb_cuda_ozaki_gemm(const xkb_gemm_args* a, int nmod, void* stream);
 
+/* Column-panel form of the real Ozaki contraction (C full): op(A) converted
+ * once; for each panel p of columns [bounds[p], bounds[p+1]) of op(B) and C
+ * (bounds[0] = 0, bounds[npanel] = N) the stream waits on the CUDA event
+ * wait_ev[p] (if not NULL), the panel is computed, and done_ev[p] (if not
+ * NULL) is recorded.  Lets a caller overlap the panels' host<->device copies
+ * with the arithmetic.  No counterpart in the reference. */
+int xkb_cuda_ozaki_gemm_panels(const xkb_gemm_args* a, int nmod, void* stream, int npanel,
+                               const long* bounds, void* const* wait_ev,
+                               void* const* done_ev);
+
 /* The same real (XKB_D) Ozaki contraction as xkb_cuda_ozaki_gemm, for
  * callers that cannot allocate device memory at call time (a process whose
  * free GPU memory is held by its own caching allocator, a loop that must not

@@ -155,6 +155,53 @@ int gemm_async(int transA, int transB, int M, int N, int K, const T* alpha, cons
   const size_t NB = auto_tilesize(KERN_GEMM, M, N, K), es = sizeof(T);
   int err;
   const bool need_ab = !is_zero(*alpha) && K > 0;
+  // Large real Ozaki contractions with op(B) = B run panel by panel: B (and
+  // C) cross the host link in column panels, each panel is multiplied as soon
+  // as its operands landed, and coherence copies each finished panel back.
+  if (need_ab && HT<T>::dt == XKB_D && transB == CblasNoTrans && N >= 4096 &&
+      use_ozaki(XKB_D, M, N, K)) {
+    if ((err = flush_pending())) return rt_error(err);
+    Desc* dA = get_desc(A, Am, An, LDA, es, NB, &err);
+    if (!dA) return rt_error(err);
+    if ((err = make_valid(dA, 0, Am, 0, An))) return rt_error(err);  // compute waits for A
+    Desc* dB = get_desc(B, Bm, Bn, LDB, es, NB, &err);
+    if (!dB) return rt_error(err);
+    Desc* dC = get_desc(C, M, N, LDC, es, NB, &err);
+    if (!dC) return rt_error(err);
+    const long np = std::min<long>(16, std::max<long>(2, N / 2048));
+    const long w = ((N + np - 1) / np + 255) / 256 * 256;  // multiple of the INT8 tile width
+    std::vector<long> bounds{0};
+    while (bounds.back() < N) bounds.push_back(std::min<long>(N, bounds.back() + w));
+    std::vector<std::pair<Desc*, size_t>> in{{dB, (size_t)K}};
+    if (!is_zero(*beta)) in.emplace_back(dC, (size_t)M);
+    // completion events stay with C until its coherence point: owned by the
+    // descriptor, not taken from the recycled pool
+    while (dC->panel_ev.size() < bounds.size() - 1) {
+      cudaEvent_t e;
+      if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess)
+        return rt_error(XKB_ECUDA);
+      dC->panel_ev.push_back(e);
+    }
+    std::vector<cudaEvent_t> ev, done(dC->panel_ev.begin(), dC->panel_ev.begin() + (bounds.size() - 1));
+    if ((err = make_valid_panels(in, bounds, ev))) return rt_error(err);
+    xkb_gemm_args a = base_args<T>(opcode(transA), opcode(transB), M, N, K, alpha, beta);
+    a.A = dev_ptr(dA, 0, 0);
+    a.lda = (long)dA->dld;
+    a.B = dev_ptr(dB, 0, 0);
+    a.ldb = (long)dB->dld;
+    a.C = dev_ptr(dC, 0, 0);
+    a.ldc = (long)dC->dld;
+    const int nm = R.ozaki_moduli ? R.ozaki_moduli : xkb_ozaki_default_moduli(K);
+    err = xkb_cuda_ozaki_gemm_panels(&a, nm, R.s_comp, (int)done.size(), bounds.data(),
+                                     reinterpret_cast<void* const*>(ev.data()),
+                                     reinterpret_cast<void* const*>(done.data()));
+    if (err) return rt_error(err);
+    R.stats.ozaki_calls++;
+    R.stats.ozaki_moduli += (uint64_t)nm;
+    mark_full_overwrite(dC, 0, M, 0, N);
+    for (size_t p = 0; p < done.size(); ++p) dC->col_ready.emplace_back((size_t)bounds[p + 1], done[p]);
+    return 0;
+  }
   Desc *dA = nullptr, *dB = nullptr;
   if (need_ab) {
     dA = get_desc(A, Am, An, LDA, es, NB, &err);

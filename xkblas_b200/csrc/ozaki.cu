@@ -1034,6 +1034,127 @@ extern "C" int xkb_cuda_ozaki_gemm(const xkb_gemm_args* a, int nmod, void* strea
 }
 
 // ===========================================================================
+// Column-panel form of the real contraction, for callers that move op(B)
+// and C across the host link panel by panel: op(A) is scaled and converted
+// once; then for each column panel [n0, n1) of op(B) / C the stream waits on
+// wait_ev[p] (the panel's operands are on the device), the panel's column
+// shifts and residue planes are formed, multiplied on the INT8 tensor cores
+// and recombined into C[:, n0:n1), and done_ev[p] is recorded (the panel's
+// result is final).  Transfers of later panels and of finished results then
+// overlap the arithmetic.  The caller orders op(A) before the call.
+// Real, C full (no triangle mask); other calls use xkb_cuda_ozaki_gemm.
+extern "C" int xkb_cuda_ozaki_gemm_panels(const xkb_gemm_args* a, int nmod, void* stream,
+                                          int npanel, const long* bounds,
+                                          void* const* wait_ev, void* const* done_ev) {
+  if (!a || a->dtype != XKB_D || a->uplo != XKB_FULL || npanel < 1 || !bounds)
+    return XKB_EINVAL;
+  if (a->M < 0 || a->N < 0 || a->K < 0) return XKB_EINVAL;
+  if (bounds[0] != 0 || bounds[npanel] != a->N) return XKB_EINVAL;
+  for (int q = 0; q < npanel; ++q)
+    if (bounds[q + 1] <= bounds[q]) return XKB_EINVAL;
+  cudaStream_t st = resolve_stream(stream);
+  auto wait = [&](int q) {
+    if (wait_ev && wait_ev[q]) cudaStreamWaitEvent(st, static_cast<cudaEvent_t>(wait_ev[q]), 0);
+  };
+  auto done = [&](int q) {
+    if (done_ev && done_ev[q]) cudaEventRecord(static_cast<cudaEvent_t>(done_ev[q]), st);
+  };
+  if (a->M == 0) {
+    for (int q = 0; q < npanel; ++q) done(q);
+    return XKB_OK;
+  }
+  if (a->K == 0 || a->alpha[0] == 0.0 || a->K > 131072) {  // no split product to pipeline
+    for (int q = 0; q < npanel; ++q) wait(q);
+    const int r = a->K > 131072 ? XKB_ERANGE : xkb_cuda_gemm(a, st);
+    for (int q = 0; q < npanel; ++q) done(q);
+    return r;
+  }
+  if (nmod == 0) nmod = default_moduli(a->K);
+  const Consts* c = consts_for(nmod);
+  if (!c) return XKB_ERANGE;
+  const int M = a->M, K = a->K;
+  const long Kpad = (long)rup(K, BKB), Mpad = (long)rup(M, BM);
+  long wmax = 0;
+  for (int q = 0; q < npanel; ++q) wmax = std::max(wmax, bounds[q + 1] - bounds[q]);
+  const long Wpad = (long)rup((size_t)wmax, BN);
+  const bool akc = a->opA != XKB_OP_N, bkc = a->opB == XKB_OP_N;
+  const int nch = (int)((K + kNormChunk - 1) / kNormChunk);
+  int8_t *Ap = nullptr, *Bp = nullptr;
+  uint8_t* R = nullptr;
+  int *mu = nullptr, *nu = nullptr;
+  double2* part = nullptr;
+  auto alloc = [&](void** p, size_t n) {
+    return cudaMallocAsync(p, std::max<size_t>(n, 256), st) == cudaSuccess;
+  };
+  bool ok = alloc((void**)&Ap, (size_t)nmod * Mpad * Kpad) &&
+            alloc((void**)&Bp, (size_t)nmod * Wpad * Kpad) &&
+            alloc((void**)&R, (size_t)nmod * Mpad * Wpad) && alloc((void**)&mu, sizeof(int) * M) &&
+            alloc((void**)&nu, sizeof(int) * a->N) &&
+            alloc((void**)&part, sizeof(double2) * (size_t)nch * (size_t)std::max<long>(M, wmax));
+  int err = ok ? XKB_OK : XKB_ENOMEM;
+  if (!ok) cudaGetLastError();
+  const double* Ad = static_cast<const double*>(a->A);
+  const double* Bd = static_cast<const double*>(a->B);
+  const int slot = trace_begin("ozaki_panels", a->dtype, M, a->N, K, nmod, st);
+  if (!err) {
+    View va{Ad, a->lda, akc, 1, 0, 1.0};
+    err = launch_norm(va, M, K, 0, c, part, mu, st);
+    if (!err) err = launch_res(va, M, K, mu, c, Ap, Mpad, Kpad, 0, st);
+    if (!err && Kpad > (long)rup(K, 64)) {
+      const size_t kz = rup(K, 64);
+      if (cudaMemset2DAsync(Ap + kz, Kpad, 0, Kpad - kz, (size_t)nmod * Mpad, st) != cudaSuccess)
+        err = XKB_ECUDA;
+    }
+  }
+  trace_mark(slot, 1, st);
+  for (int q = 0; q < npanel; ++q) {
+    wait(q);
+    const long n0 = bounds[q], nw = bounds[q + 1] - bounds[q];
+    const long npad = (long)rup((size_t)nw, BN);
+    if (!err) {
+      // columns n0.. of op(B): opB == N -> B[k + j ldb]; else B[j + k ldb]
+      View vb{bkc ? Bd + n0 * a->ldb : Bd + n0, a->ldb, bkc, 1, 0, 1.0};
+      err = launch_norm(vb, (int)nw, K, 0, c, part, nu + n0, st);
+      if (!err) err = launch_res(vb, (int)nw, K, nu + n0, c, Bp, npad, Kpad, 0, st);
+      if (!err && Kpad > (long)rup(K, 64)) {
+        const size_t kz = rup(K, 64);
+        if (cudaMemset2DAsync(Bp + kz, Kpad, 0, Kpad - kz, (size_t)nmod * npad, st) != cudaSuccess)
+          err = XKB_ECUDA;
+      }
+      if (!err) err = launch_gemm(Ap, Mpad, Bp, npad, Mpad, npad, Kpad, c, R, XKB_FULL, 0, st);
+      if (!err) {
+        CrtP cp;
+        std::memset(&cp, 0, sizeof(cp));
+        cp.M = M;
+        cp.N = (int)nw;
+        cp.R = R;
+        cp.Mpad = Mpad;
+        cp.Npad = npad;
+        cp.mu = mu;
+        cp.nu = nu + n0;
+        cp.C = static_cast<double*>(a->C) + n0 * a->ldc;
+        cp.ldc = a->ldc;
+        cp.ar = a->alpha[0];
+        cp.br = a->beta[0];
+        cp.uplo = XKB_FULL;
+        const dim3 cg((unsigned)((M / 4 + 1 + 255) / 256), (unsigned)std::min<long>(nw, 65535));
+        err = launch_crt(cg, st, cp, *c, nullptr);
+      }
+    }
+    done(q);  // recorded on every path: waiters never hang on an error
+  }
+  trace_mark(slot, 2, st);
+  trace_mark(slot, 3, st);
+  if (Ap) cudaFreeAsync(Ap, st);
+  if (Bp) cudaFreeAsync(Bp, st);
+  if (R) cudaFreeAsync(R, st);
+  if (mu) cudaFreeAsync(mu, st);
+  if (nu) cudaFreeAsync(nu, st);
+  if (part) cudaFreeAsync(part, st);
+  return err;
+}
+
+// ===========================================================================
 // Scratch-free variant of the real Ozaki contraction.
 //
 // Who needs it: callers that cannot ask the CUDA allocator for memory at call

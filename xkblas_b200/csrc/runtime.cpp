@@ -127,6 +127,7 @@ static void free_desc_memory(Desc* d) {
 void drop_desc(Desc* d) {
   Runtime& R = rt();
   free_desc_memory(d);
+  for (cudaEvent_t e : d->panel_ev) cudaEventDestroy(e);
   R.descs.erase(d->host);
   delete d;
 }
@@ -329,6 +330,7 @@ static bool tile_in_uplo(const Desc* d, size_t i, size_t j, int uplo) {
 
 void mark_written(Desc* d, size_t r0, size_t r1, size_t c0, size_t c1, int uplo) {
   if (r1 <= r0 || c1 <= c0) return;
+  d->col_ready.clear();  // this write is ordered by the compute stream only
   const size_t tr0 = r0 / d->mb, tr1 = (r1 + d->mb - 1) / d->mb;
   const size_t tc0 = c0 / d->nb, tc1 = (c1 + d->nb - 1) / d->nb;
   for (size_t j = tc0; j < tc1; ++j)
@@ -399,20 +401,101 @@ int defer_op(const xkb_batch_op& o, Desc* r0, Desc* r1, Desc* r2, Desc* w) {
   return XKB_OK;
 }
 
+int make_valid_panels(const std::vector<std::pair<Desc*, size_t>>& ds,
+                      const std::vector<long>& bounds, std::vector<cudaEvent_t>& ev) {
+  Runtime& R = rt();
+  const size_t np = bounds.size() - 1, ncol = (size_t)bounds.back();
+  ev.assign(np, nullptr);
+  // snapshot of the tiles that need a copy: tile rows covering [0, rows),
+  // tile columns covering [0, ncol); whole tiles are copied, as make_valid does
+  std::vector<std::vector<uint8_t>> need(ds.size());
+  std::vector<size_t> tr1(ds.size()), tc1(ds.size());
+  for (size_t m = 0; m < ds.size(); ++m) {
+    Desc* d = ds[m].first;
+    tr1[m] = std::min(d->mt, (ds[m].second + d->mb - 1) / d->mb);
+    tc1[m] = std::min(d->nt, (ncol + d->nb - 1) / d->nb);
+    need[m].assign(d->mt * d->nt, 0);
+    for (size_t j = 0; j < tc1[m]; ++j)
+      for (size_t i = 0; i < tr1[m]; ++i) {
+        const bool miss = !(d->tile(i, j) & kDevValid);
+        need[m][i + j * d->mt] = miss;
+        miss ? ++R.stats.misses : ++R.stats.hits;
+      }
+  }
+  for (size_t p = 0; p < np; ++p) {
+    for (size_t m = 0; m < ds.size(); ++m) {
+      Desc* d = ds[m].first;
+      // the last panel also takes the rest of its last tile column
+      const size_t c0 = std::min((size_t)bounds[p], d->N);
+      const size_t c1 = p + 1 == np ? std::min(tc1[m] * d->nb, d->N)
+                                    : std::min((size_t)bounds[p + 1], d->N);
+      for (size_t tj = c0 / d->nb; tj * d->nb < c1; ++tj) {
+        const size_t a = std::max(c0, tj * d->nb), b = std::min(c1, (tj + 1) * d->nb);
+        size_t i = 0;
+        while (i < tr1[m]) {  // runs of tile rows needing a copy in this tile column
+          if (!need[m][i + tj * d->mt]) {
+            ++i;
+            continue;
+          }
+          size_t i1 = i;
+          while (i1 < tr1[m] && need[m][i1 + tj * d->mt]) ++i1;
+          if (int e = copy_h2d(d, i * d->mb, std::min(i1 * d->mb, d->M), a, b)) return e;
+          i = i1;
+        }
+      }
+    }
+    ev[p] = next_event();
+    cudaEventRecord(ev[p], R.s_h2d);
+  }
+  for (size_t m = 0; m < ds.size(); ++m)
+    for (size_t j = 0; j < tc1[m]; ++j)
+      for (size_t i = 0; i < tr1[m]; ++i) ds[m].first->tile(i, j) |= kDevValid;
+  return XKB_OK;
+}
+
 int coherent(Desc* d, int uplo, int memflag) {
   Runtime& R = rt();
   if (int e = flush_pending()) return e;
-  // D2H after everything already queued on the compute stream
-  cudaEvent_t ev = next_event();
-  cudaEventRecord(ev, R.s_comp);
-  cudaStreamWaitEvent(R.s_d2h, ev, 0);
-  int e = for_runs(
-      d, 0, d->mt, 0, d->nt,
-      [&](uint8_t s, size_t i, size_t j) {
-        return (s & kHostStale) && (uplo == 0 || tile_in_uplo(d, i, j, uplo));
-      },
-      [&](size_t a, size_t b, size_t c, size_t dd) { return copy_d2h(d, a, b, c, dd); });
+  int e;
+  if (uplo == 0 && !d->col_ready.empty()) {
+    // written panel by panel: copy each panel back once its event fired;
+    // columns past the last panel after all work queued so far
+    cudaEvent_t tail = nullptr;
+    e = for_runs(
+        d, 0, d->mt, 0, d->nt, [&](uint8_t s, size_t, size_t) { return (s & kHostStale) != 0; },
+        [&](size_t a, size_t b, size_t c, size_t dd) {
+          size_t from = 0;
+          for (auto& cr : d->col_ready) {
+            const size_t lo = std::max(c, from), hi = std::min(dd, cr.first);
+            from = cr.first;
+            if (lo >= hi) continue;
+            cudaStreamWaitEvent(R.s_d2h, cr.second, 0);
+            if (int r = copy_d2h(d, a, b, lo, hi)) return r;
+          }
+          if (dd > std::max(c, from)) {
+            if (!tail) {
+              tail = next_event();
+              cudaEventRecord(tail, R.s_comp);
+            }
+            cudaStreamWaitEvent(R.s_d2h, tail, 0);
+            if (int r = copy_d2h(d, a, b, std::max(c, from), dd)) return r;
+          }
+          return XKB_OK;
+        });
+  } else {
+    // D2H after everything already queued on the compute stream
+    cudaEvent_t ev = next_event();
+    cudaEventRecord(ev, R.s_comp);
+    cudaStreamWaitEvent(R.s_d2h, ev, 0);
+    e = for_runs(
+        d, 0, d->mt, 0, d->nt,
+        [&](uint8_t s, size_t i, size_t j) {
+          return (s & kHostStale) && (uplo == 0 || tile_in_uplo(d, i, j, uplo));
+        },
+        [&](size_t a, size_t b, size_t c, size_t dd) { return copy_d2h(d, a, b, c, dd); });
+  }
   if (e) return e;
+  d->col_ready.clear();
   for (size_t j = 0; j < d->nt; ++j)
     for (size_t i = 0; i < d->mt; ++i) {
       uint8_t& s = d->tile(i, j);

@@ -36,6 +36,12 @@ struct Desc {
   std::vector<uint8_t> st;                // mt*nt tile states, column major
   bool registered_init = false;           // handle initialised (isinit)
   uint8_t pend = 0;                       // deferred calls: 1 read, 2 written
+  // columns finished panel by panel on the compute stream: (end column,
+  // event recorded when columns [previous end, end) are final), ascending.
+  // Lets coherence copy each panel back as soon as it is done.  Cleared by
+  // any other write to the matrix.
+  std::vector<std::pair<size_t, cudaEvent_t>> col_ready;
+  std::vector<cudaEvent_t> panel_ev;  // owned events behind col_ready
   std::string name;
   uint8_t& tile(size_t i, size_t j) { return st[i + j * mt]; }
 };
@@ -91,6 +97,13 @@ void mark_written(Desc* d, size_t r0, size_t r1, size_t c0, size_t c1, int uplo)
 // Mark a region as produced on the device without reading the host copy.
 void mark_full_overwrite(Desc* d, size_t r0, size_t r1, size_t c0, size_t c1);
 int coherent(Desc* d, int uplo, int memflag);
+// Column-panel upload: for each panel [bounds[p], bounds[p+1]) and every
+// (matrix, row count) in `ds`, copy the panel's columns of the tiles (covering
+// rows [0, row count)) that are not valid on the device, in panel order, and
+// record ev[p] on the copy stream after panel p.  The compute stream is NOT
+// made to wait: the caller waits per panel.  The tiles become valid.
+int make_valid_panels(const std::vector<std::pair<Desc*, size_t>>& ds,
+                      const std::vector<long>& bounds, std::vector<cudaEvent_t>& ev);
 // Launch the deferred calls (caller holds rt().mu); returns an XKB_* code.
 int flush_pending();
 // Queue a call for the executor; reads: the buffers it reads (nullptr
