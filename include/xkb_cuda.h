@@ -192,6 +192,9 @@ int xkb_cuda_batch_release(void);
  *                           tiles (96)
  *   oz_group_m              Ozaki INT8 GEMM raster: M tiles per group of the
  *                           persistent tile walk (8)
+ *   batch_flush_mb          public async API: queued calls are launched once
+ *                           their operands reach this many MiB (2048), so the
+ *                           executor overlaps the uploads of later calls
  * xkb_tune_load returns the number of entries read or XKB_EINVAL. */
 int xkb_tune_set(const char* key, double value);
 double xkb_tune_get(const char* key, double dflt);

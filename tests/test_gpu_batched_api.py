@@ -37,7 +37,18 @@ def _call_trsm(xk, uplo, tr, dg, alpha, A, B):
              xk._ptr(B), B.shape[0])
 
 
-def test_many_independent_calls_one_batch(xk):
+@pytest.fixture(params=[None, 1.0], ids=["one_batch", "flush_1MiB"])
+def flush_mb(xk, request):
+    """None: the default threshold (all calls in one batch); 1.0: the queue
+    is launched whenever its operands reach 1 MiB (many batches, results made
+    coherent against each batch's own completion event)."""
+    if request.param is not None:
+        xk.lib().xkb_tune_set(b"batch_flush_mb", request.param)
+    yield request.param
+    xk.lib().xkb_tune_set(b"batch_flush_mb", 2048.0)
+
+
+def test_many_independent_calls_one_batch(xk, flush_mb):
     rng = np.random.default_rng(5)
     xk.reset_stats()
     calls = []
@@ -69,11 +80,14 @@ def test_many_independent_calls_one_batch(xk):
             al = (2.0 + 0.5j) if cplx else 2.0
             assert _call_trsm(xk, uplo, tr, dg, al, A, B) == 0
             calls.append(("trsm", (uplo, tr, dg, al, A, B0, M, N), B))
-    for _, _, out in calls:
+    for _, _, out in reversed(calls):
         xk.coherent(out)
     xk.sync()
     st = xk.stats()
-    assert st["batches"] >= 1 and st["batched_calls"] == len(calls)
+    if flush_mb is None:
+        assert st["batches"] == 1 and st["batched_calls"] == len(calls), st
+    else:  # lone calls run outside the executor and are not counted
+        assert st["batches"] > 1 and st["batched_calls"] <= len(calls), st
     for kind, args, out in calls:
         if kind == "gemm":
             ta, tb, al, A, B, be, C0, K = args

@@ -174,15 +174,14 @@ int gemm_async(int transA, int transB, int M, int N, int K, const T* alpha, cons
     while (bounds.back() < N) bounds.push_back(std::min<long>(N, bounds.back() + w));
     std::vector<std::pair<Desc*, size_t>> in{{dB, (size_t)K}};
     if (!is_zero(*beta)) in.emplace_back(dC, (size_t)M);
-    // completion events stay with C until its coherence point: owned by the
-    // descriptor, not taken from the recycled pool
-    while (dC->panel_ev.size() < bounds.size() - 1) {
-      cudaEvent_t e;
-      if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess)
-        return rt_error(XKB_ECUDA);
-      dC->panel_ev.push_back(e);
+    // completion events stay with C until its coherence point: not taken
+    // from the recycled pool
+    std::vector<EventRef> fin(bounds.size() - 1);
+    std::vector<cudaEvent_t> ev, done(fin.size());
+    for (size_t p = 0; p < fin.size(); ++p) {
+      if (!(fin[p] = new_event_ref())) return rt_error(XKB_ECUDA);
+      done[p] = fin[p]->e;
     }
-    std::vector<cudaEvent_t> ev, done(dC->panel_ev.begin(), dC->panel_ev.begin() + (bounds.size() - 1));
     if ((err = make_valid_panels(in, bounds, ev))) return rt_error(err);
     xkb_gemm_args a = base_args<T>(opcode(transA), opcode(transB), M, N, K, alpha, beta);
     a.A = dev_ptr(dA, 0, 0);
@@ -199,23 +198,24 @@ int gemm_async(int transA, int transB, int M, int N, int K, const T* alpha, cons
     R.stats.ozaki_calls++;
     R.stats.ozaki_moduli += (uint64_t)nm;
     mark_full_overwrite(dC, 0, M, 0, N);
-    for (size_t p = 0; p < done.size(); ++p) dC->col_ready.emplace_back((size_t)bounds[p + 1], done[p]);
+    for (size_t p = 0; p < fin.size(); ++p) dC->col_ready.emplace_back((size_t)bounds[p + 1], fin[p]);
     return 0;
   }
   Desc *dA = nullptr, *dB = nullptr;
   if (need_ab) {
     dA = get_desc(A, Am, An, LDA, es, NB, &err);
     if (!dA) return rt_error(err);
-    if ((err = make_valid(dA, 0, Am, 0, An))) return rt_error(err);
+    if ((err = make_valid(dA, 0, Am, 0, An, false))) return rt_error(err);
     dB = get_desc(B, Bm, Bn, LDB, es, NB, &err);
     if (!dB) return rt_error(err);
-    if ((err = make_valid(dB, 0, Bm, 0, Bn))) return rt_error(err);
+    if ((err = make_valid(dB, 0, Bm, 0, Bn, false))) return rt_error(err);
   }
   Desc* dC = get_desc(C, M, N, LDC, es, NB, &err);
   if (!dC) return rt_error(err);
   if (!is_zero(*beta)) {
-    if ((err = make_valid(dC, 0, M, 0, N))) return rt_error(err);
+    if ((err = make_valid(dC, 0, M, 0, N, false))) return rt_error(err);
   }
+  if ((err = comp_wait_h2d())) return rt_error(err);  // one wait for the three uploads
   xkb_gemm_args a = base_args<T>(opcode(transA), opcode(transB), M, N, K, alpha, beta);
   a.A = dA ? dev_ptr(dA, 0, 0) : nullptr;
   a.lda = dA ? (long)dA->dld : 1;
@@ -245,10 +245,13 @@ int gemm_async(int transA, int transB, int M, int N, int K, const T* alpha, cons
     o.alpha[1] = a.alpha[1];
     o.beta[0] = a.beta[0];
     o.beta[1] = a.beta[1];
+    // marked before queueing: a flush inside defer_op then leaves C's
+    // completion event in place
+    mark_full_overwrite(dC, 0, M, 0, N);
     if ((err = defer_op(o, dA, dB, is_zero(*beta) ? nullptr : dC, dC))) return rt_error(err);
-  } else if ((err = run_gemm(a))) {
-    return rt_error(err);
+    return 0;
   }
+  if ((err = run_gemm(a))) return rt_error(err);
   mark_full_overwrite(dC, 0, M, 0, N);
   return 0;
 }
@@ -489,8 +492,9 @@ int tr_async(int is_trsm, int side, int uplo, int transA, int diag, int M, int N
   Desc* dA = nullptr;
   if (!zero) {
     if (!(dA = get_desc(A, NA, NA, LDA, es, NB, &err))) return rt_error(err);
-    if ((err = make_valid(dA, 0, NA, 0, NA))) return rt_error(err);
-    if ((err = make_valid(dB, 0, M, 0, N))) return rt_error(err);
+    if ((err = make_valid(dA, 0, NA, 0, NA, false))) return rt_error(err);
+    if ((err = make_valid(dB, 0, M, 0, N, false))) return rt_error(err);
+    if ((err = comp_wait_h2d())) return rt_error(err);
   }
   double al[2];
   sc(*alpha, al);
@@ -516,8 +520,10 @@ int tr_async(int is_trsm, int side, int uplo, int transA, int diag, int M, int N
     o.ldc = (long)dB->dld;
     o.alpha[0] = al[0];
     o.alpha[1] = al[1];
-    if ((err = defer_op(o, dA, dB, nullptr, dB))) return rt_error(err);
+    // marked before queueing: a flush inside defer_op then leaves B's
+    // completion event in place
     mark_full_overwrite(dB, 0, M, 0, N);
+    if ((err = defer_op(o, dA, dB, nullptr, dB))) return rt_error(err);
     return 0;
   }
   if ((err = flush_pending())) return rt_error(err);

@@ -76,12 +76,22 @@ int ensure_init() {
   R.ozaki_min_dim = (long)xkb_tune_get("ozaki_min_dim", (double)R.ozaki_min_dim);
   if (const char* s = getenv("XKBLAS_OZAKI_SLICES")) R.ozaki_moduli = atoi(s);
   if (const char* s = getenv("XKBLAS_OZAKI_MIN_DIM")) R.ozaki_min_dim = atol(s);
+  if (const char* s = getenv("XKBLAS_BATCH_FLUSH_MB")) R.batch_flush_env = (size_t)atol(s) << 20;
   R.ready = true;
   return XKB_OK;
 }
 
 // Events are recycled round-robin; 64 in flight is far more than any call
 // sequence keeps outstanding between two stream waits.
+EventRef new_event_ref() {
+  auto r = std::make_shared<SharedEvent>();
+  if (cudaEventCreateWithFlags(&r->e, cudaEventDisableTiming) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  return r;
+}
+
 cudaEvent_t next_event() {
   Runtime& R = rt();
   cudaEvent_t e = R.ev_pool[R.ev_next];
@@ -127,7 +137,6 @@ static void free_desc_memory(Desc* d) {
 void drop_desc(Desc* d) {
   Runtime& R = rt();
   free_desc_memory(d);
-  for (cudaEvent_t e : d->panel_ev) cudaEventDestroy(e);
   R.descs.erase(d->host);
   delete d;
 }
@@ -142,8 +151,12 @@ static int flush_sync(Desc* d) {
 
 static int alloc_desc(Desc* d) {
   Runtime& R = rt();
-  const size_t align = std::max<size_t>(1, 128 / d->esz);  // 128-byte columns
-  d->dld = round_up(std::max<size_t>(d->M, 1), align);
+  // a host matrix with contiguous columns keeps its layout on the device, so
+  // that every transfer of it is one contiguous copy; otherwise columns are
+  // padded to 128 bytes (the kernels take any leading dimension and repack
+  // for TMA where they need to)
+  const size_t align = std::max<size_t>(1, 128 / d->esz);
+  d->dld = d->ld == d->M ? std::max<size_t>(d->M, 1) : round_up(std::max<size_t>(d->M, 1), align);
   const size_t bytes = d->dld * std::max<size_t>(d->N, 1) * d->esz;
   void* p = nullptr;
   if (cudaMallocAsync(&p, bytes, R.s_comp) != cudaSuccess) {
@@ -151,10 +164,7 @@ static int alloc_desc(Desc* d) {
     return XKB_ENOMEM;
   }
   d->dev = p;
-  // the copy stream must see the allocation
-  cudaEvent_t e = next_event();
-  cudaEventRecord(e, R.s_comp);
-  cudaStreamWaitEvent(R.s_h2d, e, 0);
+  R.alloc_unsynced = true;  // the copy stream waits for it before its next copy
   return XKB_OK;
 }
 
@@ -195,34 +205,26 @@ Desc* get_desc(const void* host, size_t M, size_t N, size_t ld, size_t esz, size
 // crosses the host link as one contiguous copy through a stream-ordered
 // staging buffer and is re-pitched on the device: pitched copies of short
 // rows move far below the link's bandwidth.
-constexpr size_t kStagedMaxRowBytes = 32768;
-
-static bool staged(const Desc* d, size_t r0, size_t r1) {
-  return r0 == 0 && r1 == d->M && d->ld == d->M && d->dld != d->ld &&
-         d->M * d->esz <= kStagedMaxRowBytes;
-}
-
 static int copy_h2d(Desc* d, size_t r0, size_t r1, size_t c0, size_t c1) {
   Runtime& R = rt();
   if (r1 <= r0 || c1 <= c0) return XKB_OK;
+  if (R.alloc_unsynced) {  // buffers allocated on the compute stream since the last copy
+    cudaEvent_t e = next_event();
+    cudaEventRecord(e, R.s_comp);
+    cudaStreamWaitEvent(R.s_h2d, e, 0);
+    R.alloc_unsynced = false;
+  }
   const char* src = static_cast<const char*>(d->host) + (r0 + c0 * d->ld) * d->esz;
   char* dst = static_cast<char*>(dev_ptr(d, r0, c0));
   const size_t w = (r1 - r0) * d->esz;
   R.stats.h2d += w * (c1 - c0);
-  if (staged(d, r0, r1)) {
-    void* tmp = nullptr;
-    if (cudaMallocAsync(&tmp, w * (c1 - c0), R.s_h2d) == cudaSuccess) {
-      cudaError_t e = cudaMemcpyAsync(tmp, src, w * (c1 - c0), cudaMemcpyHostToDevice, R.s_h2d);
-      if (e == cudaSuccess)
-        e = cudaMemcpy2DAsync(dst, d->dld * d->esz, tmp, w, w, c1 - c0,
-                              cudaMemcpyDeviceToDevice, R.s_h2d);
-      cudaFreeAsync(tmp, R.s_h2d);
-      return cuda_ok(e);
-    }
-    cudaGetLastError();  // no staging memory: pitched copy below
-  }
-  cudaError_t e = cudaMemcpy2DAsync(dst, d->dld * d->esz, src, d->ld * d->esz, w, c1 - c0,
-                                    cudaMemcpyHostToDevice, R.s_h2d);
+  cudaError_t e;
+  if (d->ld == d->dld && (r1 - r0 == d->M || c1 - c0 == 1))  // one contiguous range
+    e = cudaMemcpyAsync(dst, src, ((c1 - c0 - 1) * d->ld + (r1 - r0)) * d->esz,
+                        cudaMemcpyHostToDevice, R.s_h2d);
+  else
+    e = cudaMemcpy2DAsync(dst, d->dld * d->esz, src, d->ld * d->esz, w, c1 - c0,
+                          cudaMemcpyHostToDevice, R.s_h2d);
   return cuda_ok(e);
 }
 
@@ -233,20 +235,13 @@ static int copy_d2h(Desc* d, size_t r0, size_t r1, size_t c0, size_t c1) {
   const char* src = static_cast<const char*>(dev_ptr(d, r0, c0));
   const size_t w = (r1 - r0) * d->esz;
   R.stats.d2h += w * (c1 - c0);
-  if (staged(d, r0, r1)) {
-    void* tmp = nullptr;
-    if (cudaMallocAsync(&tmp, w * (c1 - c0), R.s_d2h) == cudaSuccess) {
-      cudaError_t e = cudaMemcpy2DAsync(tmp, w, src, d->dld * d->esz, w, c1 - c0,
-                                        cudaMemcpyDeviceToDevice, R.s_d2h);
-      if (e == cudaSuccess)
-        e = cudaMemcpyAsync(dst, tmp, w * (c1 - c0), cudaMemcpyDeviceToHost, R.s_d2h);
-      cudaFreeAsync(tmp, R.s_d2h);
-      return cuda_ok(e);
-    }
-    cudaGetLastError();
-  }
-  cudaError_t e = cudaMemcpy2DAsync(dst, d->ld * d->esz, src, d->dld * d->esz, w, c1 - c0,
-                                    cudaMemcpyDeviceToHost, R.s_d2h);
+  cudaError_t e;
+  if (d->ld == d->dld && (r1 - r0 == d->M || c1 - c0 == 1))
+    e = cudaMemcpyAsync(dst, src, ((c1 - c0 - 1) * d->ld + (r1 - r0)) * d->esz,
+                        cudaMemcpyDeviceToHost, R.s_d2h);
+  else
+    e = cudaMemcpy2DAsync(dst, d->ld * d->esz, src, d->dld * d->esz, w, c1 - c0,
+                          cudaMemcpyDeviceToHost, R.s_d2h);
   return cuda_ok(e);
 }
 
@@ -296,7 +291,7 @@ static int for_runs(Desc* d, size_t tr0, size_t tr1, size_t tc0, size_t tc1, Pre
   return flush();
 }
 
-int make_valid(Desc* d, size_t r0, size_t r1, size_t c0, size_t c1) {
+int make_valid(Desc* d, size_t r0, size_t r1, size_t c0, size_t c1, bool wait) {
   Runtime& R = rt();
   if (r1 <= r0 || c1 <= c0) return XKB_OK;
   const size_t tr0 = r0 / d->mb, tr1 = (r1 + d->mb - 1) / d->mb;
@@ -313,6 +308,14 @@ int make_valid(Desc* d, size_t r0, size_t r1, size_t c0, size_t c1) {
   if (e) return e;
   for (size_t j = tc0; j < tc1; ++j)
     for (size_t i = tr0; i < tr1; ++i) d->tile(i, j) |= kDevValid;
+  R.h2d_unsynced = true;
+  return wait ? comp_wait_h2d() : XKB_OK;
+}
+
+int comp_wait_h2d() {
+  Runtime& R = rt();
+  if (!R.h2d_unsynced) return XKB_OK;
+  R.h2d_unsynced = false;
   cudaEvent_t ev = next_event();
   cudaEventRecord(ev, R.s_h2d);
   return cuda_ok(cudaStreamWaitEvent(R.s_comp, ev, 0));
@@ -347,8 +350,26 @@ int flush_pending() {
   if (R.pending.empty()) return XKB_OK;
   std::vector<xkb_batch_op> ops;
   ops.swap(R.pending);
-  for (Desc* d : R.pend_descs) d->pend = 0;
+  std::vector<Desc*> written;
+  for (Desc* d : R.pend_descs) {
+    if (d->pend & 2) written.push_back(d);
+    d->pend = 0;
+  }
   R.pend_descs.clear();
+  R.pend_bytes = 0;
+  const int e = launch_ops(ops);
+  if (e) return e;
+  // the outputs are final once this launch is: coherence need not wait for
+  // work queued after it
+  if (EventRef ev = new_event_ref()) {
+    cudaEventRecord(ev->e, R.s_comp);
+    for (Desc* d : written) d->col_ready.assign(1, {d->N, ev});
+  }
+  return XKB_OK;
+}
+
+int launch_ops(const std::vector<xkb_batch_op>& ops) {
+  Runtime& R = rt();
   if (ops.size() == 1) {  // a lone call: the whole-matrix kernels
     const xkb_batch_op& o = ops[0];
     if (o.kind == XKB_BATCH_TRSM)
@@ -389,6 +410,10 @@ int defer_op(const xkb_batch_op& o, Desc* r0, Desc* r1, Desc* r2, Desc* w) {
     if (int e = flush_pending()) return e;
   }
   R.pending.push_back(o);
+  const size_t es = (o.dtype == XKB_S ? 4 : (o.dtype == XKB_Z ? 16 : 8));
+  R.pend_bytes += es * (o.kind == XKB_BATCH_TRSM
+                            ? (size_t)o.M * o.M + (size_t)o.M * o.N
+                            : (size_t)o.M * o.K + (size_t)o.K * o.N + (size_t)o.M * o.N);
   auto mark = [&](Desc* d, uint8_t bit) {
     if (!d) return;
     if (!d->pend) R.pend_descs.push_back(d);
@@ -398,6 +423,11 @@ int defer_op(const xkb_batch_op& o, Desc* r0, Desc* r1, Desc* r2, Desc* w) {
   mark(r1, 1);
   mark(r2, 1);
   mark(w, 2);
+  if (w) w->col_ready.clear();  // set again when this call is launched
+  const size_t lim = R.batch_flush_env
+                         ? R.batch_flush_env
+                         : (size_t)(xkb_tune_get("batch_flush_mb", 2048.0) * 1048576.0);
+  if (R.pend_bytes >= lim) return flush_pending();
   return XKB_OK;
 }
 
@@ -469,7 +499,7 @@ int coherent(Desc* d, int uplo, int memflag) {
             const size_t lo = std::max(c, from), hi = std::min(dd, cr.first);
             from = cr.first;
             if (lo >= hi) continue;
-            cudaStreamWaitEvent(R.s_d2h, cr.second, 0);
+            cudaStreamWaitEvent(R.s_d2h, cr.second->e, 0);
             if (int r = copy_d2h(d, a, b, lo, hi)) return r;
           }
           if (dd > std::max(c, from)) {

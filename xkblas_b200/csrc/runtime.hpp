@@ -6,6 +6,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <unordered_map>
@@ -27,6 +28,18 @@ enum : uint8_t {
 // xkblas_init_matrix_handle, blas/xkblas.c:458-510).  Unlike the reference,
 // the device copy is ONE column-major buffer for the whole matrix; tiles are
 // the unit of coherence (valid / dirty bits) and of host<->device copies.
+// A CUDA event held by every descriptor whose results it marks; destroyed
+// with its last holder (CUDA releases a recorded event once it completed).
+struct SharedEvent {
+  cudaEvent_t e = nullptr;
+  ~SharedEvent() {
+    if (e) cudaEventDestroy(e);
+  }
+};
+using EventRef = std::shared_ptr<SharedEvent>;
+// A fresh event (nullptr if CUDA cannot create one).
+EventRef new_event_ref();
+
 struct Desc {
   void* host = nullptr;
   size_t M = 0, N = 0, ld = 0, esz = 0;   // host view
@@ -36,12 +49,13 @@ struct Desc {
   std::vector<uint8_t> st;                // mt*nt tile states, column major
   bool registered_init = false;           // handle initialised (isinit)
   uint8_t pend = 0;                       // deferred calls: 1 read, 2 written
-  // columns finished panel by panel on the compute stream: (end column,
-  // event recorded when columns [previous end, end) are final), ascending.
-  // Lets coherence copy each panel back as soon as it is done.  Cleared by
-  // any other write to the matrix.
-  std::vector<std::pair<size_t, cudaEvent_t>> col_ready;
-  std::vector<cudaEvent_t> panel_ev;  // owned events behind col_ready
+  // columns finished on the compute stream: (end column, event recorded when
+  // columns [previous end, end) are final), ascending.  Set by the panel
+  // contraction (one entry per panel) and by an executor batch (one entry for
+  // the whole matrix); lets coherence copy results back as soon as their
+  // producer is done instead of after all queued work.  Cleared by any write
+  // that does not set it.
+  std::vector<std::pair<size_t, std::shared_ptr<struct SharedEvent>>> col_ready;
   std::string name;
   uint8_t& tile(size_t i, size_t j) { return st[i + j * mt]; }
 };
@@ -59,6 +73,8 @@ struct Runtime {
   int device = 0;
   cudaStream_t s_comp = nullptr, s_h2d = nullptr, s_d2h = nullptr;
   cudaEvent_t ev_pool[64];
+  bool alloc_unsynced = false;  // device buffers allocated since the last host->device copy
+  bool h2d_unsynced = false;    // copies the compute stream does not wait for yet
   int ev_next = 0;
   std::unordered_map<const void*, Desc*> descs;
   size_t nb_param = 0;        // preset tile size (0 = automatic)
@@ -76,6 +92,11 @@ struct Runtime {
   // that touches what a queued call writes or writes what one reads.
   bool batch_on = true;
   size_t batch_max = 8192;
+  // queued calls are launched once their operands reach batch_flush_mb
+  // (tuning key, default 2048) MiB, so that the executor starts while later
+  // calls' operands are still uploading; XKBLAS_BATCH_FLUSH_MB overrides
+  size_t batch_flush_env = 0;
+  size_t pend_bytes = 0;  // operand bytes of the queued calls
   std::vector<xkb_batch_op> pending;
   std::vector<Desc*> pend_descs;  // buffers the queued calls touch (Desc::pend set)
   uint64_t batches = 0, batched_calls = 0;
@@ -91,7 +112,11 @@ Desc* get_desc(const void* host, size_t M, size_t N, size_t ld, size_t esz, size
                int* err);
 // Make the tiles covering rows [r0,r1) x cols [c0,c1) valid on the device
 // (H2D on the copy stream; the compute stream then waits).
-int make_valid(Desc* d, size_t r0, size_t r1, size_t c0, size_t c1);
+// wait = false: the compute stream is not yet made to wait for the copies;
+// the caller calls comp_wait_h2d() before its next launch.
+int make_valid(Desc* d, size_t r0, size_t r1, size_t c0, size_t c1, bool wait = true);
+// Make the compute stream wait for the copies issued by make_valid(.., false).
+int comp_wait_h2d();
 // Mark a region as written by the compute stream (device newer than host).
 void mark_written(Desc* d, size_t r0, size_t r1, size_t c0, size_t c1, int uplo);
 // Mark a region as produced on the device without reading the host copy.
@@ -106,6 +131,9 @@ int make_valid_panels(const std::vector<std::pair<Desc*, size_t>>& ds,
                       const std::vector<long>& bounds, std::vector<cudaEvent_t>& ev);
 // Launch the deferred calls (caller holds rt().mu); returns an XKB_* code.
 int flush_pending();
+// Launch a list of calls on the compute stream: one call through the
+// whole-matrix kernels, more as one executor batch.
+int launch_ops(const std::vector<xkb_batch_op>& ops);
 // Queue a call for the executor; reads: the buffers it reads (nullptr
 // entries ignored), w: the buffer it writes.  Flushes first on a conflict.
 int defer_op(const xkb_batch_op& o, Desc* r0, Desc* r1, Desc* r2, Desc* w);
