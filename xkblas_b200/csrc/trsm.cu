@@ -8,11 +8,11 @@
 // TRSM is solved recursively on the system index: the triangle is split in
 // two (split points multiple of 64), the leading half is solved, the coupling
 // block is applied to the trailing half as one GEMM (DMMA, or Ozaki when
-// requested and large), and the trailing half is solved.  Leaves of <= 64
-// unknowns are solved in FP64 by k_trsm_leaf (trsm_leaf.cuh): each
-// right-hand side held in the registers of a few lanes, the 64x64 triangle in
-// shared memory, about two CTAs per SM.
-// This keeps every flop except O(n * 64 * nrhs) inside large GEMMs.
+// requested and large), and the trailing half is solved.  Diagonal blocks of
+// <= 256 unknowns are solved in one launch of k_trsm_block (8-unknown
+// substitution steps in registers + rank-8 DMMA updates, right-hand sides in
+// shared memory).  This keeps every flop except O(n * 256 * nrhs) inside
+// large GEMMs.
 #include <algorithm>
 
 #include "trsm_leaf.cuh"
@@ -20,7 +20,7 @@
 
 namespace xkb {
 
-constexpr int kLeaf = 64;
+constexpr int kSplit = 64;  // recursion split points are multiples of this
 
 template <class T>
 struct TT;
@@ -69,26 +69,324 @@ __device__ __forceinline__ void stv(T* p, size_t i, double re, double im) {
   }
 }
 
-// Leaf solve: T x = alpha b for the right-hand sides of this CTA's column
-// range, T (n x n, n <= 64) the effective triangle: T(i,j) = A[swap ? j + i*lda
-// : i + j*lda] (conjugated when conj), lower when LOWER.  RHS c, unknown i
-// lives at B[rhs_rows ? c + i*ldb : i + c*ldb] (rhs_rows: the right-side
-// form).  Body: trsm_leaf.cuh (register-resident substitution).
-constexpr int kLeafThreads = 128;
-constexpr int kLeafRplReal = 8;  // many right-hand sides: more lanes per column
+// Solve of one diagonal block of <= kBlk unknowns for all right-hand sides
+// in one launch.  Each CTA takes CW right-hand sides and keeps them in shared
+// memory (FP64, alpha applied on load).  The block is walked in steps of 8
+// unknowns (forward for a lower effective triangle, backward for an upper
+// one).  At the start the inverses of the block's 8 x 8 diagonal sub-blocks
+// are formed in parallel, one thread per column (substitution against a unit
+// vector); each step then takes Y = inv(T_ss) X_s with one DMMA per 8
+// right-hand sides and applies the rank-8 update of the unknowns still to
+// solve with DMMA (m16n8k8; complex: four real products).  The coupling strip
+// T(rows still to solve, 8 columns) of each step is copied with cp.async two
+// steps ahead into a ring of three buffers.
+constexpr int kBlk = 256;
+constexpr int kBlkThreads = 256;
+
+template <class T>
+struct BlkShape {
+  using S = typename St<T>::S;
+  static constexpr bool CP = St<T>::CPLX;
+  static constexpr int CW = CP ? 8 : 16;      // right-hand sides per CTA
+  static constexpr int NT = CW / 8;           // 8-column MMA tiles
+  static constexpr int XROWS = kBlk + 16;     // rows incl. the last partial 16-row tile
+  static constexpr int XS = XROWS + 2;        // column stride, = 2 mod 16
+  static constexpr int YW = CW + 2;           // solved rows [8][YW]
+  static constexpr int SRL = kBlk + 16 + 2;   // strip column stride (elements of S)
+  static constexpr int PL = CP ? 2 : 1;       // real planes
+  static constexpr int NBUF = 3;
+  static constexpr size_t X_D = (size_t)PL * CW * XS;         // doubles
+  static constexpr size_t Y_D = (size_t)PL * 8 * YW;          // doubles
+  static constexpr size_t V_D = (size_t)PL * (kBlk / 8) * 64;  // doubles: inverses, [blk][i][j]
+  static constexpr size_t S_B = sizeof(S) * PL * 8 * SRL;    // bytes per strip buffer
+  static constexpr size_t SMEM = sizeof(double) * (X_D + Y_D + V_D) + NBUF * S_B;
+  static constexpr int PE = kBlk * 8 / kBlkThreads;  // strip elements per thread
+  static_assert(sizeof(S) * PL * kBlk * 8 <= S_B, "diagonal blocks are staged in one buffer");
+};
+
+template <int BYTES>
+__device__ __forceinline__ void cp_async_zfill(void* smem, const void* gmem, bool valid) {
+  static_assert(BYTES == 4 || BYTES == 8, "element copy");
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;" ::"r"(smem_u32(smem)), "l"(gmem),
+               "n"(BYTES), "r"(valid ? BYTES : 0)
+               : "memory");
+}
 
 template <class T, bool LOWER>
-__global__ void __launch_bounds__(kLeafThreads)
-    k_trsm_leaf(int n, int nrhs, int cols_per_cta, const typename St<T>::S* A, long lda, int swap,
-                int conj, int unit, typename St<T>::S* B, long ldb, int rhs_rows, double ar,
-                double ai) {
-  extern __shared__ double sm_leaf[];
-  leaf_stage<T, kLeafThreads, kLeafRplReal>(A, lda, n, swap != 0, conj != 0, LOWER, unit != 0,
-                                            sm_leaf);
-  const int c0 = blockIdx.x * cols_per_cta;
-  const int c1 = min(nrhs, c0 + cols_per_cta);
-  leaf_solve<T, kLeafThreads, LOWER, kLeafRplReal>(B, ldb, rhs_rows != 0, n, c0, c1, ar, ai,
-                                                   sm_leaf);
+__global__ void __launch_bounds__(kBlkThreads, 2)
+    k_trsm_block(int nb, int nrhs, const typename St<T>::S* A, long lda, int swap, int conj,
+                 int unit, typename St<T>::S* B, long ldb, int rhs_rows, double ar, double ai) {
+  using Sh = BlkShape<T>;
+  using S = typename St<T>::S;
+  constexpr bool CP = Sh::CP;
+  constexpr int CW = Sh::CW, XS = Sh::XS, YW = Sh::YW, SRL = Sh::SRL, PE = Sh::PE;
+  constexpr int W = CP ? 2 : 1;
+  extern __shared__ double sm_blk[];
+  double* Xr = sm_blk;  // X[c * XS + row]
+  double* Xi = Xr + (CP ? CW * XS : 0);
+  double* Yr = sm_blk + Sh::X_D;  // Y[k * YW + c]: the 8 rows just solved
+  double* Yi = Yr + (CP ? 8 * YW : 0);
+  double* Vr = Yr + Sh::Y_D;  // inverse of diagonal sub-block m: V[m * 64 + i * 8 + j]
+  double* Vi = Vr + (CP ? (kBlk / 8) * 64 : 0);
+  S* strips = reinterpret_cast<S*>(Vr + Sh::V_D);
+  auto strip_buf = [&](int q) { return strips + (size_t)q * (Sh::S_B / sizeof(S)); };
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const int c0 = blockIdx.x * CW;
+  const int cols = min(CW, nrhs - c0);
+  const int nsub = (nb + 7) / 8;
+  auto sub_of = [&](int s) { return LOWER ? s : nsub - 1 - s; };
+
+  // ---- coupling strips: step s covers unknowns b = 8 sub(s) .. b+7; strip
+  // row j is matrix row r0 + j (lower r0 = b, rows b..nb-1; upper r0 = 0,
+  // rows 0..b+7), column k is matrix column b + k; stored [plane][k][row]
+  // as raw elements of A.  This thread's elements, q = 0..PE-1: no swap
+  // (columns of A contiguous) row tid, column q; swap (rows contiguous) row
+  // 32 q + tid / 8, column tid % 8: consecutive threads, consecutive addresses.
+  const int jt = swap ? tid >> 3 : tid, kt = swap ? tid & 7 : 0;
+  const int jq = swap ? 32 : 0, kq = swap ? 0 : 1;
+  auto strip_issue = [&](int s) {
+    if (s < nsub) {
+      const int b = 8 * sub_of(s), r0 = LOWER ? b : 0;
+      const int rows = LOWER ? nb - b : min(nb, b + 8);
+      S* dst = strip_buf(s % Sh::NBUF);
+#pragma unroll
+      for (int q = 0; q < PE; ++q) {
+        const int j = jt + q * jq, k = kt + q * kq;
+        const bool ok = j < rows && b + k < nb;
+        const size_t idx = swap ? (size_t)(b + k) + (size_t)(r0 + j) * lda
+                                : (size_t)(r0 + j) + (size_t)(b + k) * lda;
+        const S* src = ok ? A + W * idx : A;
+        cp_async_zfill<sizeof(S)>(dst + k * SRL + j, src, ok);
+        if (CP) cp_async_zfill<sizeof(S)>(dst + 8 * SRL + k * SRL + j, ok ? src + 1 : A, ok);
+      }
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");  // possibly empty: uniform counting
+  };
+  strip_issue(0);
+  strip_issue(1);
+
+  // ---- right-hand sides into shared memory (zero past nb rows / cols) ----
+  for (int e = tid; e < CW * (Sh::XROWS - nb); e += kBlkThreads) {
+    const int c = e / (Sh::XROWS - nb), r = nb + e % (Sh::XROWS - nb);
+    Xr[c * XS + r] = 0.0;
+    if (CP) Xi[c * XS + r] = 0.0;
+  }
+  {
+    constexpr int GRP = kBlk * CW / kBlkThreads;  // one round of loads
+    for (int e0 = 0; e0 < nb * CW; e0 += kBlkThreads * GRP) {
+      double br[GRP], bi[GRP];
+#pragma unroll
+      for (int q = 0; q < GRP; ++q) {
+        const int e = e0 + q * kBlkThreads + tid;
+        const int i = rhs_rows ? e / CW : e % nb, c = rhs_rows ? e % CW : e / nb;
+        br[q] = bi[q] = 0.0;
+        if (e < nb * CW && c < cols) {
+          const size_t idx = leaf_at(i, c0 + c, ldb, rhs_rows != 0);
+          br[q] = (double)__ldcg(B + W * idx);
+          if (CP) bi[q] = (double)__ldcg(B + 2 * idx + 1);
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < GRP; ++q) {
+        const int e = e0 + q * kBlkThreads + tid;
+        const int i = rhs_rows ? e / CW : e % nb, c = rhs_rows ? e % CW : e / nb;
+        if (e < nb * CW) {
+          Xr[c * XS + i] = ar * br[q] - ai * bi[q];
+          if (CP) Xi[c * XS + i] = ar * bi[q] + ai * br[q];
+        }
+      }
+    }
+  }
+
+  // ---- inverses of the diagonal 8 x 8 sub-blocks ----
+  {
+    // stage the sub-blocks (raw, [m][plane][i][j]) in the third strip buffer
+    S* D = strip_buf(2);
+    constexpr int DE = kBlk * 8 / kBlkThreads;
+#pragma unroll
+    for (int q = 0; q < DE; ++q) {
+      const int e = q * kBlkThreads + tid;
+      const int m = e >> 6, i = (e >> 3) & 7, j = e & 7;
+      const int rr = 8 * m + i, qq = 8 * m + j;
+      S vr = S(0), vi = S(0);
+      if (m < nsub && rr < nb && qq < nb && (LOWER ? rr >= qq : rr <= qq)) {
+        const size_t idx = swap ? (size_t)qq + (size_t)rr * lda : (size_t)rr + (size_t)qq * lda;
+        vr = __ldcg(A + W * idx);
+        if (CP) vi = __ldcg(A + 2 * idx + 1);
+      }
+      D[m * 64 * Sh::PL + i * 8 + j] = vr;
+      if (CP) D[m * 128 + 64 + i * 8 + j] = vi;
+    }
+    __syncthreads();
+    // thread (m, kk): column kk of inv(T_m), T_m z = e_kk by substitution;
+    // rows / columns past nb (zero when staged) act as the identity.  Every
+    // thread takes part (the shuffles below span whole warps); sub-blocks
+    // past the last one invert the identity.
+    const int m = tid >> 3, kk = tid & 7;
+    {
+      const S* Dm = D + m * 64 * Sh::PL;
+      auto tv = [&](int i, int j, double& re, double& im) {
+        re = (double)Dm[i * 8 + j];
+        im = CP ? (conj ? -(double)Dm[64 + i * 8 + j] : (double)Dm[64 + i * 8 + j]) : 0.0;
+      };
+      // reciprocal diagonal: thread kk forms entry kk, the 8 threads of the
+      // sub-block (consecutive lanes) share them
+      double rk = 1.0, ik = 0.0;
+      {
+        double dr, di;
+        tv(kk, kk, dr, di);
+        if (!(unit || 8 * m + kk >= nb)) {
+          if (CP) {
+            const double den = dr * dr + di * di;
+            rk = dr / den;
+            ik = -di / den;
+          } else {
+            rk = 1.0 / dr;
+          }
+        }
+      }
+      double rr_[8], ri_[8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        rr_[i] = __shfl_sync(0xffffffffu, rk, (lane & ~7) | i);
+        ri_[i] = CP ? __shfl_sync(0xffffffffu, ik, (lane & ~7) | i) : 0.0;
+      }
+      // column form: each step one multiply, then independent updates.  All
+      // register arrays are indexed by unrolled loop counters (kk only enters
+      // predicates), so they stay in registers.
+      double zr[8], zi[8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        zr[i] = i == kk ? 1.0 : 0.0;
+        zi[i] = 0.0;
+      }
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const int jj = LOWER ? q : 7 - q;
+        if (LOWER ? jj >= kk : jj <= kk) {
+          const double vr = zr[jj] * rr_[jj] - zi[jj] * ri_[jj];
+          const double vi = zr[jj] * ri_[jj] + zi[jj] * rr_[jj];
+          zr[jj] = vr;
+          zi[jj] = vi;
+#pragma unroll
+          for (int i = 0; i < 8; ++i) {
+            if (LOWER ? i > jj : i < jj) {
+              double tr, ti;
+              tv(i, jj, tr, ti);
+              zr[i] -= tr * vr - ti * vi;
+              zi[i] -= tr * vi + ti * vr;
+            }
+          }
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        Vr[m * 64 + i * 8 + kk] = zr[i];
+        if (CP) Vi[m * 64 + i * 8 + kk] = zi[i];
+      }
+    }
+  }
+
+  for (int s = 0; s < nsub; ++s) {
+    const int b = 8 * sub_of(s), r0 = LOWER ? b : 0;
+    // strip s landed (strip s+1 may still be in flight); the barrier also
+    // ends the previous step's update (X, Y free) and the inverses
+    asm volatile("cp.async.wait_group 1;" ::: "memory");
+    __syncthreads();
+    strip_issue(s + 2);  // into the buffer step s-1 read
+    // 1. Y = inv(T_ss) X(b..b+7): warp 0, one DMMA per 8 right-hand sides
+    // (rows 8..15 of the 16-row operand are zero)
+    if (warp == 0) {
+      const int m = b / 8, k0 = 2 * t, k1 = k0 + 1;
+      const double* vr = Vr + m * 64;
+      const double* vi = Vi + m * 64;
+#pragma unroll
+      for (int nt = 0; nt < Sh::NT; ++nt) {
+        const int n0 = nt * 8;
+        const double a_r[4] = {vr[g * 8 + k0], 0.0, vr[g * 8 + k1], 0.0};
+        const double b_r[2] = {Xr[(n0 + g) * XS + b + k0], Xr[(n0 + g) * XS + b + k1]};
+        double yr[4] = {0.0, 0.0, 0.0, 0.0}, yi[4] = {0.0, 0.0, 0.0, 0.0};
+        if constexpr (CP) {
+          const double a_i[4] = {vi[g * 8 + k0], 0.0, vi[g * 8 + k1], 0.0};
+          const double a_ni[4] = {-a_i[0], 0.0, -a_i[2], 0.0};
+          const double b_i[2] = {Xi[(n0 + g) * XS + b + k0], Xi[(n0 + g) * XS + b + k1]};
+          dmma_k8(yr, a_r, b_r);
+          dmma_k8(yr, a_ni, b_i);
+          dmma_k8(yi, a_r, b_i);
+          dmma_k8(yi, a_i, b_r);
+        } else {
+          dmma_k8(yr, a_r, b_r);
+        }
+        // rows 0..7 of the result: (g, n0 + 2t + v)
+#pragma unroll
+        for (int v = 0; v < 2; ++v) {
+          const int c = n0 + 2 * t + v;
+          Yr[g * YW + c] = yr[v];
+          Xr[c * XS + b + g] = yr[v];
+          if (CP) {
+            Yi[g * YW + c] = yi[v];
+            Xi[c * XS + b + g] = yi[v];
+          }
+        }
+      }
+    }
+    __syncthreads();
+    // 2. rows still to solve -= T(rows, b..b+7) Y: 16 x 8 DMMA tiles
+    const S* str = strip_buf(s % Sh::NBUF);
+    const S* sti = str + 8 * SRL;
+    const int u0 = LOWER ? b + 8 : 0, u1 = LOWER ? nb : b;
+    const int mt = (u1 - u0 + 15) / 16;
+    for (int tile = warp; tile < mt * Sh::NT; tile += kBlkThreads / 32) {
+      const int m0 = u0 + (tile / Sh::NT) * 16, n0 = (tile % Sh::NT) * 8;
+      const int ra = m0 + g - r0, rb = ra + 8;  // strip rows of this lane
+      const int k0 = 2 * t, k1 = k0 + 1;
+      const double a_r[4] = {-(double)str[k0 * SRL + ra], -(double)str[k0 * SRL + rb],
+                             -(double)str[k1 * SRL + ra], -(double)str[k1 * SRL + rb]};
+      const double b_r[2] = {Yr[k0 * YW + n0 + g], Yr[k1 * YW + n0 + g]};
+      double cr[4], ci[4];
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        const int row = m0 + g + ((v >> 1) << 3), col = n0 + 2 * t + (v & 1);
+        cr[v] = Xr[col * XS + row];
+        ci[v] = CP ? Xi[col * XS + row] : 0.0;
+      }
+      if constexpr (CP) {
+        // T = A or conj(A); C -= T Y: re += (-Tr) Yr + Ti Yi, im += (-Tr) Yi + (-Ti) Yr
+        const double sg = conj ? 1.0 : -1.0;  // -Ti
+        const double a_i[4] = {sg * (double)sti[k0 * SRL + ra], sg * (double)sti[k0 * SRL + rb],
+                               sg * (double)sti[k1 * SRL + ra], sg * (double)sti[k1 * SRL + rb]};
+        const double a_ni[4] = {-a_i[0], -a_i[1], -a_i[2], -a_i[3]};
+        const double b_i[2] = {Yi[k0 * YW + n0 + g], Yi[k1 * YW + n0 + g]};
+        dmma_k8(cr, a_r, b_r);
+        dmma_k8(cr, a_ni, b_i);
+        dmma_k8(ci, a_r, b_i);
+        dmma_k8(ci, a_i, b_r);
+      } else {
+        dmma_k8(cr, a_r, b_r);
+      }
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        const int row = m0 + g + ((v >> 1) << 3), col = n0 + 2 * t + (v & 1);
+        if (row < u1) {
+          Xr[col * XS + row] = cr[v];
+          if (CP) Xi[col * XS + row] = ci[v];
+        }
+      }
+    }
+  }
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
+  __syncthreads();
+
+  // ---- store ----
+#pragma unroll 4
+  for (int e = tid; e < nb * CW; e += kBlkThreads) {
+    const int i = rhs_rows ? e / CW : e % nb, c = rhs_rows ? e % CW : e / nb;
+    if (c >= cols) continue;
+    const size_t idx = leaf_at(i, c0 + c, ldb, rhs_rows != 0);
+    B[W * idx] = static_cast<S>(Xr[c * XS + i]);
+    if (CP) B[2 * idx + 1] = static_cast<S>(Xi[c * XS + i]);
+  }
 }
 
 template <class T>
@@ -151,40 +449,34 @@ static unsigned grid_for(size_t total, int per_block = 256) {
 }
 
 template <class T>
-static int launch_diag(int n, int nrhs, const void* A, long lda, int swap, int conj, int lower,
-                       int unit, void* B, long ldb, int rhs_rows, const double* al,
-                       cudaStream_t st) {
+static int launch_block(int n, int nrhs, const void* A, long lda, int swap, int conj, int lower,
+                        int unit, void* B, long ldb, int rhs_rows, const double* al,
+                        cudaStream_t st) {
   using S = typename St<T>::S;
-  constexpr int cpp = kLeafThreads / LeafShape<T, kLeafRplReal>::G;  // right-hand sides per pass
-  // about two CTAs per SM; each stages the block once for all its passes
-  const long want = 2L * sm_count();
-  long per = ((long)nrhs + want - 1) / want;
-  per = std::max<long>(cpp, (per + cpp - 1) / cpp * cpp);
-  const unsigned grid = (unsigned)std::max<long>(1, ((long)nrhs + per - 1) / per);
-  const size_t smem = LeafShape<T, kLeafRplReal>::SMEM;
-  auto kl = lower ? k_trsm_leaf<T, true> : k_trsm_leaf<T, false>;
+  using Sh = BlkShape<T>;
+  const unsigned grid = (unsigned)((nrhs + Sh::CW - 1) / Sh::CW);
+  auto kb = lower ? k_trsm_block<T, true> : k_trsm_block<T, false>;
   static bool attr[2] = {false, false};
   if (!attr[lower ? 1 : 0]) {
-    if (cudaFuncSetAttribute(kl, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+    if (cudaFuncSetAttribute(kb, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Sh::SMEM) !=
         cudaSuccess)
       return XKB_ECUDA;
     attr[lower ? 1 : 0] = true;
   }
-  kl<<<grid, kLeafThreads, smem, st>>>(n, nrhs, (int)per, static_cast<const S*>(A), lda, swap,
-                                       conj, unit, static_cast<S*>(B), ldb, rhs_rows, al[0],
-                                       al[1]);
+  kb<<<grid, kBlkThreads, Sh::SMEM, st>>>(n, nrhs, static_cast<const S*>(A), lda, swap, conj,
+                                          unit, static_cast<S*>(B), ldb, rhs_rows, al[0], al[1]);
   count_launch();
   return cudaPeekAtLastError() == cudaSuccess ? XKB_OK : XKB_ECUDA;
 }
 
-static int diag_dispatch(int dt, int n, int nrhs, const void* A, long lda, int swap, int conj,
-                         int lower, int unit, void* B, long ldb, int rhs_rows, const double* al,
-                         cudaStream_t st) {
+static int block_dispatch(int dt, int n, int nrhs, const void* A, long lda, int swap, int conj,
+                          int lower, int unit, void* B, long ldb, int rhs_rows, const double* al,
+                          cudaStream_t st) {
   switch (dt) {
-    case XKB_S: return launch_diag<float>(n, nrhs, A, lda, swap, conj, lower, unit, B, ldb, rhs_rows, al, st);
-    case XKB_D: return launch_diag<double>(n, nrhs, A, lda, swap, conj, lower, unit, B, ldb, rhs_rows, al, st);
-    case XKB_C: return launch_diag<float2>(n, nrhs, A, lda, swap, conj, lower, unit, B, ldb, rhs_rows, al, st);
-    case XKB_Z: return launch_diag<double2>(n, nrhs, A, lda, swap, conj, lower, unit, B, ldb, rhs_rows, al, st);
+    case XKB_S: return launch_block<float>(n, nrhs, A, lda, swap, conj, lower, unit, B, ldb, rhs_rows, al, st);
+    case XKB_D: return launch_block<double>(n, nrhs, A, lda, swap, conj, lower, unit, B, ldb, rhs_rows, al, st);
+    case XKB_C: return launch_block<float2>(n, nrhs, A, lda, swap, conj, lower, unit, B, ldb, rhs_rows, al, st);
+    case XKB_Z: return launch_block<double2>(n, nrhs, A, lda, swap, conj, lower, unit, B, ldb, rhs_rows, al, st);
   }
   return XKB_EINVAL;
 }
@@ -253,15 +545,15 @@ static int update(const TrsmCtx& c, long p0, long p1, long q0, long q1, const do
 
 static int solve(const TrsmCtx& c, long i0, long i1, const double* alpha) {
   const long n = i1 - i0;
-  if (n <= kLeaf) {
-    // leaf: diagonal block of the effective triangle
+  if (n <= kBlk) {
+    // diagonal block of the effective triangle: one launch
     const char* Ad = aptr(c, i0, i0);
     char* Bd = c.left ? c.B + i0 * (long)c.es : c.B + i0 * c.ldb * (long)c.es;
-    return diag_dispatch(c.dt, (int)n, c.nrhs, Ad, c.lda, c.swap, c.conj, c.lower_eff, c.unit, Bd,
-                         c.ldb, c.left ? 0 : 1, alpha, c.st);
+    return block_dispatch(c.dt, (int)n, c.nrhs, Ad, c.lda, c.swap, c.conj, c.lower_eff, c.unit,
+                          Bd, c.ldb, c.left ? 0 : 1, alpha, c.st);
   }
-  long h = i0 + ((n / 2 + kLeaf - 1) / kLeaf) * kLeaf;
-  if (h >= i1) h = i1 - kLeaf;
+  long h = i0 + ((n / 2 + kSplit - 1) / kSplit) * kSplit;
+  if (h >= i1) h = i1 - kSplit;
   const double one[2] = {1.0, 0.0};
   int e;
   if (c.fwd) {
@@ -300,7 +592,7 @@ extern "C" int xkb_cuda_trsm(int dtype, int side, int uplo, int trans, int diag,
   c.st = resolve_stream(stream);
   const bool lower = uplo == XKB_LOWER;
   const bool op_lower = lower ^ (c.trans != XKB_OP_N);  // op(A) lower?
-  // effective triangle element access, as in k_trsm_leaf
+  // effective triangle element access, as in k_trsm_block
   if (c.left) {
     c.swap = c.trans != XKB_OP_N;
     c.conj = c.trans == XKB_OP_C;

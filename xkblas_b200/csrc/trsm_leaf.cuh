@@ -113,17 +113,17 @@ __device__ __forceinline__ void leaf_stage(const typename St<T>::S* A, long lda,
   __syncthreads();
 }
 
-// Solve right-hand sides c0 .. c1-1 in place (alpha applied on load).  All
-// NT threads take part (every warp runs the same number of passes).
-template <class T, int NT, bool LOWER, int RPL_REAL = 16>
-__device__ __forceinline__ void leaf_solve(typename St<T>::S* B, long ldb, bool rhs_rows, int n,
-                                           int c0, int c1, double ar, double ai,
-                                           const double* sm) {
+// Substitution core: right-hand sides c0 .. c1-1, unknown `row` of rhs `c`
+// read by ld(row, c, re, im) (rows < n of live columns only; zero elsewhere)
+// and written back by sto(row, c, re, im).  All NT threads take part (every
+// warp runs the same number of passes).
+template <class T, int NT, bool LOWER, int RPL_REAL, class Ld, class Sto>
+__device__ __forceinline__ void leaf_solve_core(int n, int c0, int c1, const double* sm, Ld ld,
+                                                Sto sto) {
   using Sh = LeafShape<T, RPL_REAL>;
   constexpr int RPL = Sh::RPL, G = Sh::G, GS = Sh::GS, COL = Sh::COL;
   constexpr int CPP = NT / G;  // right-hand sides per pass
   constexpr bool CP = Sh::CPLX;
-  using S = typename St<T>::S;
   const double* Tr = sm;
   const double* Ti = Tr + kLeafRows * COL;
   const double* Dr = Ti + (CP ? kLeafRows * COL : 0);
@@ -139,13 +139,7 @@ __device__ __forceinline__ void leaf_solve(typename St<T>::S* B, long ldb, bool 
     for (int r = 0; r < RPL; ++r) {
       const int row = q * RPL + r;
       xr[r] = xi[r] = 0.0;
-      if (row < n && live) {
-        const size_t idx = leaf_at(row, c, ldb, rhs_rows);
-        const double br = CP ? (double)__ldcg(B + 2 * idx) : (double)__ldcg(B + idx);
-        const double bi = CP ? (double)__ldcg(B + 2 * idx + 1) : 0.0;
-        xr[r] = ar * br - ai * bi;
-        if (CP) xi[r] = ar * bi + ai * br;
-      }
+      if (row < n && live) ld(row, c, xr[r], xi[r]);
     }
     // steps in G rounds of RPL: the register index is a compile-time constant
     // within a round, the owning lane a run-time one
@@ -200,17 +194,36 @@ __device__ __forceinline__ void leaf_solve(typename St<T>::S* B, long ldb, bool 
 #pragma unroll
     for (int r = 0; r < RPL; ++r) {
       const int row = q * RPL + r;
-      if (row < n && live) {
-        const size_t idx = leaf_at(row, c, ldb, rhs_rows);
-        if (CP) {
-          B[2 * idx] = static_cast<S>(xr[r]);
-          B[2 * idx + 1] = static_cast<S>(xi[r]);
-        } else {
-          B[idx] = static_cast<S>(xr[r]);
-        }
-      }
+      if (row < n && live) sto(row, c, xr[r], xi[r]);
     }
   }
+}
+
+// Solve right-hand sides c0 .. c1-1 of B in place (alpha applied on load).
+template <class T, int NT, bool LOWER, int RPL_REAL = 16>
+__device__ __forceinline__ void leaf_solve(typename St<T>::S* B, long ldb, bool rhs_rows, int n,
+                                           int c0, int c1, double ar, double ai,
+                                           const double* sm) {
+  constexpr bool CP = St<T>::CPLX;
+  using S = typename St<T>::S;
+  leaf_solve_core<T, NT, LOWER, RPL_REAL>(
+      n, c0, c1, sm,
+      [&](int row, int c, double& xr, double& xi) {
+        const size_t idx = leaf_at(row, c, ldb, rhs_rows);
+        const double br = CP ? (double)__ldcg(B + 2 * idx) : (double)__ldcg(B + idx);
+        const double bi = CP ? (double)__ldcg(B + 2 * idx + 1) : 0.0;
+        xr = ar * br - ai * bi;
+        if (CP) xi = ar * bi + ai * br;
+      },
+      [&](int row, int c, double xr, double xi) {
+        const size_t idx = leaf_at(row, c, ldb, rhs_rows);
+        if (CP) {
+          B[2 * idx] = static_cast<S>(xr);
+          B[2 * idx + 1] = static_cast<S>(xi);
+        } else {
+          B[idx] = static_cast<S>(xr);
+        }
+      });
 }
 
 }  // namespace xkb
