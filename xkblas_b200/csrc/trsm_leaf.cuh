@@ -1,13 +1,12 @@
 // trsm_leaf.cuh -- FP64 solve of one diagonal block of a triangular system
-// (n <= 64 unknowns) against a range of right-hand sides, shared by the
-// recursive solver (trsm.cu) and the tile-task executor (sched.cu).  It is
-// the body the reference hands to cublasZtrsm for a diagonal tile
-// (blas/ztask_trsm.c:162-180).
+// (n <= 64 unknowns) against a range of right-hand sides, used by the
+// tile-task executor's solve tasks (sched.cu); leaf_at is shared with the
+// whole-matrix solver (trsm.cu).  It is the body the reference hands to
+// cublasZtrsm for a diagonal tile (blas/ztask_trsm.c:162-180).
 //
 // X = alpha op(T)^-1 B by substitution.  A right-hand side is held by G lanes
-// of one warp, lane g keeping rows RPL*g .. RPL*g + RPL-1 in registers (the
-// executor: real RPL 16, G 4, complex RPL 8, G 8; the recursive solver, with
-// thousands of right-hand sides: real 8 / 8, complex 4 / 16).  At step i the owner of row i scales it
+// of one warp, lane g keeping rows RPL*g .. RPL*g + RPL-1 in registers (real
+// RPL 16, G 4; complex RPL 8, G 8).  At step i the owner of row i scales it
 // by the reciprocal of T(i,i) (the packed-reciprocal form CPU BLAS kernels
 // use), the G lanes share it by shuffle, and each lane updates its rows below
 // (lower) or above (upper) i.  op(T) is staged column by column in shared
