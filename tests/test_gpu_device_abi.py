@@ -104,3 +104,28 @@ def test_ozaki_unaligned(xk):
     scale = 1.5 * A.abs().max().item() * B.abs().max().item() * K + 0.5
     assert (C - ref).abs().max().item() <= 4 * EPS * scale
     assert xk.lib().xkb_cuda_take_device_error() == 0
+
+
+def test_ozaki_panels_ragged(xk):
+    """xkb_cuda_ozaki_gemm_panels with ragged column panels (widths 256, 44,
+    700) and no events, on unaligned operands; bad boundaries are EINVAL."""
+    import torch
+    g = torch.Generator(device="cuda").manual_seed(43)
+    M, N, K = 300, 1000, 700
+    bufA, pA, A = _mat(torch, M, K, M + 1, 1, 1, g)
+    bufB, pB, B = _mat(torch, K, N, K + 2, 1, 1, g)
+    bufC, pC, C = _mat(torch, M, N, M + 3, 1, 1, g)
+    C0 = C.clone()
+    ga = GemmArgs(1, 0, 0, M, N, K, pA, M + 1, pB, K + 2, pC, M + 3)
+    ga.alpha[0], ga.beta[0] = 1.5, -0.5
+    lib = xk.lib()
+    bounds = (ctypes.c_long * 4)(0, 256, 300, N)
+    torch.cuda.synchronize()
+    assert lib.xkb_cuda_ozaki_gemm_panels(ctypes.byref(ga), 0, None, 3, bounds, None, None) == 0
+    xk.sync()
+    ref = 1.5 * (A @ B) - 0.5 * C0
+    scale = 1.5 * A.abs().max().item() * B.abs().max().item() * K + 0.5
+    assert (C - ref).abs().max().item() <= 4 * EPS * scale
+    bad = (ctypes.c_long * 3)(0, 600, 500)
+    assert lib.xkb_cuda_ozaki_gemm_panels(ctypes.byref(ga), 0, None, 2, bad, None, None) != 0
+    assert lib.xkb_cuda_take_device_error() == 0

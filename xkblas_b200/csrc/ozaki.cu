@@ -49,6 +49,9 @@ struct Consts {
   double invp_d[kMaxMod];
   uint32_t wlo[kMaxMod], whi[kMaxMod];  // bytes of 2^(8t) mod p, t = 0..3, 4..7
   uint32_t off[kMaxMod];                // p - (2^62 mod p): undoes the +2^62 offset
+  uint32_t offh[kMaxMod];               // off + floor(p/2): symmetric residues
+  uint32_t magic[kMaxMod];              // ceil(2^32 / p): exact quotients below 2^21
+  int half[kMaxMod];                    // floor(p/2)
   uint32_t crt[kMaxMod][4];             // (P/p)((P/p)^-1 mod p) mod P, 32-bit limbs
   uint32_t P[4], Ph[4];                 // P and floor(P/2)
   double Pd, invPd;
@@ -140,6 +143,9 @@ static bool make_consts(int n, Consts* c) {
     uint64_t t62 = 1;
     for (int s2 = 0; s2 < 62; ++s2) t62 = (t62 * 2) % (uint64_t)p;
     c->off[i] = (uint32_t)((uint64_t)p - t62);
+    c->half[i] = p / 2;
+    c->offh[i] = c->off[i] + (uint32_t)(p / 2);
+    c->magic[i] = (uint32_t)(((1ull << 32) + (uint64_t)p - 1) / (uint64_t)p);
     const u128 Mi = P / (u128)p;
     const int inv = inv_mod((int)(Mi % (u128)p), p);
     const u128 w = mulmod(Mi, (u128)inv, P);
@@ -274,22 +280,26 @@ __global__ void __launch_bounds__(256) k_oz_residues(int L, int K, const double*
   // X element (l,k) = esign * X[eoff + estride*(KC ? k + l*ld : l + k*ld)]
   __shared__ double tile[64][65];
   const int l0 = blockIdx.x * 64, k0 = blockIdx.y * 64;
-  for (int e = threadIdx.x; e < 64 * 64; e += 256) {
-    int ll, kk;
-    if (KC) {
-      kk = e & 63;
-      ll = e >> 6;
-    } else {
-      ll = e & 63;
-      kk = e >> 6;
+  {
+    // all 16 loads of a thread in flight before the shared stores
+    double v[16];
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+      const int e = threadIdx.x + q * 256;
+      const int ll = KC ? e >> 6 : e & 63, kk = KC ? e & 63 : e >> 6;
+      const int l = l0 + ll, k = k0 + kk;
+      v[q] = 0.0;
+      if (l < L && k < K) {
+        const size_t idx = KC ? (size_t)k + (size_t)l * ld : (size_t)l + (size_t)k * ld;
+        v[q] = esign * X[eoff + estride * idx];
+      }
     }
-    const int l = l0 + ll, k = k0 + kk;
-    double v = 0.0;
-    if (l < L && k < K) {
-      const size_t idx = KC ? (size_t)k + (size_t)l * ld : (size_t)l + (size_t)k * ld;
-      v = esign * X[eoff + estride * idx];
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+      const int e = threadIdx.x + q * 256;
+      const int ll = KC ? e >> 6 : e & 63, kk = KC ? e & 63 : e >> 6;
+      tile[ll][kk] = v[q];
     }
-    tile[ll][kk] = v;
   }
   __syncthreads();
   const size_t plane = (size_t)Lpad * (size_t)Kpad;
@@ -311,29 +321,26 @@ __global__ void __launch_bounds__(256) k_oz_residues(int L, int K, const double*
       hi[v] = (uint32_t)(u >> 32);
     }
     int8_t* dst = planes + (size_t)l * Kpad + kofs + k0 + kq;
+    // p_0 = 256: the two's complement low byte (the offset 2^62 is 0 mod 256)
+    *reinterpret_cast<uint32_t*>(dst) =
+        __byte_perm(__byte_perm(lo[0], lo[1], 0x0040), __byte_perm(lo[2], lo[3], 0x0040), 0x5410);
 #pragma unroll
-    for (int m = 0; m < NM; ++m) {
-      uint32_t packed = 0;
-      const int p = c.p[m];
+    for (int m = 1; m < NM; ++m) {
+      const uint32_t p = (uint32_t)c.p[m];
+      uint32_t r[4];
 #pragma unroll
       for (int v = 0; v < 4; ++v) {
-        int r;
-        if (m == 0) {  // p_0 = 256: the two's complement low byte
-          r = (int)(int8_t)(uint8_t)(unsigned long long)a[v];  // offset 2^62 = 0 mod 256
-        } else {
-          // a' mod p from its bytes: off + sum_t byte_t (2^(8t) mod p), where
-          // off = p - (2^62 mod p) removes the offset (total < 2^20)
-          unsigned int sacc = __dp4a(lo[v], c.wlo[m], c.off[m]);
-          sacc = __dp4a(hi[v], c.whi[m], sacc);
-          // invp_f <= 1/p, round toward zero: q in {floor(s/p) - 1, floor(s/p)}
-          const unsigned int q = __float2uint_rz(__fmul_rz(__uint2float_rn(sacc), c.invp_f[m]));
-          int rr = (int)(sacc - q * (unsigned int)p);
-          if (rr >= p) rr -= p;
-          r = rr > (p >> 1) ? rr - p : rr;  // symmetric residue
-        }
-        packed |= ((uint32_t)(uint8_t)(int8_t)r) << (8 * v);
+        // s = a' mod p + h (mod p) from the bytes of a': offh + sum_t byte_t
+        // (2^(8t) mod p) < 2^21; q = floor(s / p) exactly by the 32-bit
+        // reciprocal ceil(2^32 / p) (error s * 2^-32 < 1/p); s - q p - h is
+        // the symmetric residue in [-h, h]
+        uint32_t sacc = __dp4a(lo[v], c.wlo[m], c.offh[m]);
+        sacc = __dp4a(hi[v], c.whi[m], sacc);
+        const uint32_t q = __umulhi(sacc, c.magic[m]);
+        r[v] = sacc - q * p - (uint32_t)c.half[m];
       }
-      *reinterpret_cast<uint32_t*>(dst + (size_t)m * plane) = packed;
+      *reinterpret_cast<uint32_t*>(dst + (size_t)m * plane) =
+          __byte_perm(__byte_perm(r[0], r[1], 0x0040), __byte_perm(r[2], r[3], 0x0040), 0x5410);
     }
   }
 }
@@ -643,12 +650,12 @@ __device__ __forceinline__ double scale2(double x, int e) {
   return x * pow2(e1) * pow2(e2);
 }
 
+// The four rows of a thread are reconstructed unconditionally (rows past M
+// reuse the last row's shift and are not stored), so their independent
+// integer chains interleave; the stores are predicated afterwards.
 template <int NM>
-__global__ void __launch_bounds__(256) k_oz_crt(const CrtP p, const Consts c) {
-  const long iq = (long)blockIdx.x * blockDim.x + threadIdx.x;  // row quad
-  const long i0 = iq * 4;
-  if (i0 >= p.M) return;
-  for (int j = blockIdx.y; j < p.N; j += gridDim.y) {
+__device__ __forceinline__ void crt_quad(const CrtP& p, const Consts& c, long i0, int j,
+                                         double (&y)[4]) {
   const size_t plane = (size_t)p.Mpad * (size_t)p.Npad;
   uint32_t words[NM];
 #pragma unroll
@@ -657,39 +664,70 @@ __global__ void __launch_bounds__(256) k_oz_crt(const CrtP p, const Consts c) {
   const int nuj = p.nu[j];
 #pragma unroll
   for (int v = 0; v < 4; ++v) {
-    const long i = i0 + v;
-    if (i >= p.M) break;
-    if (p.uplo == XKB_LOWER && i + p.diag < j) continue;
-    if (p.uplo == XKB_UPPER && i + p.diag > j) continue;
     uint32_t r[NM];
 #pragma unroll
-    for (int m = 0; m < NM; ++m) r[m] = (words[m] >> (8 * v)) & 0xffu;
-    const int mui = p.mu[i];
-    double y;
-    if (mui == kShiftNonFinite || nuj == kShiftNonFinite) y = __longlong_as_double(0x7ff8000000000000ll);
-    else y = scale2(crt_value<NM>(r, c), -(mui + nuj));
-    const size_t idx = (size_t)i + (size_t)j * p.ldc;
-    if (!p.cplx) {
-      double out = p.ar * y;
-      if (p.br != 0.0) out = fma(p.br, p.C[idx], out);
-      p.C[idx] = out;
-    } else {
-      // complex: part 0 stores Re(AB) into the scratch `other` buffer role is
-      // reversed: see ozaki_complex() -- here C holds (Re,Im) pairs and the
-      // first pass wrote Re(AB) into p.other[i + j*M].
-      const double xr = p.other[(size_t)i + (size_t)j * p.M], xi = y;
-      double vr = p.ar * xr - p.ai * xi;
-      double vi = p.ar * xi + p.ai * xr;
-      if (p.br != 0.0 || p.bi != 0.0) {
-        const double cr = p.C[2 * idx], ci = p.C[2 * idx + 1];
-        vr += p.br * cr - p.bi * ci;
-        vi += p.br * ci + p.bi * cr;
-      }
-      if (p.herm_diag && i + p.diag == j) vi = 0.0;
-      p.C[2 * idx] = vr;
-      p.C[2 * idx + 1] = vi;
-    }
+    for (int m = 0; m < NM; ++m) r[m] = __byte_perm(words[m], 0u, 0x4440 + v);
+    const int mui = p.mu[min(i0 + v, (long)p.M - 1)];
+    if (mui == kShiftNonFinite || nuj == kShiftNonFinite) y[v] = __longlong_as_double(0x7ff8000000000000ll);
+    else y[v] = scale2(crt_value<NM>(r, c), -(mui + nuj));
   }
+}
+
+template <int NM>
+__global__ void __launch_bounds__(256) k_oz_crt(const CrtP p, const Consts c) {
+  const long iq = (long)blockIdx.x * blockDim.x + threadIdx.x;  // row quad
+  const long i0 = iq * 4;
+  if (i0 >= p.M) return;
+  for (int j = blockIdx.y; j < p.N; j += gridDim.y) {
+    double y[4];
+    crt_quad<NM>(p, c, i0, j, y);
+    const size_t idx0 = (size_t)i0 + (size_t)j * p.ldc;
+    if (!p.cplx) {
+      const bool full = i0 + 3 < p.M && p.uplo == XKB_FULL &&
+                        (reinterpret_cast<uintptr_t>(p.C + idx0) & 15) == 0;
+      if (full) {  // two 16-byte loads / stores for the quad
+        double2* cp2 = reinterpret_cast<double2*>(p.C + idx0);
+        double2 o0 = make_double2(p.ar * y[0], p.ar * y[1]);
+        double2 o1 = make_double2(p.ar * y[2], p.ar * y[3]);
+        if (p.br != 0.0) {
+          const double2 c0 = cp2[0], c1 = cp2[1];
+          o0.x = fma(p.br, c0.x, o0.x);
+          o0.y = fma(p.br, c0.y, o0.y);
+          o1.x = fma(p.br, c1.x, o1.x);
+          o1.y = fma(p.br, c1.y, o1.y);
+        }
+        cp2[0] = o0;
+        cp2[1] = o1;
+        continue;
+      }
+    }
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      const long i = i0 + v;
+      if (i >= p.M) break;
+      if (p.uplo == XKB_LOWER && i + p.diag < j) continue;
+      if (p.uplo == XKB_UPPER && i + p.diag > j) continue;
+      const size_t idx = (size_t)i + (size_t)j * p.ldc;
+      if (!p.cplx) {
+        double out = p.ar * y[v];
+        if (p.br != 0.0) out = fma(p.br, p.C[idx], out);
+        p.C[idx] = out;
+      } else {
+        // complex: the first pass wrote Re(AB) into p.other[i + j*M]; this
+        // pass reconstructs Im(AB) and writes the (Re, Im) pairs of C
+        const double xr = p.other[(size_t)i + (size_t)j * p.M], xi = y[v];
+        double vr = p.ar * xr - p.ai * xi;
+        double vi = p.ar * xi + p.ai * xr;
+        if (p.br != 0.0 || p.bi != 0.0) {
+          const double cr = p.C[2 * idx], ci = p.C[2 * idx + 1];
+          vr += p.br * cr - p.bi * ci;
+          vi += p.br * ci + p.bi * cr;
+        }
+        if (p.herm_diag && i + p.diag == j) vi = 0.0;
+        p.C[2 * idx] = vr;
+        p.C[2 * idx + 1] = vi;
+      }
+    }
   }
 }
 
@@ -700,27 +738,16 @@ __global__ void __launch_bounds__(256) k_oz_crt_store(const CrtP p, const Consts
   const long i0 = iq * 4;
   if (i0 >= p.M) return;
   for (int j = blockIdx.y; j < p.N; j += gridDim.y) {
-  const size_t plane = (size_t)p.Mpad * (size_t)p.Npad;
-  uint32_t words[NM];
+    double y[4];
+    crt_quad<NM>(p, c, i0, j, y);
 #pragma unroll
-  for (int m = 0; m < NM; ++m)
-    words[m] = *reinterpret_cast<const uint32_t*>(p.R + (size_t)m * plane + (size_t)j * p.Mpad + i0);
-  const int nuj = p.nu[j];
-#pragma unroll
-  for (int v = 0; v < 4; ++v) {
-    const long i = i0 + v;
-    if (i >= p.M) break;
-    if (p.uplo == XKB_LOWER && i + p.diag < j) continue;
-    if (p.uplo == XKB_UPPER && i + p.diag > j) continue;
-    uint32_t r[NM];
-#pragma unroll
-    for (int m = 0; m < NM; ++m) r[m] = (words[m] >> (8 * v)) & 0xffu;
-    const int mui = p.mu[i];
-    double y;
-    if (mui == kShiftNonFinite || nuj == kShiftNonFinite) y = __longlong_as_double(0x7ff8000000000000ll);
-    else y = scale2(crt_value<NM>(r, c), -(mui + nuj));
-    out[(size_t)i + (size_t)j * p.M] = y;
-  }
+    for (int v = 0; v < 4; ++v) {
+      const long i = i0 + v;
+      if (i >= p.M) break;
+      if (p.uplo == XKB_LOWER && i + p.diag < j) continue;
+      if (p.uplo == XKB_UPPER && i + p.diag > j) continue;
+      out[(size_t)i + (size_t)j * p.M] = y[v];
+    }
   }
 }
 
@@ -1000,7 +1027,7 @@ extern "C" int xkb_cuda_ozaki_gemm(const xkb_gemm_args* a, int nmod, void* strea
   cp.uplo = a->uplo;
   cp.herm_diag = a->herm_diag;
   cp.diag = a->diag;
-  const dim3 cg((unsigned)((M / 4 + 1 + 255) / 256), (unsigned)std::min(N, 65535));
+  const dim3 cg((unsigned)(((M + 3) / 4 + 255) / 256), (unsigned)std::min(N, 65535));
   trace_mark(slot, 1, st);
   if (err == XKB_OK) {
     err = same ? launch_gemm(Ap, Arows, Ap, Arows, Mpad, Npad, Kpad, c, R, a->uplo, a->diag, st)
@@ -1137,7 +1164,7 @@ extern "C" int xkb_cuda_ozaki_gemm_panels(const xkb_gemm_args* a, int nmod, void
         cp.ar = a->alpha[0];
         cp.br = a->beta[0];
         cp.uplo = XKB_FULL;
-        const dim3 cg((unsigned)((M / 4 + 1 + 255) / 256), (unsigned)std::min<long>(nw, 65535));
+        const dim3 cg((unsigned)(((M + 3) / 4 + 255) / 256), (unsigned)std::min<long>(nw, 65535));
         err = launch_crt(cg, st, cp, *c, nullptr);
       }
     }
@@ -1275,7 +1302,7 @@ extern "C" int xkb_cuda_ozaki_gemm_noalloc(const xkb_gemm_args* a, int nmod, voi
     cp.br = a->beta[0];
     cp.uplo = a->uplo;
     cp.diag = a->diag;
-    const dim3 cg((unsigned)((M / 4 + 1 + 255) / 256), (unsigned)N);
+    const dim3 cg((unsigned)(((M + 3) / 4 + 255) / 256), (unsigned)N);
     err = launch_crt(cg, st, cp, *c, nullptr);
   }
   return err;
