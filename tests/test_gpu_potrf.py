@@ -38,7 +38,7 @@ def _potrf(xk, A, uplo):
 
 @pytest.mark.parametrize("dt", [np.float64, np.complex128, np.float32, np.complex64])
 @pytest.mark.parametrize("uplo", [LO, UP])
-@pytest.mark.parametrize("n", [1, 64, 65, 200, 700])
+@pytest.mark.parametrize("n", [1, 7, 64, 65, 127, 128, 129, 200, 700])
 def test_potrf_factor(xk, dt, uplo, n):
     A0 = _spd(n, dt, 10 + n)
     A = A0.copy(order="F")
@@ -67,6 +67,17 @@ def test_potrf_reports_first_bad_pivot(xk):
     A = _spd(n, np.float64, 3)
     A[150, 150] = -5.0  # leading 150x150 block stays positive definite
     assert _potrf(xk, A, LO) == 151
+
+
+@pytest.mark.parametrize("dt,uplo,col", [(np.float64, UP, 6), (np.complex128, LO, 70),
+                                          (np.complex128, UP, 1), (np.float64, LO, 129)])
+def test_potrf_reports_bad_pivot_in_block(xk, dt, uplo, col):
+    """A non-positive pivot inside a diagonal block (first column of a step,
+    mid-step, past the first block) is reported 1-based."""
+    n = 160
+    A = _spd(n, dt, 5)
+    A[col - 1, col - 1] = -5.0  # the leading (col-1) x (col-1) block stays positive definite
+    assert _potrf(xk, A, uplo) == col
 
 
 def test_potrf_argument_codes(xk):

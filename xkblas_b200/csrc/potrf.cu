@@ -6,11 +6,12 @@
 // gemm of the trailing tiles) and its diagonal-tile body (cuSOLVER potrf in
 // ztask_potrf.c).  Here the factorization is recursive on the matrix index
 // (split points multiple of 64): factor the leading block, solve the panel
-// against it with xkb_cuda_trsm (FP64 leaves + DMMA GEMMs), update the
+// against it with xkb_cuda_trsm (block solves + DMMA GEMMs), update the
 // trailing block with one triangle-masked GEMM (the HERK/SYRK of the
 // reference: C = C - P P^H, only the stored triangle written), factor the
-// trailing block.  Blocks of <= 64 are factored in FP64 by k_potrf_leaf
-// (register-resident elements, one CTA).
+// trailing block.  Blocks of <= 128 columns (64 complex) are factored in
+// FP64 by one CTA of k_potrf_block (the block in shared memory, 8-column
+// steps with DMMA panel solves and updates).
 // A non-positive (or non-finite) pivot stops nothing on the device -- later
 // blocks become NaN as in LAPACK's unchecked use -- but the first failing
 // column (1-based, over the whole matrix) is recorded in *d_info (0 = none).
@@ -21,121 +22,225 @@
 
 namespace xkb {
 
-constexpr int kPotrfLeaf = 64;
-
-// Factor the n x n (n <= 64) Hermitian block at A in place.  The block is
-// read as its lower triangle L (upper: L = U^H, read transposed and
-// conjugated) and factored right-looking column by column.  Element (i, k)
-// of the triangle lives in a register of thread ((i + k) mod 256) -- 8 or 9
-// elements per thread; per column j the pivot and the scaled column go
-// through shared memory (two barriers), and every thread updates its own
-// elements L(i,k) -= L(i,j) conj(L(k,j)), k > j.  Written back to the stored
-// triangle only.
-constexpr int kPotrfThreads = 256;
-constexpr int kPotrfPer = (kPotrfLeaf * (kPotrfLeaf + 1) / 2 + kPotrfThreads - 1) / kPotrfThreads;
+// Diagonal blocks of up to NMAX (128 real, 64 complex) columns are factored
+// by one CTA with the block in shared memory (FP64), 8 columns per step:
+//   1. warp 0 factors the 8 x 8 diagonal block in registers (lane l holds row
+//      l; per column: pivot by shuffle, square root, reciprocal, rank-1
+//      update by shuffles) and forms the inverse of that factor (lane c
+//      solves for column c);
+//   2. all warps solve the panel below, L(rows, s) = A(rows, s) L_ss^-H,
+//      with FP64 DMMA (16 x 8 tiles, K = 8);
+//   3. all warps apply the rank-8 update to the trailing lower triangle,
+//      A(i, j) -= L(i, s) L(j, s)^H, with DMMA tiles that meet the triangle.
+// Same operations as the blocked right-looking Cholesky; the 8 x 8 panel
+// solve goes through the explicit inverse of the 8 x 8 factor.
+constexpr int kPoThreads = 256;
 
 template <class T>
-__global__ void __launch_bounds__(kPotrfThreads) k_potrf_leaf(int n, typename St<T>::S* A,
-                                                              long lda, int upper, int col0,
-                                                              int* info) {
-  constexpr bool CP = St<T>::CPLX;
+struct PoShape {
+  static constexpr bool CP = St<T>::CPLX;
+  static constexpr int NMAX = CP ? 64 : 128;
+  static constexpr int ROWS = NMAX + 16;  // rows incl. the last partial 16-row tile
+  static constexpr int COLS = NMAX + 8;   // columns incl. the last partial 8-column tile
+  static constexpr int LD = ROWS + 2;     // column stride, = 2 mod 16
+  static constexpr int PL = CP ? 2 : 1;
+  static constexpr size_t SMEM = sizeof(double) * ((size_t)PL * COLS * LD + PL * 64 * 2);
+};
+
+template <class T>
+__global__ void __launch_bounds__(kPoThreads, 1)
+    k_potrf_block(int n, typename St<T>::S* A, long lda, int upper, int col0, int* info) {
+  using Sh = PoShape<T>;
   using S = typename St<T>::S;
-  __shared__ double cr[kPotrfLeaf], ci[kPotrfLeaf];  // column j after scaling
-  __shared__ int s_bad;
-  // this thread's elements: the e-th element of the packed lower triangle
-  // (column-major, (i, k) with i >= k) for e = tid + 256 q
-  int ei[kPotrfPer], ek[kPotrfPer];
-  double vr[kPotrfPer], vi[kPotrfPer];
-#pragma unroll
-  for (int q = 0; q < kPotrfPer; ++q) {
-    const int e = threadIdx.x + q * kPotrfThreads;
-    // column k holds n - k elements: find k, i for packed index e
-    int k = 0, base = 0;
-    while (k < kPotrfLeaf && base + (kPotrfLeaf - k) <= e) {
-      base += kPotrfLeaf - k;
-      ++k;
-    }
-    const int i = k + (e - base);
-    ei[q] = i;
-    ek[q] = k;
-    vr[q] = vi[q] = 0.0;
-    if (k < kPotrfLeaf && i < n && k < n) {
+  constexpr bool CP = Sh::CP;
+  constexpr int LD = Sh::LD;
+  constexpr int W = CP ? 2 : 1;
+  extern __shared__ double sm_po[];
+  double* Xr = sm_po;  // L(i, k) at X[k * LD + i], lower part only
+  double* Xi = Xr + (CP ? Sh::COLS * LD : 0);
+  double* Lsr = sm_po + (size_t)Sh::PL * Sh::COLS * LD;  // 8 x 8 factor, [i][k]
+  double* Lsi = Lsr + 64;
+  double* Vr = Lsr + Sh::PL * 64;  // its inverse, [i][k]
+  double* Vi = Vr + 64;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int g = lane >> 2, t = lane & 3;
+
+  // ---- load the effective lower triangle (upper: L = U^H) ----
+  for (int e = tid; e < Sh::COLS * LD; e += kPoThreads) {
+    const int k = e / LD, i = e % LD;
+    double vr = 0.0, vi = 0.0;
+    if (i < n && k < n && i >= k) {
       const size_t idx = upper ? (size_t)k + (size_t)i * lda : (size_t)i + (size_t)k * lda;
-      if (CP) {
-        vr[q] = (double)A[2 * idx];
-        vi[q] = (i == k) ? 0.0 : (upper ? -(double)A[2 * idx + 1] : (double)A[2 * idx + 1]);
+      vr = (double)A[W * idx];
+      if (CP) vi = (i == k) ? 0.0 : (upper ? -(double)A[2 * idx + 1] : (double)A[2 * idx + 1]);
+    }
+    Xr[e] = vr;
+    if (CP) Xi[e] = vi;
+  }
+  __syncthreads();
+
+  const int nsteps = (n + 7) / 8;
+  for (int s = 0; s < nsteps; ++s) {
+    const int b = 8 * s, w = min(8, n - b);
+    // 1. 8 x 8 diagonal factor and its inverse (warp 0)
+    if (warp == 0) {
+      const int l = lane & 7;  // lanes 8..31 mirror lanes 0..7 (shuffles span the warp)
+      double ar[8], ai[8], rinv[8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const bool in = k <= l && l < w;
+        ar[k] = in ? Xr[(b + k) * LD + b + l] : (k == l ? 1.0 : 0.0);
+        ai[k] = (in && CP) ? Xi[(b + k) * LD + b + l] : 0.0;
+      }
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const double d = __shfl_sync(0xffffffffu, ar[j], j);
+        if (!(d > 0.0) && lane == 0 && j < w && info) atomicCAS(info, 0, col0 + b + j + 1);
+        const double ljj = sqrt(d), r = 1.0 / ljj;
+        rinv[j] = r;
+        if (l == j) {
+          ar[j] = ljj;
+          ai[j] = 0.0;
+        } else if (l > j) {
+          ar[j] *= r;
+          ai[j] *= r;
+        }
+#pragma unroll
+        for (int k = j + 1; k < 8; ++k) {
+          const double vr = __shfl_sync(0xffffffffu, ar[j], k);  // L(k, j)
+          const double vi = CP ? __shfl_sync(0xffffffffu, ai[j], k) : 0.0;
+          if (l >= k) {  // A(l, k) -= L(l, j) conj(L(k, j))
+            ar[k] -= ar[j] * vr + ai[j] * vi;
+            if (CP) ai[k] -= ai[j] * vr - ar[j] * vi;
+          }
+        }
+      }
+      if (lane < 8) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+          Lsr[l * 8 + k] = k <= l ? ar[k] : 0.0;
+          if (CP) Lsi[l * 8 + k] = k <= l ? ai[k] : 0.0;
+          if (k <= l && l < w) {
+            Xr[(b + k) * LD + b + l] = ar[k];
+            if (CP) Xi[(b + k) * LD + b + l] = ai[k];
+          }
+        }
+      }
+      __syncwarp();
+      if (lane < 8) {
+        // column c = lane of inv(L_ss): L_ss z = e_c, column form
+        const int c = lane;
+        double zr[8], zi[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+          zr[i] = i == c ? 1.0 : 0.0;
+          zi[i] = 0.0;
+        }
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          if (j >= c) {
+            zr[j] *= rinv[j];  // the diagonal of the factor is real
+            zi[j] *= rinv[j];
+#pragma unroll
+            for (int i = j + 1; i < 8; ++i) {
+              const double lr = Lsr[i * 8 + j], li = CP ? Lsi[i * 8 + j] : 0.0;
+              zr[i] -= lr * zr[j] - li * zi[j];
+              if (CP) zi[i] -= lr * zi[j] + li * zr[j];
+            }
+          }
+        }
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+          Vr[i * 8 + c] = zr[i];
+          if (CP) Vi[i * 8 + c] = zi[i];
+        }
+      }
+    }
+    __syncthreads();
+    const int r0 = b + 8, R = n - r0;
+    if (R <= 0) break;
+    const int mt = (R + 15) / 16;
+    const int k0 = 2 * t, k1 = k0 + 1;
+    // 2. panel: L(i, b..b+7) = A(i, b..b+7) inv(L_ss)^H, in place
+    //    B operand (k, c) = conj(V(c, k))
+    for (int tile = warp; tile < mt; tile += kPoThreads / 32) {
+      const int m0 = r0 + tile * 16;
+      const double a_r[4] = {Xr[(b + k0) * LD + m0 + g], Xr[(b + k0) * LD + m0 + g + 8],
+                             Xr[(b + k1) * LD + m0 + g], Xr[(b + k1) * LD + m0 + g + 8]};
+      const double b_r[2] = {Vr[g * 8 + k0], Vr[g * 8 + k1]};
+      double dr[4] = {0.0, 0.0, 0.0, 0.0}, di[4] = {0.0, 0.0, 0.0, 0.0};
+      if constexpr (CP) {
+        const double a_i[4] = {Xi[(b + k0) * LD + m0 + g], Xi[(b + k0) * LD + m0 + g + 8],
+                               Xi[(b + k1) * LD + m0 + g], Xi[(b + k1) * LD + m0 + g + 8]};
+        const double a_ni[4] = {-a_i[0], -a_i[1], -a_i[2], -a_i[3]};
+        const double b_i[2] = {-Vi[g * 8 + k0], -Vi[g * 8 + k1]};  // conj
+        dmma_k8(dr, a_r, b_r);
+        dmma_k8(dr, a_ni, b_i);
+        dmma_k8(di, a_r, b_i);
+        dmma_k8(di, a_i, b_r);
       } else {
-        vr[q] = (double)A[idx];
+        dmma_k8(dr, a_r, b_r);
       }
-    } else {
-      ei[q] = -1;  // padding slot
-    }
-  }
-  if (threadIdx.x == 0) s_bad = 0;
-  int j = 0;
-  for (; j < n; ++j) {
-    // 1. the owner of (j, j) publishes the pivot; owners of column j publish it
+      __syncwarp();  // all lanes read the tile before any lane writes it
 #pragma unroll
-    for (int q = 0; q < kPotrfPer; ++q)
-      if (ek[q] == j && ei[q] >= 0) {
-        cr[ei[q]] = vr[q];
-        if (CP) ci[ei[q]] = vi[q];
+      for (int v = 0; v < 4; ++v) {
+        const int row = m0 + g + ((v >> 1) << 3), col = b + 2 * t + (v & 1);
+        Xr[col * LD + row] = dr[v];
+        if (CP) Xi[col * LD + row] = di[v];
       }
-    __syncthreads();
-    const double d = cr[j];
-    if (!(d > 0.0)) {  // non-positive or NaN pivot: uniform decision
-      if (threadIdx.x == 0 && info) atomicCAS(info, 0, col0 + j + 1);
-      break;
-    }
-    const double ljj = sqrt(d), inv = 1.0 / ljj;
-    // 2. scale column j in place (owners) and in the shared copy
-#pragma unroll
-    for (int q = 0; q < kPotrfPer; ++q)
-      if (ek[q] == j && ei[q] >= 0) {
-        if (ei[q] == j) {
-          vr[q] = ljj;
-        } else {
-          vr[q] *= inv;
-          if (CP) vi[q] *= inv;
-        }
-      }
-    __syncthreads();  // everyone read cr[j] before it is overwritten below
-    if (threadIdx.x < kPotrfLeaf && threadIdx.x > j && threadIdx.x < n) {
-      cr[threadIdx.x] *= inv;
-      if (CP) ci[threadIdx.x] *= inv;
     }
     __syncthreads();
-    // 3. trailing update of this thread's elements, column k > j
+    // 3. trailing update of the lower triangle: A(i, j) -= L(i, s) L(j, s)^H
+    //    16 x 8 tiles (i rows, j columns) meeting the triangle
+    const int nt = (R + 7) / 8;
+    for (int tile = warp; tile < mt * nt; tile += kPoThreads / 32) {
+      const int ti = tile / nt, tj = tile % nt;
+      if (8 * tj > 16 * ti + 15) continue;  // wholly above the diagonal (warp-uniform)
+      const int m0 = r0 + 16 * ti, n0 = r0 + 8 * tj;
+      const double a_r[4] = {-Xr[(b + k0) * LD + m0 + g], -Xr[(b + k0) * LD + m0 + g + 8],
+                             -Xr[(b + k1) * LD + m0 + g], -Xr[(b + k1) * LD + m0 + g + 8]};
+      // B (k, c) = conj(L(n0 + c, b + k))
+      const double b_r[2] = {Xr[(b + k0) * LD + n0 + g], Xr[(b + k1) * LD + n0 + g]};
+      double cr[4], ci[4];
 #pragma unroll
-    for (int q = 0; q < kPotrfPer; ++q) {
-      const int i = ei[q], k = ek[q];
-      if (i >= 0 && k > j && i < n) {
-        const double ar = cr[i], br = cr[k];
-        if (CP) {
-          const double ai = ci[i], bi = ci[k];
-          vr[q] -= ar * br + ai * bi;  // L(i,j) conj(L(k,j))
-          if (i != k) vi[q] -= ai * br - ar * bi;
-        } else {
-          vr[q] -= ar * br;
+      for (int v = 0; v < 4; ++v) {
+        const int row = m0 + g + ((v >> 1) << 3), col = n0 + 2 * t + (v & 1);
+        cr[v] = Xr[col * LD + row];
+        ci[v] = CP ? Xi[col * LD + row] : 0.0;
+      }
+      if constexpr (CP) {
+        // C += (-L_i)(conj L_j): re += (-Lr)(Ljr) - (-Li)(-Lji) ; im += (-Lr)(-Lji) + (-Li)(Ljr)
+        const double a_i[4] = {-Xi[(b + k0) * LD + m0 + g], -Xi[(b + k0) * LD + m0 + g + 8],
+                               -Xi[(b + k1) * LD + m0 + g], -Xi[(b + k1) * LD + m0 + g + 8]};
+        const double a_ni[4] = {-a_i[0], -a_i[1], -a_i[2], -a_i[3]};
+        const double b_i[2] = {-Xi[(b + k0) * LD + n0 + g], -Xi[(b + k1) * LD + n0 + g]};
+        dmma_k8(cr, a_r, b_r);
+        dmma_k8(cr, a_ni, b_i);
+        dmma_k8(ci, a_r, b_i);
+        dmma_k8(ci, a_i, b_r);
+      } else {
+        dmma_k8(cr, a_r, b_r);
+      }
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        const int row = m0 + g + ((v >> 1) << 3), col = n0 + 2 * t + (v & 1);
+        if (row >= col) {  // lower part only (the diagonal's imaginary part is dropped at the end)
+          Xr[col * LD + row] = cr[v];
+          if (CP) Xi[col * LD + row] = ci[v];
         }
       }
     }
-    __syncthreads();  // column j + 1 is published next
+    __syncthreads();
   }
-  // write back the stored triangle (columns past a failure hold partial values)
-#pragma unroll
-  for (int q = 0; q < kPotrfPer; ++q) {
-    const int i = ei[q], k = ek[q];
-    if (i < 0 || i >= n || k >= n) continue;
+
+  // ---- store the factor (the stored triangle only) ----
+  for (int e = tid; e < n * n; e += kPoThreads) {
+    const int i = e % n, k = e / n;
+    if (i < k) continue;
     const size_t idx = upper ? (size_t)k + (size_t)i * lda : (size_t)i + (size_t)k * lda;
-    if (CP) {
-      A[2 * idx] = static_cast<S>(vr[q]);
-      A[2 * idx + 1] = static_cast<S>(upper ? -vi[q] : vi[q]);
-    } else {
-      A[idx] = static_cast<S>(vr[q]);
-    }
+    A[W * idx] = static_cast<S>(Xr[k * LD + i]);
+    if (CP) A[2 * idx + 1] = static_cast<S>(i == k ? 0.0 : (upper ? -Xi[k * LD + i] : Xi[k * LD + i]));
   }
-  (void)s_bad;
 }
 
 struct PotrfCtx {
@@ -148,7 +253,15 @@ struct PotrfCtx {
 
 template <class T>
 static int launch_leaf(const PotrfCtx& c, char* Ad, long n, long i0) {
-  k_potrf_leaf<T><<<1, kPotrfThreads, 0, c.st>>>(
+  using Sh = PoShape<T>;
+  static bool attr = false;
+  if (!attr) {
+    if (cudaFuncSetAttribute(k_potrf_block<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)Sh::SMEM) != cudaSuccess)
+      return XKB_ECUDA;
+    attr = true;
+  }
+  k_potrf_block<T><<<1, kPoThreads, Sh::SMEM, c.st>>>(
       (int)n, reinterpret_cast<typename St<T>::S*>(Ad), c.lda, c.upper, (int)i0, c.info);
   count_launch();
   return cudaPeekAtLastError() == cudaSuccess ? XKB_OK : XKB_ECUDA;
@@ -167,13 +280,15 @@ static int leaf(const PotrfCtx& c, long i0, long n) {
 
 static int factor(const PotrfCtx& c, long i0, long i1) {
   const long n = i1 - i0;
-  if (n <= kPotrfLeaf) return leaf(c, i0, n);
-  long h = i0 + ((n / 2 + kPotrfLeaf - 1) / kPotrfLeaf) * kPotrfLeaf;
-  if (h >= i1) h = i1 - kPotrfLeaf;
+  const bool cplx = c.dt == XKB_C || c.dt == XKB_Z;
+  const long nmax = cplx ? PoShape<double2>::NMAX : PoShape<double>::NMAX;
+  if (n <= nmax) return leaf(c, i0, n);
+  constexpr long kSplit = 64;
+  long h = i0 + ((n / 2 + kSplit - 1) / kSplit) * kSplit;
+  if (h >= i1) h = i1 - kSplit;
   const long n1 = h - i0, n2 = i1 - h;
   int e;
   if ((e = factor(c, i0, h))) return e;
-  const bool cplx = c.dt == XKB_C || c.dt == XKB_Z;
   const int ctr = cplx ? XKB_OP_C : XKB_OP_T;
   const double one[2] = {1.0, 0.0};
   char* A11 = c.A + (i0 + i0 * c.lda) * (long)c.es;
