@@ -192,9 +192,6 @@ int xkb_cuda_batch_release(void);
  *                           tiles (96)
  *   oz_group_m              Ozaki INT8 GEMM raster: M tiles per group of the
  *                           persistent tile walk (8)
- *   trsm_block_min_rhs      whole-matrix TRSM solves diagonal blocks of 65..256
- *                           unknowns in one fused launch when it has at least
- *                           this many right-hand sides, else recurses to 64 (0)
  *   batch_flush_mb          public async API: queued calls are launched once
  *                           their operands reach this many MiB (2048), so the
  *                           executor overlaps the uploads of later calls

@@ -5,8 +5,8 @@
 dmma    DGEMM NN 4096^3 through xkb_cuda_gemm (k_gemm_dmma), two calls
 ozaki   the same through xkb_cuda_ozaki_gemm, 16 moduli (k_oz_* kernels)
 repack  the DGEMM with lda = ldb = 4097 (k_repack, then k_gemm_dmma)
-trsm    DTRSM L/L/N/N 4096 x 4096, diagonally dominant (k_trsm_leaf, GEMMs)
-potrf   DPOTRF lower 4096 (k_potrf_leaf, k_trsm_leaf, GEMMs)
+trsm    DTRSM L/L/N/N 4096 x 4096, diagonally dominant (k_trsm_block, GEMMs)
+potrf   DPOTRF lower 4096 (k_potrf_block, k_trsm_block, GEMMs)
 batch   150 mixed calls (70% DGEMM, 20% DTRSM, 10% ZGEMM; M, N, K
         log-uniform in [64, 2048]) as one xkb_cuda_batch launch (k_sched)
 
