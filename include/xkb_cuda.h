@@ -205,8 +205,11 @@ int xkb_tune_clear(void);
  * (XKB_UPPER), s/d/c/z, only the stored triangle read and written
  * (replaces the reference's tile driver blas/zpotrf.c:46-220).  d_info: a
  * device int (may be NULL) that receives the first column, 1-based, whose
- * pivot is not positive; it is not cleared here. */
-int xkb_cuda_potrf(int dtype, int uplo, int N, void* A, long lda, int* d_info, void* stream);
+ * pivot is not positive; it is not cleared here.  ozaki > 0 (XKB_D/XKB_Z):
+ * trailing updates and panel-solve updates whose dimensions are all
+ * >= ozaki use the Ozaki INT8 form (tensor-op mode); 0: plain FP64. */
+int xkb_cuda_potrf(int dtype, int uplo, int N, void* A, long lda, int* d_info, int ozaki,
+                   void* stream);
 
 /* Device error word written by bounded waits (0 = none); clears it. */
 int xkb_cuda_take_device_error(void);

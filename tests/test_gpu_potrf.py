@@ -62,6 +62,30 @@ def test_potrf_factor(xk, dt, uplo, n):
     assert np.abs(got - ref).max() <= 64 * n * EPS[dt] * max(1.0, np.abs(ref).max())
 
 
+@pytest.mark.parametrize("dt,uplo", [(np.float64, LO), (np.complex128, UP)])
+def test_potrf_tensor_op_mode(xk, dt, uplo):
+    """XKBLAS_TENSOR_OP_MATH: the top-level trailing update and the panel
+    solve's coupling updates (all dimensions >= 2048 at n = 4200) run in the
+    Ozaki INT8 form; same backward-error bound as the plain factorization."""
+    n = 4200
+    A0 = _spd(n, dt, 11)
+    A = A0.copy(order="F")
+    xk.set_modemath(xk.XKBLAS_TENSOR_OP_MATH)
+    try:
+        assert _potrf(xk, A, uplo) == 0
+    finally:
+        xk.set_modemath(xk.XKBLAS_DEFAULT_MATH)
+    up = np.complex128 if np.iscomplexobj(A0) else np.float64
+    if uplo == LO:
+        L = np.tril(A)
+        R = L @ L.conj().T
+    else:
+        U = np.triu(A)
+        R = U.conj().T @ U
+    scale = np.abs(A0).max() * n * EPS[dt]
+    assert np.abs(R - A0.astype(up)).max() <= 16 * scale
+
+
 def test_potrf_reports_first_bad_pivot(xk):
     n = 300
     A = _spd(n, np.float64, 3)

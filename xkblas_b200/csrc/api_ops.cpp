@@ -573,8 +573,10 @@ int potrf_async(int uplo, int N, T* A, int LDA) {
     }
   }
   cudaMemsetAsync(R.d_potrf_info, 0, sizeof(int), R.s_comp);
+  const bool tc = R.math == XKBLAS_TENSOR_OP_MATH && (HT<T>::dt == XKB_D || HT<T>::dt == XKB_Z);
   err = xkb_cuda_potrf(HT<T>::dt, uplo == CblasLower ? XKB_LOWER : XKB_UPPER, N,
-                       dev_ptr(dA, 0, 0), (long)dA->dld, R.d_potrf_info, R.s_comp);
+                       dev_ptr(dA, 0, 0), (long)dA->dld, R.d_potrf_info,
+                       tc ? (int)std::max<long>(R.ozaki_min_dim, 1) : 0, R.s_comp);
   if (err) return rt_error(err);
   mark_written(dA, 0, N, 0, N, uplo);
   return 0;

@@ -245,6 +245,7 @@ __global__ void __launch_bounds__(kPoThreads, 1)
 
 struct PotrfCtx {
   int dt, es, upper;
+  int ozaki;  // > 0: updates whose dimensions are all >= ozaki use the Ozaki form
   char* A;
   long lda;
   int* info;
@@ -307,7 +308,7 @@ static int factor(const PotrfCtx& c, long i0, long i1) {
     // A21 = A21 L11^-H; A22 -= A21 A21^H (lower triangle)
     P = c.A + (h + i0 * c.lda) * (long)c.es;
     if ((e = xkb_cuda_trsm(c.dt, 1, XKB_LOWER, ctr, 0, (int)n2, (int)n1, one, A11, c.lda, P,
-                           c.lda, 0, c.st)))
+                           c.lda, c.ozaki, c.st)))
       return e;
     g.opA = XKB_OP_N;
     g.opB = ctr;
@@ -316,7 +317,7 @@ static int factor(const PotrfCtx& c, long i0, long i1) {
     // A12 = U11^-H A12; A22 -= A12^H A12 (upper triangle)
     P = c.A + (i0 + h * c.lda) * (long)c.es;
     if ((e = xkb_cuda_trsm(c.dt, 0, XKB_UPPER, ctr, 0, (int)n1, (int)n2, one, A11, c.lda, P,
-                           c.lda, 0, c.st)))
+                           c.lda, c.ozaki, c.st)))
       return e;
     g.opA = ctr;
     g.opB = XKB_OP_N;
@@ -326,6 +327,13 @@ static int factor(const PotrfCtx& c, long i0, long i1) {
   g.lda = c.lda;
   g.B = P;
   g.ldb = c.lda;
+  if (c.ozaki > 0 && std::min(n1, n2) >= c.ozaki) {
+    e = xkb_cuda_ozaki_gemm(&g, 0, c.st);
+    if (e != XKB_ERANGE) {
+      if (e) return e;
+      return factor(c, h, i1);
+    }
+  }
   if ((e = xkb_cuda_gemm(&g, c.st))) return e;
   return factor(c, h, i1);
 }
@@ -335,7 +343,7 @@ static int factor(const PotrfCtx& c, long i0, long i1) {
 using namespace xkb;
 
 extern "C" int xkb_cuda_potrf(int dtype, int uplo, int N, void* A, long lda, int* d_info,
-                              void* stream) {
+                              int ozaki, void* stream) {
   if (dtype < XKB_S || dtype > XKB_Z || (uplo != XKB_LOWER && uplo != XKB_UPPER) || N < 0 ||
       lda < std::max(1, N) || (!A && N > 0))
     return XKB_EINVAL;
@@ -347,6 +355,7 @@ extern "C" int xkb_cuda_potrf(int dtype, int uplo, int N, void* A, long lda, int
   c.A = static_cast<char*>(A);
   c.lda = lda;
   c.info = d_info;
+  c.ozaki = (dtype == XKB_D || dtype == XKB_Z) ? std::max(ozaki, 0) : 0;
   c.st = resolve_stream(stream);
   return factor(c, 0, N);
 }

@@ -66,7 +66,7 @@ def main(case):
         keep += [A0, A, info]
         for _ in range(2):
             A.copy_(A0)
-            assert lib.xkb_cuda_potrf(1, 1, n, A.data_ptr(), n, info.data_ptr(), sp) == 0
+            assert lib.xkb_cuda_potrf(1, 1, n, A.data_ptr(), n, info.data_ptr(), 0, sp) == 0
     elif case == "batch":
         rng = np.random.default_rng(2024)
 
