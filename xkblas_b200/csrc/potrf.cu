@@ -65,103 +65,120 @@ __global__ void __launch_bounds__(kPoThreads, 1)
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int g = lane >> 2, t = lane & 3;
 
-  // ---- load the effective lower triangle (upper: L = U^H) ----
-  for (int e = tid; e < Sh::COLS * LD; e += kPoThreads) {
-    const int k = e / LD, i = e % LD;
-    double vr = 0.0, vi = 0.0;
-    if (i < n && k < n && i >= k) {
-      const size_t idx = upper ? (size_t)k + (size_t)i * lda : (size_t)i + (size_t)k * lda;
-      vr = (double)A[W * idx];
-      if (CP) vi = (i == k) ? 0.0 : (upper ? -(double)A[2 * idx + 1] : (double)A[2 * idx + 1]);
+  // ---- load the effective lower triangle (upper: L = U^H); loads in
+  // groups of 8 per thread before their stores ----
+  constexpr int GRP = 8;
+  for (int e0 = 0; e0 < Sh::COLS * LD; e0 += kPoThreads * GRP) {
+    double vr[GRP], vi[GRP];
+#pragma unroll
+    for (int q = 0; q < GRP; ++q) {
+      const int e = e0 + q * kPoThreads + tid;
+      const int k = e / LD, i = e % LD;
+      vr[q] = vi[q] = 0.0;
+      if (i < n && k < n && i >= k) {
+        const size_t idx = upper ? (size_t)k + (size_t)i * lda : (size_t)i + (size_t)k * lda;
+        vr[q] = (double)A[W * idx];
+        if (CP) vi[q] = (i == k) ? 0.0 : (upper ? -(double)A[2 * idx + 1] : (double)A[2 * idx + 1]);
+      }
     }
-    Xr[e] = vr;
-    if (CP) Xi[e] = vi;
+#pragma unroll
+    for (int q = 0; q < GRP; ++q) {
+      const int e = e0 + q * kPoThreads + tid;
+      if (e < Sh::COLS * LD) {
+        Xr[e] = vr[q];
+        if (CP) Xi[e] = vi[q];
+      }
+    }
   }
-  __syncthreads();
 
-  const int nsteps = (n + 7) / 8;
-  for (int s = 0; s < nsteps; ++s) {
-    const int b = 8 * s, w = min(8, n - b);
-    // 1. 8 x 8 diagonal factor and its inverse (warp 0)
-    if (warp == 0) {
-      const int l = lane & 7;  // lanes 8..31 mirror lanes 0..7 (shuffles span the warp)
-      double ar[8], ai[8], rinv[8];
+  // warp 0: factor the 8 x 8 diagonal block at b (final values in X) and
+  // invert the factor into V
+  auto diag_factor = [&](int b) {
+    const int w = min(8, n - b);
+    const int l = lane & 7;  // lanes 8..31 mirror lanes 0..7 (shuffles span the warp)
+    double ar[8], ai[8], rinv[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const bool in = k <= l && l < w;
+      ar[k] = in ? Xr[(b + k) * LD + b + l] : (k == l ? 1.0 : 0.0);
+      ai[k] = (in && CP) ? Xi[(b + k) * LD + b + l] : 0.0;
+    }
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const double d = __shfl_sync(0xffffffffu, ar[j], j);
+      if (!(d > 0.0) && lane == 0 && j < w && info) atomicCAS(info, 0, col0 + b + j + 1);
+      const double ljj = sqrt(d), r = 1.0 / ljj;
+      rinv[j] = r;
+      if (l == j) {
+        ar[j] = ljj;
+        ai[j] = 0.0;
+      } else if (l > j) {
+        ar[j] *= r;
+        ai[j] *= r;
+      }
+#pragma unroll
+      for (int k = j + 1; k < 8; ++k) {
+        const double vr = __shfl_sync(0xffffffffu, ar[j], k);  // L(k, j)
+        const double vi = CP ? __shfl_sync(0xffffffffu, ai[j], k) : 0.0;
+        if (l >= k) {  // A(l, k) -= L(l, j) conj(L(k, j))
+          ar[k] -= ar[j] * vr + ai[j] * vi;
+          if (CP) ai[k] -= ai[j] * vr - ar[j] * vi;
+        }
+      }
+    }
+    if (lane < 8) {
 #pragma unroll
       for (int k = 0; k < 8; ++k) {
-        const bool in = k <= l && l < w;
-        ar[k] = in ? Xr[(b + k) * LD + b + l] : (k == l ? 1.0 : 0.0);
-        ai[k] = (in && CP) ? Xi[(b + k) * LD + b + l] : 0.0;
+        Lsr[l * 8 + k] = k <= l ? ar[k] : 0.0;
+        if (CP) Lsi[l * 8 + k] = k <= l ? ai[k] : 0.0;
+        if (k <= l && l < w) {
+          Xr[(b + k) * LD + b + l] = ar[k];
+          if (CP) Xi[(b + k) * LD + b + l] = ai[k];
+        }
+      }
+    }
+    __syncwarp();
+    if (lane < 8) {
+      // column c = lane of inv(L_ss): L_ss z = e_c, column form
+      const int c = lane;
+      double zr[8], zi[8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        zr[i] = i == c ? 1.0 : 0.0;
+        zi[i] = 0.0;
       }
 #pragma unroll
       for (int j = 0; j < 8; ++j) {
-        const double d = __shfl_sync(0xffffffffu, ar[j], j);
-        if (!(d > 0.0) && lane == 0 && j < w && info) atomicCAS(info, 0, col0 + b + j + 1);
-        const double ljj = sqrt(d), r = 1.0 / ljj;
-        rinv[j] = r;
-        if (l == j) {
-          ar[j] = ljj;
-          ai[j] = 0.0;
-        } else if (l > j) {
-          ar[j] *= r;
-          ai[j] *= r;
-        }
+        if (j >= c) {
+          zr[j] *= rinv[j];  // the diagonal of the factor is real
+          zi[j] *= rinv[j];
 #pragma unroll
-        for (int k = j + 1; k < 8; ++k) {
-          const double vr = __shfl_sync(0xffffffffu, ar[j], k);  // L(k, j)
-          const double vi = CP ? __shfl_sync(0xffffffffu, ai[j], k) : 0.0;
-          if (l >= k) {  // A(l, k) -= L(l, j) conj(L(k, j))
-            ar[k] -= ar[j] * vr + ai[j] * vi;
-            if (CP) ai[k] -= ai[j] * vr - ar[j] * vi;
+          for (int i = j + 1; i < 8; ++i) {
+            const double lr = Lsr[i * 8 + j], li = CP ? Lsi[i * 8 + j] : 0.0;
+            zr[i] -= lr * zr[j] - li * zi[j];
+            if (CP) zi[i] -= lr * zi[j] + li * zr[j];
           }
         }
       }
-      if (lane < 8) {
 #pragma unroll
-        for (int k = 0; k < 8; ++k) {
-          Lsr[l * 8 + k] = k <= l ? ar[k] : 0.0;
-          if (CP) Lsi[l * 8 + k] = k <= l ? ai[k] : 0.0;
-          if (k <= l && l < w) {
-            Xr[(b + k) * LD + b + l] = ar[k];
-            if (CP) Xi[(b + k) * LD + b + l] = ai[k];
-          }
-        }
-      }
-      __syncwarp();
-      if (lane < 8) {
-        // column c = lane of inv(L_ss): L_ss z = e_c, column form
-        const int c = lane;
-        double zr[8], zi[8];
-#pragma unroll
-        for (int i = 0; i < 8; ++i) {
-          zr[i] = i == c ? 1.0 : 0.0;
-          zi[i] = 0.0;
-        }
-#pragma unroll
-        for (int j = 0; j < 8; ++j) {
-          if (j >= c) {
-            zr[j] *= rinv[j];  // the diagonal of the factor is real
-            zi[j] *= rinv[j];
-#pragma unroll
-            for (int i = j + 1; i < 8; ++i) {
-              const double lr = Lsr[i * 8 + j], li = CP ? Lsi[i * 8 + j] : 0.0;
-              zr[i] -= lr * zr[j] - li * zi[j];
-              if (CP) zi[i] -= lr * zi[j] + li * zr[j];
-            }
-          }
-        }
-#pragma unroll
-        for (int i = 0; i < 8; ++i) {
-          Vr[i * 8 + c] = zr[i];
-          if (CP) Vi[i * 8 + c] = zi[i];
-        }
+      for (int i = 0; i < 8; ++i) {
+        Vr[i * 8 + c] = zr[i];
+        if (CP) Vi[i * 8 + c] = zi[i];
       }
     }
-    __syncthreads();
+  };
+
+  __syncthreads();
+  if (warp == 0) diag_factor(0);
+  __syncthreads();
+  const int nsteps = (n + 7) / 8;
+  for (int s = 0; s < nsteps; ++s) {
+    const int b = 8 * s;
     const int r0 = b + 8, R = n - r0;
     if (R <= 0) break;
     const int mt = (R + 15) / 16;
     const int k0 = 2 * t, k1 = k0 + 1;
-    // 2. panel: L(i, b..b+7) = A(i, b..b+7) inv(L_ss)^H, in place
+    // 1. panel: L(i, b..b+7) = A(i, b..b+7) inv(L_ss)^H, in place
     //    B operand (k, c) = conj(V(c, k))
     for (int tile = warp; tile < mt; tile += kPoThreads / 32) {
       const int m0 = r0 + tile * 16;
@@ -190,12 +207,14 @@ __global__ void __launch_bounds__(kPoThreads, 1)
       }
     }
     __syncthreads();
-    // 3. trailing update of the lower triangle: A(i, j) -= L(i, s) L(j, s)^H
-    //    16 x 8 tiles (i rows, j columns) meeting the triangle
+    // 2. trailing update of the lower triangle: A(i, j) -= L(i, s) L(j, s)^H
+    //    over 16 x 8 tiles (i rows, j columns) meeting the triangle.  Tile 0
+    //    holds the next diagonal block: warp 0 updates it and factors that
+    //    block while warps 1..7 update the rest (look-ahead).
     const int nt = (R + 7) / 8;
-    for (int tile = warp; tile < mt * nt; tile += kPoThreads / 32) {
+    auto upd_tile = [&](int tile) {
       const int ti = tile / nt, tj = tile % nt;
-      if (8 * tj > 16 * ti + 15) continue;  // wholly above the diagonal (warp-uniform)
+      if (8 * tj > 16 * ti + 15) return;  // wholly above the diagonal (warp-uniform)
       const int m0 = r0 + 16 * ti, n0 = r0 + 8 * tj;
       const double a_r[4] = {-Xr[(b + k0) * LD + m0 + g], -Xr[(b + k0) * LD + m0 + g + 8],
                              -Xr[(b + k1) * LD + m0 + g], -Xr[(b + k1) * LD + m0 + g + 8]};
@@ -209,7 +228,7 @@ __global__ void __launch_bounds__(kPoThreads, 1)
         ci[v] = CP ? Xi[col * LD + row] : 0.0;
       }
       if constexpr (CP) {
-        // C += (-L_i)(conj L_j): re += (-Lr)(Ljr) - (-Li)(-Lji) ; im += (-Lr)(-Lji) + (-Li)(Ljr)
+        // C += (-L_i)(conj L_j)
         const double a_i[4] = {-Xi[(b + k0) * LD + m0 + g], -Xi[(b + k0) * LD + m0 + g + 8],
                                -Xi[(b + k1) * LD + m0 + g], -Xi[(b + k1) * LD + m0 + g + 8]};
         const double a_ni[4] = {-a_i[0], -a_i[1], -a_i[2], -a_i[3]};
@@ -229,6 +248,13 @@ __global__ void __launch_bounds__(kPoThreads, 1)
           if (CP) Xi[col * LD + row] = ci[v];
         }
       }
+    };
+    if (warp == 0) {
+      upd_tile(0);
+      __syncwarp();
+      diag_factor(r0);  // step s + 1 (its block is final after tile 0)
+    } else {
+      for (int tile = 1 + (warp - 1); tile < mt * nt; tile += kPoThreads / 32 - 1) upd_tile(tile);
     }
     __syncthreads();
   }

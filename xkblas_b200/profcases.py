@@ -1,12 +1,14 @@
 """Small, self-contained cases for profiling single kernels with ncu:
 
-    python -m xkblas_b200.profcases dmma|ozaki|repack|trsm|potrf|batch
+    python -m xkblas_b200.profcases dmma|ozaki|repack|trsm|potrf|batch|copy
 
 dmma    DGEMM NN 4096^3 through xkb_cuda_gemm (k_gemm_dmma), two calls
 ozaki   the same through xkb_cuda_ozaki_gemm, 16 moduli (k_oz_* kernels)
 repack  the DGEMM with lda = ldb = 4097 (k_repack, then k_gemm_dmma)
 trsm    DTRSM L/L/N/N 4096 x 4096, diagonally dominant (k_trsm_block, GEMMs)
 potrf   DPOTRF lower 4096 (k_potrf_block, k_trsm_block, GEMMs)
+copy    beta scaling (k_scale, 8192^2) and the TRMM / SYMM materialisations
+        (k_tri_fill, k_copy2d, k_sym_fill, 4096^2)
 batch   150 mixed calls (70% DGEMM, 20% DTRSM, 10% ZGEMM; M, N, K
         log-uniform in [64, 2048]) as one xkb_cuda_batch launch (k_sched)
 
@@ -99,6 +101,26 @@ def main(case):
         arr = (X.BatchOp * len(ops))(*ops)
         for _ in range(2):
             assert lib.xkb_cuda_batch(arr, len(ops), 0, sp) == 0
+    elif case == "copy":
+        # HBM-bound helpers: beta scaling of C (k_scale, 8192^2), the
+        # triangle and symmetric materialisations of TRMM / SYMM
+        # (k_tri_fill, k_copy2d, k_sym_fill, 4096^2)
+        n = 8192
+        C = rnd(n, n)
+        keep += [C]
+        be = (ctypes.c_double * 2)(0.5, 0.0)
+        bp = ctypes.cast(be, ctypes.POINTER(ctypes.c_double))
+        for _ in range(2):
+            assert lib.xkb_cuda_scale(1, n, n, bp, C.data_ptr(), n, 0, 0, 0, sp) == 0
+        n = 4096
+        A, B, D = rnd(n, n), rnd(n, n), rnd(n, n)
+        keep += [A, B, D]
+        al = (ctypes.c_double * 2)(1.0, 0.0)
+        ap = ctypes.cast(al, ctypes.POINTER(ctypes.c_double))
+        for _ in range(2):
+            assert lib.xkb_cuda_trmm(1, 0, 1, 0, 0, n, n, ap, A.data_ptr(), n, B.data_ptr(), n, sp) == 0
+            assert lib.xkb_cuda_symm(1, 0, 0, 1, n, n, ap, A.data_ptr(), n, B.data_ptr(), n, bp,
+                                     D.data_ptr(), n, sp) == 0
     else:
         raise SystemExit("unknown case %r" % case)
     torch.cuda.synchronize()
