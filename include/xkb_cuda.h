@@ -211,6 +211,14 @@ int xkb_tune_clear(void);
 int xkb_cuda_potrf(int dtype, int uplo, int N, void* A, long lda, int* d_info, int ozaki,
                    void* stream);
 
+/* LU factorization without pivoting in place, A = L U (L unit lower, U
+ * upper), square N x N, s/d/c/z (replaces the reference's tile driver
+ * blas/zgetrf_nopiv.c:48-101).  d_info: a device int (may be NULL) that
+ * receives the first zero pivot, 1-based; it is not cleared here.  ozaki as
+ * for xkb_cuda_potrf. */
+int xkb_cuda_getrf_nopiv(int dtype, int N, void* A, long lda, int* d_info, int ozaki,
+                         void* stream);
+
 /* Device error word written by bounded waits (0 = none); clears it. */
 int xkb_cuda_take_device_error(void);
 

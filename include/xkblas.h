@@ -250,6 +250,19 @@ int xkblas_cpotrf_async(int uplo, int N, Complex32_t* A, int LDA);
 int xkblas_zpotrf_async(int uplo, int N, Complex64_t* A, int LDA);
 int xkblas_potrf_info(void);
 
+/* ---- LU factorization without pivoting (reference blas/zgetrf_nopiv.c:
+ * 48-101, a tile driver the reference builds but does not declare here).
+ * A = L U in place, L unit lower, U upper; square matrices only (M == N,
+ * else -2).  Stable for diagonally dominant or otherwise well-conditioned
+ * leading blocks, as any LU without pivoting.  The factors become final on
+ * the host after memory_coherent_async + sync; xkblas_getrf_info then gives
+ * the first zero pivot (1-based, 0 = none). */
+int xkblas_sgetrf_nopiv_async(int M, int N, float* A, int LDA);
+int xkblas_dgetrf_nopiv_async(int M, int N, double* A, int LDA);
+int xkblas_cgetrf_nopiv_async(int M, int N, Complex32_t* A, int LDA);
+int xkblas_zgetrf_nopiv_async(int M, int N, Complex64_t* A, int LDA);
+int xkblas_getrf_info(void);
+
 /* ---- synchronous forms: _async + memory_coherent_async on the output
  * (its written triangle for gemmt/syrk/herk/syr2k/her2k) + xkblas_sync +
  * xkblas_memory_invalidate_caches -- the sequence the reference's F77

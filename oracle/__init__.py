@@ -98,6 +98,14 @@ def trsm(side, uplo, trans, diag, alpha, A, B, nb=256):
     return B
 
 
+def getrf_nopiv(A, nb=256):
+    """LU without pivoting in place (tile algorithm of blas/zgetrf_nopiv.c:
+    48-101); returns the first zero pivot, 1-based (0 = none)."""
+    _f(A)
+    M, N = A.shape
+    return int(getattr(lib(), _pre(A) + "_xko_getrf_nopiv")(M, N, _p(A), A.shape[0], nb))
+
+
 def trmm(side, uplo, trans, diag, alpha, A, B, nb=256):
     _f(A), _f(B)
     M, N = B.shape

@@ -507,5 +507,48 @@ void OP(xko_trmm)(int side, int uplo, int trans, int diag, int M, int N,
   free(R);
   free(T);
 }
+/* LU factorization without pivoting, tile algorithm of
+ * blas/zgetrf_nopiv.c:48-101 (Chameleon pzgetrf_nopiv): for each diagonal
+ * tile k, the unblocked LU of A(k,k) (no pivoting), the column panel
+ * A(m,k) <- A(m,k) U(k,k)^-1 (trsm Right/Upper/NoTrans/NonUnit), the row
+ * panel A(k,n) <- L(k,k)^-1 A(k,n) (trsm Left/Lower/NoTrans/Unit), and the
+ * trailing updates A(m,n) -= A(m,k) A(k,n).  Returns the first zero pivot,
+ * 1-based (0 = none); the factorization continues past it. */
+int OP(xko_getrf_nopiv)(int M, int N, OT* A, int lda, int NB) {
+  long mt = OP(ntiles)(M, NB), nt = OP(ntiles)(N, NB);
+  long kt = mt < nt ? mt : nt;
+  int info = 0;
+  OT zone = 1, mzone = -1;
+  for (long k = 0; k < kt; k++) {
+    long tkm = (k == mt - 1) ? M - k * NB : NB;
+    long tkn = (k == nt - 1) ? N - k * NB : NB;
+    OT* Akk = OA(k, k);
+    long kmin = tkm < tkn ? tkm : tkn;
+    for (long j = 0; j < kmin; j++) {  /* unblocked right-looking LU of the tile */
+      OT d = Akk[j + j * lda];
+      if (d == (OT)0 && info == 0) info = (int)(k * NB + j + 1);
+      for (long i = j + 1; i < tkm; i++) Akk[i + j * lda] /= d;
+      for (long c = j + 1; c < tkn; c++)
+        for (long i = j + 1; i < tkm; i++) Akk[i + c * lda] -= Akk[i + j * lda] * Akk[j + c * lda];
+    }
+    for (long m = k + 1; m < mt; m++) {
+      long tmm = (m == mt - 1) ? M - m * NB : NB;
+      OP(tile_trsm)(XKO_RIGHT, XKO_UPPER, XKO_NOTRANS, XKO_NONUNIT, tmm, tkn, zone, Akk, lda,
+                    OA(m, k), lda);
+    }
+    for (long n = k + 1; n < nt; n++) {
+      long tnn = (n == nt - 1) ? N - n * NB : NB;
+      OP(tile_trsm)(XKO_LEFT, XKO_LOWER, XKO_NOTRANS, XKO_UNIT, tkm, tnn, zone, Akk, lda,
+                    OA(k, n), lda);
+      for (long m = k + 1; m < mt; m++) {
+        long tmm = (m == mt - 1) ? M - m * NB : NB;
+        OP(tile_gemm)(0, XKO_NOTRANS, XKO_NOTRANS, tmm, tnn, NB, mzone, OA(m, k), lda,
+                      OA(k, n), lda, zone, OA(m, n), lda, 0, 0);
+      }
+    }
+  }
+  return info;
+}
+
 #undef OA
 #undef OB

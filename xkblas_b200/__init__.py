@@ -109,6 +109,7 @@ def lib():
                                         c_long, c_vp]
         _lib.xkb_ozaki_default_moduli.argtypes = [c_long]
         _lib.xkb_cuda_potrf.argtypes = [c_int, c_int, c_int, c_vp, c_long, c_vp, c_int, c_vp]
+        _lib.xkb_cuda_getrf_nopiv.argtypes = [c_int, c_int, c_vp, c_long, c_vp, c_int, c_vp]
         _lib.xkb_cuda_batch.argtypes = [ctypes.POINTER(BatchOp), c_int, c_int, c_vp]
         _lib.xkb_cuda_batch_latency.argtypes = [ctypes.POINTER(ctypes.c_double), c_int]
         _lib.xkblas_get_stats.argtypes = [ctypes.POINTER(Stats)]

@@ -582,7 +582,57 @@ int potrf_async(int uplo, int N, T* A, int LDA) {
   return 0;
 }
 
+// LU without pivoting of a square matrix (reference blas/zgetrf_nopiv.c:
+// 48-101; the tile driver is built there but not declared in its headers).
+template <class T>
+int getrf_async(int M, int N, T* A, int LDA) {
+  if (M < 0) return -1;
+  if (N < 0 || N != M) return -2;
+  if (LDA < std::max(1, M)) return -4;
+  if (N == 0) return 0;
+  Guard g;
+  if (int e = ensure_init()) return rt_error(e);
+  Runtime& R = rt();
+  R.stats.calls++;
+  {
+    const double n = N;
+    R.stats.flops += (HT<T>::cplx ? 4.0 : 1.0) * (2.0 * n * n * n / 3.0 - n * n / 2.0 - n / 6.0);
+  }
+  int err;
+  if ((err = flush_pending())) return rt_error(err);
+  const size_t NB = auto_tilesize(KERN_GEMM, N, N, N), es = sizeof(T);
+  Desc* dA = get_desc(A, N, N, LDA, es, NB, &err);
+  if (!dA) return rt_error(err);
+  if ((err = make_valid(dA, 0, N, 0, N))) return rt_error(err);
+  if (!R.d_potrf_info) {
+    if (cudaMalloc(&R.d_potrf_info, sizeof(int)) != cudaSuccess) {
+      R.d_potrf_info = nullptr;
+      return rt_error(XKB_ENOMEM);
+    }
+  }
+  cudaMemsetAsync(R.d_potrf_info, 0, sizeof(int), R.s_comp);
+  const bool tc = R.math == XKBLAS_TENSOR_OP_MATH && (HT<T>::dt == XKB_D || HT<T>::dt == XKB_Z);
+  err = xkb_cuda_getrf_nopiv(HT<T>::dt, N, dev_ptr(dA, 0, 0), (long)dA->dld, R.d_potrf_info,
+                             tc ? (int)std::max<long>(R.ozaki_min_dim, 1) : 0, R.s_comp);
+  if (err) return rt_error(err);
+  mark_full_overwrite(dA, 0, N, 0, N);
+  return 0;
+}
+
 }  // namespace
+
+extern "C" int xkblas_sgetrf_nopiv_async(int M, int N, float* A, int LDA) {
+  return getrf_async<float>(M, N, A, LDA);
+}
+extern "C" int xkblas_dgetrf_nopiv_async(int M, int N, double* A, int LDA) {
+  return getrf_async<double>(M, N, A, LDA);
+}
+extern "C" int xkblas_cgetrf_nopiv_async(int M, int N, Complex32_t* A, int LDA) {
+  return getrf_async<Complex32_t>(M, N, A, LDA);
+}
+extern "C" int xkblas_zgetrf_nopiv_async(int M, int N, Complex64_t* A, int LDA) {
+  return getrf_async<Complex64_t>(M, N, A, LDA);
+}
 
 extern "C" int xkblas_spotrf_async(int uplo, int N, float* A, int LDA) {
   return potrf_async<float>(uplo, N, A, LDA);
@@ -596,6 +646,9 @@ extern "C" int xkblas_cpotrf_async(int uplo, int N, Complex32_t* A, int LDA) {
 extern "C" int xkblas_zpotrf_async(int uplo, int N, Complex64_t* A, int LDA) {
   return potrf_async<Complex64_t>(uplo, N, A, LDA);
 }
+// the factorization calls share one device info word
+extern "C" int xkblas_getrf_info(void) { return xkblas_potrf_info(); }
+
 extern "C" int xkblas_potrf_info(void) {
   Runtime& R = rt();
   std::lock_guard<std::recursive_mutex> g(R.mu);
