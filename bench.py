@@ -269,6 +269,23 @@ def other_configs(lib, torch, dev, sp, stream):
     out["dpotrf_l_8192"] = {"plain_tflops": fl / tp / 1e9, "ozaki_tflops": fl / to / 1e9,
                             "plain_ms": tp, "ozaki_ms": to, "info": max(info_p, int(info.item()))}
     del Bm, A0, A, info
+    # LU without pivoting (the zgetrf_nopiv tile driver): DGETRF 8192 on a
+    # diagonally dominant matrix; flops 2n^3/3 - n^2/2 + 5n/6 (reference flops.h)
+    A0 = u(n, n) + n * torch.eye(n, device=dev, dtype=torch.float64)
+    A = A0.clone()
+    info = torch.zeros(1, dtype=torch.int32, device=dev)
+    with torch.cuda.stream(stream):
+        rs = lambda: A.copy_(A0)
+        tp = timed(lambda: lib.xkb_cuda_getrf_nopiv(1, n, ctypes.c_void_p(A.data_ptr()), n,
+                                                    ctypes.c_void_p(info.data_ptr()), 0, sp), 3, rs)
+        info_p = int(info.item())
+        to = timed(lambda: lib.xkb_cuda_getrf_nopiv(1, n, ctypes.c_void_p(A.data_ptr()), n,
+                                                    ctypes.c_void_p(info.data_ptr()), 2048, sp), 3, rs)
+    fl = 2.0 * n ** 3 / 3.0 - n * n / 2.0 + 5.0 * n / 6.0
+    out["dgetrf_nopiv_8192"] = {"plain_tflops": fl / tp / 1e9, "ozaki_tflops": fl / to / 1e9,
+                                "plain_ms": tp, "ozaki_ms": to,
+                                "info": max(info_p, int(info.item()))}
+    del A0, A, info
     torch.cuda.empty_cache()
     return out
 

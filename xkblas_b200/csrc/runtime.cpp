@@ -65,6 +65,7 @@ int ensure_init() {
   }
   xkb::set_library_stream(R.s_comp);
   if (const char* b = getenv("XKBLAS_BATCH")) R.batch_on = atoi(b) != 0;
+  if (const char* u = getenv("XKBLAS_UNIFIED")) R.unified = R.unified || atoi(u) != 0;
   if (const char* t = getenv("XKBLAS_TILE_SIZE")) R.nb_param = (size_t)atol(t);
   else if (const char* b = getenv("XKBLAS_BLOC_SIZE")) R.nb_param = (size_t)atol(b);
   if (const char* m = getenv("XKBLAS_DEFAULT_MATH")) {
@@ -119,6 +120,11 @@ void scratch_free(void* p) {
 
 static void free_desc_memory(Desc* d) {
   Runtime& R = rt();
+  if (d->managed) {  // the caller's memory: only queued calls must run first
+    flush_pending();
+    d->dev = nullptr;
+    return;
+  }
   if (d->dev) {
     flush_pending();  // queued calls may use the buffer
     // D2H copies and kernels may still read the buffer: order the free
@@ -191,9 +197,23 @@ Desc* get_desc(const void* host, size_t M, size_t N, size_t ld, size_t esz, size
   d->nt = std::max<size_t>(1, (N + d->nb - 1) / d->nb);
   d->st.assign(d->mt * d->nt, 0);
   d->registered_init = true;
-  if ((*err = alloc_desc(d)) != XKB_OK) {
-    delete d;
-    return nullptr;
+  cudaPointerAttributes pa;
+  if (cudaPointerGetAttributes(&pa, host) == cudaSuccess && pa.type == cudaMemoryTypeManaged) {
+    // managed memory (xkblas_malloc_unified): the kernels use it in place;
+    // its pages are moved to the device ahead of the first kernel
+    d->managed = true;
+    d->dev = const_cast<void*>(host);
+    d->dld = ld;
+    d->st.assign(d->mt * d->nt, kDevValid);
+    if (cudaMemPrefetchAsync(host, ((N ? N - 1 : 0) * ld + M) * esz, R.device, R.s_comp) !=
+        cudaSuccess)
+      cudaGetLastError();  // advisory only
+  } else {
+    cudaGetLastError();
+    if ((*err = alloc_desc(d)) != XKB_OK) {
+      delete d;
+      return nullptr;
+    }
   }
   R.descs[host] = d;
   return d;
@@ -338,7 +358,8 @@ void mark_written(Desc* d, size_t r0, size_t r1, size_t c0, size_t c1, int uplo)
   const size_t tc0 = c0 / d->nb, tc1 = (c1 + d->nb - 1) / d->nb;
   for (size_t j = tc0; j < tc1; ++j)
     for (size_t i = tr0; i < tr1; ++i)
-      if (!uplo || tile_in_uplo(d, i, j, uplo)) d->tile(i, j) |= kDevValid | kHostStale;
+      if (!uplo || tile_in_uplo(d, i, j, uplo))
+        d->tile(i, j) |= d->managed ? kDevValid : (kDevValid | kHostStale);
 }
 
 void mark_full_overwrite(Desc* d, size_t r0, size_t r1, size_t c0, size_t c1) {
@@ -486,6 +507,19 @@ int make_valid_panels(const std::vector<std::pair<Desc*, size_t>>& ds,
 int coherent(Desc* d, int uplo, int memflag) {
   Runtime& R = rt();
   if (int e = flush_pending()) return e;
+  if (d->managed) {
+    // nothing to copy (the reference's unified mode returns here too,
+    // blas/xkblas.c:1959); move the pages back to the host once the queued
+    // work is done, so that host reads after xkblas_sync do not fault
+    cudaEvent_t ev = next_event();
+    cudaEventRecord(ev, R.s_comp);
+    cudaStreamWaitEvent(R.s_d2h, ev, 0);
+    if (cudaMemPrefetchAsync(d->host, ((d->N ? d->N - 1 : 0) * d->ld + d->M) * d->esz,
+                             cudaCpuDeviceId, R.s_d2h) != cudaSuccess)
+      cudaGetLastError();
+    d->col_ready.clear();
+    return XKB_OK;
+  }
   int e;
   if (uplo == 0 && !d->col_ready.empty()) {
     // written panel by panel: copy each panel back once its event fired;
@@ -656,6 +690,13 @@ int xkblas_get_device_properties(struct xkblas_dev_prop_t* prop) {
   if (!prop) return EINVAL;
   prop->device_count = xkblas_get_devicecount() > 0 ? 1 : 0;
   prop->has_unified = 0;
+  if (prop->device_count) {
+    int m = 0;
+    if (cudaDeviceGetAttribute(&m, cudaDevAttrConcurrentManagedAccess, rt().device) == cudaSuccess)
+      prop->has_unified = m ? 1 : 0;
+    else
+      cudaGetLastError();
+  }
   prop->arch = XKBLAS_ARCH_UNKNOWN;
   if (prop->device_count) {
     cudaDeviceProp p;
@@ -665,7 +706,16 @@ int xkblas_get_device_properties(struct xkblas_dev_prop_t* prop) {
   return 0;
 }
 
-int xkblas_force_set_unified(void) { return EINVAL; }
+int xkblas_force_set_unified(void) {
+  int dev = 0, managed = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&managed, cudaDevAttrManagedMemory, dev) != cudaSuccess || !managed) {
+    cudaGetLastError();
+    return EINVAL;
+  }
+  rt().unified = true;
+  return 0;
+}
 
 const char* xkblas_get_configuration(void) {
   return "xkblas-b200 0.6: sm_100a; FP64 DMMA (TMA+mbarrier) tile GEMM; Ozaki-II INT8 "
@@ -780,12 +830,38 @@ void xkblas_free(void* ptr, size_t sz) {
   free(ptr);
 }
 
+// Unified mode (reference blas/xkblas.c:155-220): managed memory when the
+// mode is on (xkblas_force_set_unified or XKBLAS_UNIFIED=1), else malloc.
+// Managed matrices are used in place by the kernels (no tile copies).
 int xkblas_malloc_unified(void** ptr, size_t size) {
   if (!ptr) return EINVAL;
-  *ptr = malloc(std::max<size_t>(size, 1));  // no unified memory path on B200+x86
-  return *ptr ? 0 : EINVAL;
+  Runtime& R = rt();
+  if (R.unified) {
+    if (cudaMallocManaged(ptr, std::max<size_t>(size, 1), cudaMemAttachGlobal) != cudaSuccess) {
+      cudaGetLastError();
+      *ptr = nullptr;
+      return ENOMEM;
+    }
+    return 0;
+  }
+  *ptr = malloc(std::max<size_t>(size, 1));
+  return *ptr ? 0 : ENOMEM;
 }
 int xkblas_free_unified(void* ptr) {
+  if (!ptr) return 0;
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, ptr) == cudaSuccess && a.type == cudaMemoryTypeManaged) {
+    Runtime& R = rt();
+    {
+      std::lock_guard<std::recursive_mutex> g(R.mu);
+      auto it = R.descs.find(ptr);  // a directory entry must not outlive the memory
+      if (it != R.descs.end()) drop_desc(it->second);
+      if (R.ready) cudaDeviceSynchronize();
+    }
+    cudaFree(ptr);
+    return 0;
+  }
+  cudaGetLastError();
   free(ptr);
   return 0;
 }

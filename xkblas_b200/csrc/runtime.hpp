@@ -49,6 +49,7 @@ struct Desc {
   std::vector<uint8_t> st;                // mt*nt tile states, column major
   bool registered_init = false;           // handle initialised (isinit)
   uint8_t pend = 0;                       // deferred calls: 1 read, 2 written
+  bool managed = false;                   // CUDA managed memory: used in place, never copied
   // columns finished on the compute stream: (end column, event recorded when
   // columns [previous end, end) are final), ascending.  Set by the panel
   // contraction (one entry per panel) and by an executor batch (one entry for
@@ -81,6 +82,7 @@ struct Runtime {
   size_t prec_param = 8;
   int math = XKBLAS_DEFAULT_MATH;
   int ozaki_moduli = 0;       // 0 = automatic
+  bool unified = false;       // xkblas_malloc_unified returns managed memory (XKBLAS_UNIFIED)
   long ozaki_min_dim = 2048;  // contractions smaller than this stay plain
                               // (measured crossover on a B200, autotune.py)
   Stats stats;
