@@ -184,7 +184,8 @@ int xkb_cuda_batch_release(void);
  * XKBLAS_TUNE_FILE at init).  Keys (built-in default):
  *   gemm_big_min_tiles      whole-matrix GEMM uses 128-wide tiles when it has
  *                           at least this many of them (SM count)
- *   ozaki_min_dim           tensor-op mode uses Ozaki when min(M,N,K) >= (2048)
+ *   ozaki_min_dim           tensor-op mode uses Ozaki when min(M,N,K) >= (2048;
+ *                           read per call; XKBLAS_OZAKI_MIN_DIM overrides)
  *   ozaki_moduli_k<=<K>     moduli count for contractions with inner size <= K
  *                           (the smallest band covering K; else the K rule)
  *   batch_schedule          executor claim order, 0 solves first / 1 gemms (0)

@@ -81,3 +81,4 @@ def test_getrf_nopiv_argument_codes(xk):
     assert lib.xkblas_dgetrf_nopiv_async(-1, 4, xk._ptr(A), 4) == -1
     assert lib.xkblas_dgetrf_nopiv_async(4, 3, xk._ptr(A), 4) == -2
     assert lib.xkblas_dgetrf_nopiv_async(4, 4, xk._ptr(A), 3) == -4
+    assert lib.xkblas_dgetrf_nopiv_async(0, 0, xk._ptr(A), 1) == 0  # empty: nothing to do

@@ -108,6 +108,7 @@ def test_potrf_argument_codes(xk):
     lib = xk.lib()
     A = np.zeros((4, 4), order="F")
     assert lib.xkblas_dpotrf_async(120, 4, xk._ptr(A), 4) == -2
+    assert lib.xkblas_dpotrf_async(122, 0, xk._ptr(A), 1) == 0  # empty: nothing to do
     assert lib.xkblas_dpotrf_async(LO, -1, xk._ptr(A), 4) == -5
     assert lib.xkblas_dpotrf_async(LO, 4, xk._ptr(A), 3) == -8
     assert lib.xkblas_dpotrf_async(LO, 0, xk._ptr(A), 1) == 0

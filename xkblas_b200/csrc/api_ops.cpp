@@ -95,7 +95,7 @@ bool use_ozaki(int dt, long m, long n, long k) {
   Runtime& R = rt();
   if (R.math != XKBLAS_TENSOR_OP_MATH) return false;
   if (dt != XKB_D && dt != XKB_Z) return false;
-  return std::min(m, std::min(n, k)) >= R.ozaki_min_dim && xkb_ozaki_default_moduli(k) > 0;
+  return std::min(m, std::min(n, k)) >= ozaki_min_dim() && xkb_ozaki_default_moduli(k) > 0;
 }
 
 // One contraction on device operands: plain DMMA or Ozaki.
@@ -532,7 +532,7 @@ int tr_async(int is_trsm, int side, int uplo, int transA, int diag, int M, int N
     err = xkb_cuda_scale(HT<T>::dt, M, N, z, dev_ptr(dB, 0, 0), (long)dB->dld, XKB_FULL, 0, 0,
                          R.s_comp);
   } else if (is_trsm) {
-    const int oz = tc ? (int)std::max<long>(R.ozaki_min_dim, 1) : 0;
+    const int oz = tc ? (int)std::max<long>(ozaki_min_dim(), 1) : 0;
     err = xkb_cuda_trsm(HT<T>::dt, sd, ul, opcode(transA), dg, M, N, al, dev_ptr(dA, 0, 0),
                         (long)dA->dld, dev_ptr(dB, 0, 0), (long)dB->dld, oz, R.s_comp);
   } else {
@@ -576,7 +576,7 @@ int potrf_async(int uplo, int N, T* A, int LDA) {
   const bool tc = R.math == XKBLAS_TENSOR_OP_MATH && (HT<T>::dt == XKB_D || HT<T>::dt == XKB_Z);
   err = xkb_cuda_potrf(HT<T>::dt, uplo == CblasLower ? XKB_LOWER : XKB_UPPER, N,
                        dev_ptr(dA, 0, 0), (long)dA->dld, R.d_potrf_info,
-                       tc ? (int)std::max<long>(R.ozaki_min_dim, 1) : 0, R.s_comp);
+                       tc ? (int)std::max<long>(ozaki_min_dim(), 1) : 0, R.s_comp);
   if (err) return rt_error(err);
   mark_written(dA, 0, N, 0, N, uplo);
   return 0;
@@ -613,7 +613,7 @@ int getrf_async(int M, int N, T* A, int LDA) {
   cudaMemsetAsync(R.d_potrf_info, 0, sizeof(int), R.s_comp);
   const bool tc = R.math == XKBLAS_TENSOR_OP_MATH && (HT<T>::dt == XKB_D || HT<T>::dt == XKB_Z);
   err = xkb_cuda_getrf_nopiv(HT<T>::dt, N, dev_ptr(dA, 0, 0), (long)dA->dld, R.d_potrf_info,
-                             tc ? (int)std::max<long>(R.ozaki_min_dim, 1) : 0, R.s_comp);
+                             tc ? (int)std::max<long>(ozaki_min_dim(), 1) : 0, R.s_comp);
   if (err) return rt_error(err);
   mark_full_overwrite(dA, 0, N, 0, N);
   return 0;

@@ -74,9 +74,9 @@ int ensure_init() {
   }
   // autotuner output (python -m xkblas_b200.autotune), then explicit settings
   if (const char* f = getenv("XKBLAS_TUNE_FILE")) xkb_tune_load(f);
-  R.ozaki_min_dim = (long)xkb_tune_get("ozaki_min_dim", (double)R.ozaki_min_dim);
+
   if (const char* s = getenv("XKBLAS_OZAKI_SLICES")) R.ozaki_moduli = atoi(s);
-  if (const char* s = getenv("XKBLAS_OZAKI_MIN_DIM")) R.ozaki_min_dim = atol(s);
+  if (const char* s = getenv("XKBLAS_OZAKI_MIN_DIM")) R.ozaki_min_env = atol(s);
   if (const char* s = getenv("XKBLAS_BATCH_FLUSH_MB")) R.batch_flush_env = (size_t)atol(s) << 20;
   R.ready = true;
   return XKB_OK;
@@ -91,6 +91,11 @@ EventRef new_event_ref() {
     return nullptr;
   }
   return r;
+}
+
+long ozaki_min_dim() {
+  const Runtime& R = rt();
+  return R.ozaki_min_env >= 0 ? R.ozaki_min_env : (long)xkb_tune_get("ozaki_min_dim", 2048.0);
 }
 
 cudaEvent_t next_event() {

@@ -83,7 +83,9 @@ struct Runtime {
   int math = XKBLAS_DEFAULT_MATH;
   int ozaki_moduli = 0;       // 0 = automatic
   bool unified = false;       // xkblas_malloc_unified returns managed memory (XKBLAS_UNIFIED)
-  long ozaki_min_dim = 2048;  // contractions smaller than this stay plain
+  // contractions smaller than this stay plain: XKBLAS_OZAKI_MIN_DIM, else the
+  // tuning key ozaki_min_dim (read per call), else 2048; see ozaki_min_dim()
+  long ozaki_min_env = -1;
                               // (measured crossover on a B200, autotune.py)
   Stats stats;
   int sticky_error = 0;
@@ -131,6 +133,9 @@ int coherent(Desc* d, int uplo, int memflag);
 // made to wait: the caller waits per panel.  The tiles become valid.
 int make_valid_panels(const std::vector<std::pair<Desc*, size_t>>& ds,
                       const std::vector<long>& bounds, std::vector<cudaEvent_t>& ev);
+// The Ozaki crossover in effect (min(M, N, K) at or above it: tensor-op mode
+// uses the Ozaki form).
+long ozaki_min_dim();
 // Launch the deferred calls (caller holds rt().mu); returns an XKB_* code.
 int flush_pending();
 // Launch a list of calls on the compute stream: one call through the
