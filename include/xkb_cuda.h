@@ -193,6 +193,9 @@ int xkb_cuda_batch_release(void);
  *                           tiles (96)
  *   oz_group_m              Ozaki INT8 GEMM raster: M tiles per group of the
  *                           persistent tile walk (8)
+ *   ozaki_panel_cols        public async API: column width of the panels a
+ *                           large Ozaki DGEMM streams through (1024; 2..32
+ *                           panels, multiples of 256 columns)
  *   batch_flush_mb          public async API: queued calls are launched once
  *                           their operands reach this many MiB (2048), so the
  *                           executor overlaps the uploads of later calls

@@ -168,7 +168,8 @@ int gemm_async(int transA, int transB, int M, int N, int K, const T* alpha, cons
     if (!dB) return rt_error(err);
     Desc* dC = get_desc(C, M, N, LDC, es, NB, &err);
     if (!dC) return rt_error(err);
-    const long np = std::min<long>(16, std::max<long>(2, N / 2048));
+    const long pc = std::max<long>(256, (long)xkb_tune_get("ozaki_panel_cols", 1024.0));
+    const long np = std::min<long>(32, std::max<long>(2, N / pc));
     const long w = ((N + np - 1) / np + 255) / 256 * 256;  // multiple of the INT8 tile width
     std::vector<long> bounds{0};
     while (bounds.back() < N) bounds.push_back(std::min<long>(N, bounds.back() + w));
