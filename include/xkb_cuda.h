@@ -193,6 +193,8 @@ int xkb_cuda_batch_release(void);
  *                           tiles (96)
  *   oz_group_m              Ozaki INT8 GEMM raster: M tiles per group of the
  *                           persistent tile walk (8)
+ *   oz_2cta                 Ozaki INT8 GEMM on CTA pairs (tcgen05 cta_group::2,
+ *                           256 x 256 tiles) instead of single CTAs (0)
  *   ozaki_panel_cols        public async API: column width of the panels a
  *                           large Ozaki DGEMM streams through (1024; 2..32
  *                           panels, multiples of 256 columns)

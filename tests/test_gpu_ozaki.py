@@ -207,3 +207,32 @@ def test_ozaki_k_beyond_int32_limit(tc):
         lib.xkb_tune_set(b"ozaki_min_dim", 2048.0)
     tc.invalidate_caches()
     assert checks.gemm_ratio(C, A @ B, A, B, np.zeros((M, N)), 1.0, 0.0, K) <= 3.0
+
+
+@pytest.mark.parametrize("mnk", [(300, 200, 513), (1024, 1024, 1024)])
+def test_ozaki_cta_pair_kernel_matches(xk, mnk):
+    """The CTA-pair INT8 GEMM (tuning key oz_2cta = 1) gives bit-identical
+    results to the single-CTA kernel (same residue products, exact)."""
+    import torch
+    M, N, K = mnk
+    lib = xk.lib()
+    g = torch.Generator(device="cuda").manual_seed(5)
+    dA = torch.rand(K, M, generator=g, dtype=torch.float64, device="cuda") - 0.5
+    dB = torch.rand(N, K, generator=g, dtype=torch.float64, device="cuda") - 0.5
+    out = []
+    for flag in (0.0, 1.0):
+        dC = torch.zeros(N, M, dtype=torch.float64, device="cuda")
+        ga = GemmArgs(1, 0, 0, M, N, K, dA.data_ptr(), M, dB.data_ptr(), K, dC.data_ptr(), M)
+        ga.alpha[0] = 1.0
+        lib.xkb_tune_set(b"oz_2cta", flag)
+        try:
+            torch.cuda.synchronize()
+            assert lib.xkb_cuda_ozaki_gemm(ctypes.byref(ga), 0, None) == 0
+            xk.sync()
+        finally:
+            lib.xkb_tune_set(b"oz_2cta", 0.0)
+        out.append(dC.clone())
+    assert torch.equal(out[0], out[1])
+    ref = dB @ dA  # row-major N x M view of the column-major C = A B
+    assert (out[0] - ref).abs().max().item() <= 4 * 2.0 ** -53 * K * 0.25 * 2
+    assert lib.xkb_cuda_take_device_error() == 0

@@ -586,6 +586,251 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
 }
 
 // ---------------------------------------------------------------------------
+// 3b. The same product on CTA pairs (a cluster of 2): tcgen05.mma.cta_group::2
+//     computes a 256 x 256 tile per pair, each CTA holding 128 rows of A and
+//     128 rows of B (its half of N) in shared memory and 128 rows of the
+//     accumulator in its TMEM.  Per CTA and stage: 16 KB of A + 16 KB of B
+//     for the work that takes 16 + 32 KB in the single-CTA kernel, so a third
+//     less operand traffic from L2 per MMA.  Both CTAs load their halves with
+//     TMA (no multicast); the loads signal the even CTA's stage barrier, the
+//     even CTA issues the MMAs and commits to the barriers of both CTAs, and
+//     the odd CTA's epilogue warps release the accumulator on the even CTA's
+//     barrier.
+constexpr int BM2 = 256, BN2 = 256;                 // pair tile
+constexpr int S2 = 6;                               // stages
+constexpr uint32_t H_STAGE = 128 * BKB;             // one 128-row operand half per stage
+constexpr uint32_t kPeerMask = 0xFEFFFFFFu;         // shared::cluster address of the even CTA
+
+__device__ __forceinline__ uint32_t cluster_rank() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+__device__ __forceinline__ uint32_t mapa_rank(uint32_t addr, uint32_t rank) {
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(addr), "r"(rank));
+  return r;
+}
+__device__ __forceinline__ void cluster_sync() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::
+                   : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_cluster(uint32_t cluster_addr) {
+  asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(cluster_addr)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx_cluster(uint32_t cluster_addr, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.release.cluster.shared::cluster.b64 _, [%0], %1;" ::"r"(
+                   cluster_addr),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void tma_load_3d_pair(void* dst, const CUtensorMap* m, int x, int y,
+                                                 int z, uint32_t bar_even) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(m)), "r"(x), "r"(y), "r"(z), "r"(bar_even)
+      : "memory");
+}
+__device__ __forceinline__ void tc_mma_i8_pair(uint32_t tmem, uint64_t ad, uint64_t bd,
+                                               uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::2.kind::i8 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
+      "l"(ad), "l"(bd), "r"(idesc), "r"(acc)
+      : "memory");
+}
+// commit the MMAs issued so far to the barrier at this offset in both CTAs
+__device__ __forceinline__ void tc_commit_pair(uint64_t* bar) {
+  asm volatile(
+      "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64"
+      " [%0], %1;" ::"r"(smem_u32(bar)),
+      "h"((uint16_t)3)
+      : "memory");
+}
+
+__device__ __forceinline__ bool oz_tile2(const GemmP& p, int t, int& mod, int& m0, int& n0) {
+  const int tiles_mn = p.tiles_m * p.tiles_n;
+  mod = t / tiles_mn;
+  const int r = t - mod * tiles_mn;
+  const int GROUP = p.group;
+  const int span = GROUP * p.tiles_n;
+  const int first_m = (r / span) * GROUP;
+  const int gsz = min(p.tiles_m - first_m, GROUP);
+  const int tm = first_m + (r % span) % gsz;
+  const int tn = (r % span) / gsz;
+  m0 = tm * BM2;
+  n0 = tn * BN2;
+  if (p.uplo == XKB_LOWER && (long)(m0 + BM2 - 1) + p.diag < (long)n0) return false;
+  if (p.uplo == XKB_UPPER && (long)m0 + p.diag > (long)(n0 + BN2 - 1)) return false;
+  return true;
+}
+
+__global__ void __launch_bounds__(kGemmThreads, 1)
+    k_oz_gemm2(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUtensorMap tB,
+               const GemmP p) {
+  extern __shared__ uint8_t sm_raw[];
+  uint8_t* sm =
+      reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(sm_raw) + 1023) & ~uintptr_t(1023));
+  uint8_t* sA = sm;
+  uint8_t* sB = sm + S2 * H_STAGE;
+  uint64_t* full = reinterpret_cast<uint64_t*>(sB + S2 * H_STAGE);
+  uint64_t* empty = full + S2;
+  uint64_t* accf = empty + S2;  // [2] accumulator ready (both CTAs)
+  uint64_t* acce = accf + 2;    // [2] accumulator drained (even CTA: both epilogues)
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(acce + 2);
+
+  const uint32_t rank = cluster_rank();
+  const int pair = blockIdx.x >> 1, npairs = gridDim.x >> 1;
+  const int total = p.tiles_m * p.tiles_n * p.nmod;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < S2; ++s) {
+      mbar_init(&full[s], 2);  // one arrive.expect_tx per CTA of the pair
+      mbar_init(&empty[s], 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&accf[b], 1);
+      mbar_init(&acce[b], 2 * kEpiWarps);
+    }
+    fence_barrier_init();
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(tslot)),
+                 "r"(kTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::: "memory");
+    tc_fence_before();
+  }
+  __syncthreads();
+  cluster_sync();  // barriers of both CTAs initialised before any cross-CTA signal
+  tc_fence_after();
+  const uint32_t tmem = *reinterpret_cast<volatile uint32_t*>(tslot);
+  const int KB = p.kblocks;
+
+  if (warp == 0) {
+    if (lane == 0) {  // ---- TMA producer (both CTAs): this CTA's halves of A and B
+      tma_prefetch(&tA);
+      tma_prefetch(&tB);
+      uint32_t it = 0;
+      bool ok = true;
+      for (int t = pair; t < total && ok; t += npairs) {
+        int mod, m0, n0;
+        if (!oz_tile2(p, t, mod, m0, n0)) continue;
+        for (int kb = 0; kb < KB; ++kb, ++it) {
+          const int s = it % S2;
+          const uint32_t ph = (it / S2) & 1;
+          if (!mbar_wait(&empty[s], ph ^ 1, kErrEmptyWait)) {
+            ok = false;
+            break;
+          }
+          // the even CTA's stage barrier: arrive through its cluster address,
+          // the pair-form TMA names it with the peer bit cleared
+          mbar_expect_tx_cluster(mapa_rank(smem_u32(&full[s]), 0), 2 * H_STAGE);
+          const uint32_t fe = smem_u32(&full[s]) & kPeerMask;
+          tma_load_3d_pair(sA + s * H_STAGE, &tA, kb * BKB, m0 + 128 * (int)rank, mod, fe);
+          tma_load_3d_pair(sB + s * H_STAGE, &tB, kb * BKB, n0 + 128 * (int)rank, mod, fe);
+        }
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0 && rank == 0) {  // ---- MMA issuer (even CTA)
+      // kind::i8: D s32, A s8, B s8, K-major; N = 256, M = 256 (the pair)
+      const uint32_t idesc = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN2 >> 3) << 17) |
+                             ((uint32_t)(BM2 >> 4) << 24);
+      uint32_t it = 0, tl = 0;
+      bool ok = true;
+      for (int t = pair; t < total && ok; t += npairs) {
+        int mod, m0, n0;
+        if (!oz_tile2(p, t, mod, m0, n0)) continue;
+        const int b = tl & 1;
+        const uint32_t aph = (tl >> 1) & 1;
+        if (!mbar_wait(&acce[b], aph ^ 1, kErrAccWait)) break;  // drained in both CTAs
+        tc_fence_after();
+        const uint32_t d = tmem + (uint32_t)(b * BN2);
+        for (int kb = 0; kb < KB; ++kb, ++it) {
+          const int s = it % S2;
+          const uint32_t ph = (it / S2) & 1;
+          if (!mbar_wait(&full[s], ph, kErrFullWait)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t a0 = smem_u32(sA + s * H_STAGE), b0 = smem_u32(sB + s * H_STAGE);
+#pragma unroll
+          for (int k = 0; k < BKB / 32; ++k)
+            tc_mma_i8_pair(d, desc_sw128(a0 + 32 * k), desc_sw128(b0 + 32 * k), idesc,
+                           (kb | k) != 0 ? 1u : 0u);
+          tc_commit_pair(&empty[s]);  // stage s free in both CTAs once read
+        }
+        tc_commit_pair(&accf[b]);  // accumulator b complete in both CTAs
+        ++tl;
+      }
+    }
+  } else {
+    // ---- epilogue (both CTAs): warps 2..5, TMEM lanes 32*(warp%4) .. +31
+    const int q = warp & 3;
+    const uint32_t ae0 = mapa_rank(smem_u32(&acce[0]), 0), ae1 = mapa_rank(smem_u32(&acce[1]), 0);
+    uint32_t tl = 0;
+    for (int t = pair; t < total; t += npairs) {
+      int mod, m0, n0;
+      if (!oz_tile2(p, t, mod, m0, n0)) continue;
+      const int b = tl & 1;
+      const uint32_t aph = (tl >> 1) & 1;
+      const bool got = mbar_wait(&accf[b], aph, kErrAccWait);
+      if (!__all_sync(0xffffffffu, got)) break;  // uniform and converged for tcgen05.ld
+      tc_fence_after();
+      const int row = m0 + 128 * (int)rank + q * 32 + lane;
+      const uint32_t tbase = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * BN2);
+      const int pm = p.p[mod];
+      const double ip = p.invp[mod];
+      uint8_t* plane = p.R + (size_t)mod * (size_t)p.Mpad * (size_t)p.Npad;
+      for (int c = 0; c < BN2 / 16; ++c) {
+        uint32_t v[16];
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
+            "%14,%15}, [%16];"
+            : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+              "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]),
+              "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+            : "r"(tbase + (uint32_t)(c * 16)));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        if (c == BN2 / 16 - 1) {
+          // every column of buffer b is in registers: release it to the even CTA
+          tc_fence_before();
+          __syncwarp();
+          if (lane == 0) mbar_arrive_cluster(b ? ae1 : ae0);
+        }
+#pragma unroll
+        for (int e = 0; e < 16; ++e) {
+          const int acc = (int)v[e];
+          const int qq = (int)floor((double)acc * ip);
+          int r = acc - qq * pm;
+          if (r < 0) r += pm;
+          else if (r >= pm) r -= pm;
+          const size_t col = (size_t)(n0 + c * 16 + e);
+          __stcs(plane + col * (size_t)p.Mpad + (size_t)row, (unsigned char)r);
+        }
+      }
+      ++tl;
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  cluster_sync();  // both CTAs done with the pair's TMEM and barriers
+  if (warp == 1) {
+    __syncwarp();
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(kTmemCols)
+                 : "memory");
+  }
+}
+
+// ---------------------------------------------------------------------------
 // 4. CRT reconstruction + scaling + alpha/beta, 4 consecutive rows per thread.
 struct CrtP {
   int M, N;
@@ -871,6 +1116,41 @@ static int launch_gemm(const int8_t* Ap, long a_rows, const int8_t* Bp, long b_r
     p.p[m] = c->p[m];
     p.invp[m] = c->invp_d[m];
   }
+  const long total2 = (Mpad % BM2 == 0 && Npad % BN2 == 0)
+                         ? (Mpad / BM2) * (Npad / BN2) * (long)c->nmod : 0;
+  if (total2 > 0 && tune("oz_2cta", 0.0) != 0.0 && sm_count() >= 2) {
+    // CTA pairs: 256 x 256 tiles, each CTA loading 128-row halves of A and B
+    CUtensorMap tB2;
+    if (!encode_planes(&tB2, Bp, Kpad, b_rows, c->nmod, 128)) return XKB_EINVAL;
+    p.tiles_m = (int)(Mpad / BM2);
+    p.tiles_n = (int)(Npad / BN2);
+    p.group = std::max(1, std::min(p.tiles_m, (int)tune("oz_group_m", 8.0)));
+    const size_t smem2 = 1024 + S2 * (size_t)(2 * H_STAGE) + (2 * S2 + 4) * 8 + 16;
+    static bool attr2 = false;
+    if (!attr2) {
+      if (cudaFuncSetAttribute(k_oz_gemm2, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)smem2) != cudaSuccess)
+        return XKB_ECUDA;
+      attr2 = true;
+    }
+    const long pairs = std::min<long>(total2, sm_count() / 2);
+    cudaLaunchConfig_t cfg;
+    std::memset(&cfg, 0, sizeof(cfg));
+    cfg.gridDim = dim3((unsigned)(2 * pairs));
+    cfg.blockDim = dim3(kGemmThreads);
+    cfg.dynamicSmemBytes = smem2;
+    cfg.stream = st;
+    cudaLaunchAttribute la[1];
+    la[0].id = cudaLaunchAttributeClusterDimension;
+    la[0].val.clusterDim.x = 2;
+    la[0].val.clusterDim.y = 1;
+    la[0].val.clusterDim.z = 1;
+    cfg.attrs = la;
+    cfg.numAttrs = 1;
+    if (cudaLaunchKernelEx(&cfg, k_oz_gemm2, tA, tB2, p) != cudaSuccess) return XKB_ECUDA;
+    count_launch();
+    return cudaPeekAtLastError() == cudaSuccess ? XKB_OK : XKB_ECUDA;
+  }
   const size_t smem = 1024 + S * (size_t)(A_STAGE + B_STAGE) + (2 * S + 4) * 8 + 16;
   static bool attr = false;
   if (!attr) {
@@ -931,7 +1211,7 @@ extern "C" int xkb_cuda_ozaki_gemm(const xkb_gemm_args* a, int nmod, void* strea
   // kernel); the zero pads contribute nothing to the products
   const long kofs2 = (long)rup(K, 64);
   const long Kpad = cplx ? (long)rup(2 * kofs2, BKB) : (long)rup(K, BKB);
-  const long Mpad = (long)rup(M, BM), Npad = (long)rup(N, BN);
+  const long Mpad = (long)rup(M, BM2), Npad = (long)rup(N, BN);  // BM2: CTA-pair tiles
   const bool akc = a->opA != XKB_OP_N, bkc = a->opB == XKB_OP_N;
   // C = A A^T (or A^T A): op(B)^T's rows are op(A)'s rows, one residue buffer
   // serves both operands; it then holds max(Mpad, Npad) rows per plane
@@ -1100,7 +1380,7 @@ extern "C" int xkb_cuda_ozaki_gemm_panels(const xkb_gemm_args* a, int nmod, void
   const Consts* c = consts_for(nmod);
   if (!c) return XKB_ERANGE;
   const int M = a->M, K = a->K;
-  const long Kpad = (long)rup(K, BKB), Mpad = (long)rup(M, BM);
+  const long Kpad = (long)rup(K, BKB), Mpad = (long)rup(M, BM2);
   long wmax = 0;
   for (int q = 0; q < npanel; ++q) wmax = std::max(wmax, bounds[q + 1] - bounds[q]);
   const long Wpad = (long)rup((size_t)wmax, BN);
