@@ -592,8 +592,8 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
 //     accumulator in its TMEM.  Per CTA and stage: 16 KB of A + 16 KB of B
 //     for the work that takes 16 + 32 KB in the single-CTA kernel, so a third
 //     less operand traffic from L2 per MMA.  Both CTAs load their halves with
-//     TMA (no multicast); the loads signal the even CTA's stage barrier, the
-//     even CTA issues the MMAs and commits to the barriers of both CTAs, and
+//     TMA; the loads signal the even CTA's stage barrier, the even CTA
+//     issues the MMAs and commits to the barriers of both CTAs, and
 //     the odd CTA's epilogue warps release the accumulator on the even CTA's
 //     barrier.
 constexpr int BM2 = 256, BN2 = 256;                 // pair tile
@@ -643,12 +643,13 @@ __device__ __forceinline__ void tc_mma_i8_pair(uint32_t tmem, uint64_t ad, uint6
       : "memory");
 }
 // commit the MMAs issued so far to the barrier at this offset in both CTAs
+// (one commit per CTA, addressed through the cluster window)
 __device__ __forceinline__ void tc_commit_pair(uint64_t* bar) {
-  asm volatile(
-      "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64"
-      " [%0], %1;" ::"r"(smem_u32(bar)),
-      "h"((uint16_t)3)
-      : "memory");
+#pragma unroll
+  for (uint32_t r = 0; r < 2; ++r)
+    asm volatile("tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::
+                     "r"(mapa_rank(smem_u32(bar), r))
+                 : "memory");
 }
 
 __device__ __forceinline__ bool oz_tile2(const GemmP& p, int t, int& mod, int& m0, int& n0) {
