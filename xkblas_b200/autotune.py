@@ -15,15 +15,22 @@ Choices (keys of the table, see include/xkb_cuda.h):
                           product is at most half the plain FP64 kernel's on
                           inputs with exponents spread over [-20, 20] per row
                           of A and per column of B);
+  oz_2cta                 Ozaki INT8 GEMM on single CTAs or CTA pairs (timed
+                          on a square Ozaki DGEMM);
+  ozaki_panel_cols        column width of the panels a public-API Ozaki DGEMM
+                          streams through (timed end to end with pinned host
+                          matrices, 8192^3, caches dropped per call);
   batch_schedule,         tile-task executor: claim order and 128-row tile
   batch_tile128_min_rows  threshold (timed on a mixed batch of uneven calls).
 
-Each measurement uses seeded synthetic device matrices and CUDA events; the
-table records the measured times beside each choice.
+Each measurement uses seeded synthetic matrices and CUDA events (the panel
+sweep: host clock around the public calls); the table records the measured
+times beside each choice.
 """
 import argparse
 import ctypes
 import math
+import time
 import sys
 
 import numpy as np
@@ -220,11 +227,73 @@ class Tuner:
         self.table["batch_schedule"] = (best[1], "%.2f ms best of the sweep" % best[0])
         self.table["batch_tile128_min_rows"] = (best[2], "%.2f ms best of the sweep" % best[0])
 
+    def ozaki_kernel(self):
+        """Single-CTA or CTA-pair INT8 GEMM (oz_2cta)."""
+        lib = self.lib
+        n = 2048 if self.quick else 4096
+        A, B, C = self.rnd(n, n), self.rnd(n, n), self.rnd(n, n)
+        a = self.args(A, B, C, n, n, n)
+        tm = {}
+        for v in (0.0, 1.0):
+            lib.xkb_tune_set(b"oz_2cta", v)
+            tm[v] = self.time(lambda: lib.xkb_cuda_ozaki_gemm(ctypes.byref(a), 0, self.sp), 5)
+        best = 1 if tm[1.0] < tm[0.0] else 0
+        lib.xkb_tune_set(b"oz_2cta", float(best))
+        self.log("ozaki %d: single CTA %.3f ms, CTA pair %.3f ms" % (n, tm[0.0], tm[1.0]))
+        self.table["oz_2cta"] = (best, "%d^3: single %.3f ms, pair %.3f ms" % (n, tm[0.0], tm[1.0]))
+
+    def ozaki_panels(self):
+        """Column-panel width of the public-API Ozaki DGEMM (ozaki_panel_cols),
+        timed end to end with pinned host matrices, caches dropped per call."""
+        t, X, lib = self.torch, self.X, self.lib
+        n = 4096 if self.quick else 8192
+        hs = [t.empty((n, n), dtype=t.float64, pin_memory=True).numpy() for _ in range(3)]
+        rng = np.random.default_rng(3)
+        for h in hs[:2]:
+            h[...] = rng.random((n, n)) - 0.5
+        one, zero = np.array([1.0]), np.array([0.0])
+        P = ctypes.c_void_p
+        old_min = lib.xkb_tune_get(b"ozaki_min_dim", 2048.0)
+        lib.xkb_tune_set(b"ozaki_min_dim", float(min(old_min, n)))
+        X.set_modemath(X.XKBLAS_TENSOR_OP_MATH)
+
+        def call():
+            assert lib.xkblas_dgemm_async(111, 111, n, n, n, P(one.ctypes.data), P(hs[0].ctypes.data),
+                                          n, P(hs[1].ctypes.data), n, P(zero.ctypes.data),
+                                          P(hs[2].ctypes.data), n) == 0
+            lib.xkblas_memory_coherent_async(0, 0, n, n, P(hs[2].ctypes.data), n, 8)
+            assert lib.xkblas_sync() == 0
+            lib.xkblas_memory_invalidate_caches()
+
+        res = {}
+        try:
+            for cols in (512, 1024, 2048):
+                if n // cols < 2:
+                    continue
+                lib.xkb_tune_set(b"ozaki_panel_cols", float(cols))
+                call()
+                best = math.inf
+                for _ in range(2 if self.quick else 3):
+                    t0 = time.perf_counter()
+                    call()
+                    best = min(best, time.perf_counter() - t0)
+                res[cols] = best * 1e3
+                self.log("ozaki panels %d^3, %d columns: %.2f ms" % (n, cols, res[cols]))
+        finally:
+            X.set_modemath(X.XKBLAS_DEFAULT_MATH)
+            lib.xkb_tune_set(b"ozaki_min_dim", old_min)
+        cols = min(res, key=res.get)
+        lib.xkb_tune_set(b"ozaki_panel_cols", float(cols))
+        self.table["ozaki_panel_cols"] = (cols, "%d^3 e2e: " % n + ", ".join(
+            "%d: %.1f ms" % (c, v) for c, v in res.items()))
+
     def run(self):
         self.lib.xkb_tune_clear()
         self.gemm_tiles()
         self.ozaki_crossover()
         self.moduli()
+        self.ozaki_kernel()
+        self.ozaki_panels()
         self.batch()
         return self.table
 
