@@ -52,9 +52,11 @@ struct Consts {
   uint32_t offh[kMaxMod];               // off + floor(p/2): symmetric residues
   uint32_t magic[kMaxMod];              // ceil(2^32 / p): exact quotients below 2^21
   int half[kMaxMod];                    // floor(p/2)
-  uint32_t crt[kMaxMod][4];             // (P/p)((P/p)^-1 mod p) mod P, 32-bit limbs
-  uint32_t P[4], Ph[4];                 // P and floor(P/2)
-  double Pd, invPd;
+  // CRT weights w = (P/p)((P/p)^-1 mod p) mod P split as w = w1 + w2: w1 the
+  // bits of w from 2^csplit up (exact double, <= 41 significant bits), w2
+  // the rest rounded to double; P = P1 + P2 the same way
+  double w1[kMaxMod], w2[kMaxMod];
+  double P1d, P2d, Pd, invPd;
 };
 
 // ---------------------------------------------------------------------------
@@ -126,6 +128,12 @@ static bool make_consts(int n, Consts* c) {
   for (int i = 0; i < n; ++i) P *= (u128)m[i];
   // budget: ||A'_i||_2 ||B'_j||_2 <= 2^(2H) (1+tiny) < P/2
   c->H = (int)std::floor((log2P(n) - 1.0) / 2.0) - 1;
+  // split point of the CRT weights: sum_l r_l w1_l < 4080 P < 2^(bits(P)+12)
+  // must be an integer multiple of 2^csplit below 2^(53+csplit)
+  int bitsP = 0;
+  for (u128 t = P; t; t >>= 1) ++bitsP;
+  const int csplit = std::max(0, bitsP + 12 - 53);
+  const u128 low = csplit ? (((u128)1 << csplit) - 1) : 0;
   for (int i = 0; i < n; ++i) {
     const int p = m[i];
     c->p[i] = p;
@@ -149,13 +157,11 @@ static bool make_consts(int n, Consts* c) {
     const u128 Mi = P / (u128)p;
     const int inv = inv_mod((int)(Mi % (u128)p), p);
     const u128 w = mulmod(Mi, (u128)inv, P);
-    for (int t = 0; t < 4; ++t) c->crt[i][t] = (uint32_t)(w >> (32 * t));
+    c->w1[i] = std::ldexp((double)(uint64_t)(w >> csplit), csplit);  // < 2^41 units: exact
+    c->w2[i] = (double)(w & low);
   }
-  const u128 Ph = P >> 1;
-  for (int t = 0; t < 4; ++t) {
-    c->P[t] = (uint32_t)(P >> (32 * t));
-    c->Ph[t] = (uint32_t)(Ph >> (32 * t));
-  }
+  c->P1d = std::ldexp((double)(uint64_t)(P >> csplit), csplit);
+  c->P2d = (double)(P & low);
   c->Pd = (double)P;
   c->invPd = 1.0 / c->Pd;
   return true;
@@ -848,50 +854,42 @@ struct CrtP {
   long diag;
 };
 
-// Exact recombination.  S = sum_l r_l w_l (< 2^12 P, 160 bits as 32-bit
-// limbs).  The shifts keep |C'| <= P/8, so the wanted value is S - qP with
-// q = round(S / P): a double estimate of S/P is within 2^-38 of the truth and
-// S/P lies within 1/8 of an integer, so q is exact and no correction or
-// range mapping is needed.  |S - qP| < 2^124: it is computed modulo 2^128 and
-// read as a signed 128-bit integer, then converted to double (two roundings).
+// Recombination on the FP64 pipe.  S = sum_l r_l w_l < 4080 P; the shifts
+// keep |C'| <= P/8, so the wanted value is S - qP with q = round(S / P).
+// With w = w1 + w2 (w1: multiples of 2^csplit, <= 41 significant bits):
+//  - S1 = sum r_l w1_l is exact (8-bit x 41-bit products, multiples of
+//    2^csplit, sum below 2^(53+csplit));
+//  - q = rint(S1 / P) is exact: S2 / P < 2^-28 and S / P lies within 1/8 of
+//    an integer (q < 2^12);
+//  - S1 - q P1 is exact (a 53-bit product, the difference a multiple of
+//    2^csplit below 2^(42+csplit));
+//  - S2 - q P2 carries absolute errors of order 2^(csplit-37) plus the
+//    rounding of w2 (2^43 at 16 moduli), far below the 2^(2H-61) sqrt(K)
+//    already left by rounding the scaled operands to integers.
+// 2 FP64 FMAs per modulus and element against 4 64-bit integer multiply-adds
+// for a 128-bit limb sum: the kernel moves from the integer multiply pipe to
+// the FP64 pipe, which nothing else here uses.
 template <int NM>
 __device__ __forceinline__ double crt_value(const uint32_t (&r)[NM], const Consts& c) {
-  unsigned long long a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+  double s1 = 0.0, s2 = 0.0;
 #pragma unroll
   for (int m = 0; m < NM; ++m) {
-    const unsigned long long rv = r[m];
-    a0 += rv * c.crt[m][0];
-    a1 += rv * c.crt[m][1];
-    a2 += rv * c.crt[m][2];
-    a3 += rv * c.crt[m][3];
+    const double rv = (double)r[m];
+    s1 = fma(rv, c.w1[m], s1);
+    s2 = fma(rv, c.w2[m], s2);
   }
-  a1 += a0 >> 32;
-  a2 += a1 >> 32;
-  a3 += a2 >> 32;
-  const unsigned long long lo = (a0 & 0xffffffffull) | (a1 << 32);
-  const unsigned long long hi = (a2 & 0xffffffffull) | (a3 << 32);  // S mod 2^128
-  const double Sd = (double)(a3 >> 32) * 340282366920938463463374607431768211456.0 +
-                    (double)(a3 & 0xffffffffull) * 79228162514264337593543950336.0 +
-                    (double)(a2 & 0xffffffffull) * 18446744073709551616.0;
-  const unsigned long long q = (unsigned long long)rint(Sd * c.invPd);
-  const unsigned long long Plo = ((unsigned long long)c.P[1] << 32) | c.P[0];
-  const unsigned long long Phi = ((unsigned long long)c.P[3] << 32) | c.P[2];
-  const unsigned long long qlo = q * Plo;
-  const unsigned long long qhi = q * Phi + __umul64hi(q, Plo);
-  unsigned long long rlo = lo - qlo;
-  unsigned long long rhi = hi - qhi - (lo < qlo ? 1ull : 0ull);
-  const bool neg = (long long)rhi < 0;
-  if (neg) {
-    rlo = ~rlo + 1ull;
-    rhi = ~rhi + (rlo == 0 ? 1ull : 0ull);
-  }
-  const double v = fma((double)rhi, 18446744073709551616.0, (double)rlo);
-  return neg ? -v : v;
+  const double q = rint(s1 * c.invPd);
+  return fma(-q, c.P1d, s1) + fma(-q, c.P2d, s2);
 }
 
 // x * 2^e for the shift range used here (|e| <= 2000), exact unless the
 // result under/overflows
 __device__ __forceinline__ double scale2(double x, int e) {
+  // x normal and x 2^e normal: add e to the exponent field
+  const int hi = __double2hiint(x);
+  const int ex = (hi >> 20) & 0x7ff;
+  if (ex != 0 && (unsigned)(ex + e - 1) < 2046u)
+    return __hiloint2double(hi + (int)((unsigned)e << 20), __double2loint(x));
   const int e1 = e / 2, e2 = e - e1;
   return x * pow2(e1) * pow2(e2);
 }
@@ -920,7 +918,7 @@ __device__ __forceinline__ void crt_quad(const CrtP& p, const Consts& c, long i0
 }
 
 template <int NM>
-__global__ void __launch_bounds__(256) k_oz_crt(const CrtP p, const Consts c) {
+__global__ void __launch_bounds__(256, 4) k_oz_crt(const CrtP p, const Consts c) {
   const long iq = (long)blockIdx.x * blockDim.x + threadIdx.x;  // row quad
   const long i0 = iq * 4;
   if (i0 >= p.M) return;
@@ -979,7 +977,7 @@ __global__ void __launch_bounds__(256) k_oz_crt(const CrtP p, const Consts c) {
 
 // Complex first pass: Re(op(A)op(B)) (unscaled by alpha) into a scratch M x N.
 template <int NM>
-__global__ void __launch_bounds__(256) k_oz_crt_store(const CrtP p, const Consts c, double* out) {
+__global__ void __launch_bounds__(256, 4) k_oz_crt_store(const CrtP p, const Consts c, double* out) {
   const long iq = (long)blockIdx.x * blockDim.x + threadIdx.x;
   const long i0 = iq * 4;
   if (i0 >= p.M) return;
