@@ -323,6 +323,25 @@ void xkblas_reset_stats(void);
 /* Last device-side error word (0 = none); set by bounded waits in kernels. */
 int  xkblas_last_device_error(void);
 
+/* ---- added: event trace as the CSV tables of the reference's trace
+ * converter (bin/ukilli.cpp:875-1115; the reference records with
+ * KAAPI_RECORD_TRACE=1, kaapi/kaapi_trace_lib.c:754-840, and converts post
+ * mortem).  Recording is off by default; XKBLAS_TRACE_DIR=<dir> turns it on
+ * at initialisation and writes the tables into <dir> at the last
+ * xkblas_finalize.  Tables (same headers and columns as the converter):
+ *   kern.csv      kernel launches: Resource,Type,Stream,Push,Start,End,
+ *                 Duration,Name ("<call>/<kernel>"),TaskId
+ *   cpy.csv       host<->device copies: ...,Size (bytes),Dir (1 H2D, 2 D2H)
+ *   call.csv      API calls: Resource,Level,Start,End (the xkblas_sync that
+ *                 completed it),Duration,Name,NParam,Param0..Param15
+ *   task.csv      API calls as host tasks (entry to return)
+ *   parallel.csv  the host threads and the GPU over the recording
+ * Times are seconds since recording started; device times come from CUDA
+ * events on the launching stream.  Export drains what it wrote. */
+int      xkblas_trace_record(int on);           /* returns the previous state */
+int      xkblas_trace_export(const char* dir);  /* 0, EINVAL or EIO */
+uint64_t xkblas_trace_dropped(void);            /* events not recorded (table full) */
+
 #ifdef __cplusplus
 }
 #endif

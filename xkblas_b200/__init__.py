@@ -113,6 +113,8 @@ def lib():
         _lib.xkb_cuda_batch.argtypes = [ctypes.POINTER(BatchOp), c_int, c_int, c_vp]
         _lib.xkb_cuda_batch_latency.argtypes = [ctypes.POINTER(ctypes.c_double), c_int]
         _lib.xkblas_get_stats.argtypes = [ctypes.POINTER(Stats)]
+        _lib.xkblas_trace_export.argtypes = [ctypes.c_char_p]
+        _lib.xkblas_trace_dropped.restype = ctypes.c_uint64
     return _lib
 
 
@@ -152,6 +154,20 @@ def reset_stats():
 
 def invalidate_caches():
     return lib().xkblas_memory_invalidate_caches()
+
+
+def trace_record(on=True):
+    """Switch event recording on or off; returns the previous state."""
+    return bool(lib().xkblas_trace_record(1 if on else 0))
+
+
+def trace_export(directory):
+    """Write the recorded events as kern.csv, cpy.csv, call.csv, task.csv and
+    parallel.csv into `directory` (the column layout of the reference's trace
+    converter, bin/ukilli.cpp); raises on failure."""
+    r = lib().xkblas_trace_export(os.fsencode(directory))
+    if r != 0:
+        raise XkblasError("xkblas_trace_export failed: %d" % r)
 
 
 def kernel_count():

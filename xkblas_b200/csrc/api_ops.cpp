@@ -21,6 +21,7 @@
 #include <cerrno>
 #include <cmath>
 #include <complex>
+#include <cstring>
 
 #include "runtime.hpp"
 
@@ -50,6 +51,18 @@ struct HT<Complex64_t> {
   static constexpr int dt = XKB_Z;
   static constexpr bool cplx = true;
 };
+
+// Call name for the trace (reference names: precision letter + operation,
+// e.g. "dgemm", blas/zgemm.c:262), 7 characters at most.
+struct OpName {
+  char s[8];
+  OpName(int dt, const char* op) {
+    s[0] = "sdcz"[dt == XKB_S ? 0 : dt == XKB_D ? 1 : dt == XKB_C ? 2 : 3];
+    std::strncpy(s + 1, op, 6);
+    s[7] = 0;
+  }
+};
+using U64 = uint64_t;
 
 template <class T>
 void sc(const T& v, double out[2]) {
@@ -147,6 +160,11 @@ int gemm_async(int transA, int transB, int M, int N, int K, const T* alpha, cons
   if (LDB < std::max(1, Bm)) return -10;
   if (LDC < std::max(1, M)) return -13;
   if (M == 0 || N == 0 || ((is_zero(*alpha) || K == 0) && is_one(*beta))) return 0;
+  const OpName op_name(HT<T>::dt, "gemm");
+  xkb::EvCall ev_call(op_name.s,
+                      {U64(M), U64(N), U64(K),
+                       U64(xkb::evlog_on() ? auto_tilesize(KERN_GEMM, M, N, K) : 0), U64(transA),
+                       U64(transB), 0});
   Guard g;
   if (int e = ensure_init()) return rt_error(e);
   Runtime& R = rt();
@@ -275,6 +293,10 @@ int gemmt_async(int uplo, int transA, int transB, int N, int K, const T* alpha, 
   if (LDC < std::max(1, N)) return -13;
   if (N == 0 || ((is_zero(*alpha) || K == 0) && is_one(*beta))) return 0;
   if (uplo == 0) return gemm_async<T>(transA, transB, N, N, K, alpha, A, LDA, B, LDB, beta, C, LDC);
+  const OpName op_name(HT<T>::dt, "gemmt");
+  xkb::EvCall ev_call(op_name.s,
+                      {U64(N), U64(K), U64(xkb::evlog_on() ? auto_tilesize(KERN_GEMMT, N, N, K) : 0),
+                       U64(transA), U64(transB), 0, 0});
   Guard g;
   if (int e = ensure_init()) return rt_error(e);
   Runtime& R = rt();
@@ -323,6 +345,8 @@ int rk_async(int herm, int uplo, int trans, int N, int K, const T& alpha, const 
   if (LDA < std::max(1, Am)) return -7;
   if (LDC < std::max(1, N)) return -10;
   if (N == 0 || ((is_zero(alpha) || K == 0) && is_one(beta))) return 0;
+  const OpName op_name(HT<T>::dt, herm ? "herk" : "syrk");
+  xkb::EvCall ev_call(op_name.s, {U64(N), U64(K), U64(uplo), U64(trans), 0, 0, 0});
   Guard g;
   if (int e = ensure_init()) return rt_error(e);
   Runtime& R = rt();
@@ -374,6 +398,8 @@ int r2k_async(int herm, int uplo, int trans, int N, int K, const T& alpha, const
   if (LDB < std::max(1, Am)) return -9;
   if (LDC < std::max(1, N)) return -12;
   if (N == 0 || ((is_zero(alpha) || K == 0) && is_one(beta))) return 0;
+  const OpName op_name(HT<T>::dt, herm ? "her2k" : "syr2k");
+  xkb::EvCall ev_call(op_name.s, {U64(N), U64(K), U64(uplo), U64(trans), 0, 0, 0});
   Guard g;
   if (int e = ensure_init()) return rt_error(e);
   Runtime& R = rt();
@@ -433,6 +459,8 @@ int sm_async(int herm, int side, int uplo, int M, int N, const T* alpha, const T
   if (LDB < std::max(1, M)) return -9;
   if (LDC < std::max(1, M)) return -12;
   if (M == 0 || N == 0 || (is_zero(*alpha) && is_one(*beta))) return 0;
+  const OpName op_name(HT<T>::dt, herm ? "hemm" : "symm");
+  xkb::EvCall ev_call(op_name.s, {U64(M), U64(N), U64(side), U64(uplo), 0, 0, 0});
   Guard g;
   if (int e = ensure_init()) return rt_error(e);
   Runtime& R = rt();
@@ -477,6 +505,9 @@ int tr_async(int is_trsm, int side, int uplo, int transA, int diag, int M, int N
   if (LDA < std::max(1, NA)) return -8;
   if (LDB < std::max(1, M)) return -10;
   if (std::min(M, N) == 0) return 0;
+  const OpName op_name(HT<T>::dt, is_trsm ? "trsm" : "trmm");
+  xkb::EvCall ev_call(op_name.s,
+                      {U64(M), U64(N), U64(side), U64(uplo), U64(transA), U64(diag), 0});
   Guard g;
   if (int e = ensure_init()) return rt_error(e);
   Runtime& R = rt();
@@ -553,6 +584,8 @@ int potrf_async(int uplo, int N, T* A, int LDA) {
   if (N < 0) return -5;
   if (LDA < std::max(1, N)) return -8;
   if (N == 0) return 0;
+  const OpName op_name(HT<T>::dt, "potrf");
+  xkb::EvCall ev_call(op_name.s, {U64(N), U64(uplo)});
   Guard g;
   if (int e = ensure_init()) return rt_error(e);
   Runtime& R = rt();
@@ -591,6 +624,8 @@ int getrf_async(int M, int N, T* A, int LDA) {
   if (N < 0 || N != M) return -2;
   if (LDA < std::max(1, M)) return -4;
   if (N == 0) return 0;
+  const OpName op_name(HT<T>::dt, "getrf");
+  xkb::EvCall ev_call(op_name.s, {U64(M), U64(N)});
   Guard g;
   if (int e = ensure_init()) return rt_error(e);
   Runtime& R = rt();

@@ -315,7 +315,9 @@ static int launch_dmma(const xkb_gemm_args* a, cudaStream_t st) {
     attr_done = true;
   }
   const long grid = (long)p.tiles_m * p.tiles_n;
+  const long long tv = evlog_kern_begin(st, "k_gemm_dmma");
   kern<<<(unsigned)grid, kThreads, smem, st>>>(tA, tB, p);
+  evlog_kern_end(tv, st);
   count_launch();
   return cudaPeekAtLastError() == cudaSuccess ? XKB_OK : XKB_ECUDA;
 }
@@ -373,6 +375,7 @@ static int repack(const void* src, long ld, int rows, int cols, int es, void** o
   const size_t total = (size_t)rows * cols;
   const unsigned grid = (unsigned)std::max<size_t>(
       1, std::min<size_t>((total + 255) / 256, (size_t)sm_count() * 16));
+  const long long tv = evlog_kern_begin(st, "k_repack");
   if (es % 8 == 0 && reinterpret_cast<uintptr_t>(src) % 8 == 0)
     k_repack<double><<<grid, 256, 0, st>>>(rows * (es / 8), cols,
                                            static_cast<const double*>(src), ld * (es / 8),
@@ -381,6 +384,7 @@ static int repack(const void* src, long ld, int rows, int cols, int es, void** o
     k_repack<float><<<grid, 256, 0, st>>>(rows * (es / 4), cols, static_cast<const float*>(src),
                                           ld * (es / 4), static_cast<float*>(*out),
                                           ldp * (es / 4));
+  evlog_kern_end(tv, st);
   count_launch();
   return cudaPeekAtLastError() == cudaSuccess ? XKB_OK : XKB_ECUDA;
 }
@@ -392,9 +396,11 @@ static int launch_scale(int M, int N, const double* beta, void* C, long ldc, int
   if (total == 0) return XKB_OK;
   long blocks = (long)((total + 255) / 256);
   if (blocks > 4L * sm_count() * 8) blocks = 4L * sm_count() * 8;
+  const long long tv = evlog_kern_begin(st, "k_scale");
   k_scale<T><<<(unsigned)blocks, 256, 0, st>>>(M, N, beta[0], St<T>::CPLX ? beta[1] : 0.0,
                                                reinterpret_cast<T*>(C), ldc, uplo, herm_diag,
                                                diag);
+  evlog_kern_end(tv, st);
   count_launch();
   return cudaPeekAtLastError() == cudaSuccess ? XKB_OK : XKB_ECUDA;
 }

@@ -337,8 +337,10 @@ static int launch_block(const LuCtx& c, char* Ad, long n, long i0) {
       return XKB_ECUDA;
     attr = true;
   }
+  const long long tv = evlog_kern_begin(c.st, "k_getrf_block");
   k_getrf_block<T><<<1, kLuThreads, Sh::SMEM, c.st>>>(
       (int)n, reinterpret_cast<typename St<T>::S*>(Ad), c.lda, (int)i0, c.info);
+  evlog_kern_end(tv, c.st);
   count_launch();
   return cudaPeekAtLastError() == cudaSuccess ? XKB_OK : XKB_ECUDA;
 }

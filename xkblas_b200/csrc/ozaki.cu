@@ -1002,6 +1002,8 @@ static void crt_launch(dim3 g, cudaStream_t st, const CrtP& cp, const Consts& c,
   else k_oz_crt<NM><<<g, 256, 0, st>>>(cp, c);
 }
 static int launch_crt(dim3 g, cudaStream_t st, const CrtP& cp, const Consts& c, double* store) {
+  if (c.nmod < 2 || c.nmod > kMaxMod) return XKB_EINVAL;
+  const long long tv = evlog_kern_begin(st, store ? "k_oz_crt_store" : "k_oz_crt");
   switch (c.nmod) {
 #define XKB_CRT_CASE(NM) \
   case NM:               \
@@ -1010,8 +1012,9 @@ static int launch_crt(dim3 g, cudaStream_t st, const CrtP& cp, const Consts& c, 
     XKB_CRT_CASE(7) XKB_CRT_CASE(8) XKB_CRT_CASE(9) XKB_CRT_CASE(10) XKB_CRT_CASE(11)
     XKB_CRT_CASE(12) XKB_CRT_CASE(13) XKB_CRT_CASE(14) XKB_CRT_CASE(15) XKB_CRT_CASE(16)
 #undef XKB_CRT_CASE
-    default: return XKB_EINVAL;
+    default: break;
   }
+  evlog_kern_end(tv, st);
   count_launch();
   return cudaPeekAtLastError() == cudaSuccess ? XKB_OK : XKB_ECUDA;
 }
@@ -1047,6 +1050,7 @@ struct View {
 static int launch_norm(const View& v, int L, int K, int cplx, const Consts* c, double2* part,
                        int* mu, cudaStream_t st) {
   const int nch = (K + kNormChunk - 1) / kNormChunk;
+  const long long tv = evlog_kern_begin(st, "k_oz_norm+k_oz_shift");
   if (v.kc) {
     dim3 g((unsigned)((L + 7) / 8), (unsigned)nch);
     k_oz_norm<true><<<g, 256, 0, st>>>(L, K, v.X, v.ld, cplx, part);
@@ -1055,6 +1059,7 @@ static int launch_norm(const View& v, int L, int K, int cplx, const Consts* c, d
     k_oz_norm<false><<<g, 256, 0, st>>>(L, K, v.X, v.ld, cplx, part);
   }
   k_oz_shift<<<(unsigned)((L + 255) / 256), 256, 0, st>>>(L, K, nch, part, c->H, mu);
+  evlog_kern_end(tv, st);
   count_launch(2);
   return cudaPeekAtLastError() == cudaSuccess ? XKB_OK : XKB_ECUDA;
 }
@@ -1072,13 +1077,16 @@ static int launch_res(const View& v, int L, int K, const int* mu, const Consts* 
       k_oz_residues<false, NM><<<g, 256, 0, st>>>(L, K, v.X, v.ld, v.estride, v.eoff,       \
                                                   v.sign, mu, *c, planes, Lpad, Kpad, kofs); \
     break;
+  if (c->nmod < 2 || c->nmod > kMaxMod) return XKB_EINVAL;
+  const long long tv = evlog_kern_begin(st, "k_oz_residues");
   switch (c->nmod) {
     XKB_RES_CASE(2) XKB_RES_CASE(3) XKB_RES_CASE(4) XKB_RES_CASE(5) XKB_RES_CASE(6)
     XKB_RES_CASE(7) XKB_RES_CASE(8) XKB_RES_CASE(9) XKB_RES_CASE(10) XKB_RES_CASE(11)
     XKB_RES_CASE(12) XKB_RES_CASE(13) XKB_RES_CASE(14) XKB_RES_CASE(15) XKB_RES_CASE(16)
-    default: return XKB_EINVAL;
+    default: break;
   }
 #undef XKB_RES_CASE
+  evlog_kern_end(tv, st);
   count_launch();
   return cudaPeekAtLastError() == cudaSuccess ? XKB_OK : XKB_ECUDA;
 }
@@ -1146,7 +1154,10 @@ static int launch_gemm(const int8_t* Ap, long a_rows, const int8_t* Bp, long b_r
     la[0].val.clusterDim.z = 1;
     cfg.attrs = la;
     cfg.numAttrs = 1;
-    if (cudaLaunchKernelEx(&cfg, k_oz_gemm2, tA, tB2, p) != cudaSuccess) return XKB_ECUDA;
+    const long long tv = evlog_kern_begin(st, "k_oz_gemm2");
+    const cudaError_t le = cudaLaunchKernelEx(&cfg, k_oz_gemm2, tA, tB2, p);
+    evlog_kern_end(tv, st);
+    if (le != cudaSuccess) return XKB_ECUDA;
     count_launch();
     return cudaPeekAtLastError() == cudaSuccess ? XKB_OK : XKB_ECUDA;
   }
@@ -1160,7 +1171,9 @@ static int launch_gemm(const int8_t* Ap, long a_rows, const int8_t* Bp, long b_r
   }
   const long total = (long)p.tiles_m * p.tiles_n * c->nmod;
   const unsigned grid = (unsigned)std::min<long>(total, sm_count());  // persistent
+  const long long tv = evlog_kern_begin(st, "k_oz_gemm");
   k_oz_gemm<<<grid, kGemmThreads, smem, st>>>(tA, tB, p);
+  evlog_kern_end(tv, st);
   count_launch();
   return cudaPeekAtLastError() == cudaSuccess ? XKB_OK : XKB_ECUDA;
 }

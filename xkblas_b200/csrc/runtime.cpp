@@ -51,6 +51,8 @@ int ensure_init() {
   if (prop.major != 10) return XKB_ENODEV;  // kernels are built for sm_100a only
   if (cudaSetDevice(dev) != cudaSuccess) return XKB_ENODEV;
   R.device = dev;
+  if (const char* dir = getenv("XKBLAS_TRACE_DIR"))
+    if (*dir) xkblas_trace_record(1);
   if (cudaStreamCreateWithFlags(&R.s_comp, cudaStreamNonBlocking) != cudaSuccess ||
       cudaStreamCreateWithFlags(&R.s_h2d, cudaStreamNonBlocking) != cudaSuccess ||
       cudaStreamCreateWithFlags(&R.s_d2h, cudaStreamNonBlocking) != cudaSuccess)
@@ -243,6 +245,7 @@ static int copy_h2d(Desc* d, size_t r0, size_t r1, size_t c0, size_t c1) {
   char* dst = static_cast<char*>(dev_ptr(d, r0, c0));
   const size_t w = (r1 - r0) * d->esz;
   R.stats.h2d += w * (c1 - c0);
+  const long long tv = xkb::evlog_copy_begin(R.s_h2d, w * (c1 - c0), 1);
   cudaError_t e;
   if (d->ld == d->dld && (r1 - r0 == d->M || c1 - c0 == 1))  // one contiguous range
     e = cudaMemcpyAsync(dst, src, ((c1 - c0 - 1) * d->ld + (r1 - r0)) * d->esz,
@@ -250,6 +253,7 @@ static int copy_h2d(Desc* d, size_t r0, size_t r1, size_t c0, size_t c1) {
   else
     e = cudaMemcpy2DAsync(dst, d->dld * d->esz, src, d->ld * d->esz, w, c1 - c0,
                           cudaMemcpyHostToDevice, R.s_h2d);
+  xkb::evlog_copy_end(tv, R.s_h2d);
   return cuda_ok(e);
 }
 
@@ -260,6 +264,7 @@ static int copy_d2h(Desc* d, size_t r0, size_t r1, size_t c0, size_t c1) {
   const char* src = static_cast<const char*>(dev_ptr(d, r0, c0));
   const size_t w = (r1 - r0) * d->esz;
   R.stats.d2h += w * (c1 - c0);
+  const long long tv = xkb::evlog_copy_begin(R.s_d2h, w * (c1 - c0), 2);
   cudaError_t e;
   if (d->ld == d->dld && (r1 - r0 == d->M || c1 - c0 == 1))
     e = cudaMemcpyAsync(dst, src, ((c1 - c0 - 1) * d->ld + (r1 - r0)) * d->esz,
@@ -267,6 +272,7 @@ static int copy_d2h(Desc* d, size_t r0, size_t r1, size_t c0, size_t c1) {
   else
     e = cudaMemcpy2DAsync(dst, d->ld * d->esz, src, d->dld * d->esz, w, c1 - c0,
                           cudaMemcpyDeviceToHost, R.s_d2h);
+  xkb::evlog_copy_end(tv, R.s_d2h);
   return cuda_ok(e);
 }
 
@@ -396,6 +402,12 @@ int flush_pending() {
 
 int launch_ops(const std::vector<xkb_batch_op>& ops) {
   Runtime& R = rt();
+  // trace name of the launched work: the deferred call, not the call whose
+  // flush launches it
+  static const char* const kNames[2][2] = {{"dgemm", "zgemm"}, {"dtrsm", "ztrsm"}};
+  const xkb_batch_op& o0 = ops[0];
+  xkb::EvName ev_name(ops.size() > 1 ? "batch"
+                                     : kNames[o0.kind == XKB_BATCH_TRSM][o0.dtype == XKB_Z]);
   if (ops.size() == 1) {  // a lone call: the whole-matrix kernels
     const xkb_batch_op& o = ops[0];
     if (o.kind == XKB_BATCH_TRSM)
@@ -682,6 +694,8 @@ int xkblas_finalize(void) {
   for (Desc* d : all) drop_desc(d);
   cudaStreamSynchronize(R.s_comp);
   xkb_cuda_batch_release();
+  if (const char* dir = getenv("XKBLAS_TRACE_DIR"))
+    if (*dir) xkblas_trace_export(dir);
   return 0;
 }
 
@@ -732,7 +746,10 @@ void xkblas_load_sym(void** ptr, const char* name);  // native.cpp
 int xkblas_sync(void) {
   Runtime& R = rt();
   std::lock_guard<std::recursive_mutex> g(R.mu);
-  if (!R.ready) return 0;
+  if (!R.ready) {
+    xkb::evlog_sync_done();
+    return 0;
+  }
   int e = flush_pending();
   if (cudaStreamSynchronize(R.s_comp) != cudaSuccess) e = XKB_ECUDA;
   if (cudaStreamSynchronize(R.s_h2d) != cudaSuccess) e = XKB_ECUDA;
@@ -742,6 +759,7 @@ int xkblas_sync(void) {
     R.sticky_error = de;
     e = XKB_ETIMEDOUT;
   }
+  xkb::evlog_sync_done();
   return e;
 }
 

@@ -12,6 +12,7 @@
 #include <unordered_map>
 #include <vector>
 
+#include "evlog.hpp"
 #include "xkb_cuda.h"
 #include "xkblas.h"
 

@@ -946,7 +946,10 @@ static int launch_entry(Batch& B, GraphEntry* e, cudaStream_t st) {
   B.ncalls = e->L.nops;
   B.call_tasks = e->call_tasks;
   B.cur_times = e->d_times;
-  if (cudaGraphLaunch(e->exec, st) != cudaSuccess) return XKB_ECUDA;
+  const long long tv = evlog_kern_begin(st, "k_sched(graph)");
+  const cudaError_t le = cudaGraphLaunch(e->exec, st);
+  evlog_kern_end(tv, st);
+  if (le != cudaSuccess) return XKB_ECUDA;
   count_launch();
   return XKB_OK;
 }
@@ -1162,9 +1165,11 @@ extern "C" int xkb_cuda_batch(const xkb_batch_op* ops, int nops, int schedule, v
   B.cur_times = B.d_times;
   KArgs a(d, L, schedule, B.d_times);
   const int grid = std::min(grid_size(), std::max(1, ntasks));
+  const long long tv = evlog_kern_begin(st, "k_sched");
   k_sched<<<grid, kThreads, kSmemBytes, st>>>(a.tasks, a.ndep, a.succ, a.bulk, a.nbulk, a.urq,
                                               a.nurg, a.ctl, a.urgent_first, a.left,
                                               a.call_end, a.t_start);
+  evlog_kern_end(tv, st);
   count_launch();
   // the pinned staging buffer must outlive the copy: the copy is ordered
   // before the kernel, and the next batch synchronises before reusing it

@@ -463,8 +463,10 @@ static int launch_block(int n, int nrhs, const void* A, long lda, int swap, int 
       return XKB_ECUDA;
     attr[lower ? 1 : 0] = true;
   }
+  const long long tv = evlog_kern_begin(st, "k_trsm_block");
   kb<<<grid, kBlkThreads, Sh::SMEM, st>>>(n, nrhs, static_cast<const S*>(A), lda, swap, conj,
                                           unit, static_cast<S*>(B), ldb, rhs_rows, al[0], al[1]);
+  evlog_kern_end(tv, st);
   count_launch();
   return cudaPeekAtLastError() == cudaSuccess ? XKB_OK : XKB_ECUDA;
 }
@@ -624,6 +626,7 @@ extern "C" int xkb_cuda_trmm(int dtype, int side, int uplo, int trans, int diag,
   }
   const unsigned g1 = grid_for((size_t)na * na), g2 = grid_for((size_t)M * N);
   const int lower = uplo == XKB_LOWER, unit = diag != 0;
+  const long long tv = evlog_kern_begin(st, "k_tri_fill+k_copy2d");
   switch (dtype) {
     case XKB_S:
       k_tri_fill<float><<<g1, 256, 0, st>>>((int)na, (const float*)A, lda, lower, unit, (float*)T, ldt);
@@ -642,6 +645,7 @@ extern "C" int xkb_cuda_trmm(int dtype, int side, int uplo, int trans, int diag,
       k_copy2d<double2><<<g2, 256, 0, st>>>(M, N, (const double2*)B, ldb, (double2*)Bc, ldc);
       break;
   }
+  evlog_kern_end(tv, st);
   count_launch(2);
   xkb_gemm_args g{};
   g.dtype = dtype;
@@ -689,12 +693,14 @@ extern "C" int xkb_cuda_symm(int dtype, int herm, int side, int uplo, int M, int
   const unsigned g1 = grid_for((size_t)na * na);
   const int lower = uplo == XKB_LOWER;
   const int hm = herm && (dtype == XKB_C || dtype == XKB_Z);
+  const long long tv = evlog_kern_begin(st, "k_sym_fill");
   switch (dtype) {
     case XKB_S: k_sym_fill<float><<<g1, 256, 0, st>>>((int)na, (const float*)A, lda, lower, 0, (float*)S, ldt); break;
     case XKB_D: k_sym_fill<double><<<g1, 256, 0, st>>>((int)na, (const double*)A, lda, lower, 0, (double*)S, ldt); break;
     case XKB_C: k_sym_fill<float2><<<g1, 256, 0, st>>>((int)na, (const float2*)A, lda, lower, hm, (float2*)S, ldt); break;
     case XKB_Z: k_sym_fill<double2><<<g1, 256, 0, st>>>((int)na, (const double2*)A, lda, lower, hm, (double2*)S, ldt); break;
   }
+  evlog_kern_end(tv, st);
   count_launch();
   xkb_gemm_args g{};
   g.dtype = dtype;

@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "evlog.hpp"
 #include "xkb_cuda.h"
 
 namespace xkb {
