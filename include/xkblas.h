@@ -317,6 +317,7 @@ typedef struct xkblas_stats_t {
   double   flops;          /* algorithmic flops (reference blas/flops.h) */
   uint64_t batches;        /* deferred-call batches run as one executor launch */
   uint64_t batched_calls;  /* calls those batches held */
+  uint64_t evictions;      /* matrices evicted under the cache limit */
 } xkblas_stats_t;
 int  xkblas_get_stats(xkblas_stats_t* st);
 void xkblas_reset_stats(void);

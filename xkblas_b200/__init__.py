@@ -64,7 +64,7 @@ class Stats(ctypes.Structure):
                 ("tile_hits", ctypes.c_uint64), ("tile_misses", ctypes.c_uint64),
                 ("ozaki_calls", ctypes.c_uint64), ("ozaki_moduli", ctypes.c_uint64),
                 ("flops", ctypes.c_double), ("batches", ctypes.c_uint64),
-                ("batched_calls", ctypes.c_uint64)]
+                ("batched_calls", ctypes.c_uint64), ("evictions", ctypes.c_uint64)]
 
 
 def lib():

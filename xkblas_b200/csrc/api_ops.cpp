@@ -101,7 +101,7 @@ int rt_error(int xkb) {
 
 struct Guard {
   std::lock_guard<std::recursive_mutex> g;
-  Guard() : g(rt().mu) {}
+  Guard() : g(rt().mu) { rt().call_epoch++; }  // operands of this call are not evicted by it
 };
 
 bool use_ozaki(int dt, long m, long n, long k) {

@@ -51,6 +51,19 @@ int ensure_init() {
   if (prop.major != 10) return XKB_ENODEV;  // kernels are built for sm_100a only
   if (cudaSetDevice(dev) != cudaSuccess) return XKB_ENODEV;
   R.device = dev;
+  {
+    size_t fr = 0, total = 0;
+    if (cudaMemGetInfo(&fr, &total) != cudaSuccess) {
+      cudaGetLastError();
+      total = prop.totalGlobalMem;
+    }
+    double pct = 98.0;
+    if (const char* s = getenv("XKBLAS_CACHE_LIMIT")) pct = std::min(100.0, std::max(1.0, atof(s)));
+    R.cache_limit = (size_t)((double)total * pct / 100.0);
+    // extension: an absolute limit in MiB
+    if (const char* s = getenv("XKBLAS_CACHE_LIMIT_MB"))
+      if (atof(s) > 0) R.cache_limit = (size_t)(atof(s) * 1048576.0);
+  }
   if (const char* dir = getenv("XKBLAS_TRACE_DIR"))
     if (*dir) xkblas_trace_record(1);
   if (cudaStreamCreateWithFlags(&R.s_comp, cudaStreamNonBlocking) != cudaSuccess ||
@@ -144,6 +157,8 @@ static void free_desc_memory(Desc* d) {
     cudaStreamWaitEvent(R.s_comp, e2, 0);
     cudaFreeAsync(d->dev, R.s_comp);
     d->dev = nullptr;
+    R.dev_bytes -= std::min(R.dev_bytes, d->bytes);
+    d->bytes = 0;
   }
 }
 
@@ -162,6 +177,36 @@ static int flush_sync(Desc* d) {
   return cuda_ok(cudaStreamSynchronize(rt().s_d2h));
 }
 
+// Evict one matrix: its dirty tiles go back to the host, later uploads of it
+// wait for that copy, and its device buffer is released (stream ordered).
+static void evict(Desc* d) {
+  Runtime& R = rt();
+  coherent(d, 0, 0);
+  cudaEvent_t e = next_event();
+  cudaEventRecord(e, R.s_d2h);
+  cudaStreamWaitEvent(R.s_h2d, e, 0);
+  R.stats.evictions++;
+  drop_desc(d);
+}
+
+// Evict least recently used matrices not touched by the current call until
+// `need` more bytes fit under the cache limit; false if that cannot be
+// reached (the allocation then goes ahead above the limit if it can).
+static bool evict_for(size_t need) {
+  Runtime& R = rt();
+  while (R.dev_bytes + need > R.cache_limit) {
+    Desc* v = nullptr;
+    for (auto& kv : R.descs) {
+      Desc* d = kv.second;
+      if (d->managed || !d->dev || d->epoch == R.call_epoch) continue;
+      if (!v || d->last_use < v->last_use) v = d;
+    }
+    if (!v) return false;
+    evict(v);
+  }
+  return true;
+}
+
 static int alloc_desc(Desc* d) {
   Runtime& R = rt();
   // a host matrix with contiguous columns keeps its layout on the device, so
@@ -171,12 +216,21 @@ static int alloc_desc(Desc* d) {
   const size_t align = std::max<size_t>(1, 128 / d->esz);
   d->dld = d->ld == d->M ? std::max<size_t>(d->M, 1) : round_up(std::max<size_t>(d->M, 1), align);
   const size_t bytes = d->dld * std::max<size_t>(d->N, 1) * d->esz;
+  if (R.cache_limit) evict_for(bytes);
   void* p = nullptr;
   if (cudaMallocAsync(&p, bytes, R.s_comp) != cudaSuccess) {
     cudaGetLastError();
-    return XKB_ENOMEM;
+    // out of device memory below the limit: evict what the call does not use
+    // and try once more
+    evict_for(R.cache_limit);
+    if (cudaMallocAsync(&p, bytes, R.s_comp) != cudaSuccess) {
+      cudaGetLastError();
+      return XKB_ENOMEM;
+    }
   }
   d->dev = p;
+  d->bytes = bytes;
+  R.dev_bytes += bytes;
   R.alloc_unsynced = true;  // the copy stream waits for it before its next copy
   return XKB_OK;
 }
@@ -188,7 +242,11 @@ Desc* get_desc(const void* host, size_t M, size_t N, size_t ld, size_t esz, size
   auto it = R.descs.find(host);
   if (it != R.descs.end()) {
     Desc* d = it->second;
-    if (d->ld == ld && d->esz == esz && M <= d->M && N <= d->N) return d;
+    if (d->ld == ld && d->esz == esz && M <= d->M && N <= d->N) {
+      d->last_use = ++R.use_clock;
+      d->epoch = R.call_epoch;
+      return d;
+    }
     // Same pointer, different geometry: write back, rebuild.
     if ((*err = flush_sync(d)) != XKB_OK) return nullptr;
     drop_desc(d);
@@ -204,6 +262,8 @@ Desc* get_desc(const void* host, size_t M, size_t N, size_t ld, size_t esz, size
   d->nt = std::max<size_t>(1, (N + d->nb - 1) / d->nb);
   d->st.assign(d->mt * d->nt, 0);
   d->registered_init = true;
+  d->last_use = ++R.use_clock;
+  d->epoch = R.call_epoch;
   cudaPointerAttributes pa;
   if (cudaPointerGetAttributes(&pa, host) == cudaSuccess && pa.type == cudaMemoryTypeManaged) {
     // managed memory (xkblas_malloc_unified): the kernels use it in place;
@@ -1049,6 +1109,7 @@ int xkblas_get_stats(xkblas_stats_t* st) {
   st->kernels = xkb_cuda_kernel_count();
   st->h2d_bytes = R.stats.h2d;
   st->d2h_bytes = R.stats.d2h;
+  st->evictions = R.stats.evictions;
   st->tile_hits = R.stats.hits;
   st->tile_misses = R.stats.misses;
   st->ozaki_calls = R.stats.ozaki_calls;

@@ -51,6 +51,9 @@ struct Desc {
   bool registered_init = false;           // handle initialised (isinit)
   uint8_t pend = 0;                       // deferred calls: 1 read, 2 written
   bool managed = false;                   // CUDA managed memory: used in place, never copied
+  size_t bytes = 0;                       // device buffer size (counted against the cache limit)
+  uint64_t last_use = 0;                  // LRU stamp: the runtime's use clock at the last touch
+  uint64_t epoch = 0;                     // API call that last touched it (never evicted by it)
   // columns finished on the compute stream: (end column, event recorded when
   // columns [previous end, end) are final), ascending.  Set by the panel
   // contraction (one entry per panel) and by an executor batch (one entry for
@@ -63,7 +66,7 @@ struct Desc {
 };
 
 struct Stats {
-  uint64_t calls = 0, h2d = 0, d2h = 0, hits = 0, misses = 0;
+  uint64_t calls = 0, h2d = 0, d2h = 0, hits = 0, misses = 0, evictions = 0;
   uint64_t ozaki_calls = 0, ozaki_moduli = 0;
   double flops = 0;
 };
@@ -106,6 +109,13 @@ struct Runtime {
   std::vector<Desc*> pend_descs;  // buffers the queued calls touch (Desc::pend set)
   uint64_t batches = 0, batched_calls = 0;
   int* d_potrf_info = nullptr;  // device word for the last factorization
+  // Device cache limit (reference: XKBLAS_CACHE_LIMIT -> KAAPI_CUDA_CACHE_LIMIT,
+  // percent of device memory, default 98, clamped to [1, 100],
+  // kaapi/kaapi_impl.c:208,311-316; kaapi_plugin_cuda.c:2306).  Matrix
+  // buffers beyond it evict the least recently used matrices not touched by
+  // the current call (dirty tiles written back first).
+  size_t cache_limit = 0, dev_bytes = 0;
+  uint64_t use_clock = 0, call_epoch = 0;
 };
 
 Runtime& rt();
