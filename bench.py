@@ -681,7 +681,11 @@ def main():
 
     # ---- roofline of the dominant kernel (INT8 tensor-core GEMM, all moduli)
     pk, pk_src = peaks()
-    int8_peak = 2.0 * pk["bf16_tflops"]  # dense INT8 rate = 2x dense BF16 on B200
+    # dense INT8 rate = 2x dense BF16 on B200.  The INT8 GEMM runs ~50 ms per
+    # launch, back to back inside a long step under the 1 kW power cap: the
+    # sustained BF16 figure is its denominator (the burst one is reported too)
+    int8_peak = 2.0 * pk.get("bf16_tflops_sustained", pk["bf16_tflops"])
+    int8_peak_burst = 2.0 * pk["bf16_tflops"]
     gm = statistics.mean(gemm_ms) if gemm_ms else float("nan")
     int8_ops = 2.0 * M * N * K * nmod  # algorithmic INT8 ops per launch (one launch, all moduli)
     achieved = int8_ops / (gm * 1e-3) / 1e12
@@ -760,7 +764,9 @@ def main():
         "roofline": {"bound": "tensor", "kernel": "k_oz_gemm (INT8 tcgen05, all moduli)",
                      "achieved": achieved, "peak": int8_peak, "unit": "TFLOP/s",
                      "frac": achieved / int8_peak, "traffic": traffic,
-                     "peak_source": "%s bf16 dense x2 (INT8:BF16 dense rate 2:1)" % pk_src,
+                     "peak_source": "%s bf16 dense sustained x2 (INT8:BF16 dense rate 2:1)"
+                                    % pk_src,
+                     "peak_burst": int8_peak_burst, "frac_of_burst": achieved / int8_peak_burst,
                      "ms_per_launch": gm},
         "plain_dmma": {"value": plain_tflops, "unit": "TFLOP/s", "ms_per_step": ms_plain,
                        "frac_of_fp64_nominal": plain_tflops / fp64_nominal,
