@@ -1,12 +1,15 @@
 """Small, self-contained cases for profiling single kernels with ncu:
 
-    python -m xkblas_b200.profcases dmma|ozaki|repack|trsm|potrf|batch|copy
+    python -m xkblas_b200.profcases dmma|ozaki|ozaki2|repack|trsm|potrf|getrf|batch|copy
 
 dmma    DGEMM NN 4096^3 through xkb_cuda_gemm (k_gemm_dmma), two calls
 ozaki   the same through xkb_cuda_ozaki_gemm, 16 moduli (k_oz_* kernels)
+ozaki2  the same with the CTA-pair INT8 kernel (tuning key oz_2cta = 1, k_oz_gemm2)
 repack  the DGEMM with lda = ldb = 4097 (k_repack, then k_gemm_dmma)
 trsm    DTRSM L/L/N/N 4096 x 4096, diagonally dominant (k_trsm_block, GEMMs)
 potrf   DPOTRF lower 4096 (k_potrf_block, k_trsm_block, GEMMs)
+getrf   DGETRF without pivoting 4096, diagonally dominant (k_getrf_block,
+        k_trsm_block, GEMMs)
 copy    beta scaling (k_scale, 8192^2) and the TRMM / SYMM materialisations
         (k_tri_fill, k_copy2d, k_sym_fill, 4096^2)
 batch   150 mixed calls (70% DGEMM, 20% DTRSM, 10% ZGEMM; M, N, K
@@ -38,7 +41,9 @@ def main(case):
         return torch.rand(c, r, generator=g, device="cuda", dtype=f64) - 0.5
 
     keep = []
-    if case in ("dmma", "ozaki", "repack"):
+    if case == "ozaki2":
+        lib.xkb_tune_set(b"oz_2cta", 1.0)
+    if case in ("dmma", "ozaki", "ozaki2", "repack"):
         n = 4096
         ld = n + 1 if case == "repack" else n
         A, B, C = rnd(ld, n), rnd(ld, n), rnd(n, n)
@@ -46,7 +51,7 @@ def main(case):
         ga = _GemmArgs(1, 0, 0, n, n, n, A.data_ptr(), ld, B.data_ptr(), ld, C.data_ptr(), n)
         ga.alpha[0] = ga.beta[0] = 1.0
         for _ in range(2):
-            rc = (lib.xkb_cuda_ozaki_gemm(ctypes.byref(ga), 0, sp) if case == "ozaki"
+            rc = (lib.xkb_cuda_ozaki_gemm(ctypes.byref(ga), 0, sp) if case.startswith("ozaki")
                   else lib.xkb_cuda_gemm(ctypes.byref(ga), sp))
             assert rc == 0, rc
     elif case == "trsm":
@@ -69,6 +74,15 @@ def main(case):
         for _ in range(2):
             A.copy_(A0)
             assert lib.xkb_cuda_potrf(1, 1, n, A.data_ptr(), n, info.data_ptr(), 0, sp) == 0
+    elif case == "getrf":
+        n = 4096
+        A0 = rnd(n, n) + n * torch.eye(n, device="cuda", dtype=f64)
+        A = A0.clone()
+        info = torch.zeros(1, dtype=torch.int32, device="cuda")
+        keep += [A0, A, info]
+        for _ in range(2):
+            A.copy_(A0)
+            assert lib.xkb_cuda_getrf_nopiv(1, n, A.data_ptr(), n, info.data_ptr(), 0, sp) == 0
     elif case == "batch":
         rng = np.random.default_rng(2024)
 
