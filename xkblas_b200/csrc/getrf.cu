@@ -15,7 +15,6 @@
 // with LAPACK's unchecked use); the first one (1-based, over the whole
 // matrix) is recorded in *d_info (0 = none).
 #include <algorithm>
-#include <mutex>
 
 #include "dmma_common.cuh"
 #include "xkb_dev.cuh"
@@ -357,30 +356,6 @@ static int block(const LuCtx& c, long i0, long n) {
   return XKB_EINVAL;
 }
 
-// Side stream for the L21 solve, which is independent of the U12 solve at
-// the same level: the small, latency-bound triangular solves of the
-// recursion then run two at a time.  nullptr (both on the caller's stream)
-// if it cannot be created.
-struct SideStream {
-  cudaStream_t s = nullptr;
-  cudaEvent_t fork = nullptr, join = nullptr;
-};
-static const SideStream& side_stream() {
-  static SideStream ss;
-  static std::once_flag once;
-  std::call_once(once, [] {
-    SideStream t;
-    if (cudaStreamCreateWithFlags(&t.s, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaEventCreateWithFlags(&t.fork, cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&t.join, cudaEventDisableTiming) != cudaSuccess) {
-      cudaGetLastError();
-      return;
-    }
-    ss = t;
-  });
-  return ss;
-}
-
 static int factor(const LuCtx& c, long i0, long i1) {
   const long n = i1 - i0;
   const bool cplx = c.dt == XKB_C || c.dt == XKB_Z;
@@ -398,22 +373,18 @@ static int factor(const LuCtx& c, long i0, long i1) {
   char* A21 = c.A + (h + i0 * c.lda) * (long)c.es;
   char* A22 = c.A + (h + h * c.lda) * (long)c.es;
   // U12 = L11^-1 A12 (left, lower, unit) on the caller's stream and
-  // L21 = A21 U11^-1 (right, upper, non-unit) on the side stream; both read
-  // only the factored A11, and the update below waits for both
-  const SideStream& ss = side_stream();
-  cudaStream_t s2 = c.st;
-  if (ss.s && cudaEventRecord(ss.fork, c.st) == cudaSuccess &&
-      cudaStreamWaitEvent(ss.s, ss.fork, 0) == cudaSuccess)
-    s2 = ss.s;
-  if ((e = xkb_cuda_trsm(c.dt, 0, XKB_LOWER, XKB_OP_N, 1, (int)n1, (int)n2, one, A11, c.lda, A12,
-                         c.lda, c.ozaki, c.st)))
+  // L21 = A21 U11^-1 (right, upper, non-unit) on a side stream: both read
+  // only the factored A11 (the small, latency-bound solves of the deep
+  // levels then run two at a time); the update below waits for both
+  const SideStream& ss = side_stream(0);
+  cudaStream_t s2 = side_fork(ss, c.st);
+  if ((e = trsm_entry(c.dt, 0, XKB_LOWER, XKB_OP_N, 1, (int)n1, (int)n2, one, A11, c.lda, A12,
+                      c.lda, c.ozaki, c.st, false)))
     return e;
-  if ((e = xkb_cuda_trsm(c.dt, 1, XKB_UPPER, XKB_OP_N, 0, (int)n2, (int)n1, one, A11, c.lda, A21,
-                         c.lda, c.ozaki, s2)))
+  if ((e = trsm_entry(c.dt, 1, XKB_UPPER, XKB_OP_N, 0, (int)n2, (int)n1, one, A11, c.lda, A21,
+                      c.lda, c.ozaki, s2, false)))
     return e;
-  if (s2 != c.st && (cudaEventRecord(ss.join, s2) != cudaSuccess ||
-                     cudaStreamWaitEvent(c.st, ss.join, 0) != cudaSuccess))
-    return XKB_ECUDA;
+  if (!side_join(ss, s2, c.st)) return XKB_ECUDA;
   // A22 -= L21 U12
   xkb_gemm_args g{};
   g.dtype = c.dt;

@@ -83,6 +83,37 @@ cudaStream_t resolve_stream(void* s) {
 
 void count_launch(int n) { g_launches.fetch_add((uint64_t)n, std::memory_order_relaxed); }
 
+const SideStream& side_stream(int slot) {
+  static SideStream ss[2];
+  static std::once_flag once[2];
+  slot = slot ? 1 : 0;
+  std::call_once(once[slot], [slot] {
+    SideStream t;
+    if (cudaStreamCreateWithFlags(&t.s, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&t.fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&t.join, cudaEventDisableTiming) != cudaSuccess) {
+      cudaGetLastError();
+      return;
+    }
+    ss[slot] = t;
+  });
+  return ss[slot];
+}
+
+cudaStream_t side_fork(const SideStream& side, cudaStream_t st) {
+  if (side.s && cudaEventRecord(side.fork, st) == cudaSuccess &&
+      cudaStreamWaitEvent(side.s, side.fork, 0) == cudaSuccess)
+    return side.s;
+  cudaGetLastError();
+  return st;
+}
+
+bool side_join(const SideStream& side, cudaStream_t forked, cudaStream_t st) {
+  if (forked == st) return true;
+  return cudaEventRecord(side.join, forked) == cudaSuccess &&
+         cudaStreamWaitEvent(st, side.join, 0) == cudaSuccess;
+}
+
 int sm_count() {
   static int n = 0;
   if (n == 0) {

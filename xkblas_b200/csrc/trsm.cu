@@ -572,9 +572,10 @@ static int solve(const TrsmCtx& c, long i0, long i1, const double* alpha) {
 
 using namespace xkb;
 
-extern "C" int xkb_cuda_trsm(int dtype, int side, int uplo, int trans, int diag, int M, int N,
-                             const double* alpha, const void* A, long lda, void* B, long ldb,
-                             int ozaki, void* stream) {
+namespace xkb {
+int trsm_entry(int dtype, int side, int uplo, int trans, int diag, int M, int N,
+               const double* alpha, const void* A, long lda, void* B, long ldb, int ozaki,
+               cudaStream_t st, bool split_rhs) {
   if (dtype < XKB_S || dtype > XKB_Z || M < 0 || N < 0 || !alpha) return XKB_EINVAL;
   if (trans < XKB_OP_N || trans > XKB_OP_C) return XKB_EINVAL;
   if (M == 0 || N == 0) return XKB_OK;
@@ -591,7 +592,7 @@ extern "C" int xkb_cuda_trsm(int dtype, int side, int uplo, int trans, int diag,
   c.B = static_cast<char*>(B);
   c.ldb = ldb;
   c.nrhs = c.left ? N : M;
-  c.st = resolve_stream(stream);
+  c.st = st;
   const bool lower = uplo == XKB_LOWER;
   const bool op_lower = lower ^ (c.trans != XKB_OP_N);  // op(A) lower?
   // effective triangle element access, as in k_trsm_block
@@ -606,7 +607,34 @@ extern "C" int xkb_cuda_trsm(int dtype, int side, int uplo, int trans, int diag,
   }
   c.fwd = c.lower_eff;
   const long n = c.left ? M : N;
+  // Many right-hand sides: two independent halves, the second on a side
+  // stream, so that one half's latency-bound diagonal-block solves overlap
+  // the other half's coupling GEMMs.  Halves are multiples of 64.  In the
+  // Ozaki form each half converts the coupling blocks of A again, which pays
+  // only with more right-hand sides than unknowns.
+  constexpr long kSplitRhs = 2048;
+  if (split_rhs && c.nrhs >= kSplitRhs && (c.ozaki == 0 || c.nrhs > n)) {
+    const long h = (c.nrhs / 2 + 63) / 64 * 64;
+    TrsmCtx c2 = c;
+    c2.nrhs = c.nrhs - h;
+    c2.B = c.B + (c.left ? h * ldb : h) * (long)c.es;
+    c.nrhs = h;
+    const SideStream& ss = side_stream(1);
+    c2.st = side_fork(ss, c.st);
+    int e = solve(c, 0, n, alpha);
+    const int e2 = solve(c2, 0, n, alpha);
+    if (!side_join(ss, c2.st, c.st) && !e) e = XKB_ECUDA;
+    return e ? e : e2;
+  }
   return solve(c, 0, n, alpha);
+}
+}  // namespace xkb
+
+extern "C" int xkb_cuda_trsm(int dtype, int side, int uplo, int trans, int diag, int M, int N,
+                             const double* alpha, const void* A, long lda, void* B, long ldb,
+                             int ozaki, void* stream) {
+  return trsm_entry(dtype, side, uplo, trans, diag, M, N, alpha, A, lda, B, ldb, ozaki,
+                    resolve_stream(stream), true);
 }
 
 extern "C" int xkb_cuda_trmm(int dtype, int side, int uplo, int trans, int diag, int M, int N,

@@ -135,6 +135,25 @@ cudaStream_t resolve_stream(void* s);
 int trace_begin(const char* op, int dtype, int M, int N, int K, int nmod, cudaStream_t st);
 void trace_mark(int slot, int k, cudaStream_t st);
 void count_launch(int n = 1);
+// A lazily created non-blocking stream with a fork and a join event, for
+// work that is independent of what the caller's stream runs meanwhile
+// (slot 0: the LU's column-panel solves, slot 1: the TRSM's second half of
+// the right-hand sides).  s is nullptr if CUDA could not create it.
+struct SideStream {
+  cudaStream_t s = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
+};
+const SideStream& side_stream(int slot);
+// Fork: `side` waits for what `st` queued so far; returns `side`'s stream,
+// or `st` itself (run in order) when there is no side stream.
+cudaStream_t side_fork(const SideStream& side, cudaStream_t st);
+// Join: `st` waits for what the forked stream queued; false on a CUDA error.
+bool side_join(const SideStream& side, cudaStream_t forked, cudaStream_t st);
+// xkb_cuda_trsm with the choice to split many right-hand sides into two
+// concurrent halves (off where the caller already runs solves side by side)
+int trsm_entry(int dtype, int side, int uplo, int trans, int diag, int M, int N,
+               const double* alpha, const void* A, long lda, void* B, long ldb, int ozaki,
+               cudaStream_t st, bool split_rhs);
 double tune(const char* key, double dflt);   // tuning table (runtime_cuda.cu)
 int tune_band(const char* prefix, long K);
 int sm_count();
