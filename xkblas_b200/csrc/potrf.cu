@@ -307,17 +307,42 @@ static int leaf(const PotrfCtx& c, long i0, long n) {
   return XKB_EINVAL;
 }
 
-static int factor(const PotrfCtx& c, long i0, long i1) {
+// Trailing update C -= op(P) op(P)^H on `st`: Ozaki in tensor-op mode above
+// the crossover, else the DMMA kernel.
+static int update(const PotrfCtx& c, xkb_gemm_args g, cudaStream_t st) {
+  if (c.ozaki > 0 && std::min<long>(g.K, std::min(g.M, g.N)) >= c.ozaki) {
+    const int e = xkb_cuda_ozaki_gemm(&g, 0, st);
+    if (e != XKB_ERANGE) return e;
+  }
+  return xkb_cuda_gemm(&g, st);
+}
+
+static long split_point(long i0, long i1) {
+  constexpr long kSplit = 64;
+  const long n = i1 - i0;
+  long h = i0 + ((n / 2 + kSplit - 1) / kSplit) * kSplit;
+  if (h >= i1) h = i1 - kSplit;
+  return h;
+}
+
+// Recursive Cholesky of rows / columns [i0, i1).  Look-ahead (la): the
+// trailing update is split at the next level's split point; the part the
+// next level factors first (its leading column block, lower; row block,
+// upper) is updated on the caller's stream, the rest of the trailing
+// triangle on a side stream, so that the next level's leading factorization
+// and panel solve overlap that larger update.  pend: the caller forked such
+// an update over this call's trailing triangle; it is joined before this
+// call's own update.  Left subtrees run without look-ahead, so that they do
+// not queue behind the side stream's update.
+static int factor(const PotrfCtx& c, long i0, long i1, bool la, bool pend) {
   const long n = i1 - i0;
   const bool cplx = c.dt == XKB_C || c.dt == XKB_Z;
   const long nmax = cplx ? PoShape<double2>::NMAX : PoShape<double>::NMAX;
-  if (n <= nmax) return leaf(c, i0, n);
-  constexpr long kSplit = 64;
-  long h = i0 + ((n / 2 + kSplit - 1) / kSplit) * kSplit;
-  if (h >= i1) h = i1 - kSplit;
+  if (n <= nmax) return leaf(c, i0, n);  // never pending: callers fork only above nmax
+  const long h = split_point(i0, i1);
   const long n1 = h - i0, n2 = i1 - h;
   int e;
-  if ((e = factor(c, i0, h))) return e;
+  if ((e = factor(c, i0, h, false, false))) return e;
   const int ctr = cplx ? XKB_OP_C : XKB_OP_T;
   const double one[2] = {1.0, 0.0};
   char* A11 = c.A + (i0 + i0 * c.lda) * (long)c.es;
@@ -355,15 +380,30 @@ static int factor(const PotrfCtx& c, long i0, long i1) {
   g.lda = c.lda;
   g.B = P;
   g.ldb = c.lda;
-  if (c.ozaki > 0 && std::min(n1, n2) >= c.ozaki) {
-    e = xkb_cuda_ozaki_gemm(&g, 0, c.st);
-    if (e != XKB_ERANGE) {
-      if (e) return e;
-      return factor(c, h, i1);
-    }
+  const SideStream& ss = side_stream(0);
+  if (pend && !side_join(ss, ss.s, c.st)) return XKB_ECUDA;
+  if (!la || n2 <= nmax || !ss.s) {
+    if ((e = update(c, g, c.st))) return e;
+    return factor(c, h, i1, la, false);
   }
-  if ((e = xkb_cuda_gemm(&g, c.st))) return e;
-  return factor(c, h, i1);
+  // part 1: the next level's leading block of columns (rows) [0, m1) of A22
+  const long m1 = split_point(h, i1) - h;
+  xkb_gemm_args g1 = g, g2 = g;
+  if (!c.upper) {
+    g1.N = (int)m1;  // rows [0, n2) x cols [0, m1), lower mask
+  } else {
+    g1.M = (int)m1;  // rows [0, m1) x cols [0, n2), upper mask
+  }
+  // part 2: the trailing triangle [m1, n2)^2
+  const long off = m1 * (c.upper ? c.lda : 1) * (long)c.es;  // panel rows (lower) / cols (upper)
+  g2.M = g2.N = (int)(n2 - m1);
+  g2.A = static_cast<const char*>(g.A) + off;
+  g2.B = static_cast<const char*>(g.B) + off;
+  g2.C = A22 + (m1 + m1 * c.lda) * (long)c.es;
+  if ((e = update(c, g1, c.st))) return e;
+  cudaStream_t s2 = side_fork(ss, c.st);
+  if ((e = update(c, g2, s2))) return e;
+  return factor(c, h, i1, la, s2 != c.st);
 }
 
 }  // namespace xkb
@@ -385,5 +425,5 @@ extern "C" int xkb_cuda_potrf(int dtype, int uplo, int N, void* A, long lda, int
   c.info = d_info;
   c.ozaki = (dtype == XKB_D || dtype == XKB_Z) ? std::max(ozaki, 0) : 0;
   c.st = resolve_stream(stream);
-  return factor(c, 0, N);
+  return factor(c, 0, N, true, false);
 }
