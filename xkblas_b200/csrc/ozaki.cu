@@ -18,9 +18,10 @@
 //      accumulation in TMEM; K * 128^2 < 2^31 for K <= 131072), then reduced
 //      mod p_l;
 //   3. the n residues of each C entry are recombined by the Chinese remainder
-//      theorem in exact multi-limb integer arithmetic, mapped to the
-//      symmetric range, converted to double and scaled back by
-//      2^-(mu_i + nu_j); alpha/beta are applied in FP64.
+//      theorem on the FP64 pipe (CRT weights split into an exact high part
+//      and a rounded low part, the quotient by P exact; see crt_value),
+//      mapped to the symmetric range and scaled back by 2^-(mu_i + nu_j);
+//      alpha/beta are applied in FP64.
 // With n = 16 moduli P ~ 2^125.4, so each operand keeps ~61 bits relative to
 // its row / column 2-norm: the contraction error is below FP64 DGEMM's.
 //
@@ -866,9 +867,9 @@ struct CrtP {
 //  - S2 - q P2 carries absolute errors of order 2^(csplit-37) plus the
 //    rounding of w2 (2^43 at 16 moduli), far below the 2^(2H-61) sqrt(K)
 //    already left by rounding the scaled operands to integers.
-// 2 FP64 FMAs per modulus and element against 4 64-bit integer multiply-adds
-// for a 128-bit limb sum: the kernel moves from the integer multiply pipe to
-// the FP64 pipe, which nothing else here uses.
+// 2 FP64 FMAs per modulus and element (a 128-bit integer sum would take 4
+// 64-bit integer multiply-adds): the kernel runs on the FP64 pipe, which
+// nothing else here uses.
 template <int NM>
 __device__ __forceinline__ double crt_value(const uint32_t (&r)[NM], const Consts& c) {
   double s1 = 0.0, s2 = 0.0;
