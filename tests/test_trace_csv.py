@@ -85,3 +85,45 @@ def test_call_recorded_and_closed_by_sync(lib, tmp_path):
     again.mkdir()
     assert lib.xkblas_trace_export(os.fsencode(str(again))) == 0
     assert _rows(again / "task.csv") == [] and _rows(again / "call.csv") == []
+
+
+def test_calls_from_two_threads(lib, tmp_path):
+    """Each host thread is its own CPU resource (the reference's kproc id) and
+    its xkblas_sync closes only its own calls (ukilli.cpp:762-775)."""
+    import threading
+    if X.lib().xkblas_get_devicecount() > 0:
+        pytest.skip("host-only case")
+    lib.xkblas_trace_export(os.fsencode(str(tmp_path)))  # drain earlier events
+    lib.xkblas_trace_record(1)
+    a = np.ones((4, 4), order="F")
+    one = np.ones(1)
+    p = lambda v: ctypes.c_void_p(v.ctypes.data)
+    barrier = threading.Barrier(2)
+
+    def work(n_calls, do_sync):
+        barrier.wait()
+        for _ in range(n_calls):
+            lib.xkblas_dtrsm_async(141, 122, 111, 131, 4, 4, p(one), p(a), 4, p(a), 4)
+        if do_sync:
+            assert lib.xkblas_sync() == 0
+
+    t1 = threading.Thread(target=work, args=(3, True))
+    t2 = threading.Thread(target=work, args=(2, False))
+    t1.start(); t2.start(); t1.join(); t2.join()
+    out = tmp_path / "t2"
+    out.mkdir()
+    assert lib.xkblas_trace_export(os.fsencode(str(out))) == 0
+    tasks = _rows(out / "task.csv")
+    calls = _rows(out / "call.csv")
+    by_res = {}
+    for t in tasks:
+        by_res.setdefault(t["Resource"], []).append(t["Name"])
+    assert sorted(len(v) for v in by_res.values()) == [2, 3]
+    assert all(n == "dtrsm" for v in by_res.values() for n in v)
+    # only the syncing thread's three calls are closed, at levels 0..2
+    assert len(calls) == 3
+    assert sorted(c["Level"] for c in calls) == ["0", "1", "2"]
+    assert len({c["Resource"] for c in calls}) == 1
+    assert [int(calls[0]["Param%d" % i]) for i in range(6)] == [4, 4, 141, 122, 111, 131]
+    # the other thread's calls stay open until its own sync
+    lib.xkblas_trace_record(0)
