@@ -87,6 +87,38 @@ def test_trsm_unaligned(xk, uplo, trans):
     assert lib.xkb_cuda_take_device_error() == 0
 
 
+@pytest.mark.parametrize("dt", [1, 3])
+@pytest.mark.parametrize("side,uplo,trans", [(0, 1, 0), (0, 2, 1), (1, 2, 0), (1, 1, 2)])
+def test_trsm_many_rhs_halves(xk, dt, side, uplo, trans):
+    """2113 right-hand sides (at least 2048: solved as two concurrent halves,
+    1088 + 1025) on both sides, both triangles, transposed, complex, with
+    unaligned leading dimensions: the residual of op(T) X = alpha B (left) /
+    X op(T) = alpha B (right)."""
+    import torch
+    if dt == 1 and trans == 2:
+        pytest.skip("conjugate transpose is complex only")
+    g = torch.Generator(device="cuda").manual_seed(300 + 10 * side + uplo + dt)
+    na, nrhs = 200, 2113
+    M, N = (na, nrhs) if side == 0 else (nrhs, na)
+    bufA, pA, A = _mat(torch, na, na, na + 1, 1, dt, g)
+    A.mul_(1.0 / na)
+    A.add_(torch.eye(na, device="cuda", dtype=A.dtype))
+    bufB, pB, B = _mat(torch, M, N, M + 2, 1, dt, g)
+    B0 = B.clone()
+    al = (ctypes.c_double * 2)(2.0, 0.0)
+    torch.cuda.synchronize()
+    lib = xk.lib()
+    assert lib.xkb_cuda_trsm(dt, side, uplo, trans, 0, M, N,
+                             ctypes.cast(al, ctypes.POINTER(ctypes.c_double)), pA, na + 1, pB,
+                             M + 2, 0, None) == 0
+    xk.sync()
+    T = _op(torch.tril(A) if uplo == 1 else torch.triu(A), trans)
+    lhs = T @ B if side == 0 else B @ T
+    res = (lhs - 2.0 * B0).abs().max().item()
+    assert res <= 64 * EPS * na * (1 + B0.abs().max().item()), res
+    assert lib.xkb_cuda_take_device_error() == 0
+
+
 def test_ozaki_unaligned(xk):
     import torch
     g = torch.Generator(device="cuda").manual_seed(42)
