@@ -168,7 +168,7 @@ class TraceRec(ctypes.Structure):
 
 
 def other_configs(lib, torch, dev, sp, stream):
-    """The remaining BASELINE configurations, device resident, plain FP64
+    """The remaining benchmark workloads, device resident, plain FP64
     DMMA vs Ozaki: DGEMM 1024^3 (alpha 1.5, beta -0.5), DTRSM L/L/N/N 4096
     (alpha 2, A lower + 4096 on the diagonal), DSYRK and ZHERK L/N
     N = K = 8192 (alpha = beta = 1).  Flops: reference blas/flops.h."""
@@ -799,7 +799,7 @@ def main():
                                      "value": flops / (min(t16) * 1e-3) / 1e12,
                                      "unit": "TFLOP/s", "ms": min(t16)}
         # accuracy against the double-double oracle and the CPU baseline
-        # (bounded samples; checker / baseline only)
+        # (bounded samples: the oracle only compares and times the CPU leg)
         Co = np.asfortranarray(dC.cpu().numpy().T)
         Cp = np.asfortranarray(dP.cpu().numpy().T)
         C16 = np.asfortranarray(d16.cpu().numpy().T)

@@ -1,7 +1,8 @@
 """ctypes binding of the CPU oracle (libxkb_oracle.so).
 
 TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and
-the CPU-baseline leg of bench.py, always as the checker.  The library under
+the CPU-baseline leg of bench.py, always as the reference results are
+compared with.  The library under
 test (xkblas_b200 / libxkblas.so) never imports or links this package.
 """
 import ctypes

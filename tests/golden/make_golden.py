@@ -29,7 +29,7 @@ def main():
     O.blas_open(threads=1)
     rec = {}
     seed = 11
-    # GEMM: all trans pairs, ragged sizes, alpha/beta from the BASELINE config 1
+    # GEMM: all trans pairs, ragged sizes, alpha 1.5 / beta -0.5 as in the DGEMM 1024^3 workload
     for cplx in (False, True):
         ops = (O.NOTRANS, O.TRANS, O.CONJTRANS) if cplx else (O.NOTRANS, O.TRANS)
         for ta in ops:
