@@ -331,7 +331,9 @@ int  xkblas_last_device_error(void);
  * at initialisation and writes the tables into <dir> at the last
  * xkblas_finalize.  Tables (same headers and columns as the converter):
  *   kern.csv      kernel launches: Resource,Type,Stream,Push,Start,End,
- *                 Duration,Name ("<call>/<kernel>"),TaskId
+ *                 Duration,Name ("<call>/<kernel>"),TaskId; an executor
+ *                 launch ("batch/k_sched") is followed by one row per call
+ *                 ("batch/<call>#<i>", ending at the call's completion)
  *   cpy.csv       host<->device copies: ...,Size (bytes),Dir (1 H2D, 2 D2H)
  *   call.csv      API calls: Resource,Level,Start,End (the xkblas_sync that
  *                 completed it),Duration,Name,NParam,Param0..Param15

@@ -7,6 +7,7 @@ B200."""
 import csv
 import ctypes
 import os
+import re
 import subprocess
 import sys
 
@@ -80,13 +81,26 @@ def test_tables_describe_the_work(xk, rec, tmp_path):
     cpy = _rows(tmp_path / "cpy.csv")
     calls = _rows(tmp_path / "call.csv")
     assert kern, "no kernel recorded"
+    per_call = []
     for r in kern:
         call, _, kname = r["Name"].partition("/")
         assert call in ("dgemm", "dtrsm", "batch"), r["Name"]
-        assert kname in KERNELS, r["Name"]
+        if re.fullmatch(r"(dgemm|zgemm|dtrsm|ztrsm)#\d+", kname):
+            per_call.append(r)  # one call of an executor launch
+        else:
+            assert kname in KERNELS, r["Name"]
         assert r["Type"] == "CUDA" and r["Stream"] == "3"
         assert _f(r, "End") >= _f(r, "Start") >= _f(r, "Push") - 1e-3
         assert abs(_f(r, "Duration") - (_f(r, "End") - _f(r, "Start"))) < 1e-9
+    # the two independent calls were queued and ran as one executor launch
+    # (flushed by the first coherence call): one row per call inside it
+    launches = [r for r in kern if r["Name"] in ("batch/k_sched", "batch/k_sched(graph)")]
+    assert len(launches) == 1, [r["Name"] for r in kern]
+    assert sorted(r["Name"] for r in per_call) == ["batch/dgemm#0", "batch/dtrsm#1"]
+    k = launches[0]
+    for r in per_call:
+        assert r["Start"] == k["Start"]
+        assert _f(r, "End") <= _f(k, "End") + 1e-4
     # the copies are exactly the bytes the directory moved
     h2d = [r for r in cpy if r["Dir"] == "1"]
     d2h = [r for r in cpy if r["Dir"] == "2"]

@@ -37,6 +37,12 @@ struct DevRec {  // a kernel or a copy, bracketed by two events
   int dir = 0;
   bool ended = false;
   char name[64] = {0};
+  // executor launch: per-call completion stamps copied back after it
+  unsigned long long* h_times = nullptr;  // pinned, n + 1 entries
+  cudaEvent_t e_times = nullptr;
+  int ncalls = 0;
+  std::vector<std::string> call_names;
+  uint64_t first_call_id = 0;
 };
 
 struct CallRec {
@@ -168,6 +174,13 @@ void dev_end(std::vector<DevRec>& tab, long long id, cudaStream_t st) {
     }
 }
 
+void release_calls(DevRec& r, Log& l) {
+  if (r.h_times) cudaFreeHost(r.h_times);
+  if (r.e_times) l.spare.push_back(r.e_times);
+  r.h_times = nullptr;
+  r.e_times = nullptr;
+}
+
 // device time of `e` in seconds since t0; false if it cannot be read
 bool dev_time(Log& l, cudaEvent_t e, double* t) {
   float ms = 0;
@@ -194,6 +207,39 @@ long long evlog_kern_begin(cudaStream_t st, const char* kernel) {
   return dev_begin(L().kern, st, 3, kernel, 0, 0);
 }
 void evlog_kern_end(long long id, cudaStream_t st) { dev_end(L().kern, id, st); }
+
+void evlog_kern_calls(long long id, cudaStream_t st, const unsigned long long* d_times, int n,
+                      const char* const* names) {
+  if (id < 0 || n <= 0 || !d_times) return;
+  Log& l = L();
+  std::lock_guard<std::mutex> g(l.mu);
+  for (size_t i = l.kern.size(); i-- > 0;) {
+    DevRec& r = l.kern[i];
+    if (r.id != (uint64_t)id) continue;
+    void* h = nullptr;
+    if (cudaMallocHost(&h, ((size_t)n + 1) * sizeof(unsigned long long)) != cudaSuccess) {
+      cudaGetLastError();
+      ++l.dropped;
+      return;
+    }
+    r.h_times = static_cast<unsigned long long*>(h);
+    r.e_times = take_event(l);
+    if (!r.e_times ||
+        cudaMemcpyAsync(r.h_times, d_times, ((size_t)n + 1) * sizeof(unsigned long long),
+                        cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaEventRecord(r.e_times, st) != cudaSuccess) {
+      cudaGetLastError();
+      release_calls(r, l);
+      ++l.dropped;
+      return;
+    }
+    r.ncalls = n;
+    r.call_names.assign(names, names + n);
+    r.first_call_id = l.next_id;
+    l.next_id += (uint64_t)n;
+    return;
+  }
+}
 
 long long evlog_copy_begin(cudaStream_t st, size_t bytes, int dir) {
   return dev_begin(L().cpy, st, dir == 1 ? 0 : 1, nullptr, bytes, dir);
@@ -298,6 +344,19 @@ extern "C" int xkblas_trace_export(const char* dir) {
       }
       std::fprintf(fk, "%i,CUDA,%i,%.15f,%.15f,%.15f,%.15f,%s,%llu\n", r.device, r.stream, r.push,
                    s, e, e - s, r.name, (unsigned long long)r.id);
+      if (r.h_times && r.e_times && cudaEventSynchronize(r.e_times) == cudaSuccess) {
+        const unsigned long long t0 = r.h_times[r.ncalls];
+        for (int i = 0; i < r.ncalls; ++i) {
+          const unsigned long long ti = r.h_times[i];
+          if (!ti || ti < t0) continue;  // a call without tasks
+          const double ce = s + 1e-9 * (double)(ti - t0);
+          std::fprintf(fk, "%i,CUDA,%i,%.15f,%.15f,%.15f,%.15f,batch/%s#%i,%llu\n", r.device,
+                       r.stream, r.push, s, ce, ce - s, r.call_names[i].c_str(), i,
+                       (unsigned long long)(r.first_call_id + (uint64_t)i));
+        }
+      } else if (r.h_times) {
+        cudaGetLastError();
+      }
     }
     for (const DevRec& r : l.cpy) {
       double s, e;
@@ -342,6 +401,7 @@ extern "C" int xkblas_trace_export(const char* dir) {
         if (r.ended) {
           l.spare.push_back(r.b);
           l.spare.push_back(r.e);
+          release_calls(r, l);
         }
     l.kern.swap(kept_k);
     l.cpy.swap(kept_c);

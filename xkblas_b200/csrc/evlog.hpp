@@ -20,6 +20,13 @@ bool evlog_on();
 // Returns -1 (and records nothing) while recording is off.
 long long evlog_kern_begin(cudaStream_t st, const char* kernel);
 void evlog_kern_end(long long id, cudaStream_t st);
+// The executor launch `id` ran `n` calls: `d_times` holds, in globaltimer
+// nanoseconds, each call's completion (0 if it had no task) followed by the
+// launch's first task start; they are copied back on `st` after the launch
+// and written as one row per call ("batch/<name>#<i>", start = the launch's
+// start, end = start + the call's completion delay).
+void evlog_kern_calls(long long id, cudaStream_t st, const unsigned long long* d_times, int n,
+                      const char* const* names);
 // A host<->device copy of `bytes` on `st`; dir uses the reference's
 // direction table (bin/ukilli.cpp:223): 1 = H2D, 2 = D2H.
 long long evlog_copy_begin(cudaStream_t st, size_t bytes, int dir);

@@ -941,6 +941,17 @@ static int set_smem_attr() {
   return XKB_OK;
 }
 
+// Per-call rows of an executor launch in the event trace (recording on).
+static void trace_calls(long long tv, cudaStream_t st, const unsigned long long* d_times,
+                        const xkb_batch_op* ops, int n) {
+  if (tv < 0) return;
+  static const char* const kNames[2][2] = {{"dgemm", "zgemm"}, {"dtrsm", "ztrsm"}};
+  std::vector<const char*> names((size_t)n);
+  for (int i = 0; i < n; ++i)
+    names[i] = kNames[ops[i].kind == XKB_BATCH_TRSM][ops[i].dtype == XKB_Z];
+  evlog_kern_calls(tv, st, d_times, n, names.data());
+}
+
 static int launch_entry(Batch& B, GraphEntry* e, cudaStream_t st) {
   e->last_use = ++B.tick;
   B.ncalls = e->L.nops;
@@ -950,6 +961,7 @@ static int launch_entry(Batch& B, GraphEntry* e, cudaStream_t st) {
   const cudaError_t le = cudaGraphLaunch(e->exec, st);
   evlog_kern_end(tv, st);
   if (le != cudaSuccess) return XKB_ECUDA;
+  trace_calls(tv, st, e->d_times, e->ops.data(), e->L.nops);
   count_launch();
   return XKB_OK;
 }
@@ -1170,6 +1182,7 @@ extern "C" int xkb_cuda_batch(const xkb_batch_op* ops, int nops, int schedule, v
                                               a.nurg, a.ctl, a.urgent_first, a.left,
                                               a.call_end, a.t_start);
   evlog_kern_end(tv, st);
+  trace_calls(tv, st, B.d_times, ops, nops);
   count_launch();
   // the pinned staging buffer must outlive the copy: the copy is ordered
   // before the kernel, and the next batch synchronises before reusing it
