@@ -340,7 +340,9 @@ int  xkblas_last_device_error(void);
  *   task.csv      API calls as host tasks (entry to return)
  *   parallel.csv  the host threads and the GPU over the recording
  * Times are seconds since recording started; device times come from CUDA
- * events on the launching stream.  Export drains what it wrote. */
+ * events on the launching stream.  Export drains what it wrote.  Record
+ * eager execution only: inside a caller's CUDA-graph capture the recorder's
+ * events and copies would become part of the graph. */
 int      xkblas_trace_record(int on);           /* returns the previous state */
 int      xkblas_trace_export(const char* dir);  /* 0, EINVAL or EIO */
 uint64_t xkblas_trace_dropped(void);            /* events not recorded (table full) */
