@@ -116,8 +116,11 @@ int xkb_cuda_ozaki_gemm_panels(const xkb_gemm_args* a, int nmod, void* stream, i
  * inside the library (about 12.6 MiB per GPU that loads it, held until the
  * process exits).  M, N, K <= 512, otherwise XKB_ERANGE; nmod as above.
  * Every call uses the same array, so calls that overlap on the GPU race:
- * serialise them.  The first call on a device looks the array up (once per
- * device); make it before any stream capture. */
+ * serialise them.  The array and this path's kernels are placed in device
+ * memory by xkblas_init() (for its device) or else by the first call on a
+ * device, which looks the array up once per device (again after a
+ * cudaDeviceReset); make that call, or xkblas_init(), before handing the
+ * free device memory to another allocator and before any stream capture. */
 int xkb_cuda_ozaki_gemm_noalloc(const xkb_gemm_args* a, int nmod, void* stream);
 
 /* Number of moduli the Ozaki path uses for contraction length K (0 if K is

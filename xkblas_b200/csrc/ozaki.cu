@@ -1494,9 +1494,19 @@ extern "C" int xkb_cuda_ozaki_gemm_panels(const xkb_gemm_args* a, int nmod, void
 //   * all calls share it: two calls whose kernels overlap on the GPU (other
 //     streams, other host threads) race on it and corrupt each other --
 //     serialise them;
-//   * the first call on a device looks the array's device address up with
-//     cudaGetSymbolAddress (once per device, with that device current); make
-//     that first call before capturing a stream.
+//   * the array is placed in device memory when this file's CUDA module is
+//     loaded, which with lazy module loading (the CUDA 12 default) happens
+//     at its first use, not when the library is opened.  noalloc_prepare()
+//     -- run by xkblas_init() for its device, or else by the first call of
+//     this entry point on a device -- looks the array's address up with
+//     cudaGetSymbolAddress (that device current), which loads the module, and
+//     loads every kernel this entry point launches.  A caller that is about
+//     to hand the free device memory to its own allocator therefore calls
+//     xkblas_init() (or this entry point once) first; that first call should
+//     also come before any stream capture;
+//   * the address is cached per device together with the CUDA context's
+//     unique ID; after cudaDeviceReset() the next call sees a new context and
+//     looks the (reloaded) array up again.
 // Nothing in the array has to start at zero: every byte a call reads is
 // written earlier in the same call (planes padded by the residue kernel and a
 // 2-D memset, shifts and partials fully rewritten).
@@ -1516,25 +1526,104 @@ constexpr size_t kNoAllocBytes =
 
 static __device__ __align__(256) unsigned char g_oz_noalloc_scratch[kNoAllocBytes];
 
-// Device address of the array, looked up once per device.
+// C <- beta C on the masked part (beta == 0 writes zeros without reading),
+// for K == 0 or alpha == 0: kept in this file so that the scratch-free path
+// launches only kernels of this module (loaded by noalloc_prepare).
+__global__ void k_oz_beta(int M, int N, double beta, double* C, long ldc, int uplo, long diag) {
+  const size_t total = (size_t)M * (size_t)N;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total;
+       e += (size_t)gridDim.x * blockDim.x) {
+    const long i = (long)(e % (size_t)M), j = (long)(e / (size_t)M);
+    if (uplo == XKB_LOWER && i + diag < j) continue;
+    if (uplo == XKB_UPPER && i + diag > j) continue;
+    double* c = C + (size_t)i + (size_t)j * (size_t)ldc;
+    *c = beta != 0.0 ? beta * *c : 0.0;
+  }
+}
+
+typedef CUresult (*PFN_ctxGetCurrent)(CUcontext*);
+typedef CUresult (*PFN_ctxGetId)(CUcontext, unsigned long long*);
+
+// Unique ID of the calling thread's current CUDA context (0 if unknown or
+// none is current).
+static unsigned long long current_ctx_id() {
+  static PFN_ctxGetCurrent get_cur = nullptr;
+  static PFN_ctxGetId get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_cur = reinterpret_cast<PFN_ctxGetCurrent>(p);
+    p = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<PFN_ctxGetId>(p);
+    cudaGetLastError();
+  });
+  CUcontext ctx = nullptr;
+  unsigned long long id = 0;
+  if (!get_cur || !get_id || get_cur(&ctx) != CUDA_SUCCESS || !ctx) return 0;
+  if (get_id(ctx, &id) != CUDA_SUCCESS) return 0;
+  return id;
+}
+
+// Kernels the scratch-free path launches, loaded up front (with lazy loading
+// a kernel's code is otherwise placed in device memory at its first launch).
+template <int NM>
+static bool load_nm_kernels() {
+  cudaFuncAttributes fa;
+  return cudaFuncGetAttributes(&fa, k_oz_residues<true, NM>) == cudaSuccess &&
+         cudaFuncGetAttributes(&fa, k_oz_residues<false, NM>) == cudaSuccess &&
+         cudaFuncGetAttributes(&fa, k_oz_crt<NM>) == cudaSuccess;
+}
+static bool load_noalloc_kernels() {
+  cudaFuncAttributes fa;
+  bool ok = cudaFuncGetAttributes(&fa, k_oz_norm<true>) == cudaSuccess &&
+            cudaFuncGetAttributes(&fa, k_oz_norm<false>) == cudaSuccess &&
+            cudaFuncGetAttributes(&fa, k_oz_shift) == cudaSuccess &&
+            cudaFuncGetAttributes(&fa, k_oz_gemm) == cudaSuccess &&
+            cudaFuncGetAttributes(&fa, k_oz_beta) == cudaSuccess;
+  ok = ok && load_nm_kernels<2>() && load_nm_kernels<3>() && load_nm_kernels<4>() &&
+       load_nm_kernels<5>() && load_nm_kernels<6>() && load_nm_kernels<7>() &&
+       load_nm_kernels<8>() && load_nm_kernels<9>() && load_nm_kernels<10>() &&
+       load_nm_kernels<11>() && load_nm_kernels<12>() && load_nm_kernels<13>() &&
+       load_nm_kernels<14>() && load_nm_kernels<15>() && load_nm_kernels<16>();
+  return ok;
+}
+
+// Device address of the array for the current device, looked up when the
+// device's context is seen for the first time (once per device, unless the
+// context is reset).
 static int noalloc_base(unsigned char** out) {
   static std::mutex mu;
   static unsigned char* ptr[64] = {nullptr};
+  static unsigned long long ctx_of[64] = {0};
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return XKB_ECUDA;
   std::lock_guard<std::mutex> g(mu);
-  if (!ptr[dev]) {
+  const unsigned long long id = current_ctx_id();
+  if (!ptr[dev] || id == 0 || id != ctx_of[dev]) {
     void* p = nullptr;
-    if (cudaGetSymbolAddress(&p, g_oz_noalloc_scratch) != cudaSuccess || !p) {
+    if (cudaGetSymbolAddress(&p, g_oz_noalloc_scratch) != cudaSuccess || !p ||
+        !load_noalloc_kernels()) {
       cudaGetLastError();
+      ptr[dev] = nullptr;
       return XKB_ECUDA;
     }
     ptr[dev] = static_cast<unsigned char*>(p);
+    ctx_of[dev] = current_ctx_id();  // the lookup made the primary context current
   }
   *out = ptr[dev];
   return XKB_OK;
 }
 }  // namespace oz
+
+int noalloc_prepare() {
+  unsigned char* p = nullptr;
+  return oz::noalloc_base(&p);
+}
 }  // namespace xkb
 
 extern "C" int xkb_cuda_ozaki_gemm_noalloc(const xkb_gemm_args* a, int nmod, void* stream) {
@@ -1542,14 +1631,26 @@ extern "C" int xkb_cuda_ozaki_gemm_noalloc(const xkb_gemm_args* a, int nmod, voi
   if (a->M < 0 || a->N < 0 || a->K < 0) return XKB_EINVAL;
   if (a->M > kNoAllocMaxDim || a->N > kNoAllocMaxDim || a->K > kNoAllocMaxDim) return XKB_ERANGE;
   if (a->M == 0 || a->N == 0) return XKB_OK;
-  if (a->K == 0 || a->alpha[0] == 0.0) return xkb_cuda_gemm(a, stream);  // beta*C only
-  if (nmod == 0) nmod = default_moduli(a->K);
+  if (a->K > 0 && a->alpha[0] != 0.0 && (a->opA < XKB_OP_N || a->opA > XKB_OP_C ||
+                                         a->opB < XKB_OP_N || a->opB > XKB_OP_C))
+    return XKB_EINVAL;
+  if (nmod == 0) nmod = default_moduli(a->K > 0 ? a->K : 1);
   const Consts* c = consts_for(nmod);
   if (!c) return XKB_ERANGE;
   unsigned char* base = nullptr;
   int err = noalloc_base(&base);
   if (err) return err;
   cudaStream_t st = resolve_stream(stream);
+  if (a->K == 0 || a->alpha[0] == 0.0) {  // beta C only
+    const size_t total = (size_t)a->M * (size_t)a->N;
+    const unsigned blocks = (unsigned)std::min<size_t>((total + 255) / 256, 1024);
+    const long long tv = evlog_kern_begin(st, "k_oz_beta");
+    k_oz_beta<<<blocks, 256, 0, st>>>(a->M, a->N, a->beta[0], static_cast<double*>(a->C), a->ldc,
+                                      a->uplo, a->diag);
+    evlog_kern_end(tv, st);
+    count_launch();
+    return cudaPeekAtLastError() == cudaSuccess ? XKB_OK : XKB_ECUDA;
+  }
   const int M = a->M, N = a->N, K = a->K;
   const long Kpad = (long)rup(K, BKB), Mpad = (long)rup(M, BM), Npad = (long)rup(N, BN);
   const bool akc = a->opA != XKB_OP_N, bkc = a->opB == XKB_OP_N;
@@ -1564,6 +1665,7 @@ extern "C" int xkb_cuda_ozaki_gemm_noalloc(const xkb_gemm_args* a, int nmod, voi
   double2* part = reinterpret_cast<double2*>(base + kNoAllocA + kNoAllocB + kNoAllocR + kNoAllocShift);
   const double* Ad = static_cast<const double*>(a->A);
   const double* Bd = static_cast<const double*>(a->B);
+  const int slot = trace_begin("ozaki_noalloc", a->dtype, M, N, K, nmod, st);
   View va{Ad, a->lda, akc, 1, 0, 1.0}, vb{Bd, a->ldb, bkc, 1, 0, 1.0};
   err = launch_norm(va, M, K, 0, c, part, mu, st);
   if (!err) err = launch_norm(vb, N, K, 0, c, part + kNoAllocRows, nu, st);
@@ -1576,9 +1678,11 @@ extern "C" int xkb_cuda_ozaki_gemm_noalloc(const xkb_gemm_args* a, int nmod, voi
          cudaMemset2DAsync(Bp + kz, Kpad, 0, Kpad - kz, (size_t)nmod * Npad, st) != cudaSuccess))
       err = XKB_ECUDA;
   }
+  trace_mark(slot, 1, st);
   if (!err)
     err = same ? launch_gemm(Ap, Arows, Ap, Arows, Mpad, Npad, Kpad, c, R, a->uplo, a->diag, st)
                : launch_gemm(Ap, Mpad, Bp, Npad, Mpad, Npad, Kpad, c, R, a->uplo, a->diag, st);
+  trace_mark(slot, 2, st);
   if (!err) {
     CrtP cp;
     std::memset(&cp, 0, sizeof(cp));
@@ -1598,5 +1702,6 @@ extern "C" int xkb_cuda_ozaki_gemm_noalloc(const xkb_gemm_args* a, int nmod, voi
     const dim3 cg((unsigned)(((M + 3) / 4 + 255) / 256), (unsigned)N);
     err = launch_crt(cg, st, cp, *c, nullptr);
   }
+  trace_mark(slot, 3, st);
   return err;
 }

@@ -24,6 +24,7 @@
 
 namespace xkb {
 void set_library_stream(cudaStream_t s);
+int noalloc_prepare();  // ozaki.cu: places the scratch-free path's array and kernels
 }
 
 namespace xkbrt {
@@ -51,6 +52,11 @@ int ensure_init() {
   if (prop.major != 10) return XKB_ENODEV;  // kernels are built for sm_100a only
   if (cudaSetDevice(dev) != cudaSuccess) return XKB_ENODEV;
   R.device = dev;
+  // the fixed scratch array of xkb_cuda_ozaki_gemm_noalloc and that path's
+  // kernels are placed in device memory now, while memory is free, not at
+  // their first use (lazy module loading); a failure here is reported by
+  // that entry point's first call instead
+  if (xkb::noalloc_prepare() != XKB_OK) cudaGetLastError();
   {
     size_t fr = 0, total = 0;
     if (cudaMemGetInfo(&fr, &total) != cudaSuccess) {
