@@ -114,31 +114,55 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_baseline(budget_s=12.0):
-    """The reference's CPU path: OpenBLAS dgemm_ through the Fortran symbol
-    xkblas_dgemm_native loads (restated by the oracle), all host threads, on
-    a row sample of the workload sized to ~budget_s seconds."""
+def cpu_rows(step_s):
+    """Rows of the workload's A for one OpenBLAS dgemm_ row-block step of
+    about step_s seconds on all host threads (multiple of 64, 256..M)."""
     import oracle as O
-    path = O.blas_open(threads=os.cpu_count())
+    O.blas_open(threads=os.cpu_count())
     B = gen_expspread(K, N, 2, True)
-    rows = 64
+    rows = 256
     A = gen_expspread(rows, K, 1, False)
     C = np.zeros((rows, N), order="F")
+    O.native_gemm(O.NOTRANS, O.NOTRANS, 1.0, A, B, 0.0, C)  # first call: thread start-up
     t0 = time.perf_counter()
     O.native_gemm(O.NOTRANS, O.NOTRANS, 1.0, A, B, 0.0, C)
     t1 = time.perf_counter() - t0
-    rows = int(max(64, min(M, rows * budget_s / max(t1, 1e-3))))
-    rows = rows // 64 * 64
+    rows = int(max(256, min(M, rows * step_s / max(t1, 1e-3)))) // 64 * 64
+    return rows, B
+
+
+def cpu_gemm_steps(rows, B, nsteps):
+    """Seconds of each of nsteps OpenBLAS dgemm_ calls (the call
+    xkblas_dgemm_native makes, restated by the oracle) on the first `rows`
+    rows of the workload's A times its full B."""
+    import oracle as O
     A = gen_expspread(rows, K, 1, False)
     C = np.zeros((rows, N), order="F")
-    t0 = time.perf_counter()
-    O.native_gemm(O.NOTRANS, O.NOTRANS, 1.0, A, B, 0.0, C)
-    t = time.perf_counter() - t0
+    times = []
+    for _ in range(nsteps):
+        t0 = time.perf_counter()
+        O.native_gemm(O.NOTRANS, O.NOTRANS, 1.0, A, B, 0.0, C)
+        times.append(time.perf_counter() - t0)
+    return times
+
+
+CPU_STEP_S = 2.0  # seconds of host BLAS per sampled step (both arms)
+
+
+def cpu_sample_text(path, rows, t):
+    return ("OpenBLAS %s dgemm_ (the call xkblas_dgemm_native makes) on a %d x %d x %d row "
+            "block of the %d^3 workload per step, median step %.2f s"
+            % (os.path.basename(path or "libopenblas"), rows, N, K, M, t))
+
+
+def cpu_baseline(nsteps=3):
+    """The reference's CPU path on the box's host cores: the same row-block
+    steps as the reference arm (--impl reference), median of nsteps."""
+    import oracle as O
+    rows, B = cpu_rows(CPU_STEP_S)
+    t = statistics.median(cpu_gemm_steps(rows, B, nsteps))
     return {"value": 2.0 * rows * N * K / t / 1e12, "unit": "TFLOP/s", "cores": os.cpu_count(),
-            "kind": "port",
-            "sample": "OpenBLAS %s dgemm_ via the oracle's restatement of xkblas_dgemm_native; "
-                      "%d x %d x %d row block of the 16384^3 workload, %.1f s" % (
-                          os.path.basename(path), rows, N, K, t)}
+            "kind": "port", "sample": cpu_sample_text(O.find_openblas(), rows, t)}
 
 
 def dd_errors(A, B, Cs, nrow=16, ncol=256, seed=7):
@@ -157,14 +181,44 @@ def dd_errors(A, B, Cs, nrow=16, ncol=256, seed=7):
     return out
 
 
-from xkblas_b200 import GemmArgs  # xkb_gemm_args of include/xkb_cuda.h
+from xkblas_b200 import GemmArgs, TraceRec  # include/xkb_cuda.h structs
+
+def _cm(t):
+    """Device tensor holding a column-major matrix (a row-major tensor of its
+    transpose) -> Fortran-ordered host array of that matrix."""
+    return np.asfortranarray(t.cpu().numpy().T)
 
 
-class TraceRec(ctypes.Structure):
-    _fields_ = [("op", ctypes.c_char * 16), ("dtype", ctypes.c_int), ("M", ctypes.c_int),
-                ("N", ctypes.c_int), ("K", ctypes.c_int), ("nmod", ctypes.c_int),
-                ("ms_total", ctypes.c_float), ("ms_convert", ctypes.c_float),
-                ("ms_gemm", ctypes.c_float), ("ms_crt", ctypes.c_float)]
+def _pick(n, k, seed):
+    return np.sort(np.random.default_rng(seed).choice(n, min(n, k), replace=False))
+
+
+def dd_gemm_error(C, ta, tb, alpha, A, B, beta, C0, rows, cols, mask=None):
+    """max |C - C_dd| / (|alpha||op(A)||op(B)| + |beta||C0|) over sampled
+    entries (C_dd: the double-double oracle rounded once)."""
+    import oracle as O
+    A, B = np.asfortranarray(A), np.asfortranarray(B)
+    C0 = np.asfortranarray(C0) if C0 is not None else None
+    dd = O.gemm_dd(ta, tb, alpha, A, B, beta, C0, rows, cols)
+    opA = A if ta == O.NOTRANS else (A.T if ta == O.TRANS else A.conj().T)
+    opB = B if tb == O.NOTRANS else (B.T if tb == O.TRANS else B.conj().T)
+    scale = abs(alpha) * (np.abs(opA[rows]) @ np.abs(opB[:, cols]))
+    if C0 is not None and beta != 0:
+        scale = scale + abs(beta) * np.abs(C0[np.ix_(rows, cols)])
+    e = np.abs(C[np.ix_(rows, cols)] - dd) / scale
+    return float(e[mask].max() if mask is not None else e.max())
+
+
+def dd_backward_error(L, R, P, rows, cols, alpha=1.0):
+    """Componentwise backward error of a solve or factorization on sampled
+    entries: |L R - alpha P| / (|L||R| + |alpha||P|), the residual in
+    double-double (L R - alpha P = 0 defines the exact answer)."""
+    import oracle as O
+    L, R, P = np.asfortranarray(L), np.asfortranarray(R), np.asfortranarray(P)
+    res = O.gemm_dd(O.NOTRANS, O.NOTRANS, 1.0, L, R, -alpha, P, rows, cols)
+    den = np.abs(L[rows]) @ np.abs(R[:, cols]) + abs(alpha) * np.abs(P[np.ix_(rows, cols)])
+    return float(np.max(np.abs(res) / den))
+
 
 
 def other_configs(lib, torch, dev, sp, stream):
@@ -208,10 +262,17 @@ def other_configs(lib, torch, dev, sp, stream):
     fl = 2.0 * n ** 3
     with torch.cuda.stream(stream):
         rs = lambda: C.copy_(C0)
-        tp = timed(lambda: lib.xkb_cuda_gemm(ctypes.byref(ga), sp), 10, rs)
         to = timed(lambda: lib.xkb_cuda_ozaki_gemm(ctypes.byref(ga), 0, sp), 10, rs)
-    out["dgemm_nn_1024_nb256"] = {"plain_tflops": fl / tp / 1e9, "ozaki_tflops": fl / to / 1e9,
-                                  "plain_ms": tp, "ozaki_ms": to}
+        Co = _cm(C)
+        tp = timed(lambda: lib.xkb_cuda_gemm(ctypes.byref(ga), sp), 10, rs)
+        Cp = _cm(C)
+    hA, hB, hC0 = _cm(A), _cm(B), _cm(C0)
+    r, c = _pick(n, 64, 1), _pick(n, 64, 2)
+    out["dgemm_nn_1024_nb256"] = {
+        "plain_tflops": fl / tp / 1e9, "ozaki_tflops": fl / to / 1e9, "plain_ms": tp, "ozaki_ms": to,
+        "error_vs_dd": {k: dd_gemm_error(X_, 111, 111, 1.5, hA, hB, -0.5, hC0, r, c)
+                        for k, X_ in (("plain", Cp), ("ozaki", Co))},
+        "error_kind": "componentwise |C - C_dd| / (|alpha||A||B| + |beta||C0|), 64 x 64 sampled"}
     del A, B, C, C0
     # config 2: DTRSM L/L/N/N 4096, alpha 2
     n = 4096
@@ -226,16 +287,31 @@ def other_configs(lib, torch, dev, sp, stream):
         rs = lambda: B.copy_(B0)
         tp = timed(lambda: lib.xkb_cuda_trsm(1, 0, 1, 0, 0, n, n, al, Acm.data_ptr(), n,
                                              B.data_ptr(), n, 0, sp), 5, rs)
+        Xp = _cm(B)
         to = timed(lambda: lib.xkb_cuda_trsm(1, 0, 1, 0, 0, n, n, al, Acm.data_ptr(), n,
                                              B.data_ptr(), n, 1024, sp), 5, rs)
-    out["dtrsm_llnn_4096"] = {"plain_tflops": fl / tp / 1e9, "ozaki_tflops": fl / to / 1e9,
-                              "plain_ms": tp, "ozaki_ms": to}
+        Xo = _cm(B)
+    hA, hB0 = np.asfortranarray(A.cpu().numpy()), _cm(B0)
+    r, c = _pick(n, 48, 3), _pick(n, 48, 4)
+    out["dtrsm_llnn_4096"] = {
+        "plain_tflops": fl / tp / 1e9, "ozaki_tflops": fl / to / 1e9, "plain_ms": tp, "ozaki_ms": to,
+        "error_vs_dd": {k: dd_backward_error(hA, X_, hB0, r, c, alpha=2.0)
+                        for k, X_ in (("plain", Xp), ("ozaki", Xo))},
+        "error_kind": "componentwise backward error |A X - 2 B| / (|A||X| + 2|B|), residual in "
+                      "double-double, 48 x 48 sampled"}
     del A, Acm, B, B0
     # config 3: DSYRK / ZHERK lower, no-trans, N = K = 8192
     n = 8192
     for name, cplx, code, mult in (("dsyrk_ln_8192", False, 1, 1.0), ("zherk_ln_8192", True, 3, 4.0)):
         A = u(n, n, cplx=cplx)
-        C0 = u(n, n, cplx=cplx)
+        # C symmetric / Hermitian with the same entry distribution: the lower
+        # triangle of a uniform matrix mirrored (conjugated), real diagonal
+        U = u(n, n, cplx=cplx)
+        H = torch.tril(U) + torch.tril(U, -1).conj().t()
+        if cplx:
+            H.diagonal().imag.zero_()
+        C0 = H.t().contiguous()  # column-major storage of H
+        del U, H
         C = C0.clone()
         gs = GemmArgs(code, 0, 2 if cplx else 1, n, n, n, A.data_ptr(), n, A.data_ptr(), n,
                       C.data_ptr(), n)
@@ -246,10 +322,21 @@ def other_configs(lib, torch, dev, sp, stream):
         with torch.cuda.stream(stream):
             rs = lambda: C.copy_(C0)
             tp = timed(lambda: lib.xkb_cuda_gemm(ctypes.byref(gs), sp), 2, rs)
+            Cp = _cm(C)
             to = timed(lambda: lib.xkb_cuda_ozaki_gemm(ctypes.byref(gs), 0, sp), 3, rs)
-        out[name] = {"plain_tflops": fl / tp / 1e9, "ozaki_tflops": fl / to / 1e9,
-                     "plain_ms": tp, "ozaki_ms": to}
-        del A, C, C0
+            Co = _cm(C)
+        hA, hC0 = _cm(A), _cm(C0)
+        r = _pick(n, 64, 5)
+        c = np.unique(np.concatenate([r[:32], _pick(n, 32, 6)]))
+        low = r[:, None] >= c[None, :]
+        out[name] = {
+            "plain_tflops": fl / tp / 1e9, "ozaki_tflops": fl / to / 1e9, "plain_ms": tp,
+            "ozaki_ms": to,
+            "error_vs_dd": {k: dd_gemm_error(X_, 111, 113 if cplx else 112, 1.0, hA, hA, 1.0, hC0,
+                                             r, c, mask=low)
+                            for k, X_ in (("plain", Cp), ("ozaki", Co))},
+            "error_kind": "componentwise, lower-triangle entries of a 64 x 64 sample"}
+        del A, C, C0, Cp, Co, hA, hC0
     # Cholesky (a next-row driver on the same kernels): DPOTRF lower 8192,
     # A = B B^T / n + I; flops n^3/3 + n^2/2 + n/6 (reference flops.h)
     n = 8192
@@ -262,12 +349,22 @@ def other_configs(lib, torch, dev, sp, stream):
         tp = timed(lambda: lib.xkb_cuda_potrf(1, 1, n, ctypes.c_void_p(A.data_ptr()), n,
                                               ctypes.c_void_p(info.data_ptr()), 0, sp), 3, rs)
         info_p = int(info.item())
+        Lp = np.tril(_cm(A))
         # tensor-op mode: updates with all dimensions >= 2048 in the Ozaki form
         to = timed(lambda: lib.xkb_cuda_potrf(1, 1, n, ctypes.c_void_p(A.data_ptr()), n,
                                               ctypes.c_void_p(info.data_ptr()), 2048, sp), 3, rs)
+        Lo = np.tril(_cm(A))
     fl = n ** 3 / 3.0 + n * n / 2.0 + n / 6.0
-    out["dpotrf_l_8192"] = {"plain_tflops": fl / tp / 1e9, "ozaki_tflops": fl / to / 1e9,
-                            "plain_ms": tp, "ozaki_ms": to, "info": max(info_p, int(info.item()))}
+    hA0 = _cm(A0)
+    r, c = _pick(n, 48, 7), _pick(n, 48, 8)
+    out["dpotrf_l_8192"] = {
+        "plain_tflops": fl / tp / 1e9, "ozaki_tflops": fl / to / 1e9, "plain_ms": tp, "ozaki_ms": to,
+        "info": max(info_p, int(info.item())),
+        "error_vs_dd": {k: dd_backward_error(L_, np.asfortranarray(L_.T), hA0, r, c)
+                        for k, L_ in (("plain", Lp), ("ozaki", Lo))},
+        "error_kind": "componentwise backward error |L L^T - A| / (|L||L^T| + |A|), residual in "
+                      "double-double, 48 x 48 sampled"}
+    del Lp, Lo, hA0
     del Bm, A0, A, info
     # LU without pivoting (the zgetrf_nopiv tile driver): DGETRF 8192 on a
     # diagonally dominant matrix; flops 2n^3/3 - n^2/2 + 5n/6 (reference flops.h)
@@ -279,12 +376,25 @@ def other_configs(lib, torch, dev, sp, stream):
         tp = timed(lambda: lib.xkb_cuda_getrf_nopiv(1, n, ctypes.c_void_p(A.data_ptr()), n,
                                                     ctypes.c_void_p(info.data_ptr()), 0, sp), 3, rs)
         info_p = int(info.item())
+        LUp = _cm(A)
         to = timed(lambda: lib.xkb_cuda_getrf_nopiv(1, n, ctypes.c_void_p(A.data_ptr()), n,
                                                     ctypes.c_void_p(info.data_ptr()), 2048, sp), 3, rs)
+        LUo = _cm(A)
     fl = 2.0 * n ** 3 / 3.0 - n * n / 2.0 + 5.0 * n / 6.0
-    out["dgetrf_nopiv_8192"] = {"plain_tflops": fl / tp / 1e9, "ozaki_tflops": fl / to / 1e9,
-                                "plain_ms": tp, "ozaki_ms": to,
-                                "info": max(info_p, int(info.item()))}
+    hA0 = _cm(A0)
+    r, c = _pick(n, 48, 9), _pick(n, 48, 10)
+
+    def lu_err(LU):
+        L = np.asfortranarray(np.tril(LU, -1) + np.eye(n))
+        return dd_backward_error(L, np.asfortranarray(np.triu(LU)), hA0, r, c)
+
+    out["dgetrf_nopiv_8192"] = {
+        "plain_tflops": fl / tp / 1e9, "ozaki_tflops": fl / to / 1e9, "plain_ms": tp, "ozaki_ms": to,
+        "info": max(info_p, int(info.item())),
+        "error_vs_dd": {"plain": lu_err(LUp), "ozaki": lu_err(LUo)},
+        "error_kind": "componentwise backward error |L U - A| / (|L||U| + |A|), residual in "
+                      "double-double, 48 x 48 sampled"}
+    del LUp, LUo, hA0
     del A0, A, info
     torch.cuda.empty_cache()
     return out
@@ -363,6 +473,13 @@ def batch_config(lib, torch, dev, sp, stream, ncalls=2000, seed=2024, reps=5):
     torch.cuda.synchronize()
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
+    # accuracy sample: the first calls of each kind, inputs copied before the
+    # first submission (later submissions accumulate into the outputs)
+    sample = {"dgemm": [], "dtrsm": [], "zgemm": []}
+    for i, o in enumerate(ops):
+        kind = "dtrsm" if o.kind == 1 else ("zgemm" if o.dtype == 3 else "dgemm")
+        if len(sample[kind]) < 4:
+            sample[kind].append((i, [_cm(t) for t in keep[i]]))
     # first submission: host task construction + task upload + launch; the
     # second is kept as a CUDA graph, later ones replay it
     lib.xkb_cuda_batch_release()
@@ -374,6 +491,19 @@ def batch_config(lib, torch, dev, sp, stream, ncalls=2000, seed=2024, reps=5):
     ev1.record(stream)
     torch.cuda.synchronize()
     ms_first = ev0.elapsed_time(ev1)
+    errs = {}
+    for kind, lst in sample.items():
+        e = 0.0
+        for i, host in lst:
+            out = _cm(keep[i][-1])
+            r, c = _pick(out.shape[0], 16, i), _pick(out.shape[1], 16, i + 1)
+            if kind == "dtrsm":
+                # host[0]: the lower L (its column-major storage read back)
+                e = max(e, dd_backward_error(host[0], out, host[1], r, c))
+            else:
+                A_, B_, C0_ = host
+                e = max(e, dd_gemm_error(out, 111, 111, 1.0, A_, B_, 1.0, C0_, r, c))
+        errs[kind] = e
     k0 = lib.xkb_cuda_kernel_count()
     for _ in range(3):  # warm-up
         assert lib.xkb_cuda_batch(ctypes.addressof(arr), len(ops), 0, sp) == 0
@@ -435,7 +565,11 @@ def batch_config(lib, torch, dev, sp, stream, ncalls=2000, seed=2024, reps=5):
             "latency_ms_p99": float(np.percentile(lat, 99)),
             "per_call_launches": {"tflops": flops / ms_seq / 1e9, "ms": ms_seq,
                                   "launches": len(ops), "rejected_calls": int(rejected)},
-            "speedup_vs_per_call": ms_seq / ms}
+            "speedup_vs_per_call": ms_seq / ms,
+            "error_vs_dd": errs,
+            "error_kind": "max over the first 4 calls of each kind, 16 x 16 sampled entries each: "
+                          "gemm componentwise |C - C_dd| / (|A||B| + |C0|), trsm componentwise "
+                          "backward error with the residual in double-double"}
 
 
 def batch_config_e2e(lib, torch, ncalls=2000, seed=2024, reps=2):
@@ -553,34 +687,35 @@ def batch_config_e2e(lib, torch, ncalls=2000, seed=2024, reps=2):
     return out
 
 
+def workload_config(world):
+    """The `config` both arms print (the workload only)."""
+    return {"workload": WORKLOAD, "M": M, "N": N, "K": K, "exp_spread": EMAX,
+            "parallelism": "replicas" if world > 1 else "single",
+            "l2": "inputs 2 GiB each > 126 MB L2 (no flush needed)"}
+
+
 def run_reference(args, rank, world):
+    """The reference's own CPU implementation of the path (the host BLAS
+    through xkblas_dgemm_native's Fortran symbol), all host threads, on rank
+    0: warm-up + timed steps of the same row block cpu_baseline uses; the
+    value is the median step."""
     if rank != 0:
         return
     import oracle as O
-    O.blas_open(threads=os.cpu_count())
-    B = gen_expspread(K, N, 2, True)
-    rows = 256
-    A = gen_expspread(rows, K, 1, False)
-    C = np.zeros((rows, N), order="F")
-    times = []
-    for i in range(args.warmup + args.steps):
-        t0 = time.perf_counter()
-        O.native_gemm(O.NOTRANS, O.NOTRANS, 1.0, A, B, 0.0, C)
-        dt = time.perf_counter() - t0
-        if i >= args.warmup:
-            times.append(dt)
-    t = max(times)
+    rows, B = cpu_rows(CPU_STEP_S)
+    times = cpu_gemm_steps(rows, B, args.warmup + args.steps)[args.warmup:]
+    t = statistics.median(times)
     v = 2.0 * rows * N * K / t / 1e12
+    sample = cpu_sample_text(O.find_openblas(), rows, t)
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "TFLOP/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic",
-            "config": {"workload": WORKLOAD, "M": M, "N": N, "K": K, "sample_rows": rows},
-            "cpu_baseline": {"value": v, "unit": "TFLOP/s", "cores": os.cpu_count(), "kind": "port",
-                             "sample": "OpenBLAS dgemm_ (xkblas_dgemm_native's call) on a "
-                                       "%d-row block of the workload per step" % rows},
+            "data": "synthetic", "config": workload_config(world),
+            "cpu_baseline": {"value": v, "unit": "TFLOP/s", "cores": os.cpu_count(),
+                             "kind": "port", "sample": sample},
             "e2e": {"value": v, "unit": "TFLOP/s", "h2d_bytes_per_step": 0,
-                    "d2h_bytes_per_step": 0}}
+                    "d2h_bytes_per_step": 0},
+            "step_ms": {"min": min(times) * 1e3, "median": t * 1e3, "max": max(times) * 1e3}}
     print(json.dumps(line), flush=True)
 
 
@@ -733,7 +868,7 @@ def main():
         assert lib.xkblas_sync() == 0
         lib.xkblas_memory_invalidate_caches()
 
-    e2e_steps = max(2, min(args.steps, 3))
+    e2e_steps = args.steps
     for _ in range(2):
         e2e_step()
     barrier()
@@ -749,13 +884,11 @@ def main():
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": WORKLOAD, "M": M, "N": N, "K": K, "exp_spread": EMAX,
-                   "moduli": nmod,
-                   "moduli_choice": "autotuned (xkblas_b200.autotune.choose_moduli on a 1024x1024x%d "
-                                    "sample: plain err %.2e, %s)" % (
-                                        K, tune_err_plain, ", ".join("%d: %.2e" % e for e in tune_errs)),
-                   "parallelism": "replicas" if world > 1 else "single",
-                   "l2": "inputs 2 GiB each > 126 MB L2 (no flush needed)"},
+        "config": workload_config(world),
+        "ozaki": {"moduli": nmod,
+                  "moduli_choice": "autotuned (xkblas_b200.autotune.choose_moduli on a 1024x1024x%d "
+                                   "sample: plain err %.2e, %s)" % (
+                                       K, tune_err_plain, ", ".join("%d: %.2e" % e for e in tune_errs))},
         "e2e": {"value": e2e_value, "unit": "TFLOP/s",
                 "h2d_bytes_per_step": 2 * M * K * 8, "d2h_bytes_per_step": M * N * 8,
                 "ms_per_step": t_e2e * 1e3},

@@ -75,16 +75,20 @@ int xkb_cuda_trsm(int dtype, int side, int uplo, int trans, int diag, int M,
                   int N, const double* alpha, const void* A, long lda, void* B,
                   long ldb, int ozaki, void* stream);
 
-/* B <- alpha * op(A) * B (side L) or alpha * B * op(A) (side R). */
+/* B <- alpha * op(A) * B (side L) or alpha * B * op(A) (side R): one
+ * product with the triangle materialised; when ozaki > 0 and dtype is
+ * XKB_D/XKB_Z, a product whose three dimensions are all >= ozaki runs in the
+ * Ozaki INT8 form. */
 int xkb_cuda_trmm(int dtype, int side, int uplo, int trans, int diag, int M,
                   int N, const double* alpha, const void* A, long lda, void* B,
-                  long ldb, void* stream);
+                  long ldb, int ozaki, void* stream);
 
 /* C <- alpha*A*B + beta*C (side L) or alpha*B*A + beta*C, A symmetric
- * (herm = 0) or Hermitian (herm = 1) stored in its uplo triangle. */
+ * (herm = 0) or Hermitian (herm = 1) stored in its uplo triangle; ozaki as
+ * for xkb_cuda_trmm. */
 int xkb_cuda_symm(int dtype, int herm, int side, int uplo, int M, int N,
                   const double* alpha, const void* A, long lda, const void* B,
-                  long ldb, const double* beta, void* C, long ldc,
+                  long ldb, const double* beta, void* C, long ldc, int ozaki,
                   void* stream);
 
 /* C <- beta*C on the masked part (used for K == 0 / alpha == 0). */

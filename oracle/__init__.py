@@ -158,6 +158,9 @@ def gemm_dd(ta, tb, alpha, A, B, beta, C, rows, cols):
     double-double, rounded once.  Returns an (len(rows), len(cols)) array."""
     rows = np.ascontiguousarray(rows, dtype=np.int64)
     cols = np.ascontiguousarray(cols, dtype=np.int64)
+    _f(A), _f(B)
+    if C is not None:
+        _f(C)
     K = A.shape[1] if ta == NOTRANS else A.shape[0]
     Cp = C if C is not None else None
     if np.iscomplexobj(A):

@@ -174,9 +174,49 @@ def test_no_device_reports_enodev_not_fallback():
 
 
 def test_cuda_abi_rejects_bad_arguments_without_device():
+    """The thin CUDA ABI checks its arguments before touching a device, so
+    these codes are the same with or without a GPU."""
     lib = X.lib()
+    EINVAL, ERANGE = -1, -6
+    one = (ctypes.c_double * 2)(1.0, 0.0)
+    dp = ctypes.cast(one, ctypes.POINTER(ctypes.c_double))
+    # gemm: null record, negative size, unknown element type / op code
+    assert lib.xkb_cuda_gemm(None, None) == EINVAL
+    g = X.GemmArgs(1, 0, 0, -1, 4, 4, 16, 4, 16, 4, 16, 4)
+    assert lib.xkb_cuda_gemm(ctypes.byref(g), None) == EINVAL
+    g = X.GemmArgs(7, 0, 0, 4, 4, 4, 16, 4, 16, 4, 16, 4)
+    assert lib.xkb_cuda_gemm(ctypes.byref(g), None) == EINVAL
+    g = X.GemmArgs(1, 3, 0, 4, 4, 4, 16, 4, 16, 4, 16, 4)
+    assert lib.xkb_cuda_gemm(ctypes.byref(g), None) == EINVAL
+    # Ozaki: real or complex double only; sizes checked
+    g = X.GemmArgs(0, 0, 0, 4, 4, 4, 16, 4, 16, 4, 16, 4)
+    assert lib.xkb_cuda_ozaki_gemm(ctypes.byref(g), 0, None) == EINVAL
+    g = X.GemmArgs(1, 0, 0, 4, -4, 4, 16, 4, 16, 4, 16, 4)
+    assert lib.xkb_cuda_ozaki_gemm(ctypes.byref(g), 0, None) == EINVAL
+    # the scratch-free form: beyond its fixed array, or not real double
+    g = X.GemmArgs(1, 0, 0, 4, 4, 513, 16, 4, 16, 513, 16, 4)
+    assert lib.xkb_cuda_ozaki_gemm_noalloc(ctypes.byref(g), 0, None) == ERANGE
+    g = X.GemmArgs(3, 0, 0, 4, 4, 4, 16, 4, 16, 4, 16, 4)
+    assert lib.xkb_cuda_ozaki_gemm_noalloc(ctypes.byref(g), 0, None) == EINVAL
+    # trsm / trmm / symm / scale
+    assert lib.xkb_cuda_trsm(1, 0, 1, 0, 0, -1, 4, dp, 16, 4, 16, 4, 0, None) == EINVAL
+    assert lib.xkb_cuda_trsm(1, 0, 1, 5, 0, 4, 4, dp, 16, 4, 16, 4, 0, None) == EINVAL
+    assert lib.xkb_cuda_trsm(1, 0, 1, 0, 0, 4, 4, None, 16, 4, 16, 4, 0, None) == EINVAL
+    assert lib.xkb_cuda_trmm(9, 0, 1, 0, 0, 4, 4, dp, 16, 4, 16, 4, 0, None) == EINVAL
+    assert lib.xkb_cuda_symm(1, 0, 0, 1, 4, -2, dp, 16, 4, 16, 4, dp, 16, 4, 0, None) == EINVAL
+    assert lib.xkb_cuda_scale(1, 4, 4, None, 16, 4, 0, 0, 0, None) == EINVAL
+    # batch: null list or negative count; an empty list is a no-op
+    assert lib.xkb_cuda_batch(None, 3, 0, None) == EINVAL
+    ops = (X.BatchOp * 1)()
+    assert lib.xkb_cuda_batch(ops, -1, 0, None) == EINVAL
+    assert lib.xkb_cuda_batch(ops, 0, 0, None) == 0
+    # zero-sized products are no-ops that never reach the device
+    g = X.GemmArgs(1, 0, 0, 0, 4, 4, 16, 1, 16, 4, 16, 1)
+    assert lib.xkb_cuda_gemm(ctypes.byref(g), None) == 0
+    assert lib.xkb_cuda_ozaki_gemm(ctypes.byref(g), 0, None) == 0
+    assert lib.xkb_cuda_ozaki_gemm_noalloc(ctypes.byref(g), 0, None) == 0
 
-    
+
 
 def test_tuning_table_load_and_lookup(tmp_path):
     """The autotuner's table: a file of "key value" lines is loaded, values

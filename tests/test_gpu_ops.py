@@ -326,6 +326,44 @@ def test_coherence_uplo_writeback(xk):
         xk.set_param(0)
 
 
+def test_coherence_memflag_drops_other_triangle(xk):
+    """coherent_async(uplo, memflag = 1) writes back the uplo tiles and drops
+    the device copies of the others (reference blas/xkblas.c:2016-2049): a
+    later full coherence request copies nothing back for them, and the next
+    call reads them from the host again."""
+    N, K, nb = 512, 64, 128
+    xk.set_param(nb)
+    try:
+        A = O.plrnt(N, K, 910)
+        C0 = O.plrnt(N, N, 911)
+        C = C0.copy(order="F")
+        lib = xk.lib()
+        one = xk._scal(1.0, np.float64)
+        args = (N_, T_, N, N, K, xk._ptr(one), xk._ptr(A), N, xk._ptr(A), N, xk._ptr(one),
+                xk._ptr(C), N)
+        assert lib.xkblas_dgemm_async(*args) == 0
+        assert lib.xkblas_memory_coherent_async(LO, 1, N, N, xk._ptr(C), N, 8) == 0
+        xk.sync()
+        G = A @ A.T
+        # block-upper tiles (strictly above the diagonal tiles) were dropped
+        tile_up = np.kron(np.triu(np.ones((N // nb, N // nb), bool), 1), np.ones((nb, nb), bool))
+        np.testing.assert_allclose(C[~tile_up], (G + C0)[~tile_up], rtol=1e-13, atol=1e-12)
+        np.testing.assert_array_equal(C[tile_up], C0[tile_up])
+        # nothing of the dropped tiles comes back on a full request
+        assert lib.xkblas_memory_coherent_async(0, 0, N, N, xk._ptr(C), N, 8) == 0
+        xk.sync()
+        np.testing.assert_array_equal(C[tile_up], C0[tile_up])
+        # the next call reads the dropped tiles from the host again
+        H = C.copy(order="F")
+        assert lib.xkblas_dgemm_async(*args) == 0
+        assert lib.xkblas_memory_coherent_async(0, 0, N, N, xk._ptr(C), N, 8) == 0
+        xk.sync()
+        np.testing.assert_allclose(C, G + H, rtol=1e-13, atol=1e-12)
+        xk.invalidate_caches()
+    finally:
+        xk.set_param(0)
+
+
 def test_async_chain_without_host_round_trip(xk):
     """C1 = A B; C2 = C1 B (C1 consumed on the device, never copied back in
     between); only C2 is made coherent."""

@@ -236,3 +236,99 @@ def test_ozaki_cta_pair_kernel_matches(xk, mnk):
     ref = dB @ dA  # row-major N x M view of the column-major C = A B
     assert (out[0] - ref).abs().max().item() <= 4 * 2.0 ** -53 * K * 0.25 * 2
     assert lib.xkb_cuda_take_device_error() == 0
+
+
+# ---- the remaining level-3 operations in tensor-op mode ----------------------
+# Each call must run at least one Ozaki contraction (seen in the per-call
+# trace) and meet the reference test program's bound against the oracle.
+RIGHT, UNIT = 142, 132
+
+
+def _gen(M, N, seed, cplx):
+    return O.plrnt(M, N, seed, cplx)
+
+
+def _ran_ozaki(tr):
+    return "ozaki_gemm" in tr.ops()
+
+
+@pytest.mark.parametrize("cplx", [False, True])
+@pytest.mark.parametrize("uplo", [UP, LO])
+def test_ozaki_gemmt(tc, cplx, uplo):
+    N, K = 260, 190
+    A, B, C0 = _gen(N, K, 600, cplx), _gen(K, N, 601, cplx), _gen(N, N, 602, cplx)
+    C = C0.copy(order="F")
+    with tc.contraction_trace() as tr:
+        tc.gemmt(uplo, N_, N_, 1.25, A, B, -1.0, C)
+    tc.invalidate_caches()
+    assert _ran_ozaki(tr)
+    R = O.gemmt(uplo, N_, N_, 1.25, A, B, -1.0, C0.copy(order="F"))
+    sel = np.tril if uplo == LO else np.triu
+    assert checks.gemm_ratio(sel(C), sel(R), A, B, C0, 1.25, -1.0, K) <= 3
+    other = np.triu if uplo == LO else np.tril
+    k = 1 if uplo == LO else -1
+    np.testing.assert_array_equal(other(C, k), other(C0, k))
+
+
+@pytest.mark.parametrize("cplx", [False, True])
+@pytest.mark.parametrize("uplo", [UP, LO])
+def test_ozaki_syr2k_her2k(tc, cplx, uplo):
+    N, K = 230, 170
+    for herm in ((False, True) if cplx else (False,)):
+        for tr_ in (N_, (C_ if herm else T_)):
+            A = _gen(N, K, 500, cplx) if tr_ == N_ else _gen(K, N, 500, cplx)
+            B = _gen(N, K, 501, cplx) if tr_ == N_ else _gen(K, N, 501, cplx)
+            C0 = O.plgsy(N, 502, cplx=cplx)
+            alpha = (0.75 + 0.5j) if cplx else 0.75
+            C = C0.copy(order="F")
+            with tc.contraction_trace() as tr:
+                tc.syr2k(uplo, tr_, alpha, A, B, 0.5, C, herm=herm)
+            tc.invalidate_caches()
+            assert _ran_ozaki(tr)
+            R = O.syr2k(uplo, tr_, alpha, A, B, 0.5, C0.copy(order="F"), herm=herm)
+            sel = np.tril if uplo == LO else np.triu
+            # reference bound, testing/ztesting_syr2k.c (the syrk form with ||B||)
+            assert checks.rk_ratio(sel(C), sel(R), A, C0, N, checks.ninf(B)) <= 10
+            if herm:
+                assert np.all(np.diag(C).imag == 0)
+
+
+@pytest.mark.parametrize("cplx", [False, True])
+@pytest.mark.parametrize("side", [LEFT, RIGHT])
+@pytest.mark.parametrize("uplo", [UP, LO])
+def test_ozaki_symm_hemm(tc, cplx, side, uplo):
+    M, N = 240, 200
+    na = M if side == LEFT else N
+    for herm in ((False, True) if cplx else (False,)):
+        A = _gen(na, na, 700, cplx)
+        B, C0 = _gen(M, N, 701, cplx), _gen(M, N, 702, cplx)
+        alpha = (1.5 + 0.5j) if cplx else 1.5
+        C = C0.copy(order="F")
+        with tc.contraction_trace() as tr:
+            tc.symm(side, uplo, alpha, A, B, -0.5, C, herm=herm)
+        tc.invalidate_caches()
+        assert _ran_ozaki(tr)
+        R = O.symm(side, uplo, alpha, A, B, -0.5, C0.copy(order="F"), herm=herm)
+        # reference bound, testing/ztesting_symm.c:240-246
+        den = (checks.ninf(A) + checks.ninf(B) + checks.ninf(C0)) * max(M, N) * 2.0 ** -53
+        assert checks.ninf(C - R) / den <= 10
+
+
+@pytest.mark.parametrize("cplx", [False, True])
+@pytest.mark.parametrize("side", [LEFT, RIGHT])
+def test_ozaki_trmm(tc, cplx, side):
+    M, N = 220, 180
+    na = M if side == LEFT else N
+    for uplo in (UP, LO):
+        for tr_ in ((N_, T_, C_) if cplx else (N_, T_)):
+            for dg in (NONUNIT, UNIT):
+                A = _gen(na, na, 800, cplx)
+                B0 = _gen(M, N, 801, cplx)
+                B = B0.copy(order="F")
+                with tc.contraction_trace() as tr:
+                    tc.trmm(side, uplo, tr_, dg, 1.5, A, B)
+                tc.invalidate_caches()
+                assert _ran_ozaki(tr)
+                R = O.trmm(side, uplo, tr_, dg, 1.5, A, B0.copy(order="F"))
+                # reference bound, testing/ztesting_trmm.c (as TRSM's)
+                assert checks.trsm_ratio(B, R, A, M, N) <= 10, (uplo, tr_, dg)

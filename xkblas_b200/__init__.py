@@ -54,6 +54,14 @@ class BatchOp(ctypes.Structure):
                 ("alpha", ctypes.c_double * 2), ("beta", ctypes.c_double * 2)]
 
 
+class TraceRec(ctypes.Structure):
+    """xkb_trace_rec of include/xkb_cuda.h (per-call phase timings)."""
+    _fields_ = [("op", ctypes.c_char * 16), ("dtype", ctypes.c_int), ("M", ctypes.c_int),
+                ("N", ctypes.c_int), ("K", ctypes.c_int), ("nmod", ctypes.c_int),
+                ("ms_total", ctypes.c_float), ("ms_convert", ctypes.c_float),
+                ("ms_gemm", ctypes.c_float), ("ms_crt", ctypes.c_float)]
+
+
 class XkblasError(RuntimeError):
     pass
 
@@ -102,9 +110,9 @@ def lib():
         _lib.xkb_cuda_trsm.argtypes = [c_int, c_int, c_int, c_int, c_int, c_int, c_int, dptr,
                                        c_vp, c_long, c_vp, c_long, c_int, c_vp]
         _lib.xkb_cuda_trmm.argtypes = [c_int, c_int, c_int, c_int, c_int, c_int, c_int, dptr,
-                                       c_vp, c_long, c_vp, c_long, c_vp]
+                                       c_vp, c_long, c_vp, c_long, c_int, c_vp]
         _lib.xkb_cuda_symm.argtypes = [c_int, c_int, c_int, c_int, c_int, c_int, dptr, c_vp,
-                                       c_long, c_vp, c_long, dptr, c_vp, c_long, c_vp]
+                                       c_long, c_vp, c_long, dptr, c_vp, c_long, c_int, c_vp]
         _lib.xkb_cuda_scale.argtypes = [c_int, c_int, c_int, dptr, c_vp, c_long, c_int, c_int,
                                         c_long, c_vp]
         _lib.xkb_ozaki_default_moduli.argtypes = [c_long]
@@ -115,6 +123,7 @@ def lib():
         _lib.xkblas_get_stats.argtypes = [ctypes.POINTER(Stats)]
         _lib.xkblas_trace_export.argtypes = [ctypes.c_char_p]
         _lib.xkblas_trace_dropped.restype = ctypes.c_uint64
+        _lib.xkb_trace_take.argtypes = [ctypes.POINTER(TraceRec), c_int]
     return _lib
 
 
@@ -172,6 +181,27 @@ def trace_export(directory):
 
 def kernel_count():
     return lib().xkb_cuda_kernel_count()
+
+
+class contraction_trace:
+    """Context manager collecting the per-call records (xkb_trace_rec) of the
+    contractions launched inside it: `.records` after exit."""
+
+    def __enter__(self):
+        self.prev = lib().xkb_trace_enable(1)
+        lib().xkb_trace_take(None, 0)
+        self.records = []
+        return self
+
+    def __exit__(self, *exc):
+        buf = (TraceRec * 256)()
+        n = lib().xkb_trace_take(buf, 256)
+        self.records = [buf[i] for i in range(n)]
+        lib().xkb_trace_enable(self.prev)
+        return False
+
+    def ops(self):
+        return [r.op.decode() for r in self.records]
 
 
 # ---- numpy wrappers -----------------------------------------------------------

@@ -482,10 +482,12 @@ int sm_async(int herm, int side, int uplo, int M, int N, const T* alpha, const T
   sc(*alpha, al);
   sc(*beta, be);
   if ((err = flush_pending())) return rt_error(err);
+  const bool tc = R.math == XKBLAS_TENSOR_OP_MATH && (HT<T>::dt == XKB_D || HT<T>::dt == XKB_Z);
   if ((err = xkb_cuda_symm(HT<T>::dt, herm, side == CblasLeft ? 0 : 1,
                            uplo == CblasLower ? XKB_LOWER : XKB_UPPER, M, N, al,
                            dev_ptr(dA, 0, 0), (long)dA->dld, dev_ptr(dB, 0, 0), (long)dB->dld,
-                           be, dev_ptr(dC, 0, 0), (long)dC->dld, R.s_comp)))
+                           be, dev_ptr(dC, 0, 0), (long)dC->dld,
+                           tc ? (int)std::max<long>(ozaki_min_dim(), 1) : 0, R.s_comp)))
     return rt_error(err);
   mark_full_overwrite(dC, 0, M, 0, N);
   return 0;
@@ -569,7 +571,8 @@ int tr_async(int is_trsm, int side, int uplo, int transA, int diag, int M, int N
                         (long)dA->dld, dev_ptr(dB, 0, 0), (long)dB->dld, oz, R.s_comp);
   } else {
     err = xkb_cuda_trmm(HT<T>::dt, sd, ul, opcode(transA), dg, M, N, al, dev_ptr(dA, 0, 0),
-                        (long)dA->dld, dev_ptr(dB, 0, 0), (long)dB->dld, R.s_comp);
+                        (long)dA->dld, dev_ptr(dB, 0, 0), (long)dB->dld,
+                        tc ? (int)std::max<long>(ozaki_min_dim(), 1) : 0, R.s_comp);
   }
   if (err) return rt_error(err);
   mark_full_overwrite(dB, 0, M, 0, N);

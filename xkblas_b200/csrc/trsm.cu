@@ -637,9 +637,21 @@ extern "C" int xkb_cuda_trsm(int dtype, int side, int uplo, int trans, int diag,
                     resolve_stream(stream), true);
 }
 
+// The product on the materialised operand: Ozaki INT8 form when ozaki > 0,
+// the dtype is XKB_D / XKB_Z and all three dimensions reach ozaki (falling
+// back to DMMA when the contraction is beyond the exact-INT32 limit).
+static int product(xkb_gemm_args& g, int ozaki, cudaStream_t st) {
+  if (ozaki > 0 && (g.dtype == XKB_D || g.dtype == XKB_Z) &&
+      std::min(std::min(g.M, g.N), g.K) >= ozaki) {
+    const int e = xkb_cuda_ozaki_gemm(&g, 0, st);
+    if (e != XKB_ERANGE) return e;
+  }
+  return xkb_cuda_gemm(&g, st);
+}
+
 extern "C" int xkb_cuda_trmm(int dtype, int side, int uplo, int trans, int diag, int M, int N,
                              const double* alpha, const void* A, long lda, void* B, long ldb,
-                             void* stream) {
+                             int ozaki, void* stream) {
   if (dtype < XKB_S || dtype > XKB_Z || M < 0 || N < 0 || !alpha) return XKB_EINVAL;
   if (M == 0 || N == 0) return XKB_OK;
   cudaStream_t st = resolve_stream(stream);
@@ -701,7 +713,7 @@ extern "C" int xkb_cuda_trmm(int dtype, int side, int uplo, int trans, int diag,
   }
   g.C = B;
   g.ldc = ldb;
-  int e = xkb_cuda_gemm(&g, st);
+  int e = product(g, ozaki, st);
   cudaFreeAsync(T, st);
   cudaFreeAsync(Bc, st);
   return e;
@@ -709,7 +721,8 @@ extern "C" int xkb_cuda_trmm(int dtype, int side, int uplo, int trans, int diag,
 
 extern "C" int xkb_cuda_symm(int dtype, int herm, int side, int uplo, int M, int N,
                              const double* alpha, const void* A, long lda, const void* B,
-                             long ldb, const double* beta, void* C, long ldc, void* stream) {
+                             long ldb, const double* beta, void* C, long ldc, int ozaki,
+                             void* stream) {
   if (dtype < XKB_S || dtype > XKB_Z || M < 0 || N < 0 || !alpha || !beta) return XKB_EINVAL;
   if (M == 0 || N == 0) return XKB_OK;
   cudaStream_t st = resolve_stream(stream);
@@ -755,7 +768,7 @@ extern "C" int xkb_cuda_symm(int dtype, int herm, int side, int uplo, int M, int
   }
   g.C = C;
   g.ldc = ldc;
-  int e = xkb_cuda_gemm(&g, st);
+  int e = product(g, ozaki, st);
   cudaFreeAsync(S, st);
   return e;
 }

@@ -132,9 +132,10 @@ def main(case):
         al = (ctypes.c_double * 2)(1.0, 0.0)
         ap = ctypes.cast(al, ctypes.POINTER(ctypes.c_double))
         for _ in range(2):
-            assert lib.xkb_cuda_trmm(1, 0, 1, 0, 0, n, n, ap, A.data_ptr(), n, B.data_ptr(), n, sp) == 0
+            assert lib.xkb_cuda_trmm(1, 0, 1, 0, 0, n, n, ap, A.data_ptr(), n, B.data_ptr(), n, 0,
+                                     sp) == 0
             assert lib.xkb_cuda_symm(1, 0, 0, 1, n, n, ap, A.data_ptr(), n, B.data_ptr(), n, bp,
-                                     D.data_ptr(), n, sp) == 0
+                                     D.data_ptr(), n, 0, sp) == 0
     else:
         raise SystemExit("unknown case %r" % case)
     torch.cuda.synchronize()
