@@ -779,6 +779,11 @@ def main():
     nmod_rule = lib.xkb_ozaki_default_moduli(K)
     nmod, tune_err_plain, tune_errs = choose_moduli(lib, K, 1024, 1024, sp)
     torch.cuda.synchronize()
+    # the measured count becomes the tuning table's entry for this K band:
+    # the floor of the data rule, which picks the count on the device from
+    # the operands' concentration (nmod = 0 below)
+    lib.xkb_tune_set(b"ozaki_moduli_k<=%d" % K, float(nmod))
+    X.ozaki_counts(reset=True)  # the reported counts cover the headline calls only
 
     def barrier():
         reps.barrier(torch.cuda.synchronize)
@@ -788,7 +793,7 @@ def main():
     # ---- device-resident Ozaki steps --------------------------------------
     k0 = lib.xkb_cuda_kernel_count()
     for _ in range(args.warmup):
-        assert lib.xkb_cuda_ozaki_gemm(ctypes.byref(g_oz), nmod, sp) == 0
+        assert lib.xkb_cuda_ozaki_gemm(ctypes.byref(g_oz), 0, sp) == 0
     barrier()
     lib.xkb_trace_enable(1)
     lib.xkb_trace_take(None, 0)
@@ -799,7 +804,7 @@ def main():
         barrier()
         ev0.record(stream)
         for _ in range(args.steps):
-            assert lib.xkb_cuda_ozaki_gemm(ctypes.byref(g_oz), nmod, sp) == 0
+            assert lib.xkb_cuda_ozaki_gemm(ctypes.byref(g_oz), 0, sp) == 0
         ev1.record(stream)
         barrier()
     launches = lib.xkb_cuda_kernel_count() - k1
@@ -822,7 +827,9 @@ def main():
     int8_peak = 2.0 * pk.get("bf16_tflops_sustained", pk["bf16_tflops"])
     int8_peak_burst = 2.0 * pk["bf16_tflops"]
     gm = statistics.mean(gemm_ms) if gemm_ms else float("nan")
-    int8_ops = 2.0 * M * N * K * nmod  # algorithmic INT8 ops per launch (one launch, all moduli)
+    # the count the device chose for the timed calls (same inputs every step)
+    oz_calls, oz_msum, oz_fb, nm_chosen = X.ozaki_counts()
+    int8_ops = 2.0 * M * N * K * nm_chosen  # algorithmic INT8 ops per launch (all moduli)
     achieved = int8_ops / (gm * 1e-3) / 1e12
     traffic = None
     tp = os.path.join(ROOT, "profiles", "traffic.json")
@@ -854,7 +861,6 @@ def main():
     X.set_modemath(X.XKBLAS_TENSOR_OP_MATH)
     # the same moduli count through the runtime: the tuning-table entry for
     # this K band (what XKBLAS_TUNE_FILE from the autotuner provides)
-    lib.xkb_tune_set(b"ozaki_moduli_k<=%d" % K, float(nmod))
     one = np.array([1.0])
     zero = np.array([0.0])
     P = ctypes.c_void_p
@@ -885,10 +891,17 @@ def main():
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
         "config": workload_config(world),
-        "ozaki": {"moduli": nmod,
-                  "moduli_choice": "autotuned (xkblas_b200.autotune.choose_moduli on a 1024x1024x%d "
-                                   "sample: plain err %.2e, %s)" % (
-                                       K, tune_err_plain, ", ".join("%d: %.2e" % e for e in tune_errs))},
+        "ozaki": {"moduli": nm_chosen,
+                  "moduli_choice": "chosen on the device per call (nmod = 0): the smallest count "
+                                   "with H >= 53 + log2(2.31 rho_max sigma_max), at least the "
+                                   "tuning table's %d for this K band" % nmod,
+                  "tuned_floor": nmod,
+                  "tuned_floor_choice": "xkblas_b200.autotune.choose_moduli on a 1024x1024x%d "
+                                        "sample: plain err %.2e, %s" % (
+                                            K, tune_err_plain,
+                                            ", ".join("%d: %.2e" % e for e in tune_errs)),
+                  "device_counts": {"calls": oz_calls, "moduli_sum": oz_msum,
+                                    "plain_fallbacks": oz_fb}},
         "e2e": {"value": e2e_value, "unit": "TFLOP/s",
                 "h2d_bytes_per_step": 2 * M * K * 8, "d2h_bytes_per_step": M * N * 8,
                 "ms_per_step": t_e2e * 1e3},

@@ -46,6 +46,15 @@ extern "C" {
 #define XKB_ENODEV -4     /* no usable sm_100 device                     */
 #define XKB_ETIMEDOUT -5  /* a bounded device-side wait gave up          */
 #define XKB_ERANGE -6     /* size beyond a documented maximum            */
+#define XKB_EFAULT -7     /* a device-side bounds check refused an access */
+
+/* device error words (xkb_cuda_take_device_error, xkblas_last_device_error):
+ * the first kernel problem recorded since the last read */
+#define XKB_DEV_FULL_WAIT 1   /* a consumer gave up waiting for data / a task */
+#define XKB_DEV_EMPTY_WAIT 2  /* a producer gave up waiting for a free stage  */
+#define XKB_DEV_MMA_WAIT 3    /* a tensor-core completion wait gave up        */
+#define XKB_DEV_ACC_WAIT 4    /* an epilogue gave up waiting for its results  */
+#define XKB_DEV_BOUNDS 5      /* a bounds check refused an access             */
 
 typedef struct xkb_gemm_args {
   int dtype;          /* XKB_S/D/C/Z                                          */
@@ -98,7 +107,14 @@ int xkb_cuda_scale(int dtype, int M, int N, const double* beta, void* C,
 /* Ozaki scheme II: FP64 (or complex128) C <- alpha*op(A)*op(B) + beta*C
  * computed as nmod INT8 tensor-core products modulo pairwise coprime
  * moduli (tcgen05, exact INT32 accumulation) and a Chinese-remainder
- * reconstruction.  nmod = 0 picks the count from K for FP64 accuracy.
+ * reconstruction.  nmod > 0 uses that many moduli (2..16).  nmod = 0
+ * chooses the count on the device from the operands: with rho_i =
+ * sqrt(nnz) ||row i of op(A)||_2 / ||row i||_1 and sigma_j the same for
+ * column j of op(B), the smallest count (15 or 16, at least the tuning
+ * table's count for K's band) whose exponent budget H meets
+ * 53 + log2(2.31 max rho max sigma); when even 16 moduli cannot, the call
+ * is computed by the plain FP64 kernel instead (the choice is made and
+ * acted on on the device: no host synchronisation).
  * uplo/herm_diag/diag mask C as in xkb_gemm_args.  dtype XKB_D or XKB_Z. */
 int xkb_cuda_ozaki_gemm(const xkb_gemm_args* a, int nmod, void* stream);
 
@@ -127,9 +143,18 @@ int xkb_cuda_ozaki_gemm_panels(const xkb_gemm_args* a, int nmod, void* stream, i
  * free device memory to another allocator and before any stream capture. */
 int xkb_cuda_ozaki_gemm_noalloc(const xkb_gemm_args* a, int nmod, void* stream);
 
-/* Number of moduli the Ozaki path uses for contraction length K (0 if K is
- * beyond the exact-INT32 limit). */
+/* Number of moduli the Ozaki path uses for contraction length K when the
+ * count is fixed by K alone (the column-panel form with nmod = 0): the
+ * tuning table's count for K's band, else the smallest count keeping
+ * H - log2(K)/2 >= 53 bits; 0 if K is beyond the exact-INT32 limit. */
 int xkb_ozaki_default_moduli(long K);
+
+/* Counters of the Ozaki contractions run on the device since the last reset:
+ * out[0] calls, out[1] the moduli counts summed, out[2] calls the data rule
+ * sent to the plain FP64 kernel; *last (if not NULL) the latest call's count
+ * (0: plain kernel, -1: none yet).  reset != 0 clears them afterwards.
+ * Waits for the device.  No counterpart in the reference. */
+int xkb_ozaki_counts(unsigned long long* out, int* last, int reset);
 
 /* Per-call trace (off by default): when enabled, contractions record CUDA
  * events around their phases on their own stream; xkb_trace_take() waits for
@@ -147,6 +172,13 @@ typedef struct xkb_trace_rec {
 } xkb_trace_rec;
 int xkb_trace_enable(int on);
 int xkb_trace_take(xkb_trace_rec* out, int max);
+
+/* Failure-detection check of the executor's bounded waits (no counterpart
+ * in the reference): launches one executor CTA on a ready queue whose only
+ * queued task is never written (a dependency that never resolves).  The CTA
+ * gives up after wait_ms (1..10000), records XKB_DEV_FULL_WAIT and ends;
+ * the context stays usable.  Returns once launched. */
+int xkb_cuda_sched_wait_test(int wait_ms, void* stream);
 
 /* Batched execution: a list of independent GEMM / left-TRSM calls on device
  * operands run as ONE persistent launch of tile tasks (a DAG with device

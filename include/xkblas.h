@@ -58,6 +58,40 @@ typedef enum { CblasLeft = 141, CblasRight = 142 } CBLAS_SIDE;
 typedef CBLAS_ORDER CBLAS_LAYOUT;
 #endif
 
+/* Fortran-BLAS character arguments -> CBLAS enum values (reference
+ * blas/xkblas.h:143-200, static inline there too).  First character only,
+ * either case.  Divergence: an unknown character gives -1 (which every
+ * entry point rejects with its -i argument code) instead of abort(). */
+static inline int xkblas_blas2cblas_trans(const char* trans) {
+  switch (trans[0]) {
+    case 'n': case 'N': return CblasNoTrans;
+    case 't': case 'T': return CblasTrans;
+    case 'c': case 'C': return CblasConjTrans;
+    default: return -1;
+  }
+}
+static inline int xkblas_blas2cblas_side(const char* side) {
+  switch (side[0]) {
+    case 'l': case 'L': return CblasLeft;
+    case 'r': case 'R': return CblasRight;
+    default: return -1;
+  }
+}
+static inline int xkblas_blas2cblas_fill(const char* uplo) {
+  switch (uplo[0]) {
+    case 'l': case 'L': return CblasLower;
+    case 'u': case 'U': return CblasUpper;
+    default: return -1;
+  }
+}
+static inline int xkblas_blas2cblas_diag(const char* diag) {
+  switch (diag[0]) {
+    case 'n': case 'N': return CblasNonUnit;
+    case 'u': case 'U': return CblasUnit;
+    default: return -1;
+  }
+}
+
 /* reference blas/xkblas.h:124-138 */
 typedef enum {
   KERN_VOID, KERN_GEMM, KERN_GEMMT, KERN_TRMM, KERN_TRSM, KERN_SYMM,
@@ -96,9 +130,13 @@ int  xkblas_get_device_properties(struct xkblas_dev_prop_t* prop); /* :256 */
 int  xkblas_force_set_unified(void);                       /* :267; EINVAL here */
 const char* xkblas_get_configuration(void);                /* :273 */
 void xkblas_load_sym(void** ptr, const char* name);        /* :278 */
-int  xkblas_sync(void);                                    /* :282 */
-xkblas_context_t* xkblas_context_get(void);                /* :95 */
-void xkblas_set_modemath(xkblas_mode_math_t mode);         /* :107 */
+int  xkblas_sync(void);                                    /* :282; waits for the
+                                                              work queued before it */
+xkblas_context_t* xkblas_context_get(void);                /* :95; per thread */
+void xkblas_set_modemath(xkblas_mode_math_t mode);         /* :107; per thread */
+/* the calling thread's math mode (reference blas/xkblas.c:363-366, exported
+ * there without a header declaration) */
+xkblas_mode_math_t xkblas_get_modemath(void);
 size_t xkblas_get_param(void);                             /* :470 */
 void xkblas_set_param(size_t nb, size_t p);                /* :484 */
 int  xkblas_get_ngpus(void);                               /* :476 */
@@ -312,7 +350,9 @@ typedef struct xkblas_stats_t {
   uint64_t d2h_bytes;      /* bytes copied device -> host */
   uint64_t tile_hits;      /* tiles found valid on the device */
   uint64_t tile_misses;    /* tiles fetched from the host */
-  uint64_t ozaki_calls;    /* contractions run in the Ozaki INT8 form */
+  uint64_t ozaki_calls;    /* contractions run in the Ozaki INT8 form (all of
+                              the process's, counted on the device; reading
+                              the statistics waits for the device) */
   uint64_t ozaki_moduli;   /* sum over those calls of the moduli used */
   double   flops;          /* algorithmic flops (reference blas/flops.h) */
   uint64_t batches;        /* deferred-call batches run as one executor launch */
@@ -321,7 +361,10 @@ typedef struct xkblas_stats_t {
 } xkblas_stats_t;
 int  xkblas_get_stats(xkblas_stats_t* st);
 void xkblas_reset_stats(void);
-/* Last device-side error word (0 = none); set by bounded waits in kernels. */
+/* Last device-side error word (0 = none; XKB_DEV_* of xkb_cuda.h), read and
+ * cleared.  When a kernel recorded one, xkblas_sync() returns XKB_ETIMEDOUT
+ * (-5) for a bounded wait that gave up, XKB_EFAULT (-7) for a refused
+ * out-of-bounds access, XKB_ECUDA (-2) otherwise; the context stays usable. */
 int  xkblas_last_device_error(void);
 
 /* ---- added: event trace as the CSV tables of the reference's trace

@@ -10,6 +10,7 @@ import glob
 import os
 import subprocess
 import sysconfig
+import threading
 
 import numpy as np
 
@@ -45,20 +46,18 @@ def _p(a):
     return ctypes.c_void_p(a.ctypes.data)
 
 
-_KEEP = []
+_KEEP = threading.local()
 
 
 def _s(v, dt):
-    # scalar passed by pointer: kept alive until the next _release()
+    # scalar passed by pointer: kept alive until 32 more are made in the same
+    # thread (a list per thread: another thread never frees it mid-call)
     a = np.array([v], dtype=dt)
-    _KEEP.append(a)
-    if len(_KEEP) > 64:
-        del _KEEP[:32]
+    keep = _KEEP.__dict__.setdefault("a", [])
+    keep.append(a)
+    if len(keep) > 64:
+        del keep[:32]
     return a
-
-
-def _release():
-    del _KEEP[:]
 
 
 def _pre(a):

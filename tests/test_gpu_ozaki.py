@@ -332,3 +332,93 @@ def test_ozaki_trmm(tc, cplx, side):
                 R = O.trmm(side, uplo, tr_, dg, 1.5, A, B0.copy(order="F"))
                 # reference bound, testing/ztesting_trmm.c (as TRSM's)
                 assert checks.trsm_ratio(B, R, A, M, N) <= 10, (uplo, tr_, dg)
+
+
+# ---- the data rule for the moduli count (nmod = 0) ----------------------------
+def _elem_spread(M, N, seed, emax):
+    """u 2^e with u ~ U[-1, 1] and e ~ U{-emax..emax} drawn per ENTRY: the
+    dynamic range lies inside every row and column."""
+    rng = np.random.default_rng(seed)
+    return np.asfortranarray(rng.uniform(-1.0, 1.0, (M, N))
+                             * np.ldexp(1.0, rng.integers(-emax, emax + 1, (M, N))))
+
+
+def _run_cabi(xk, A, B, nmod, plain=False):
+    """C = A B through the C ABI on device copies; returns (C, latest count)."""
+    import torch
+    M, K = A.shape
+    N = B.shape[1]
+    dA = torch.from_numpy(np.ascontiguousarray(A.T)).cuda()
+    dB = torch.from_numpy(np.ascontiguousarray(B.T)).cuda()
+    dC = torch.zeros(N, M, dtype=torch.float64, device="cuda")
+    g = GemmArgs(1, 0, 0, M, N, K, dA.data_ptr(), M, dB.data_ptr(), K, dC.data_ptr(), M)
+    g.alpha[0] = 1.0
+    torch.cuda.synchronize()
+    lib = xk.lib()
+    r = lib.xkb_cuda_gemm(ctypes.byref(g), None) if plain else \
+        lib.xkb_cuda_ozaki_gemm(ctypes.byref(g), nmod, None)
+    assert r == 0
+    xk.sync()
+    assert lib.xkb_cuda_take_device_error() == 0
+    return np.asfortranarray(dC.cpu().numpy().T), xk.ozaki_counts()[3]
+
+
+def test_data_rule_per_element_spread_takes_more_moduli(xk):
+    """Exponents in [-20, 20] per entry: the count rises to 16 and the result
+    is no less accurate than the plain FP64 kernel's against double-double,
+    while a fixed 15 is measurably less accurate."""
+    xk.lib().xkb_tune_clear()
+    n = 768
+    A, B = _elem_spread(n, n, 1, 20), _elem_spread(n, n, 2, 20)
+    Cp, _ = _run_cabi(xk, A, B, 0, plain=True)
+    Ca, nm = _run_cabi(xk, A, B, 0)
+    C15, _ = _run_cabi(xk, A, B, 15)
+    assert nm == 16
+    ep = _dd_err(Cp, A, B, 1.0, nrow=64, ncol=64)
+    ea = _dd_err(Ca, A, B, 1.0, nrow=64, ncol=64)
+    e15 = _dd_err(C15, A, B, 1.0, nrow=64, ncol=64)
+    assert ea <= ep, (ea, ep)
+    assert ea < e15, (ea, e15)
+
+
+def test_data_rule_keeps_15_moduli_on_row_column_spread(xk):
+    """The benchmark's distribution (exponents per row of A / column of B):
+    every row is of one magnitude, the count stays at 15."""
+    xk.lib().xkb_tune_clear()
+    n = 640
+    A = O.expspread(n, n, 101, emax=20, by_col=False)
+    B = O.expspread(n, n, 102, emax=20, by_col=True)
+    Ca, nm = _run_cabi(xk, A, B, 0)
+    Cp, _ = _run_cabi(xk, A, B, 0, plain=True)
+    assert nm == 15
+    assert _dd_err(Ca, A, B, 1.0, nrow=48, ncol=48) <= _dd_err(Cp, A, B, 1.0, nrow=48, ncol=48)
+
+
+def test_data_rule_falls_back_to_plain_kernel(xk):
+    """A spread no 16-moduli product can carry (exponents in [-200, 200] per
+    entry): the call is computed by the plain FP64 kernel on the device --
+    the result equals that kernel's bit for bit, and the counters say so."""
+    n = 300
+    A, B = _elem_spread(n, n, 3, 200), _elem_spread(n, n, 4, 200)
+    c0 = xk.ozaki_counts()
+    Ca, nm = _run_cabi(xk, A, B, 0)
+    c1 = xk.ozaki_counts()
+    Cp, _ = _run_cabi(xk, A, B, 0, plain=True)
+    assert nm == 0
+    assert c1[2] == c0[2] + 1 and c1[0] == c0[0] + 1
+    np.testing.assert_array_equal(Ca, Cp)
+
+
+def test_data_rule_through_public_api(tc):
+    """Tensor-op mode through xkblas_dgemm_async: per-entry spread takes 16
+    moduli and meets the reference GEMM bound."""
+    tc.lib().xkb_tune_clear()
+    M, N, K = 520, 300, 700
+    A, B = _elem_spread(M, K, 5, 20), _elem_spread(K, N, 6, 20)
+    C0 = O.plrnt(M, N, 7)
+    C = C0.copy(order="F")
+    tc.gemm(N_, N_, 1.5, A, B, -0.5, C)
+    tc.invalidate_caches()
+    assert tc.ozaki_counts()[3] == 16
+    R = O.gemm(N_, N_, 1.5, A, B, -0.5, C0.copy(order="F"))
+    assert checks.gemm_ratio(C, R, A, B, C0, 1.5, -0.5, K) <= 3.0

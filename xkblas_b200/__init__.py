@@ -9,6 +9,7 @@ is missing: there is no Python or CPU fallback for the GPU path.
 """
 import ctypes
 import os
+import threading
 
 import numpy as np
 
@@ -124,6 +125,8 @@ def lib():
         _lib.xkblas_trace_export.argtypes = [ctypes.c_char_p]
         _lib.xkblas_trace_dropped.restype = ctypes.c_uint64
         _lib.xkb_trace_take.argtypes = [ctypes.POINTER(TraceRec), c_int]
+        _lib.xkb_ozaki_counts.argtypes = [ctypes.POINTER(ctypes.c_ulonglong),
+                                          ctypes.POINTER(c_int), c_int]
     return _lib
 
 
@@ -183,6 +186,17 @@ def kernel_count():
     return lib().xkb_cuda_kernel_count()
 
 
+def ozaki_counts(reset=False):
+    """Device counters of the Ozaki contractions: (calls, moduli summed,
+    calls sent to the plain FP64 kernel, latest call's count)."""
+    out = (ctypes.c_ulonglong * 3)()
+    last = ctypes.c_int(-1)
+    r = lib().xkb_ozaki_counts(out, ctypes.byref(last), 1 if reset else 0)
+    if r != 0:
+        raise XkblasError("xkb_ozaki_counts failed: %d" % r)
+    return int(out[0]), int(out[1]), int(out[2]), int(last.value)
+
+
 class contraction_trace:
     """Context manager collecting the per-call records (xkb_trace_rec) of the
     contractions launched inside it: `.records` after exit."""
@@ -209,15 +223,17 @@ def _ptr(a):
     return ctypes.c_void_p(a.ctypes.data)
 
 
-_KEEP = []
+_KEEP = threading.local()
 
 
 def _scal(v, dt):
-    # scalar passed by pointer: kept alive until the call returns
+    # scalar passed by pointer: kept alive until the call returns (a list per
+    # thread: another thread's trimming never frees it mid-call)
     a = np.array([v], dtype=dt)
-    _KEEP.append(a)
-    if len(_KEEP) > 64:
-        del _KEEP[:32]
+    keep = _KEEP.__dict__.setdefault("a", [])
+    keep.append(a)
+    if len(keep) > 64:
+        del keep[:32]
     return a
 
 

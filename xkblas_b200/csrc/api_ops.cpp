@@ -106,7 +106,7 @@ struct Guard {
 
 bool use_ozaki(int dt, long m, long n, long k) {
   Runtime& R = rt();
-  if (R.math != XKBLAS_TENSOR_OP_MATH) return false;
+  if (thread_math() != XKBLAS_TENSOR_OP_MATH) return false;
   if (dt != XKB_D && dt != XKB_Z) return false;
   return std::min(m, std::min(n, k)) >= ozaki_min_dim() && xkb_ozaki_default_moduli(k) > 0;
 }
@@ -116,13 +116,9 @@ int run_gemm(xkb_gemm_args& a) {
   Runtime& R = rt();
   if (int e = flush_pending()) return e;  // queued calls first, in call order
   if (use_ozaki(a.dtype, a.M, a.N, a.K)) {
-    int nm = R.ozaki_moduli ? R.ozaki_moduli : xkb_ozaki_default_moduli(a.K);
-    int e = xkb_cuda_ozaki_gemm(&a, nm, R.s_comp);
-    if (e == XKB_OK) {
-      R.stats.ozaki_calls++;
-      R.stats.ozaki_moduli += (uint64_t)nm;
-      return e;
-    }
+    // XKBLAS_OZAKI_SLICES fixes the count; otherwise it is chosen on the
+    // device from the operands (xkb_cuda_ozaki_gemm with nmod = 0)
+    int e = xkb_cuda_ozaki_gemm(&a, R.ozaki_moduli, R.s_comp);
     if (e != XKB_ERANGE) return e;
   }
   return xkb_cuda_gemm(&a, R.s_comp);
@@ -168,8 +164,8 @@ int gemm_async(int transA, int transB, int M, int N, int K, const T* alpha, cons
   Guard g;
   if (int e = ensure_init()) return rt_error(e);
   Runtime& R = rt();
-  R.stats.calls++;
-  R.stats.flops += (HT<T>::cplx ? 8.0 : 2.0) * M * (double)N * K;
+  count_call(op_name.s);
+  add_flops(op_name.s, (HT<T>::cplx ? 8.0 : 2.0) * M * (double)N * K);
   const size_t NB = auto_tilesize(KERN_GEMM, M, N, K), es = sizeof(T);
   int err;
   const bool need_ab = !is_zero(*alpha) && K > 0;
@@ -214,8 +210,7 @@ int gemm_async(int transA, int transB, int M, int N, int K, const T* alpha, cons
                                      reinterpret_cast<void* const*>(ev.data()),
                                      reinterpret_cast<void* const*>(done.data()));
     if (err) return rt_error(err);
-    R.stats.ozaki_calls++;
-    R.stats.ozaki_moduli += (uint64_t)nm;
+
     mark_full_overwrite(dC, 0, M, 0, N);
     for (size_t p = 0; p < fin.size(); ++p) dC->col_ready.emplace_back((size_t)bounds[p + 1], fin[p]);
     return 0;
@@ -300,8 +295,8 @@ int gemmt_async(int uplo, int transA, int transB, int N, int K, const T* alpha, 
   Guard g;
   if (int e = ensure_init()) return rt_error(e);
   Runtime& R = rt();
-  R.stats.calls++;
-  R.stats.flops += (HT<T>::cplx ? 4.0 : 1.0) * N * (double)(N + 1) * K;
+  count_call(op_name.s);
+  add_flops(op_name.s, (HT<T>::cplx ? 4.0 : 1.0) * N * (double)(N + 1) * K);
   const size_t NB = auto_tilesize(KERN_GEMMT, N, N, K), es = sizeof(T);
   int err;
   const bool need_ab = !is_zero(*alpha) && K > 0;
@@ -350,8 +345,8 @@ int rk_async(int herm, int uplo, int trans, int N, int K, const T& alpha, const 
   Guard g;
   if (int e = ensure_init()) return rt_error(e);
   Runtime& R = rt();
-  R.stats.calls++;
-  R.stats.flops += (HT<T>::cplx ? 4.0 : 1.0) * N * (double)(N + 1) * K;
+  count_call(op_name.s);
+  add_flops(op_name.s, (HT<T>::cplx ? 4.0 : 1.0) * N * (double)(N + 1) * K);
   const size_t NB = auto_tilesize(herm ? KERN_HERK : KERN_SYRK, N, N, K), es = sizeof(T);
   int err;
   const bool need_a = !is_zero(alpha) && K > 0;
@@ -403,8 +398,8 @@ int r2k_async(int herm, int uplo, int trans, int N, int K, const T& alpha, const
   Guard g;
   if (int e = ensure_init()) return rt_error(e);
   Runtime& R = rt();
-  R.stats.calls++;
-  R.stats.flops += (HT<T>::cplx ? 8.0 : 2.0) * N * (double)N * K;
+  count_call(op_name.s);
+  add_flops(op_name.s, (HT<T>::cplx ? 8.0 : 2.0) * N * (double)N * K);
   const size_t NB = auto_tilesize(herm ? KERN_HER2K : KERN_SYR2K, N, N, K), es = sizeof(T);
   int err;
   const bool need_ab = !is_zero(alpha) && K > 0;
@@ -464,8 +459,8 @@ int sm_async(int herm, int side, int uplo, int M, int N, const T* alpha, const T
   Guard g;
   if (int e = ensure_init()) return rt_error(e);
   Runtime& R = rt();
-  R.stats.calls++;
-  R.stats.flops += (HT<T>::cplx ? 8.0 : 2.0) * (double)M * N * Am;
+  count_call(op_name.s);
+  add_flops(op_name.s, (HT<T>::cplx ? 8.0 : 2.0) * (double)M * N * Am);
   const size_t NB = auto_tilesize(herm ? KERN_HEMM : KERN_SYMM, M, N, 0), es = sizeof(T);
   int err;
   Desc* dA = get_desc(A, Am, Am, LDA, es, NB, &err);
@@ -482,7 +477,7 @@ int sm_async(int herm, int side, int uplo, int M, int N, const T* alpha, const T
   sc(*alpha, al);
   sc(*beta, be);
   if ((err = flush_pending())) return rt_error(err);
-  const bool tc = R.math == XKBLAS_TENSOR_OP_MATH && (HT<T>::dt == XKB_D || HT<T>::dt == XKB_Z);
+  const bool tc = thread_math() == XKBLAS_TENSOR_OP_MATH && (HT<T>::dt == XKB_D || HT<T>::dt == XKB_Z);
   if ((err = xkb_cuda_symm(HT<T>::dt, herm, side == CblasLeft ? 0 : 1,
                            uplo == CblasLower ? XKB_LOWER : XKB_UPPER, M, N, al,
                            dev_ptr(dA, 0, 0), (long)dA->dld, dev_ptr(dB, 0, 0), (long)dB->dld,
@@ -513,10 +508,10 @@ int tr_async(int is_trsm, int side, int uplo, int transA, int diag, int M, int N
   Guard g;
   if (int e = ensure_init()) return rt_error(e);
   Runtime& R = rt();
-  R.stats.calls++;
+  count_call(op_name.s);
   {
     const double f = side == CblasLeft ? (double)N * M * (M + 1) : (double)M * N * (N + 1);
-    R.stats.flops += (HT<T>::cplx ? 4.0 : 1.0) * f;
+    add_flops(op_name.s, (HT<T>::cplx ? 4.0 : 1.0) * f);
   }
   const size_t NB = auto_tilesize(is_trsm ? KERN_TRSM : KERN_TRMM, M, N, NA), es = sizeof(T);
   int err;
@@ -535,7 +530,7 @@ int tr_async(int is_trsm, int side, int uplo, int transA, int diag, int M, int N
   const int sd = side == CblasLeft ? 0 : 1;
   const int ul = uplo == CblasLower ? XKB_LOWER : XKB_UPPER;
   const int dg = diag == CblasUnit ? 1 : 0;
-  const bool tc = (R.math == XKBLAS_TENSOR_OP_MATH) && (HT<T>::dt == XKB_D || HT<T>::dt == XKB_Z);
+  const bool tc = (thread_math() == XKBLAS_TENSOR_OP_MATH) && (HT<T>::dt == XKB_D || HT<T>::dt == XKB_Z);
   if (!zero && is_trsm && sd == 0 && R.batch_on && !tc &&
       (HT<T>::dt == XKB_D || HT<T>::dt == XKB_Z)) {
     // left solve queued for the tile-task executor
@@ -592,10 +587,10 @@ int potrf_async(int uplo, int N, T* A, int LDA) {
   Guard g;
   if (int e = ensure_init()) return rt_error(e);
   Runtime& R = rt();
-  R.stats.calls++;
+  count_call(op_name.s);
   {
     const double n = N;
-    R.stats.flops += (HT<T>::cplx ? 4.0 : 1.0) * (n * n * n / 3.0 + n * n / 2.0 + n / 6.0);
+    add_flops(op_name.s, (HT<T>::cplx ? 4.0 : 1.0) * (n * n * n / 3.0 + n * n / 2.0 + n / 6.0));
   }
   int err;
   if ((err = flush_pending())) return rt_error(err);
@@ -610,7 +605,7 @@ int potrf_async(int uplo, int N, T* A, int LDA) {
     }
   }
   cudaMemsetAsync(R.d_potrf_info, 0, sizeof(int), R.s_comp);
-  const bool tc = R.math == XKBLAS_TENSOR_OP_MATH && (HT<T>::dt == XKB_D || HT<T>::dt == XKB_Z);
+  const bool tc = thread_math() == XKBLAS_TENSOR_OP_MATH && (HT<T>::dt == XKB_D || HT<T>::dt == XKB_Z);
   err = xkb_cuda_potrf(HT<T>::dt, uplo == CblasLower ? XKB_LOWER : XKB_UPPER, N,
                        dev_ptr(dA, 0, 0), (long)dA->dld, R.d_potrf_info,
                        tc ? (int)std::max<long>(ozaki_min_dim(), 1) : 0, R.s_comp);
@@ -632,10 +627,10 @@ int getrf_async(int M, int N, T* A, int LDA) {
   Guard g;
   if (int e = ensure_init()) return rt_error(e);
   Runtime& R = rt();
-  R.stats.calls++;
+  count_call(op_name.s);
   {
     const double n = N;
-    R.stats.flops += (HT<T>::cplx ? 4.0 : 1.0) * (2.0 * n * n * n / 3.0 - n * n / 2.0 - n / 6.0);
+    add_flops(op_name.s, (HT<T>::cplx ? 4.0 : 1.0) * (2.0 * n * n * n / 3.0 - n * n / 2.0 - n / 6.0));
   }
   int err;
   if ((err = flush_pending())) return rt_error(err);
@@ -650,7 +645,7 @@ int getrf_async(int M, int N, T* A, int LDA) {
     }
   }
   cudaMemsetAsync(R.d_potrf_info, 0, sizeof(int), R.s_comp);
-  const bool tc = R.math == XKBLAS_TENSOR_OP_MATH && (HT<T>::dt == XKB_D || HT<T>::dt == XKB_Z);
+  const bool tc = thread_math() == XKBLAS_TENSOR_OP_MATH && (HT<T>::dt == XKB_D || HT<T>::dt == XKB_Z);
   err = xkb_cuda_getrf_nopiv(HT<T>::dt, N, dev_ptr(dA, 0, 0), (long)dA->dld, R.d_potrf_info,
                              tc ? (int)std::max<long>(ozaki_min_dim(), 1) : 0, R.s_comp);
   if (err) return rt_error(err);

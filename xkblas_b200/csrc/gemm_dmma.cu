@@ -40,6 +40,7 @@ struct GemmParams {
   long diag;
   int conjA, conjB;
   int tiles_m, tiles_n, ktiles;
+  const int* run_if;  // not null: the launch does nothing unless *run_if != 0
 };
 
 constexpr int kBK = 16;      // k extent of one pipeline stage
@@ -53,6 +54,10 @@ template <class T, int BM, int BN, bool A_KC, bool B_KC>
 __global__ void __launch_bounds__(kThreads, 1)
     k_gemm_dmma(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                 const GemmParams p) {
+  // a launch predicated on a device word (the Ozaki data rule's plain
+  // fallback): every thread reads the same word, so the whole CTA leaves
+  // before touching shared memory, barriers or C
+  if (p.run_if && *p.run_if == 0) return;
   using S = typename St<T>::S;
   constexpr int W = St<T>::W;
   constexpr bool CPLX = St<T>::CPLX;
@@ -273,7 +278,7 @@ __global__ void k_scale(int M, int N, double br, double bi, T* Cv, long ldc, int
 // ---------------------------------------------------------------------------
 // host side
 template <class T, int BM, int BN, bool A_KC, bool B_KC>
-static int launch_dmma(const xkb_gemm_args* a, cudaStream_t st) {
+static int launch_dmma(const xkb_gemm_args* a, cudaStream_t st, const int* run_if) {
   using S = typename St<T>::S;
   constexpr int W = St<T>::W;
   const int es = (int)sizeof(S);
@@ -305,6 +310,7 @@ static int launch_dmma(const xkb_gemm_args* a, cudaStream_t st) {
   p.tiles_m = (a->M + BM - 1) / BM;
   p.tiles_n = (a->N + BN - 1) / BN;
   p.ktiles = (a->K + kBK - 1) / kBK;
+  p.run_if = run_if;
   const size_t smem = kStages * (size_t)(BM + BN) * kBK * sizeof(T) + 2 * kStages * 8 + 128;
   auto kern = k_gemm_dmma<T, BM, BN, A_KC, B_KC>;
   static bool attr_done = false;  // one per instantiation
@@ -323,16 +329,16 @@ static int launch_dmma(const xkb_gemm_args* a, cudaStream_t st) {
 }
 
 template <class T, int BM, int BN>
-static int dispatch_ops(const xkb_gemm_args* a, cudaStream_t st) {
+static int dispatch_ops(const xkb_gemm_args* a, cudaStream_t st, const int* run_if) {
   const bool akc = a->opA != XKB_OP_N, bkc = a->opB == XKB_OP_N;
-  if (akc && bkc) return launch_dmma<T, BM, BN, true, true>(a, st);
-  if (akc && !bkc) return launch_dmma<T, BM, BN, true, false>(a, st);
-  if (!akc && bkc) return launch_dmma<T, BM, BN, false, true>(a, st);
-  return launch_dmma<T, BM, BN, false, false>(a, st);
+  if (akc && bkc) return launch_dmma<T, BM, BN, true, true>(a, st, run_if);
+  if (akc && !bkc) return launch_dmma<T, BM, BN, true, false>(a, st, run_if);
+  if (!akc && bkc) return launch_dmma<T, BM, BN, false, true>(a, st, run_if);
+  return launch_dmma<T, BM, BN, false, false>(a, st, run_if);
 }
 
 template <class T>
-static int dispatch_type(const xkb_gemm_args* a, cudaStream_t st) {
+static int dispatch_type(const xkb_gemm_args* a, cudaStream_t st, const int* run_if) {
   constexpr bool CPLX = St<T>::CPLX;
   constexpr int BMb = CPLX ? 64 : 128, BNb = 128;
   const long tiles_big = (long)((a->M + BMb - 1) / BMb) * ((a->N + BNb - 1) / BNb);
@@ -342,8 +348,8 @@ static int dispatch_type(const xkb_gemm_args* a, cudaStream_t st) {
   static const char* force = getenv("XKBLAS_GEMM_TILE");
   const bool big = force ? (force[0] == 'b')
                          : (tiles_big >= (long)tune("gemm_big_min_tiles", (double)sm_count()));
-  if (big) return dispatch_ops<T, BMb, BNb>(a, st);
-  return dispatch_ops<T, BMb / 2, BNb / 2>(a, st);
+  if (big) return dispatch_ops<T, BMb, BNb>(a, st, run_if);
+  return dispatch_ops<T, BMb / 2, BNb / 2>(a, st, run_if);
 }
 
 // Copy a rows x cols column-major array (element size es) into a packed
@@ -351,7 +357,8 @@ static int dispatch_type(const xkb_gemm_args* a, cudaStream_t st) {
 // of an operand whose base or leading dimension is not 16-byte aligned.
 template <class W>
 __global__ void k_repack(int rows_w, int cols, const W* __restrict__ src, long lds_w,
-                         W* __restrict__ dst, long ldd_w) {
+                         W* __restrict__ dst, long ldd_w, const int* run_if) {
+  if (run_if && *run_if == 0) return;
   const size_t total = (size_t)rows_w * (size_t)cols;
   for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total;
        e += (size_t)gridDim.x * blockDim.x) {
@@ -367,7 +374,7 @@ static bool tma_ok(const void* p, long ld, int es) {
 // Packed copy of a stored operand (rows x cols, element size es); *out is a
 // stream-ordered allocation the caller frees on the same stream.
 static int repack(const void* src, long ld, int rows, int cols, int es, void** out, long* ldo,
-                  cudaStream_t st) {
+                  cudaStream_t st, const int* run_if) {
   const long ldp = (long)(((size_t)rows * es + 15) / 16 * 16 / es);
   if (cudaMallocAsync(out, std::max<size_t>((size_t)ldp * cols * es, 16), st) != cudaSuccess)
     return XKB_ENOMEM;
@@ -379,11 +386,11 @@ static int repack(const void* src, long ld, int rows, int cols, int es, void** o
   if (es % 8 == 0 && reinterpret_cast<uintptr_t>(src) % 8 == 0)
     k_repack<double><<<grid, 256, 0, st>>>(rows * (es / 8), cols,
                                            static_cast<const double*>(src), ld * (es / 8),
-                                           static_cast<double*>(*out), ldp * (es / 8));
+                                           static_cast<double*>(*out), ldp * (es / 8), run_if);
   else
     k_repack<float><<<grid, 256, 0, st>>>(rows * (es / 4), cols, static_cast<const float*>(src),
                                           ld * (es / 4), static_cast<float*>(*out),
-                                          ldp * (es / 4));
+                                          ldp * (es / 4), run_if);
   evlog_kern_end(tv, st);
   count_launch();
   return cudaPeekAtLastError() == cudaSuccess ? XKB_OK : XKB_ECUDA;
@@ -423,19 +430,23 @@ extern "C" int xkb_cuda_scale(int dtype, int M, int N, const double* beta, void*
   return XKB_EINVAL;
 }
 
-extern "C" int xkb_cuda_gemm(const xkb_gemm_args* a, void* stream) {
+namespace xkb {
+// The whole-matrix product; run_if not null: the kernel runs only where the
+// device word is non-zero (operand repacking, if any, runs regardless).
+static int gemm_impl(const xkb_gemm_args* a, cudaStream_t st, const int* run_if) {
   if (!a || a->M < 0 || a->N < 0 || a->K < 0) return XKB_EINVAL;
   if (a->dtype < XKB_S || a->dtype > XKB_Z) return XKB_EINVAL;
   if (a->opA < XKB_OP_N || a->opA > XKB_OP_C || a->opB < XKB_OP_N || a->opB > XKB_OP_C)
     return XKB_EINVAL;
   if (a->M == 0 || a->N == 0) return XKB_OK;
-  cudaStream_t st = resolve_stream(stream);
   const bool cplx = (a->dtype == XKB_C || a->dtype == XKB_Z);
   const bool alpha_zero = a->alpha[0] == 0.0 && (!cplx || a->alpha[1] == 0.0);
   if (a->K == 0 || alpha_zero)
-    return xkb_cuda_scale(a->dtype, a->M, a->N, a->beta, a->C, a->ldc, a->uplo, a->herm_diag,
-                          a->diag, stream);
-  const int slot = trace_begin("dmma_gemm", a->dtype, a->M, a->N, a->K, 0, st);
+    return run_if ? XKB_EINVAL
+                  : xkb_cuda_scale(a->dtype, a->M, a->N, a->beta, a->C, a->ldc, a->uplo,
+                                   a->herm_diag, a->diag, st);
+  const int slot = trace_begin(run_if ? "dmma_fallback" : "dmma_gemm", a->dtype, a->M, a->N,
+                               a->K, 0, st);
   trace_mark(slot, 1, st);
   // the tensor-map loads need 16-byte aligned bases and leading dimensions:
   // other operands are first copied to packed, aligned arrays (C is read and
@@ -450,19 +461,19 @@ extern "C" int xkb_cuda_gemm(const xkb_gemm_args* a, void* stream) {
   int r = XKB_OK;
   if (!tma_ok(a->A, a->lda, es))
     r = repack(a->A, a->lda, a->opA == XKB_OP_N ? a->M : a->K,
-               a->opA == XKB_OP_N ? a->K : a->M, es, &packA, &pa.lda, st);
+               a->opA == XKB_OP_N ? a->K : a->M, es, &packA, &pa.lda, st, run_if);
   if (r == XKB_OK && !tma_ok(a->B, a->ldb, es))
     r = repack(a->B, a->ldb, a->opB == XKB_OP_N ? a->K : a->N,
-               a->opB == XKB_OP_N ? a->N : a->K, es, &packB, &pa.ldb, st);
+               a->opB == XKB_OP_N ? a->N : a->K, es, &packB, &pa.ldb, st, run_if);
   if (packA) pa.A = packA;
   if (packB) pa.B = packB;
   if (r == XKB_OK) {
     r = XKB_EINVAL;
     switch (a->dtype) {
-      case XKB_S: r = dispatch_type<float>(&pa, st); break;
-      case XKB_D: r = dispatch_type<double>(&pa, st); break;
-      case XKB_C: r = dispatch_type<float2>(&pa, st); break;
-      case XKB_Z: r = dispatch_type<double2>(&pa, st); break;
+      case XKB_S: r = dispatch_type<float>(&pa, st, run_if); break;
+      case XKB_D: r = dispatch_type<double>(&pa, st, run_if); break;
+      case XKB_C: r = dispatch_type<float2>(&pa, st, run_if); break;
+      case XKB_Z: r = dispatch_type<double2>(&pa, st, run_if); break;
     }
   }
   if (packA) cudaFreeAsync(packA, st);
@@ -470,4 +481,13 @@ extern "C" int xkb_cuda_gemm(const xkb_gemm_args* a, void* stream) {
   trace_mark(slot, 2, st);
   trace_mark(slot, 3, st);
   return r;
+}
+
+int gemm_if(const xkb_gemm_args* a, const int* run_if, cudaStream_t st) {
+  return gemm_impl(a, st, run_if);
+}
+}  // namespace xkb
+
+extern "C" int xkb_cuda_gemm(const xkb_gemm_args* a, void* stream) {
+  return gemm_impl(a, resolve_stream(stream), nullptr);
 }

@@ -169,33 +169,47 @@ static bool make_consts(int n, Consts* c) {
 }
 
 // ---------------------------------------------------------------------------
-// 1. scaling exponents.  View the operand as L "rows" of length K, element
-//    (l,k) at X[l*sl + k*sk] (one of sl, sk is 1).  Partial sums of squares
-//    and maxima over k-chunks go to part[chunk][l]; k_oz_shift finalises.
+// 1. scaling exponents and the moduli count.  View the operand as L "rows"
+//    of length K, element (l,k) at X[l*sl + k*sk] (one of sl, sk is 1).
+//    Partial sums over k-chunks go to part[chunk][l] = (sum of squares,
+//    max |x|, sum |x|, nonzero count); k_oz_stat finalises each row.
 constexpr int kNormChunk = 512;
+
+// The moduli count of a call, chosen on the device (k_oz_pick) and read by
+// every later kernel of the call: n moduli (0: the plain FP64 kernel runs
+// instead), H the exponent budget of the scaled operands for that count.
+struct OzSel {
+  int n, H, fallback, pad;
+};
+
+// Counters over all contractions of the process (xkb_ozaki_counts).
+static __device__ unsigned long long g_oz_calls, g_oz_mod_sum, g_oz_fallbacks;
+static __device__ int g_oz_last = -1;
 
 template <bool KC>  // KC: k contiguous (sk == 1)
 __global__ void __launch_bounds__(256) k_oz_norm(int L, int K, const double* X, long ld, int cplx,
-                                                  double2* part) {
+                                                  double4* part) {
   // block: 32 rows x 8 lanes along k (KC: warp-cooperative along k instead)
   const int chunk = blockIdx.y;
   const int k0 = chunk * kNormChunk, k1 = min(K, k0 + kNormChunk);
+  double ss = 0.0, mx = 0.0, s1 = 0.0, nz = 0.0;
+  auto acc = [&](double v) {
+    ss = fma(v, v, ss);
+    mx = fmax(mx, fabs(v));
+    s1 += fabs(v);
+    nz += (v != 0.0) ? 1.0 : 0.0;
+  };
   if constexpr (KC) {
     // one warp per row: lanes stride along contiguous k
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int l = blockIdx.x * 8 + warp;
-    double ss = 0.0, mx = 0.0;
     if (l < L) {
       for (int k = k0 + lane; k < k1; k += 32) {
         if (cplx) {
-          const double re = X[2 * ((size_t)k + (size_t)l * ld)], im = X[2 * ((size_t)k + (size_t)l * ld) + 1];
-          ss = fma(re, re, ss);
-          ss = fma(im, im, ss);
-          mx = fmax(mx, fmax(fabs(re), fabs(im)));
+          acc(X[2 * ((size_t)k + (size_t)l * ld)]);
+          acc(X[2 * ((size_t)k + (size_t)l * ld) + 1]);
         } else {
-          const double v = X[(size_t)k + (size_t)l * ld];
-          ss = fma(v, v, ss);
-          mx = fmax(mx, fabs(v));
+          acc(X[(size_t)k + (size_t)l * ld]);
         }
       }
     }
@@ -203,37 +217,36 @@ __global__ void __launch_bounds__(256) k_oz_norm(int L, int K, const double* X, 
     for (int o = 16; o; o >>= 1) {
       ss += __shfl_xor_sync(0xffffffffu, ss, o);
       mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+      s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+      nz += __shfl_xor_sync(0xffffffffu, nz, o);
     }
-    if (lane == 0 && l < L) part[(size_t)chunk * L + l] = make_double2(ss, mx);
+    if (lane == 0 && l < L) part[(size_t)chunk * L + l] = make_double4(ss, mx, s1, nz);
   } else {
     // l contiguous: 32 consecutive rows per warp-row, 8 k-lanes
-    __shared__ double2 red[8][32];
+    __shared__ double4 red[8][32];
     const int tl = threadIdx.x & 31, tk = threadIdx.x >> 5;
     const int l = blockIdx.x * 32 + tl;
-    double ss = 0.0, mx = 0.0;
     if (l < L) {
       for (int k = k0 + tk; k < k1; k += 8) {
         if (cplx) {
-          const double re = X[2 * ((size_t)l + (size_t)k * ld)], im = X[2 * ((size_t)l + (size_t)k * ld) + 1];
-          ss = fma(re, re, ss);
-          ss = fma(im, im, ss);
-          mx = fmax(mx, fmax(fabs(re), fabs(im)));
+          acc(X[2 * ((size_t)l + (size_t)k * ld)]);
+          acc(X[2 * ((size_t)l + (size_t)k * ld) + 1]);
         } else {
-          const double v = X[(size_t)l + (size_t)k * ld];
-          ss = fma(v, v, ss);
-          mx = fmax(mx, fabs(v));
+          acc(X[(size_t)l + (size_t)k * ld]);
         }
       }
     }
-    red[tk][tl] = make_double2(ss, mx);
+    red[tk][tl] = make_double4(ss, mx, s1, nz);
     __syncthreads();
     if (tk == 0 && l < L) {
-      double s2 = 0.0, m2 = 0.0;
-      for (int i = 0; i < 8; ++i) {
-        s2 += red[i][tl].x;
-        m2 = fmax(m2, red[i][tl].y);
+      double4 t = red[0][tl];
+      for (int i = 1; i < 8; ++i) {
+        t.x += red[i][tl].x;
+        t.y = fmax(t.y, red[i][tl].y);
+        t.z += red[i][tl].z;
+        t.w += red[i][tl].w;
       }
-      part[(size_t)chunk * L + l] = make_double2(s2, m2);
+      part[(size_t)chunk * L + l] = t;
     }
   }
 }
@@ -243,35 +256,94 @@ __device__ __forceinline__ double pow2(int e) {
   return __longlong_as_double((long long)(1023 + e) << 52);
 }
 
-// Sentinel shift: the row holds Inf/NaN; the result entries become NaN.
-constexpr int kShiftNonFinite = -100000;
+// Row codes written by k_oz_stat: the exponent e of a bound nrm < 2^e of the
+// row's 2-norm, or one of two sentinels.  The shift of the row is H - e.
+constexpr int kShiftNonFinite = -100000;  // the row holds Inf/NaN: results NaN
+constexpr int kCodeZero = 100000;         // all-zero row: shift 0
 
-__global__ void k_oz_shift(int L, int K, int nchunks, const double2* part, int H, int* mu) {
+__device__ __forceinline__ int shift_of(int code, int H) {
+  if (code == kShiftNonFinite) return kShiftNonFinite;
+  if (code == kCodeZero) return 0;
+  return max(-1000, min(1000, H - code));  // scaled values stay finite
+}
+
+// Per row: the code above, and the row's concentration
+// rho = sqrt(nnz) ||x||_2 / ||x||_1 (1 for entries of one magnitude, up to
+// sqrt(nnz) for one dominant entry), whose maximum over the rows goes to
+// *rmax (a non-negative float compared as its bits).
+__global__ void k_oz_stat(int L, int K, int nchunks, const double4* part, int* code,
+                          unsigned* rmax) {
   const int l = blockIdx.x * blockDim.x + threadIdx.x;
-  if (l >= L) return;
-  double ss = 0.0, mx = 0.0;
-  for (int c = 0; c < nchunks; ++c) {  // fixed order: deterministic
-    const double2 v = part[(size_t)c * L + l];
-    ss += v.x;
-    mx = fmax(mx, v.y);
+  float rho = 0.0f;
+  if (l < L) {
+    double ss = 0.0, mx = 0.0, s1 = 0.0, nz = 0.0;
+    for (int c = 0; c < nchunks; ++c) {  // fixed order: deterministic
+      const double4 v = part[(size_t)c * L + l];
+      ss += v.x;
+      mx = fmax(mx, v.y);
+      s1 += v.z;
+      nz += v.w;
+    }
+    if (!isfinite(mx) || isnan(ss)) {
+      code[l] = kShiftNonFinite;
+    } else if (mx == 0.0) {
+      code[l] = kCodeZero;
+    } else {
+      // bound on the row 2-norm (the sum of squares may overflow for huge entries)
+      double nrm = isfinite(ss) ? sqrt(ss) : mx * sqrt((double)K);
+      nrm = fmax(nrm, mx) * (1.0 + 1e-12);
+      int e;
+      frexp(nrm, &e);  // nrm < 2^e
+      code[l] = e;
+      // scale-free form: sqrt(nnz) * (nrm / mx) / (s1 / mx), all ratios <= nnz
+      const double r = sqrt(nz) * (nrm / mx) / fmax(s1 / mx, 1.0);
+      rho = (float)fmin(r, 3.0e38);
+    }
   }
-  if (!isfinite(mx) || isnan(ss)) {
-    mu[l] = kShiftNonFinite;
-    return;
+  // warp maximum, one atomic per warp
+#pragma unroll
+  for (int o = 16; o; o >>= 1) rho = fmaxf(rho, __shfl_xor_sync(0xffffffffu, rho, o));
+  if ((threadIdx.x & 31) == 0 && rho > 0.0f) atomicMax(rmax, __float_as_uint(rho));
+}
+
+// Moduli-count rule.  The scaled, rounded operands lose at most half a unit
+// per nonzero entry; with errors of random sign the contraction error
+// relative to sum_k |a_ik||b_kj| is about 0.58 rho_i sigma_j 2^-H, and its
+// maximum over many entries about four times that (rho, sigma: the
+// concentrations of row i of op(A) and column j of op(B)).  The smallest
+// count with 2.31 rho_max sigma_max 2^-H <= 2^-53 keeps the result within
+// FP64 rounding; if the largest count cannot, the call runs the plain FP64
+// kernel instead (fallback = 1), or, where that is not allowed, the largest
+// count.  fixed > 0: that count, no data rule.
+struct PickP {
+  int fixed, lo, hi, allow_fallback;
+  int H[kMaxMod + 1];  // exponent budget per count
+};
+
+__global__ void k_oz_pick(const unsigned* rmax, OzSel* sel, const PickP q) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  int n = q.fixed, fb = 0;
+  if (n <= 0) {
+    const double ra = fmax(1.0, (double)__uint_as_float(rmax[0]));
+    const double rb = fmax(1.0, (double)__uint_as_float(rmax[1]));
+    const double need = 53.0 + log2(2.31 * ra * rb);
+    n = 0;
+#pragma unroll
+    for (int c = kMaxMod; c >= 2; --c)  // constant indices: no local copy of q.H
+      if (c >= q.lo && c <= q.hi && (double)q.H[c] >= need) n = c;
+    if (n == 0) {
+      if (q.allow_fallback) fb = 1;
+      else n = q.hi;
+    }
   }
-  if (mx == 0.0) {
-    mu[l] = 0;
-    return;
-  }
-  // bound on the row 2-norm (sum of squares may overflow for huge entries)
-  double nrm = isfinite(ss) ? sqrt(ss) : mx * sqrt((double)K);
-  nrm = fmax(nrm, mx) * (1.0 + 1e-12);
-  int e;
-  frexp(nrm, &e);  // nrm < 2^e
-  int s = H - e;
-  // keep scaled values finite and the shift representable
-  s = max(-1000, min(1000, s));
-  mu[l] = s;
+  sel->n = n;
+  sel->H = n ? q.H[n] : 0;
+  sel->fallback = fb;
+  sel->pad = 0;
+  atomicAdd(&g_oz_calls, 1ull);
+  atomicAdd(&g_oz_mod_sum, (unsigned long long)n);
+  if (fb) atomicAdd(&g_oz_fallbacks, 1ull);
+  g_oz_last = n;
 }
 
 // ---------------------------------------------------------------------------
@@ -281,10 +353,13 @@ __global__ void k_oz_shift(int L, int K, int nchunks, const double2* part, int H
 template <bool KC, int NM>
 __global__ void __launch_bounds__(256) k_oz_residues(int L, int K, const double* X, long ld,
                                                       long estride, long eoff, double esign,
-                                                      const int* mu, const Consts c,
-                                                      int8_t* planes, long Lpad, long Kpad,
-                                                      long kofs) {
-  // X element (l,k) = esign * X[eoff + estride*(KC ? k + l*ld : l + k*ld)]
+                                                      const int* code, const OzSel* sel,
+                                                      const Consts c, int8_t* planes, long Lpad,
+                                                      long Kpad, long kofs) {
+  // X element (l,k) = esign * X[eoff + estride*(KC ? k + l*ld : l + k*ld)];
+  // planes 0 .. sel->n - 1 are written (NM: the most the call may use)
+  const int nm = sel->n, H = sel->H;
+  if (nm == 0) return;  // the plain kernel computes this call
   __shared__ double tile[64][65];
   const int l0 = blockIdx.x * 64, k0 = blockIdx.y * 64;
   {
@@ -313,7 +388,7 @@ __global__ void __launch_bounds__(256) k_oz_residues(int L, int K, const double*
   for (int it = threadIdx.x; it < 64 * 16; it += 256) {
     const int ll = it >> 4, kq = (it & 15) * 4;
     const int l = l0 + ll;
-    const int s = (l < L) ? mu[l] : 0;
+    const int s = (l < L) ? shift_of(code[l], H) : 0;
     // a' = a + 2^62 >= 0 (|a| < 2^62); residues of a' are shifted back by the
     // per-modulus constant folded into c.off (no sign handling per modulus)
     const double sc = (s == kShiftNonFinite) ? 0.0 : pow2(s / 2) * pow2(s - s / 2);
@@ -333,6 +408,7 @@ __global__ void __launch_bounds__(256) k_oz_residues(int L, int K, const double*
         __byte_perm(__byte_perm(lo[0], lo[1], 0x0040), __byte_perm(lo[2], lo[3], 0x0040), 0x5410);
 #pragma unroll
     for (int m = 1; m < NM; ++m) {
+      if (m >= nm) break;
       const uint32_t p = (uint32_t)c.p[m];
       uint32_t r[4];
 #pragma unroll
@@ -367,7 +443,8 @@ constexpr uint32_t kTmemCols = 512;  // two accumulators of BN columns
 constexpr int kEpiWarps = 4;
 
 struct GemmP {
-  int tiles_m, tiles_n, kblocks, nmod;
+  int tiles_m, tiles_n, kblocks, nmod;  // nmod: planes of the operand buffers (the most used)
+  const OzSel* sel;                     // moduli multiplied: sel->n (<= nmod)
   int group;  // raster: M tiles per group (tiles in flight share A / B panels in L2)
   uint8_t* R;
   long Mpad, Npad;
@@ -449,7 +526,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
   uint64_t* acce = accf + 2;   // [2] accumulator drained
   uint32_t* tslot = reinterpret_cast<uint32_t*>(acce + 2);
 
-  const int total = p.tiles_m * p.tiles_n * p.nmod;
+  const int total = p.tiles_m * p.tiles_n * min(p.sel->n, p.nmod);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
     for (int s = 0; s < S; ++s) {
@@ -692,7 +769,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
 
   const uint32_t rank = cluster_rank();
   const int pair = blockIdx.x >> 1, npairs = gridDim.x >> 1;
-  const int total = p.tiles_m * p.tiles_n * p.nmod;
+  const int total = p.tiles_m * p.tiles_n * min(p.sel->n, p.nmod);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
     for (int s = 0; s < S2; ++s) {
@@ -844,9 +921,10 @@ struct CrtP {
   int M, N;
   const uint8_t* R;
   long Mpad, Npad;
-  const int* mu;  // rows of op(A)
-  const int* nu;  // cols of op(B)
-  double* C;      // interleaved complex when cplx: writes part `part` (0 re, 1 im)
+  const int* mu;     // row codes of op(A) (k_oz_stat)
+  const int* nu;     // column codes of op(B)
+  const OzSel* sel;  // the call's moduli count and exponent budget
+  double* C;         // interleaved complex when cplx: writes part `part` (0 re, 1 im)
   long ldc;
   int cplx, part;
   double ar, ai, br, bi;  // real: ar, br used
@@ -899,33 +977,33 @@ __device__ __forceinline__ double scale2(double x, int e) {
 // reuse the last row's shift and are not stored), so their independent
 // integer chains interleave; the stores are predicated afterwards.
 template <int NM>
-__device__ __forceinline__ void crt_quad(const CrtP& p, const Consts& c, long i0, int j,
+__device__ __forceinline__ void crt_quad(const CrtP& p, const Consts& c, int H, long i0, int j,
                                          double (&y)[4]) {
   const size_t plane = (size_t)p.Mpad * (size_t)p.Npad;
   uint32_t words[NM];
 #pragma unroll
   for (int m = 0; m < NM; ++m)
     words[m] = *reinterpret_cast<const uint32_t*>(p.R + (size_t)m * plane + (size_t)j * p.Mpad + i0);
-  const int nuj = p.nu[j];
+  const int nuj = shift_of(p.nu[j], H);
 #pragma unroll
   for (int v = 0; v < 4; ++v) {
     uint32_t r[NM];
 #pragma unroll
     for (int m = 0; m < NM; ++m) r[m] = __byte_perm(words[m], 0u, 0x4440 + v);
-    const int mui = p.mu[min(i0 + v, (long)p.M - 1)];
+    const int mui = shift_of(p.mu[min(i0 + v, (long)p.M - 1)], H);
     if (mui == kShiftNonFinite || nuj == kShiftNonFinite) y[v] = __longlong_as_double(0x7ff8000000000000ll);
     else y[v] = scale2(crt_value<NM>(r, c), -(mui + nuj));
   }
 }
 
 template <int NM>
-__global__ void __launch_bounds__(256, 4) k_oz_crt(const CrtP p, const Consts c) {
+__device__ __forceinline__ void crt_body(const CrtP& p, const Consts& c, int H) {
   const long iq = (long)blockIdx.x * blockDim.x + threadIdx.x;  // row quad
   const long i0 = iq * 4;
   if (i0 >= p.M) return;
   for (int j = blockIdx.y; j < p.N; j += gridDim.y) {
     double y[4];
-    crt_quad<NM>(p, c, i0, j, y);
+    crt_quad<NM>(p, c, H, i0, j, y);
     const size_t idx0 = (size_t)i0 + (size_t)j * p.ldc;
     if (!p.cplx) {
       const bool full = i0 + 3 < p.M && p.uplo == XKB_FULL &&
@@ -978,13 +1056,14 @@ __global__ void __launch_bounds__(256, 4) k_oz_crt(const CrtP p, const Consts c)
 
 // Complex first pass: Re(op(A)op(B)) (unscaled by alpha) into a scratch M x N.
 template <int NM>
-__global__ void __launch_bounds__(256, 4) k_oz_crt_store(const CrtP p, const Consts c, double* out) {
+__device__ __forceinline__ void crt_store_body(const CrtP& p, const Consts& c, int H,
+                                               double* out) {
   const long iq = (long)blockIdx.x * blockDim.x + threadIdx.x;
   const long i0 = iq * 4;
   if (i0 >= p.M) return;
   for (int j = blockIdx.y; j < p.N; j += gridDim.y) {
     double y[4];
-    crt_quad<NM>(p, c, i0, j, y);
+    crt_quad<NM>(p, c, H, i0, j, y);
 #pragma unroll
     for (int v = 0; v < 4; ++v) {
       const long i = i0 + v;
@@ -996,24 +1075,60 @@ __global__ void __launch_bounds__(256, 4) k_oz_crt_store(const CrtP p, const Con
   }
 }
 
-// CRT launches, dispatched on the moduli count
+// CRT kernels.  A fixed count: one instance per count.  A count chosen on the
+// device between 15 and 16 (the data rule's range, k_oz_pick): one kernel
+// holding both reconstructions, each block taking the one sel->n names.  A
+// call the pick sent to the plain kernel (sel->n == 0) writes nothing here.
+template <int NM>
+__global__ void __launch_bounds__(256, 4) k_oz_crt(const CrtP p, const Consts c) {
+  const OzSel s = *p.sel;
+  if (s.n != NM) return;
+  crt_body<NM>(p, c, s.H);
+}
+template <int NM>
+__global__ void __launch_bounds__(256, 4) k_oz_crt_store(const CrtP p, const Consts c, double* out) {
+  const OzSel s = *p.sel;
+  if (s.n != NM) return;
+  crt_store_body<NM>(p, c, s.H, out);
+}
+__global__ void __launch_bounds__(256, 4) k_oz_crt_15_16(const CrtP p, const Consts c15,
+                                                         const Consts c16) {
+  const OzSel s = *p.sel;
+  if (s.n == 15) crt_body<15>(p, c15, s.H);
+  else if (s.n == 16) crt_body<16>(p, c16, s.H);
+}
+__global__ void __launch_bounds__(256, 4) k_oz_crt_store_15_16(const CrtP p, const Consts c15,
+                                                               const Consts c16, double* out) {
+  const OzSel s = *p.sel;
+  if (s.n == 15) crt_store_body<15>(p, c15, s.H, out);
+  else if (s.n == 16) crt_store_body<16>(p, c16, s.H, out);
+}
+
 template <int NM>
 static void crt_launch(dim3 g, cudaStream_t st, const CrtP& cp, const Consts& c, double* store) {
   if (store) k_oz_crt_store<NM><<<g, 256, 0, st>>>(cp, c, store);
   else k_oz_crt<NM><<<g, 256, 0, st>>>(cp, c);
 }
-static int launch_crt(dim3 g, cudaStream_t st, const CrtP& cp, const Consts& c, double* store) {
-  if (c.nmod < 2 || c.nmod > kMaxMod) return XKB_EINVAL;
+// lo == hi: that count; (lo, hi) == (15, 16): the count the device chose.
+static int launch_crt(dim3 g, cudaStream_t st, const CrtP& cp, const Consts* lo,
+                      const Consts* hi, double* store) {
+  if (!lo || !hi) return XKB_EINVAL;
   const long long tv = evlog_kern_begin(st, store ? "k_oz_crt_store" : "k_oz_crt");
-  switch (c.nmod) {
+  if (lo->nmod != hi->nmod) {
+    if (lo->nmod != 15 || hi->nmod != 16) return XKB_EINVAL;
+    if (store) k_oz_crt_store_15_16<<<g, 256, 0, st>>>(cp, *lo, *hi, store);
+    else k_oz_crt_15_16<<<g, 256, 0, st>>>(cp, *lo, *hi);
+  } else {
+    switch (hi->nmod) {
 #define XKB_CRT_CASE(NM) \
   case NM:               \
-    crt_launch<NM>(g, st, cp, c, store); break;
-    XKB_CRT_CASE(2) XKB_CRT_CASE(3) XKB_CRT_CASE(4) XKB_CRT_CASE(5) XKB_CRT_CASE(6)
-    XKB_CRT_CASE(7) XKB_CRT_CASE(8) XKB_CRT_CASE(9) XKB_CRT_CASE(10) XKB_CRT_CASE(11)
-    XKB_CRT_CASE(12) XKB_CRT_CASE(13) XKB_CRT_CASE(14) XKB_CRT_CASE(15) XKB_CRT_CASE(16)
+    crt_launch<NM>(g, st, cp, *hi, store); break;
+      XKB_CRT_CASE(2) XKB_CRT_CASE(3) XKB_CRT_CASE(4) XKB_CRT_CASE(5) XKB_CRT_CASE(6)
+      XKB_CRT_CASE(7) XKB_CRT_CASE(8) XKB_CRT_CASE(9) XKB_CRT_CASE(10) XKB_CRT_CASE(11)
+      XKB_CRT_CASE(12) XKB_CRT_CASE(13) XKB_CRT_CASE(14) XKB_CRT_CASE(15) XKB_CRT_CASE(16)
 #undef XKB_CRT_CASE
-    default: break;
+      default: return XKB_EINVAL;
+    }
   }
   evlog_kern_end(tv, st);
   count_launch();
@@ -1048,10 +1163,44 @@ struct View {
   double sign;
 };
 
-static int launch_norm(const View& v, int L, int K, int cplx, const Consts* c, double2* part,
-                       int* mu, cudaStream_t st) {
+// Device words of one call: the moduli selection and the two concentration
+// maxima (rows of op(A), columns of op(B)); zeroed before the norms.
+struct CallWords {
+  OzSel sel;
+  unsigned rmax[2];
+  unsigned pad[2];
+};
+
+// The counts a call may use: a fixed count (lo = hi), or the data rule's
+// range [lo, 16] with lo = max(15, the tuning table's count for K's band).
+struct ModPlan {
+  int lo = 0, hi = 0;
+  bool fixed = true;
+  const Consts* clo = nullptr;
+  const Consts* chi = nullptr;
+};
+
+static bool plan_moduli(int nmod, long K, ModPlan* pl) {
+  if (nmod > 0) {
+    pl->lo = pl->hi = nmod;
+    pl->fixed = true;
+  } else {
+    const int tuned = tune_band("ozaki_moduli_k<=", K);
+    pl->lo = std::min(kMaxMod, std::max(15, (tuned >= 2 && tuned <= kMaxMod) ? tuned : 0));
+    pl->hi = kMaxMod;
+    pl->fixed = false;
+  }
+  pl->clo = consts_for(pl->lo);
+  pl->chi = consts_for(pl->hi);
+  return pl->clo && pl->chi;
+}
+
+// Row statistics of an L x K operand view: codes (k_oz_stat) and the
+// concentration maximum into *rmax.
+static int launch_norm(const View& v, int L, int K, int cplx, double4* part, int* code,
+                       unsigned* rmax, cudaStream_t st) {
   const int nch = (K + kNormChunk - 1) / kNormChunk;
-  const long long tv = evlog_kern_begin(st, "k_oz_norm+k_oz_shift");
+  const long long tv = evlog_kern_begin(st, "k_oz_norm+k_oz_stat");
   if (v.kc) {
     dim3 g((unsigned)((L + 7) / 8), (unsigned)nch);
     k_oz_norm<true><<<g, 256, 0, st>>>(L, K, v.X, v.ld, cplx, part);
@@ -1059,24 +1208,47 @@ static int launch_norm(const View& v, int L, int K, int cplx, const Consts* c, d
     dim3 g((unsigned)((L + 31) / 32), (unsigned)nch);
     k_oz_norm<false><<<g, 256, 0, st>>>(L, K, v.X, v.ld, cplx, part);
   }
-  k_oz_shift<<<(unsigned)((L + 255) / 256), 256, 0, st>>>(L, K, nch, part, c->H, mu);
+  k_oz_stat<<<(unsigned)((L + 255) / 256), 256, 0, st>>>(L, K, nch, part, code, rmax);
   evlog_kern_end(tv, st);
   count_launch(2);
   return cudaPeekAtLastError() == cudaSuccess ? XKB_OK : XKB_ECUDA;
 }
 
-static int launch_res(const View& v, int L, int K, const int* mu, const Consts* c, int8_t* planes,
-                      long Lpad, long Kpad, long kofs, cudaStream_t st) {
+static int launch_pick(CallWords* w, const ModPlan& pl, bool allow_fallback, cudaStream_t st) {
+  PickP q;
+  std::memset(&q, 0, sizeof(q));
+  q.fixed = pl.fixed ? pl.hi : 0;
+  q.lo = pl.lo;
+  q.hi = pl.hi;
+  q.allow_fallback = allow_fallback ? 1 : 0;
+  for (int n = 2; n <= kMaxMod; ++n) {
+    const Consts* c = consts_for(n);
+    if (!c) return XKB_EINVAL;
+    q.H[n] = c->H;
+  }
+  const long long tv = evlog_kern_begin(st, "k_oz_pick");
+  k_oz_pick<<<1, 32, 0, st>>>(w->rmax, &w->sel, q);
+  evlog_kern_end(tv, st);
+  count_launch();
+  return cudaPeekAtLastError() == cudaSuccess ? XKB_OK : XKB_ECUDA;
+}
+
+// Residue planes 0 .. sel->n - 1 of an operand view (c: the constants of the
+// plan's largest count; the per-modulus constants are those of every count).
+static int launch_res(const View& v, int L, int K, const int* code, const OzSel* sel,
+                      const Consts* c, int8_t* planes, long Lpad, long Kpad, long kofs,
+                      cudaStream_t st) {
   // grid covers Lpad x (K rounded to 64); kofs places the block at column kofs
   dim3 g((unsigned)(Lpad / 64), (unsigned)(rup((size_t)K, 64) / 64));
 #define XKB_RES_CASE(NM)                                                                     \
   case NM:                                                                                   \
     if (v.kc)                                                                                \
       k_oz_residues<true, NM><<<g, 256, 0, st>>>(L, K, v.X, v.ld, v.estride, v.eoff, v.sign, \
-                                                 mu, *c, planes, Lpad, Kpad, kofs);          \
+                                                 code, sel, *c, planes, Lpad, Kpad, kofs);   \
     else                                                                                     \
       k_oz_residues<false, NM><<<g, 256, 0, st>>>(L, K, v.X, v.ld, v.estride, v.eoff,       \
-                                                  v.sign, mu, *c, planes, Lpad, Kpad, kofs); \
+                                                  v.sign, code, sel, *c, planes, Lpad, Kpad, \
+                                                  kofs);                                     \
     break;
   if (c->nmod < 2 || c->nmod > kMaxMod) return XKB_EINVAL;
   const long long tv = evlog_kern_begin(st, "k_oz_residues");
@@ -1101,8 +1273,8 @@ static bool encode_planes(CUtensorMap* m, const int8_t* base, long Kpad, long Lp
 // a_rows / b_rows: rows per plane of the A / B residue buffers (>= Mpad /
 // Npad; equal when one buffer serves both operands).
 static int launch_gemm(const int8_t* Ap, long a_rows, const int8_t* Bp, long b_rows, long Mpad,
-                       long Npad, long Kpad, const Consts* c, uint8_t* R, int uplo, long diag,
-                       cudaStream_t st) {
+                       long Npad, long Kpad, const Consts* c, const OzSel* sel, uint8_t* R,
+                       int uplo, long diag, cudaStream_t st) {
   CUtensorMap tA, tB;
   if (a_rows < Mpad || b_rows < Npad) return XKB_EINVAL;
   if (!encode_planes(&tA, Ap, Kpad, a_rows, c->nmod, BM)) return XKB_EINVAL;
@@ -1113,6 +1285,7 @@ static int launch_gemm(const int8_t* Ap, long a_rows, const int8_t* Bp, long b_r
   p.tiles_n = (int)(Npad / BN);
   p.kblocks = (int)(Kpad / BKB);
   p.nmod = c->nmod;
+  p.sel = sel;
   // raster group (tuning table oz_group_m, default 8 M tiles)
   p.group = std::max(1, std::min(p.tiles_m, (int)tune("oz_group_m", 8.0)));
   p.R = R;
@@ -1202,9 +1375,36 @@ using namespace xkb::oz;
 
 extern "C" int xkb_ozaki_default_moduli(long K) { return default_moduli(K); }
 
-// Real or complex Ozaki GEMM.  Scratch (stream-ordered, from the pool):
-//   planes of op(A) and op(B) (nmod x Mpad x Kpad, nmod x Npad x Kpad int8),
-//   residue planes of C (nmod x Mpad x Npad uint8), shifts and norm partials.
+extern "C" int xkb_ozaki_counts(unsigned long long* out, int* last, int reset) {
+  if (!out) return XKB_EINVAL;
+  // the counters are written by kernels on the library's non-blocking streams
+  if (cudaDeviceSynchronize() != cudaSuccess) return XKB_ECUDA;
+  if (cudaMemcpyFromSymbol(&out[0], g_oz_calls, sizeof(out[0])) != cudaSuccess ||
+      cudaMemcpyFromSymbol(&out[1], g_oz_mod_sum, sizeof(out[1])) != cudaSuccess ||
+      cudaMemcpyFromSymbol(&out[2], g_oz_fallbacks, sizeof(out[2])) != cudaSuccess)
+    return XKB_ECUDA;
+  if (last && cudaMemcpyFromSymbol(last, g_oz_last, sizeof(int)) != cudaSuccess) return XKB_ECUDA;
+  if (reset) {
+    const unsigned long long z = 0;
+    const int none = -1;
+    if (cudaMemcpyToSymbol(g_oz_calls, &z, sizeof z) != cudaSuccess ||
+        cudaMemcpyToSymbol(g_oz_mod_sum, &z, sizeof z) != cudaSuccess ||
+        cudaMemcpyToSymbol(g_oz_fallbacks, &z, sizeof z) != cudaSuccess ||
+        cudaMemcpyToSymbol(g_oz_last, &none, sizeof none) != cudaSuccess)
+      return XKB_ECUDA;
+  }
+  return XKB_OK;
+}
+
+// Real or complex Ozaki GEMM.  nmod > 0: that many moduli.  nmod == 0: the
+// count is chosen on the device from the operands (k_oz_pick: 15 or 16, at
+// least the tuning table's count for K's band); operands whose spread 16
+// moduli cannot carry to FP64 accuracy are computed by the plain FP64
+// kernel instead, launched here and predicated on the device's choice.
+// Scratch (stream-ordered, from the pool): residue planes of op(A) and
+// op(B) for the largest count the call may use (nmod x Mpad x Kpad,
+// nmod x Npad x Kpad int8), residue planes of C (nmod x Mpad x Npad uint8),
+// row codes, norm partials and the call's device words.
 extern "C" int xkb_cuda_ozaki_gemm(const xkb_gemm_args* a, int nmod, void* stream) {
   if (!a || (a->dtype != XKB_D && a->dtype != XKB_Z)) return XKB_EINVAL;
   if (a->M < 0 || a->N < 0 || a->K < 0) return XKB_EINVAL;
@@ -1214,9 +1414,9 @@ extern "C" int xkb_cuda_ozaki_gemm(const xkb_gemm_args* a, int nmod, void* strea
   if (a->K == 0 || (a->alpha[0] == 0.0 && a->alpha[1] == 0.0))
     return xkb_cuda_gemm(a, stream);
   if (Keff > 131072) return XKB_ERANGE;
-  if (nmod == 0) nmod = default_moduli(Keff);
-  const Consts* c = consts_for(nmod);
-  if (!c) return XKB_ERANGE;
+  ModPlan pl;
+  if (!plan_moduli(nmod, Keff, &pl)) return XKB_ERANGE;
+  const int nmax = pl.hi;
   cudaStream_t st = resolve_stream(stream);
   const int M = a->M, N = a->N, K = a->K;
   // complex operands are laid out [Re | pad | Im | pad] along k, each block
@@ -1230,25 +1430,28 @@ extern "C" int xkb_cuda_ozaki_gemm(const xkb_gemm_args* a, int nmod, void* strea
   // serves both operands; it then holds max(Mpad, Npad) rows per plane
   const bool same = (a->A == a->B) && (a->lda == a->ldb) && (akc == bkc) && !cplx && M == N;
   const long Arows = same ? std::max(Mpad, Npad) : Mpad;
-  const size_t szA = (size_t)nmod * Arows * Kpad, szB = (size_t)nmod * Npad * Kpad;
-  const size_t szR = (size_t)nmod * Mpad * Npad;
+  const size_t szA = (size_t)nmax * Arows * Kpad, szB = (size_t)nmax * Npad * Kpad;
+  const size_t szR = (size_t)nmax * Mpad * Npad;
   const int nch = (int)((Keff + kNormChunk - 1) / kNormChunk);
-  const size_t szPart = sizeof(double2) * (size_t)nch * (size_t)std::max(M, N) * 2;
+  const size_t szPart = 256 + sizeof(double4) * (size_t)nch * (size_t)std::max(M, N) * 2;
   const size_t szRe = cplx ? sizeof(double) * (size_t)M * N : 0;
   int8_t *Ap = nullptr, *Bp = nullptr;
   uint8_t* R = nullptr;
   int *mu = nullptr, *nu = nullptr;
-  double2* part = nullptr;
+  unsigned char* pw = nullptr;  // CallWords, then the norm partials from byte 256
   double* re = nullptr;
   auto alloc = [&](void** p, size_t n) {
     return cudaMallocAsync(p, std::max<size_t>(n, 256), st) == cudaSuccess;
   };
   bool ok = alloc((void**)&Ap, szA) && alloc((void**)&Bp, cplx ? 2 * szB : szB) &&
             alloc((void**)&R, szR) && alloc((void**)&mu, sizeof(int) * M) &&
-            alloc((void**)&nu, sizeof(int) * N) && alloc((void**)&part, szPart) &&
+            alloc((void**)&nu, sizeof(int) * N) && alloc((void**)&pw, szPart) &&
             (!cplx || alloc((void**)&re, szRe));
   int err = ok ? XKB_OK : XKB_ENOMEM;
   if (!ok) cudaGetLastError();
+  CallWords* w = reinterpret_cast<CallWords*>(pw);
+  double4* part = reinterpret_cast<double4*>(pw + 256);
+  const OzSel* sel = w ? &w->sel : nullptr;
   // operand views ----------------------------------------------------------
   // rows of op(A): opA == N -> A is M x K, row i = A[i + k*lda] (i contiguous)
   //                else     -> A is K x M, row i = A[k + i*lda] (k contiguous)
@@ -1258,25 +1461,28 @@ extern "C" int xkb_cuda_ozaki_gemm(const xkb_gemm_args* a, int nmod, void* strea
   const double* Bd = static_cast<const double*>(a->B);
   const double sa = (a->opA == XKB_OP_C) ? -1.0 : 1.0;  // conj: negate Im
   const double sb = (a->opB == XKB_OP_C) ? -1.0 : 1.0;
-  const int slot = trace_begin("ozaki_gemm", a->dtype, M, N, K, nmod, st);
+  const int slot = trace_begin("ozaki_gemm", a->dtype, M, N, K, pl.fixed ? nmax : 0, st);
   if (err == XKB_OK) {
     // scaling: complex rows use the norm over (re, im) = the concatenated row
     View va{Ad, a->lda, akc, 1, 0, 1.0}, vb{Bd, a->ldb, bkc, 1, 0, 1.0};
-    err = launch_norm(va, M, K, cplx, c, part, mu, st);
-    if (!err) err = launch_norm(vb, N, K, cplx, c, part + (size_t)nch * std::max(M, N), nu, st);
+    if (cudaMemsetAsync(w, 0, sizeof(CallWords), st) != cudaSuccess) err = XKB_ECUDA;
+    if (!err) err = launch_norm(va, M, K, cplx, part, mu, &w->rmax[0], st);
+    if (!err)
+      err = launch_norm(vb, N, K, cplx, part + (size_t)nch * std::max(M, N), nu, &w->rmax[1], st);
+    if (!err) err = launch_pick(w, pl, !pl.fixed, st);
   }
   if (err == XKB_OK) {
     if (!cplx) {
       View va{Ad, a->lda, akc, 1, 0, 1.0}, vb{Bd, a->ldb, bkc, 1, 0, 1.0};
-      err = launch_res(va, M, K, mu, c, Ap, Arows, Kpad, 0, st);
-      if (!err && !same) err = launch_res(vb, N, K, nu, c, Bp, Npad, Kpad, 0, st);
+      err = launch_res(va, M, K, mu, sel, pl.chi, Ap, Arows, Kpad, 0, st);
+      if (!err && !same) err = launch_res(vb, N, K, nu, sel, pl.chi, Bp, Npad, Kpad, 0, st);
       if (!err && Kpad > (long)rup(K, 64)) {
         // zero the k padding beyond the last 64-column block
         const size_t kz = rup(K, 64);
-        err = cudaMemset2DAsync(Ap + kz, Kpad, 0, Kpad - kz, (size_t)nmod * Arows, st) == cudaSuccess
+        err = cudaMemset2DAsync(Ap + kz, Kpad, 0, Kpad - kz, (size_t)nmax * Arows, st) == cudaSuccess
                   ? XKB_OK : XKB_ECUDA;
         if (!err && !same)
-          err = cudaMemset2DAsync(Bp + kz, Kpad, 0, Kpad - kz, (size_t)nmod * Npad, st) == cudaSuccess
+          err = cudaMemset2DAsync(Bp + kz, Kpad, 0, Kpad - kz, (size_t)nmax * Npad, st) == cudaSuccess
                     ? XKB_OK : XKB_ECUDA;
       }
     } else {
@@ -1287,16 +1493,16 @@ extern "C" int xkb_cuda_ozaki_gemm(const xkb_gemm_args* a, int nmod, void* strea
       View bin{Bd, a->ldb, bkc, 2, 1, -sb};
       int8_t* B1 = Bp;
       int8_t* B2 = Bp + szB;
-      err = launch_res(ar, M, K, mu, c, Ap, Mpad, Kpad, 0, st);
-      if (!err) err = launch_res(ai, M, K, mu, c, Ap, Mpad, Kpad, kofs2, st);
-      if (!err) err = launch_res(br, N, K, nu, c, B1, Npad, Kpad, 0, st);
-      if (!err) err = launch_res(bin, N, K, nu, c, B1, Npad, Kpad, kofs2, st);
-      if (!err) err = launch_res(bi, N, K, nu, c, B2, Npad, Kpad, 0, st);
-      if (!err) err = launch_res(br, N, K, nu, c, B2, Npad, Kpad, kofs2, st);
+      err = launch_res(ar, M, K, mu, sel, pl.chi, Ap, Mpad, Kpad, 0, st);
+      if (!err) err = launch_res(ai, M, K, mu, sel, pl.chi, Ap, Mpad, Kpad, kofs2, st);
+      if (!err) err = launch_res(br, N, K, nu, sel, pl.chi, B1, Npad, Kpad, 0, st);
+      if (!err) err = launch_res(bin, N, K, nu, sel, pl.chi, B1, Npad, Kpad, kofs2, st);
+      if (!err) err = launch_res(bi, N, K, nu, sel, pl.chi, B2, Npad, Kpad, 0, st);
+      if (!err) err = launch_res(br, N, K, nu, sel, pl.chi, B2, Npad, Kpad, kofs2, st);
       if (!err && Kpad > 2 * kofs2) {
         const size_t kz = 2 * (size_t)kofs2;
-        if (cudaMemset2DAsync(Ap + kz, Kpad, 0, Kpad - kz, (size_t)nmod * Mpad, st) != cudaSuccess ||
-            cudaMemset2DAsync(Bp + kz, Kpad, 0, Kpad - kz, (size_t)2 * nmod * Npad, st) != cudaSuccess)
+        if (cudaMemset2DAsync(Ap + kz, Kpad, 0, Kpad - kz, (size_t)nmax * Mpad, st) != cudaSuccess ||
+            cudaMemset2DAsync(Bp + kz, Kpad, 0, Kpad - kz, (size_t)2 * nmax * Npad, st) != cudaSuccess)
           err = XKB_ECUDA;
       }
     }
@@ -1310,6 +1516,7 @@ extern "C" int xkb_cuda_ozaki_gemm(const xkb_gemm_args* a, int nmod, void* strea
   cp.Npad = Npad;
   cp.mu = mu;
   cp.nu = nu;
+  cp.sel = sel;
   cp.C = static_cast<double*>(a->C);
   cp.ldc = a->ldc;
   cp.cplx = cplx;
@@ -1323,24 +1530,29 @@ extern "C" int xkb_cuda_ozaki_gemm(const xkb_gemm_args* a, int nmod, void* strea
   const dim3 cg((unsigned)(((M + 3) / 4 + 255) / 256), (unsigned)std::min(N, 65535));
   trace_mark(slot, 1, st);
   if (err == XKB_OK) {
-    err = same ? launch_gemm(Ap, Arows, Ap, Arows, Mpad, Npad, Kpad, c, R, a->uplo, a->diag, st)
-               : launch_gemm(Ap, Mpad, Bp, Npad, Mpad, Npad, Kpad, c, R, a->uplo, a->diag, st);
+    err = same ? launch_gemm(Ap, Arows, Ap, Arows, Mpad, Npad, Kpad, pl.chi, sel, R, a->uplo,
+                             a->diag, st)
+               : launch_gemm(Ap, Mpad, Bp, Npad, Mpad, Npad, Kpad, pl.chi, sel, R, a->uplo,
+                             a->diag, st);
     if (!err) {
       if (!cplx) {
         trace_mark(slot, 2, st);
-        err = launch_crt(cg, st, cp, *c, nullptr);
+        err = launch_crt(cg, st, cp, pl.clo, pl.chi, nullptr);
       } else {
-        err = launch_crt(cg, st, cp, *c, re);
-        err = launch_gemm(Ap, Mpad, Bp + szB, Npad, Mpad, Npad, Kpad, c, R, a->uplo, a->diag,
-                          st);
+        err = launch_crt(cg, st, cp, pl.clo, pl.chi, re);
+        if (!err)
+          err = launch_gemm(Ap, Mpad, Bp + szB, Npad, Mpad, Npad, Kpad, pl.chi, sel, R, a->uplo,
+                            a->diag, st);
         trace_mark(slot, 2, st);
         if (!err) {
           cp.other = re;
-          err = launch_crt(cg, st, cp, *c, nullptr);
+          err = launch_crt(cg, st, cp, pl.clo, pl.chi, nullptr);
         }
       }
-      if (!err && cudaPeekAtLastError() != cudaSuccess) err = XKB_ECUDA;
     }
+    // the data rule may have sent the call to the plain FP64 kernel
+    if (!err && !pl.fixed) err = gemm_if(a, &w->sel.fallback, st);
+    if (!err && cudaPeekAtLastError() != cudaSuccess) err = XKB_ECUDA;
   }
   trace_mark(slot, 3, st);
   if (Ap) cudaFreeAsync(Ap, st);
@@ -1348,7 +1560,7 @@ extern "C" int xkb_cuda_ozaki_gemm(const xkb_gemm_args* a, int nmod, void* strea
   if (R) cudaFreeAsync(R, st);
   if (mu) cudaFreeAsync(mu, st);
   if (nu) cudaFreeAsync(nu, st);
-  if (part) cudaFreeAsync(part, st);
+  if (pw) cudaFreeAsync(pw, st);
   if (re) cudaFreeAsync(re, st);
   return err;
 }
@@ -1389,9 +1601,12 @@ extern "C" int xkb_cuda_ozaki_gemm_panels(const xkb_gemm_args* a, int nmod, void
     for (int q = 0; q < npanel; ++q) done(q);
     return r;
   }
+  // op(A) is converted before op(B) arrives: the count is fixed for the call
+  // (the tuning table's or the K rule's when nmod == 0)
   if (nmod == 0) nmod = default_moduli(a->K);
-  const Consts* c = consts_for(nmod);
-  if (!c) return XKB_ERANGE;
+  ModPlan pl;
+  if (!plan_moduli(nmod, a->K, &pl)) return XKB_ERANGE;
+  const Consts* c = pl.chi;
   const int M = a->M, K = a->K;
   const long Kpad = (long)rup(K, BKB), Mpad = (long)rup(M, BM2);
   long wmax = 0;
@@ -1402,7 +1617,7 @@ extern "C" int xkb_cuda_ozaki_gemm_panels(const xkb_gemm_args* a, int nmod, void
   int8_t *Ap = nullptr, *Bp = nullptr;
   uint8_t* R = nullptr;
   int *mu = nullptr, *nu = nullptr;
-  double2* part = nullptr;
+  unsigned char* pw = nullptr;  // CallWords, then the norm partials from byte 256
   auto alloc = [&](void** p, size_t n) {
     return cudaMallocAsync(p, std::max<size_t>(n, 256), st) == cudaSuccess;
   };
@@ -1410,16 +1625,21 @@ extern "C" int xkb_cuda_ozaki_gemm_panels(const xkb_gemm_args* a, int nmod, void
             alloc((void**)&Bp, (size_t)nmod * Wpad * Kpad) &&
             alloc((void**)&R, (size_t)nmod * Mpad * Wpad) && alloc((void**)&mu, sizeof(int) * M) &&
             alloc((void**)&nu, sizeof(int) * a->N) &&
-            alloc((void**)&part, sizeof(double2) * (size_t)nch * (size_t)std::max<long>(M, wmax));
+            alloc((void**)&pw, 256 + sizeof(double4) * (size_t)nch * (size_t)std::max<long>(M, wmax));
   int err = ok ? XKB_OK : XKB_ENOMEM;
   if (!ok) cudaGetLastError();
+  CallWords* w = reinterpret_cast<CallWords*>(pw);
+  double4* part = reinterpret_cast<double4*>(pw + 256);
+  const OzSel* sel = w ? &w->sel : nullptr;
   const double* Ad = static_cast<const double*>(a->A);
   const double* Bd = static_cast<const double*>(a->B);
   const int slot = trace_begin("ozaki_panels", a->dtype, M, a->N, K, nmod, st);
   if (!err) {
     View va{Ad, a->lda, akc, 1, 0, 1.0};
-    err = launch_norm(va, M, K, 0, c, part, mu, st);
-    if (!err) err = launch_res(va, M, K, mu, c, Ap, Mpad, Kpad, 0, st);
+    if (cudaMemsetAsync(w, 0, sizeof(CallWords), st) != cudaSuccess) err = XKB_ECUDA;
+    if (!err) err = launch_norm(va, M, K, 0, part, mu, &w->rmax[0], st);
+    if (!err) err = launch_pick(w, pl, false, st);
+    if (!err) err = launch_res(va, M, K, mu, sel, c, Ap, Mpad, Kpad, 0, st);
     if (!err && Kpad > (long)rup(K, 64)) {
       const size_t kz = rup(K, 64);
       if (cudaMemset2DAsync(Ap + kz, Kpad, 0, Kpad - kz, (size_t)nmod * Mpad, st) != cudaSuccess)
@@ -1434,14 +1654,15 @@ extern "C" int xkb_cuda_ozaki_gemm_panels(const xkb_gemm_args* a, int nmod, void
     if (!err) {
       // columns n0.. of op(B): opB == N -> B[k + j ldb]; else B[j + k ldb]
       View vb{bkc ? Bd + n0 * a->ldb : Bd + n0, a->ldb, bkc, 1, 0, 1.0};
-      err = launch_norm(vb, (int)nw, K, 0, c, part, nu + n0, st);
-      if (!err) err = launch_res(vb, (int)nw, K, nu + n0, c, Bp, npad, Kpad, 0, st);
+      err = launch_norm(vb, (int)nw, K, 0, part, nu + n0, &w->rmax[1], st);
+      if (!err) err = launch_res(vb, (int)nw, K, nu + n0, sel, c, Bp, npad, Kpad, 0, st);
       if (!err && Kpad > (long)rup(K, 64)) {
         const size_t kz = rup(K, 64);
         if (cudaMemset2DAsync(Bp + kz, Kpad, 0, Kpad - kz, (size_t)nmod * npad, st) != cudaSuccess)
           err = XKB_ECUDA;
       }
-      if (!err) err = launch_gemm(Ap, Mpad, Bp, npad, Mpad, npad, Kpad, c, R, XKB_FULL, 0, st);
+      if (!err)
+        err = launch_gemm(Ap, Mpad, Bp, npad, Mpad, npad, Kpad, c, sel, R, XKB_FULL, 0, st);
       if (!err) {
         CrtP cp;
         std::memset(&cp, 0, sizeof(cp));
@@ -1452,13 +1673,14 @@ extern "C" int xkb_cuda_ozaki_gemm_panels(const xkb_gemm_args* a, int nmod, void
         cp.Npad = npad;
         cp.mu = mu;
         cp.nu = nu + n0;
+        cp.sel = sel;
         cp.C = static_cast<double*>(a->C) + n0 * a->ldc;
         cp.ldc = a->ldc;
         cp.ar = a->alpha[0];
         cp.br = a->beta[0];
         cp.uplo = XKB_FULL;
         const dim3 cg((unsigned)(((M + 3) / 4 + 255) / 256), (unsigned)std::min<long>(nw, 65535));
-        err = launch_crt(cg, st, cp, *c, nullptr);
+        err = launch_crt(cg, st, cp, c, c, nullptr);
       }
     }
     done(q);  // recorded on every path: waiters never hang on an error
@@ -1470,7 +1692,7 @@ extern "C" int xkb_cuda_ozaki_gemm_panels(const xkb_gemm_args* a, int nmod, void
   if (R) cudaFreeAsync(R, st);
   if (mu) cudaFreeAsync(mu, st);
   if (nu) cudaFreeAsync(nu, st);
-  if (part) cudaFreeAsync(part, st);
+  if (pw) cudaFreeAsync(pw, st);
   return err;
 }
 
@@ -1509,7 +1731,8 @@ extern "C" int xkb_cuda_ozaki_gemm_panels(const xkb_gemm_args* a, int nmod, void
 //     looks the (reloaded) array up again.
 // Nothing in the array has to start at zero: every byte a call reads is
 // written earlier in the same call (planes padded by the residue kernel and a
-// 2-D memset, shifts and partials fully rewritten).
+// 2-D memset, row codes and partials fully rewritten, the call's moduli
+// selection words cleared by a memset first).
 namespace xkb {
 namespace oz {
 constexpr int kNoAllocMaxDim = 512;
@@ -1520,7 +1743,7 @@ constexpr size_t kNoAllocA = kMaxMod * kNoAllocPlane;                  // A plan
 constexpr size_t kNoAllocB = kMaxMod * kNoAllocPlane;                  // B planes
 constexpr size_t kNoAllocR = kMaxMod * kNoAllocRows * kNoAllocRows;    // C residues
 constexpr size_t kNoAllocShift = 2 * 4 * kNoAllocRows;                 // mu, nu
-constexpr size_t kNoAllocPart = sizeof(double2) * 2 * kNoAllocRows;    // 1 k-chunk
+constexpr size_t kNoAllocPart = sizeof(double4) * 2 * kNoAllocRows;    // 1 k-chunk
 constexpr size_t kNoAllocBytes =
     kNoAllocA + kNoAllocB + kNoAllocR + kNoAllocShift + kNoAllocPart + 4096;
 
@@ -1582,7 +1805,9 @@ static bool load_noalloc_kernels() {
   cudaFuncAttributes fa;
   bool ok = cudaFuncGetAttributes(&fa, k_oz_norm<true>) == cudaSuccess &&
             cudaFuncGetAttributes(&fa, k_oz_norm<false>) == cudaSuccess &&
-            cudaFuncGetAttributes(&fa, k_oz_shift) == cudaSuccess &&
+            cudaFuncGetAttributes(&fa, k_oz_stat) == cudaSuccess &&
+            cudaFuncGetAttributes(&fa, k_oz_pick) == cudaSuccess &&
+            cudaFuncGetAttributes(&fa, k_oz_crt_15_16) == cudaSuccess &&
             cudaFuncGetAttributes(&fa, k_oz_gemm) == cudaSuccess &&
             cudaFuncGetAttributes(&fa, k_oz_beta) == cudaSuccess;
   ok = ok && load_nm_kernels<2>() && load_nm_kernels<3>() && load_nm_kernels<4>() &&
@@ -1634,9 +1859,12 @@ extern "C" int xkb_cuda_ozaki_gemm_noalloc(const xkb_gemm_args* a, int nmod, voi
   if (a->K > 0 && a->alpha[0] != 0.0 && (a->opA < XKB_OP_N || a->opA > XKB_OP_C ||
                                          a->opB < XKB_OP_N || a->opB > XKB_OP_C))
     return XKB_EINVAL;
-  if (nmod == 0) nmod = default_moduli(a->K > 0 ? a->K : 1);
-  const Consts* c = consts_for(nmod);
-  if (!c) return XKB_ERANGE;
+  // nmod == 0: the data rule's count, at most 16 (there is no plain fallback
+  // here: the plain kernel may need scratch for unaligned operands)
+  ModPlan pl;
+  if (!plan_moduli(nmod, a->K > 0 ? a->K : 1, &pl)) return XKB_ERANGE;
+  const Consts* c = pl.chi;
+  nmod = pl.hi;
   unsigned char* base = nullptr;
   int err = noalloc_base(&base);
   if (err) return err;
@@ -1662,15 +1890,20 @@ extern "C" int xkb_cuda_ozaki_gemm_noalloc(const xkb_gemm_args* a, int nmod, voi
   uint8_t* R = base + kNoAllocA + kNoAllocB;
   int* mu = reinterpret_cast<int*>(base + kNoAllocA + kNoAllocB + kNoAllocR);
   int* nu = mu + kNoAllocRows;
-  double2* part = reinterpret_cast<double2*>(base + kNoAllocA + kNoAllocB + kNoAllocR + kNoAllocShift);
+  unsigned char* tail = base + kNoAllocA + kNoAllocB + kNoAllocR + kNoAllocShift;
+  double4* part = reinterpret_cast<double4*>(tail);
+  CallWords* w = reinterpret_cast<CallWords*>(tail + kNoAllocPart);
+  const OzSel* sel = &w->sel;
   const double* Ad = static_cast<const double*>(a->A);
   const double* Bd = static_cast<const double*>(a->B);
-  const int slot = trace_begin("ozaki_noalloc", a->dtype, M, N, K, nmod, st);
+  const int slot = trace_begin("ozaki_noalloc", a->dtype, M, N, K, pl.fixed ? nmod : 0, st);
   View va{Ad, a->lda, akc, 1, 0, 1.0}, vb{Bd, a->ldb, bkc, 1, 0, 1.0};
-  err = launch_norm(va, M, K, 0, c, part, mu, st);
-  if (!err) err = launch_norm(vb, N, K, 0, c, part + kNoAllocRows, nu, st);
-  if (!err) err = launch_res(va, M, K, mu, c, Ap, Arows, Kpad, 0, st);
-  if (!err && !same) err = launch_res(vb, N, K, nu, c, Bp, Npad, Kpad, 0, st);
+  if (cudaMemsetAsync(w, 0, sizeof(CallWords), st) != cudaSuccess) err = XKB_ECUDA;
+  if (!err) err = launch_norm(va, M, K, 0, part, mu, &w->rmax[0], st);
+  if (!err) err = launch_norm(vb, N, K, 0, part + kNoAllocRows, nu, &w->rmax[1], st);
+  if (!err) err = launch_pick(w, pl, false, st);
+  if (!err) err = launch_res(va, M, K, mu, sel, c, Ap, Arows, Kpad, 0, st);
+  if (!err && !same) err = launch_res(vb, N, K, nu, sel, c, Bp, Npad, Kpad, 0, st);
   if (!err && Kpad > (long)rup(K, 64)) {
     const size_t kz = rup(K, 64);
     if (cudaMemset2DAsync(Ap + kz, Kpad, 0, Kpad - kz, (size_t)nmod * Arows, st) != cudaSuccess ||
@@ -1680,8 +1913,10 @@ extern "C" int xkb_cuda_ozaki_gemm_noalloc(const xkb_gemm_args* a, int nmod, voi
   }
   trace_mark(slot, 1, st);
   if (!err)
-    err = same ? launch_gemm(Ap, Arows, Ap, Arows, Mpad, Npad, Kpad, c, R, a->uplo, a->diag, st)
-               : launch_gemm(Ap, Mpad, Bp, Npad, Mpad, Npad, Kpad, c, R, a->uplo, a->diag, st);
+    err = same ? launch_gemm(Ap, Arows, Ap, Arows, Mpad, Npad, Kpad, c, sel, R, a->uplo, a->diag,
+                             st)
+               : launch_gemm(Ap, Mpad, Bp, Npad, Mpad, Npad, Kpad, c, sel, R, a->uplo, a->diag,
+                             st);
   trace_mark(slot, 2, st);
   if (!err) {
     CrtP cp;
@@ -1693,6 +1928,7 @@ extern "C" int xkb_cuda_ozaki_gemm_noalloc(const xkb_gemm_args* a, int nmod, voi
     cp.Npad = Npad;
     cp.mu = mu;
     cp.nu = nu;
+    cp.sel = sel;
     cp.C = static_cast<double*>(a->C);
     cp.ldc = a->ldc;
     cp.ar = a->alpha[0];
@@ -1700,7 +1936,7 @@ extern "C" int xkb_cuda_ozaki_gemm_noalloc(const xkb_gemm_args* a, int nmod, voi
     cp.uplo = a->uplo;
     cp.diag = a->diag;
     const dim3 cg((unsigned)(((M + 3) / 4 + 255) / 256), (unsigned)N);
-    err = launch_crt(cg, st, cp, *c, nullptr);
+    err = launch_crt(cg, st, cp, pl.clo, pl.chi, nullptr);
   }
   trace_mark(slot, 3, st);
   return err;

@@ -35,6 +35,8 @@ Runtime& rt() {
 }
 
 static int cuda_ok(cudaError_t e) { return e == cudaSuccess ? XKB_OK : XKB_ECUDA; }
+static void print_configuration(const cudaDeviceProp& prop);
+static void print_statistics();
 
 int ensure_init() {
   Runtime& R = rt();
@@ -89,6 +91,18 @@ int ensure_init() {
   if (const char* u = getenv("XKBLAS_UNIFIED")) R.unified = R.unified || atoi(u) != 0;
   if (const char* t = getenv("XKBLAS_TILE_SIZE")) R.nb_param = (size_t)atol(t);
   else if (const char* b = getenv("XKBLAS_BLOC_SIZE")) R.nb_param = (size_t)atol(b);
+  // element size the tile-size rule assumes (reference blas/xkblas.c:1483-1497;
+  // an unknown value is reported and ignored instead of exiting)
+  if (const char* p = getenv("XKBLAS_PRECISION")) {
+    if (!strcmp(p, "float") || !strcmp(p, "real*4")) R.prec_param = 4;
+    else if (!strcmp(p, "double") || !strcmp(p, "real*8")) R.prec_param = 8;
+    else if (!strcmp(p, "complex32") || !strcmp(p, "complex*4")) R.prec_param = 8;
+    else if (!strcmp(p, "complex64") || !strcmp(p, "complex*8")) R.prec_param = 16;
+    else
+      fprintf(stderr, "[XKBlas] XKBLAS_PRECISION must be float|real*4|double|real*8|"
+                      "complex32|complex*4|complex64|complex*8; '%s' ignored\n", p);
+  }
+  if (const char* v = getenv("XKBLAS_VERBOSE")) R.verbose = std::max(0, atoi(v));
   if (const char* m = getenv("XKBLAS_DEFAULT_MATH")) {
     if (!strcmp(m, "TC") || !strcmp(m, "tensorcore")) R.math = XKBLAS_TENSOR_OP_MATH;
     else R.math = XKBLAS_DEFAULT_MATH;
@@ -100,7 +114,87 @@ int ensure_init() {
   if (const char* s = getenv("XKBLAS_OZAKI_MIN_DIM")) R.ozaki_min_env = atol(s);
   if (const char* s = getenv("XKBLAS_BATCH_FLUSH_MB")) R.batch_flush_env = (size_t)atol(s) << 20;
   R.ready = true;
+  if (R.verbose) print_configuration(prop);
   return XKB_OK;
+}
+
+// XKBLAS_VERBOSE at initialisation: the configuration in effect (reference
+// blas/xkblas.c:1578-1604 prints its runtime's description there).
+static void print_configuration(const cudaDeviceProp& prop) {
+  const Runtime& R = rt();
+  const char* tf = getenv("XKBLAS_TUNE_FILE");
+  printf("[XKBlas info]\n%s\n", xkblas_get_configuration());
+  printf("device %d: %s, sm_%d%d, %d SMs, %.1f GiB, L2 %.0f MiB\n", R.device, prop.name,
+         prop.major, prop.minor, prop.multiProcessorCount,
+         (double)prop.totalGlobalMem / 1073741824.0, (double)prop.l2CacheSize / 1048576.0);
+  printf("tile size: %s%zu, precision: %zu bytes\n", R.nb_param ? "" : "auto ",
+         R.nb_param, R.prec_param);
+  printf("math: %s; Ozaki moduli: %s%d, below %ld: plain\n",
+         R.math == XKBLAS_TENSOR_OP_MATH ? "tensor-op (Ozaki INT8)" : "default (FP64 DMMA)",
+         R.ozaki_moduli ? "fixed " : "data rule, 0 = ", R.ozaki_moduli, ozaki_min_dim());
+  printf("deferred-call batches: %s, cache limit: %.0f MiB, unified: %s, tuning file: %s\n",
+         R.batch_on ? "on" : "off", (double)R.cache_limit / 1048576.0, R.unified ? "on" : "off",
+         tf && *tf ? tf : "none");
+  printf("[XKBlas info]\n");
+  fflush(stdout);
+}
+
+// XKBLAS_VERBOSE at finalisation: per-operation counts and flops, then the
+// totals (reference blas/xkblas.c:1635-1700 prints per task type).
+static void print_statistics() {
+  Runtime& R = rt();
+  unsigned long long oz[3] = {0, 0, 0};
+  xkb_ozaki_counts(oz, nullptr, 0);
+  printf("[XKBlas stats]\n");
+  uint64_t calls = 0;
+  double flops = 0;
+  for (const auto& kv : R.per_op) {
+    printf("\t[%12s]: count=%12llu, flops=%10e\n", kv.first.c_str(),
+           (unsigned long long)kv.second.calls, kv.second.flops);
+    calls += kv.second.calls;
+    flops += kv.second.flops;
+  }
+  printf("\t[%12s]: count=%12llu, flops=%10e\n", "sum -->", (unsigned long long)calls, flops);
+  if (R.verbose >= 2) {
+    printf("\tkernels=%llu h2d_bytes=%llu d2h_bytes=%llu tile_hits=%llu tile_misses=%llu "
+           "evictions=%llu batches=%llu batched_calls=%llu\n",
+           (unsigned long long)xkb_cuda_kernel_count(), (unsigned long long)R.stats.h2d,
+           (unsigned long long)R.stats.d2h, (unsigned long long)R.stats.hits,
+           (unsigned long long)R.stats.misses, (unsigned long long)R.stats.evictions,
+           (unsigned long long)R.batches, (unsigned long long)R.batched_calls);
+    printf("\tozaki: contractions=%llu moduli=%llu plain_fallbacks=%llu\n", oz[0], oz[1], oz[2]);
+  }
+  fflush(stdout);
+}
+
+void count_call(const char* op) {
+  Runtime& R = rt();
+  R.stats.calls++;
+  R.per_op[op].calls++;
+}
+
+void add_flops(const char* op, double flops) {
+  Runtime& R = rt();
+  R.stats.flops += flops;
+  R.per_op[op].flops += flops;
+}
+
+ThreadCtx& tctx() {
+  static thread_local ThreadCtx t;
+  return t;
+}
+
+ThreadCtx::~ThreadCtx() {
+  // no CUDA call at thread exit: the events go back to the runtime's pool
+  if (!ev[0]) return;
+  Runtime& R = rt();
+  std::lock_guard<std::recursive_mutex> g(R.mu);
+  for (cudaEvent_t e : ev) R.ev_free.push_back(e);
+}
+
+int thread_math() {
+  const int m = tctx().math;
+  return m < 0 ? rt().math : m;
 }
 
 // Events are recycled round-robin; 64 in flight is far more than any call
@@ -762,6 +856,7 @@ int xkblas_finalize(void) {
   xkb_cuda_batch_release();
   if (const char* dir = getenv("XKBLAS_TRACE_DIR"))
     if (*dir) xkblas_trace_export(dir);
+  if (R.verbose) print_statistics();
   return 0;
 }
 
@@ -810,20 +905,50 @@ const char* xkblas_get_configuration(void) {
 void xkblas_load_sym(void** ptr, const char* name);  // native.cpp
 
 int xkblas_sync(void) {
+  // Waits for the work queued before this call -- all of the calling
+  // thread's own calls -- without holding the runtime lock while waiting, so
+  // other threads keep submitting (reference: each thread synchronises its
+  // own task list, blas/xkblas.c:1773-1850).  Deferred calls are launched
+  // first (the queue is shared by the threads).
   Runtime& R = rt();
-  std::lock_guard<std::recursive_mutex> g(R.mu);
-  if (!R.ready) {
-    xkb::evlog_sync_done();
-    return 0;
+  ThreadCtx& T = tctx();
+  int e = 0;
+  {
+    std::lock_guard<std::recursive_mutex> g(R.mu);
+    if (!R.ready) {
+      xkb::evlog_sync_done();
+      return 0;
+    }
+    e = flush_pending();
+    if (!T.ev[0]) {
+      for (auto& ev : T.ev) {
+        if (!R.ev_free.empty()) {
+          ev = R.ev_free.back();
+          R.ev_free.pop_back();
+        } else if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) {
+          cudaGetLastError();
+          ev = nullptr;
+        }
+      }
+    }
+    const cudaStream_t ss[3] = {R.s_comp, R.s_h2d, R.s_d2h};
+    for (int i = 0; i < 3; ++i)
+      if (!T.ev[i] || cudaEventRecord(T.ev[i], ss[i]) != cudaSuccess) {
+        cudaGetLastError();
+        if (cudaStreamSynchronize(ss[i]) != cudaSuccess) e = XKB_ECUDA;  // no event: drain
+      }
   }
-  int e = flush_pending();
-  if (cudaStreamSynchronize(R.s_comp) != cudaSuccess) e = XKB_ECUDA;
-  if (cudaStreamSynchronize(R.s_h2d) != cudaSuccess) e = XKB_ECUDA;
-  if (cudaStreamSynchronize(R.s_d2h) != cudaSuccess) e = XKB_ECUDA;
+  for (cudaEvent_t ev : T.ev)
+    if (ev && cudaEventSynchronize(ev) != cudaSuccess) e = XKB_ECUDA;
+  std::lock_guard<std::recursive_mutex> g(R.mu);
   int de = xkb_cuda_take_device_error();
   if (de) {
+    // a bounded device wait that gave up, or a bounds check that refused an
+    // access; xkblas_last_device_error() gives the exact word
     R.sticky_error = de;
-    e = XKB_ETIMEDOUT;
+    e = (de >= XKB_DEV_FULL_WAIT && de <= XKB_DEV_ACC_WAIT) ? XKB_ETIMEDOUT
+        : de == XKB_DEV_BOUNDS                              ? XKB_EFAULT
+                                                            : XKB_ECUDA;
   }
   xkb::evlog_sync_done();
   return e;
@@ -838,14 +963,17 @@ int xkblas_last_device_error(void) {
 }
 
 xkblas_context_t* xkblas_context_get(void) {
-  // one runtime per process; the handle is an opaque non-null token
-  return reinterpret_cast<xkblas_context_t*>(&rt());
+  // the calling thread's context (an opaque, non-null handle per thread)
+  return reinterpret_cast<xkblas_context_t*>(&tctx());
 }
 
 void xkblas_set_modemath(xkblas_mode_math_t mode) {
-  Runtime& R = rt();
-  std::lock_guard<std::recursive_mutex> g(R.mu);
-  R.math = (mode == XKBLAS_TENSOR_OP_MATH) ? XKBLAS_TENSOR_OP_MATH : XKBLAS_DEFAULT_MATH;
+  // the calling thread's mode only (reference blas/xkblas.c:356-359)
+  tctx().math = (mode == XKBLAS_TENSOR_OP_MATH) ? XKBLAS_TENSOR_OP_MATH : XKBLAS_DEFAULT_MATH;
+}
+
+xkblas_mode_math_t xkblas_get_modemath(void) {
+  return thread_math() == XKBLAS_TENSOR_OP_MATH ? XKBLAS_TENSOR_OP_MATH : XKBLAS_DEFAULT_MATH;
 }
 
 size_t xkblas_get_param(void) { return rt().nb_param; }
@@ -1118,8 +1246,14 @@ int xkblas_get_stats(xkblas_stats_t* st) {
   st->evictions = R.stats.evictions;
   st->tile_hits = R.stats.hits;
   st->tile_misses = R.stats.misses;
-  st->ozaki_calls = R.stats.ozaki_calls;
-  st->ozaki_moduli = R.stats.ozaki_moduli;
+  // Ozaki contractions are counted on the device (the moduli count of a call
+  // may be chosen there); reading the counters waits for the device
+  st->ozaki_calls = st->ozaki_moduli = 0;
+  unsigned long long oz[3];
+  if (R.ready && xkb_ozaki_counts(oz, nullptr, 0) == XKB_OK) {
+    st->ozaki_calls = oz[0] - R.stats.ozaki_calls;
+    st->ozaki_moduli = oz[1] - R.stats.ozaki_moduli;
+  }
   st->flops = R.stats.flops;
   st->batches = R.batches;
   st->batched_calls = R.batched_calls;
@@ -1130,6 +1264,12 @@ void xkblas_reset_stats(void) {
   Runtime& R = rt();
   std::lock_guard<std::recursive_mutex> g(R.mu);
   R.stats = Stats();
+  // the Ozaki counters' values at the reset (get_stats reports the growth)
+  unsigned long long oz[3];
+  if (R.ready && xkb_ozaki_counts(oz, nullptr, 0) == XKB_OK) {
+    R.stats.ozaki_calls = oz[0];
+    R.stats.ozaki_moduli = oz[1];
+  }
   R.batches = 0;
   R.batched_calls = 0;
 }

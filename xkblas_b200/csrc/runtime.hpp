@@ -6,6 +6,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -65,9 +66,17 @@ struct Desc {
   uint8_t& tile(size_t i, size_t j) { return st[i + j * mt]; }
 };
 
+// Per-operation counters ("dgemm", "ztrsm", ...): accepted calls and their
+// algorithmic flops (reference per-task-type statistics printed at
+// finalize under XKBLAS_VERBOSE, blas/xkblas.c:1635-1700).
+struct OpCount {
+  uint64_t calls = 0;
+  double flops = 0;
+};
+
 struct Stats {
   uint64_t calls = 0, h2d = 0, d2h = 0, hits = 0, misses = 0, evictions = 0;
-  uint64_t ozaki_calls = 0, ozaki_moduli = 0;
+  uint64_t ozaki_calls = 0, ozaki_moduli = 0;  // the device counters at the last reset
   double flops = 0;
 };
 
@@ -84,7 +93,8 @@ struct Runtime {
   std::unordered_map<const void*, Desc*> descs;
   size_t nb_param = 0;        // preset tile size (0 = automatic)
   size_t prec_param = 8;
-  int math = XKBLAS_DEFAULT_MATH;
+  int math = XKBLAS_DEFAULT_MATH;  // process default (XKBLAS_DEFAULT_MATH); per thread: ThreadCtx
+  std::vector<cudaEvent_t> ev_free;  // sync events of ended threads, reused
   int ozaki_moduli = 0;       // 0 = automatic
   bool unified = false;       // xkblas_malloc_unified returns managed memory (XKBLAS_UNIFIED)
   // contractions smaller than this stay plain: XKBLAS_OZAKI_MIN_DIM, else the
@@ -92,6 +102,8 @@ struct Runtime {
   long ozaki_min_env = -1;
                               // (measured crossover on a B200, autotune.py)
   Stats stats;
+  std::map<std::string, OpCount> per_op;  // since init (XKBLAS_VERBOSE report)
+  int verbose = 0;                        // XKBLAS_VERBOSE level
   int sticky_error = 0;
   // Deferred calls: async GEMM / left-TRSM calls queued as one batch for the
   // persistent tile-task executor (XKBLAS_BATCH=0 disables).  The queue is
@@ -120,6 +132,18 @@ struct Runtime {
 
 Runtime& rt();
 int ensure_init();  // lazily initialises (returns XKB_* code)
+
+// One context per calling thread (reference: an xkblas_context_t per
+// pthread, blas/xkblas.c:224-243): its math mode (the process default until
+// the thread sets one, blas/xkblas.c:356-365) and the events its
+// xkblas_sync waits for.  The events return to a pool when the thread ends.
+struct ThreadCtx {
+  int math = -1;                    // -1: the process default (Runtime::math)
+  cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};  // compute, h2d, d2h
+  ~ThreadCtx();
+};
+ThreadCtx& tctx();
+int thread_math();  // the calling thread's mode
 cudaEvent_t next_event();
 
 // Directory operations (caller holds rt().mu).
@@ -159,6 +183,10 @@ void drop_desc(Desc* d);
 void* dev_ptr(const Desc* d, size_t r, size_t c);
 
 size_t auto_tilesize(xkblas_kernel_t kernel, size_t M, size_t N, size_t K);
+
+// Statistics of an accepted level-3 call (caller holds rt().mu).
+void count_call(const char* op);
+void add_flops(const char* op, double flops);
 
 // Scratch device memory for a call, stream-ordered on the compute stream.
 void* scratch_alloc(size_t bytes);

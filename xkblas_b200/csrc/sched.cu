@@ -114,7 +114,7 @@ __device__ __forceinline__ int ld_volatile(const int* p) { return *(const volati
 // Returns the task id, -1 when every task has been claimed, -2 on timeout or
 // when another CTA recorded an error.
 __device__ __forceinline__ int claim_task(Ctl* ctl, const int* bulk, int nbulk, const int* urq,
-                                          int nurg, bool urgent_first) {
+                                          int nurg, bool urgent_first, uint64_t wait_ns) {
   uint64_t t0 = 0;
   for (uint32_t spin = 0;; ++spin) {
     for (int pass = 0; pass < 2; ++pass) {
@@ -132,7 +132,7 @@ __device__ __forceinline__ int claim_task(Ctl* ctl, const int* bulk, int nbulk, 
                 if (dev_error_set()) return -2;
                 const uint64_t now = globaltimer();
                 if (w0 == 0) w0 = now;
-                else if (now - w0 > kWaitLimitNs) {
+                else if (now - w0 > wait_ns) {
                   dev_error(kErrFullWait);
                   return -2;
                 }
@@ -151,7 +151,7 @@ __device__ __forceinline__ int claim_task(Ctl* ctl, const int* bulk, int nbulk, 
       if (dev_error_set()) return -2;
       const uint64_t now = globaltimer();
       if (t0 == 0) t0 = now;
-      else if (now - t0 > kWaitLimitNs) {
+      else if (now - t0 > wait_ns) {
         dev_error(kErrFullWait);
         return -2;
       }
@@ -523,7 +523,7 @@ __global__ void __launch_bounds__(kThreads, 2)
     k_sched(const Task* __restrict__ tasks, int* ndep, const int* __restrict__ succ,
             const int* __restrict__ bulk, int nbulk, int* urq, int nurg, Ctl* ctl,
             int urgent_first, int* call_left, unsigned long long* call_end,
-            unsigned long long* t_start) {
+            unsigned long long* t_start, unsigned long long wait_ns) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem =
       reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
@@ -533,7 +533,7 @@ __global__ void __launch_bounds__(kThreads, 2)
   if (threadIdx.x == 0) atomicMin(t_start, (unsigned long long)globaltimer());
   for (;;) {
     if (threadIdx.x == 0) {
-      const int i = claim_task(ctl, bulk, nbulk, urq, nurg, urgent_first != 0);
+      const int i = claim_task(ctl, bulk, nbulk, urq, nurg, urgent_first != 0, wait_ns);
       if (i >= 0) {
         __threadfence();  // acquire: the producers' outputs before the reads
         s_task = tasks[i];
@@ -887,6 +887,14 @@ static uint64_t op_key(const xkb_batch_op* ops, int nops, int schedule) {
 }
 
 // kernel arguments of one launch on image d
+// How long a CTA of the executor waits for a task whose dependencies are
+// not yet resolved before it records kErrFullWait and the launch ends: the
+// tuning key sched_wait_ms (default 4000 ms), a kernel parameter.
+static unsigned long long wait_limit_ns() {
+  const double ms = tune("sched_wait_ms", (double)(kWaitLimitNs / 1000000ull));
+  return (unsigned long long)(std::max(1.0, ms) * 1e6);
+}
+
 struct KArgs {
   const Task* tasks;
   int* ndep;
@@ -900,6 +908,7 @@ struct KArgs {
   int* left;
   unsigned long long* call_end;
   unsigned long long* t_start;
+  unsigned long long wait_ns;
   KArgs(uint8_t* d, const Layout& L, int schedule, unsigned long long* times)
       : tasks(reinterpret_cast<const Task*>(d)),
         ndep(reinterpret_cast<int*>(d + L.o_ndep)),
@@ -912,9 +921,10 @@ struct KArgs {
         urgent_first(schedule == 0 ? 1 : 0),
         left(reinterpret_cast<int*>(d + L.o_left)),
         call_end(times),
-        t_start(times + L.nops) {}
-  void* params[12] = {&tasks, &ndep, &succ, &bulk, &nbulk, &urq,
-                      &nurg,  &ctl,  &urgent_first, &left, &call_end, &t_start};
+        t_start(times + L.nops),
+        wait_ns(wait_limit_ns()) {}
+  void* params[13] = {&tasks, &ndep, &succ,         &bulk, &nbulk,    &urq,    &nurg,
+                      &ctl,   &urgent_first, &left, &call_end, &t_start, &wait_ns};
 };
 
 static Batch& batch() {
@@ -1180,7 +1190,7 @@ extern "C" int xkb_cuda_batch(const xkb_batch_op* ops, int nops, int schedule, v
   const long long tv = evlog_kern_begin(st, "k_sched");
   k_sched<<<grid, kThreads, kSmemBytes, st>>>(a.tasks, a.ndep, a.succ, a.bulk, a.nbulk, a.urq,
                                               a.nurg, a.ctl, a.urgent_first, a.left,
-                                              a.call_end, a.t_start);
+                                              a.call_end, a.t_start, a.wait_ns);
   evlog_kern_end(tv, st);
   trace_calls(tv, st, B.d_times, ops, nops);
   count_launch();
@@ -1220,4 +1230,47 @@ extern "C" int xkb_cuda_batch_cached(void) {
   Batch& B = batch();
   std::lock_guard<std::mutex> g(g_batch_mu);
   return (int)B.graphs.size();
+}
+
+// Exercises the bounded wait on the device: one CTA of the executor is
+// launched on a ready queue whose only slot claims a task (the queue's tail
+// was advanced) that no producer ever writes -- as if the task's last
+// dependency never resolved.  The CTA waits wait_ms, records kErrFullWait
+// and ends; the launch returns normally and the context stays usable.  The
+// caller reads the outcome with xkb_cuda_take_device_error (or xkblas_sync).
+extern "C" int xkb_cuda_sched_wait_test(int wait_ms, void* stream) {
+  if (wait_ms < 1 || wait_ms > 10000) return XKB_EINVAL;
+  cudaStream_t st = resolve_stream(stream);
+  if (int e = set_smem_attr()) return e;
+  // layout: ctl | urq[1] | ndep[1] | left[1] | times[2] | task[1]
+  const size_t o_urq = 16, o_ndep = 32, o_left = 48, o_times = 64, o_task = 128;
+  const size_t bytes = o_task + sizeof(Task);
+  uint8_t* d = nullptr;
+  if (cudaMallocAsync(&d, bytes, st) != cudaSuccess) {
+    cudaGetLastError();
+    return XKB_ENOMEM;
+  }
+  uint8_t h[o_task + sizeof(Task)];
+  std::memset(h, 0, sizeof h);
+  const Ctl ctl{0, 0, 1, 0};  // no bulk work; one queued ticket ...
+  std::memcpy(h, &ctl, sizeof ctl);
+  const int unset = -1;       // ... whose slot is never written
+  std::memcpy(h + o_urq, &unset, sizeof unset);
+  const int one = 1;
+  std::memcpy(h + o_ndep, &one, sizeof one);
+  std::memcpy(h + o_left, &one, sizeof one);
+  cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, st);
+  auto* times = reinterpret_cast<unsigned long long*>(d + o_times);
+  cudaMemsetAsync(times + 1, 0xff, sizeof(unsigned long long), st);
+  const long long tv = evlog_kern_begin(st, "k_sched");
+  k_sched<<<1, kThreads, kSmemBytes, st>>>(
+      reinterpret_cast<const Task*>(d + o_task), reinterpret_cast<int*>(d + o_ndep), nullptr,
+      nullptr, 0, reinterpret_cast<int*>(d + o_urq), 1, reinterpret_cast<Ctl*>(d), 1,
+      reinterpret_cast<int*>(d + o_left), times, times + 1, (unsigned long long)wait_ms * 1000000ull);
+  evlog_kern_end(tv, st);
+  count_launch();
+  cudaFreeAsync(d, st);
+  // the staging array h is copied by the time the host can return: pageable
+  // memory makes cudaMemcpyAsync stage it synchronously
+  return cudaPeekAtLastError() == cudaSuccess ? XKB_OK : XKB_ECUDA;
 }

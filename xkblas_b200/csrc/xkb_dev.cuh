@@ -19,13 +19,13 @@ constexpr uint64_t kWaitLimitNs = 4000000000ull;  // 4 s
 // each unit registers a reader so xkb_cuda_take_device_error() sees all.
 static __device__ int g_dev_error;
 
-enum DevErr : int {
+enum DevErr : int {  // the XKB_DEV_* words of xkb_cuda.h
   kErrNone = 0,
-  kErrFullWait = 1,    // consumer gave up waiting for a TMA stage
-  kErrEmptyWait = 2,   // producer gave up waiting for a free stage
-  kErrMmaWait = 3,     // tensor-core completion wait gave up
-  kErrAccWait = 4,     // epilogue gave up waiting for the accumulator
-  kErrBounds = 5,      // a bounds check refused an access
+  kErrFullWait = XKB_DEV_FULL_WAIT,    // consumer gave up waiting for a TMA stage / a task
+  kErrEmptyWait = XKB_DEV_EMPTY_WAIT,  // producer gave up waiting for a free stage
+  kErrMmaWait = XKB_DEV_MMA_WAIT,      // tensor-core completion wait gave up
+  kErrAccWait = XKB_DEV_ACC_WAIT,      // epilogue gave up waiting for the accumulator
+  kErrBounds = XKB_DEV_BOUNDS,         // a bounds check refused an access
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -154,6 +154,9 @@ bool side_join(const SideStream& side, cudaStream_t forked, cudaStream_t st);
 int trsm_entry(int dtype, int side, int uplo, int trans, int diag, int M, int N,
                const double* alpha, const void* A, long lda, void* B, long ldb, int ozaki,
                cudaStream_t st, bool split_rhs);
+// xkb_cuda_gemm whose kernel runs only where the device word *run_if is
+// non-zero (gemm_dmma.cu): the plain fallback of a data-chosen Ozaki call.
+int gemm_if(const xkb_gemm_args* a, const int* run_if, cudaStream_t st);
 double tune(const char* key, double dflt);   // tuning table (runtime_cuda.cu)
 int tune_band(const char* prefix, long K);
 int sm_count();
