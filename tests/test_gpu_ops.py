@@ -398,3 +398,55 @@ def test_gemm_many_ctas_per_sm(xk, mnk):
         xk.invalidate_caches()
         err = np.abs(C - ref).max() / (1.5 * np.abs(A).max() * np.abs(B).max() * K)
         assert err < 1e-15, err
+
+
+@pytest.mark.parametrize("case", [
+    # (dtype, M, N, K, opA, opB, uplo): few output tiles, long K -> split-K
+    (np.float64, 2048, 512, 2048, N_, N_, 0),
+    (np.float64, 256, 256, 4096, T_, N_, 0),
+    (np.float64, 300, 200, 2049, N_, T_, 0),
+    (np.complex128, 320, 256, 3000, C_, N_, 0),
+    (np.float64, 384, 384, 2048, N_, T_, LO),
+    (np.complex128, 256, 256, 1500, N_, C_, UP),
+])
+def test_gemm_split_k(xk, case):
+    """Too few 128 x 128 output tiles for the SMs: the k range of each tile
+    is split across CTAs and the slices are summed in a fixed order.  Same
+    bounds as every GEMM, the masked triangle only, and bit-identical
+    results on repeated calls (deterministic reduction)."""
+    import ctypes
+    import torch
+    from xkblas_b200 import GemmArgs
+    dt, M, N, K, ta, tb, uplo = case
+    cplx = dt == np.complex128
+    A = gen(M, K, 50, dt) if ta == N_ else gen(K, M, 50, dt)
+    B = gen(K, N, 51, dt) if tb == N_ else gen(N, K, 51, dt)
+    C0 = gen(M, N, 52, dt)
+    al, be = (1.5 - 0.25j, -0.5 + 0.125j) if cplx else (1.5, -0.5)
+    dev = lambda X: torch.from_numpy(np.ascontiguousarray(X.T)).cuda()
+    dA, dB = dev(A), dev(B)
+    outs = []
+    for _ in range(2):
+        dC = dev(C0)
+        g = GemmArgs(3 if cplx else 1, ta - N_, tb - N_, M, N, K, dA.data_ptr(), A.shape[0],
+                     dB.data_ptr(), B.shape[0], dC.data_ptr(), M)
+        g.alpha[0], g.alpha[1] = (al.real, al.imag) if cplx else (al, 0.0)
+        g.beta[0], g.beta[1] = (be.real, be.imag) if cplx else (be, 0.0)
+        g.uplo = {0: 0, LO: 1, UP: 2}[uplo]
+        torch.cuda.synchronize()
+        k0 = xk.kernel_count()
+        assert xk.lib().xkb_cuda_gemm(ctypes.byref(g), None) == 0
+        assert xk.kernel_count() - k0 == 2  # the split product and its reduction
+        xk.sync()
+        outs.append(np.asfortranarray(dC.cpu().numpy().T))
+    assert xk.lib().xkb_cuda_take_device_error() == 0
+    assert np.array_equal(outs[0], outs[1])
+    C = outs[0]
+    R = O.gemm(ta, tb, al, A, B, be, C0.copy(order="F"), nb=256)
+    if uplo:
+        sel = np.tril if uplo == LO else np.triu
+        other = np.triu if uplo == LO else np.tril
+        k = 1 if uplo == LO else -1
+        np.testing.assert_array_equal(other(C, k), other(C0, k))
+        C, R = sel(C), sel(R)
+    assert checks.gemm_ratio(C, R, A, B, C0, al, be, K) <= 3.0

@@ -41,7 +41,82 @@ struct GemmParams {
   int conjA, conjB;
   int tiles_m, tiles_n, ktiles;
   const int* run_if;  // not null: the launch does nothing unless *run_if != 0
+  // split-K: the k-tiles of every C tile are shared by ksplit CTAs, slice s
+  // taking [s kt_slice, (s+1) kt_slice); each writes its raw accumulators to
+  // ws and k_gemm_splitk sums the slices in order and runs the epilogue
+  int ksplit, kt_slice;
+  double* ws;
 };
+
+// Tile of CTA `bid` (< tiles_m tiles_n) in the grouped rasterisation: 8 tile
+// rows share a band of B columns in L2.  False if it lies wholly outside the
+// triangle mask (nothing to do).
+template <int BM, int BN>
+__device__ __forceinline__ bool dmma_tile(const GemmParams& p, int bid, int& m0, int& n0) {
+  const int GROUP = 8;
+  const int span = GROUP * p.tiles_n;
+  const int first_m = (bid / span) * GROUP;
+  const int gsz = min(p.tiles_m - first_m, GROUP);
+  const int tm = first_m + (bid % span) % gsz;
+  const int tn = (bid % span) / gsz;
+  m0 = tm * BM;
+  n0 = tn * BN;
+  if (p.uplo == XKB_LOWER && (long)(m0 + BM - 1) + p.diag < (long)n0) return false;
+  if (p.uplo == XKB_UPPER && (long)m0 + p.diag > (long)(n0 + BN - 1)) return false;
+  return true;
+}
+
+// Register layout of a consumer warp's accumulators (2 x 4 warps).
+template <class T, int BM, int BN>
+struct AccShape {
+  static constexpr int WTM = BM / 2, WTN = BN / 4;
+  static constexpr int MF = WTM / 16, NF = WTN / 8;
+  static constexpr int NACC = St<T>::CPLX ? 8 : 4;
+  static constexpr int NREG = MF * NF * NACC;
+};
+
+// alpha/beta, mask, Hermitian diagonal, store of one thread's accumulators.
+template <class T, int BM, int BN>
+__device__ __forceinline__ void dmma_epilogue(const GemmParams& p, int m0, int n0,
+                                              const double* acc) {
+  using S = typename St<T>::S;
+  using A = AccShape<T, BM, BN>;
+  constexpr bool CPLX = St<T>::CPLX;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int wm = warp >> 2, wn = warp & 3;
+  const int g = lane >> 2, t = lane & 3;
+  S* C = reinterpret_cast<S*>(p.C);
+  const bool use_beta = (p.br != 0.0) || (p.bi != 0.0);
+#pragma unroll
+  for (int mf = 0; mf < A::MF; ++mf)
+#pragma unroll
+    for (int nf = 0; nf < A::NF; ++nf)
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const double* a = acc + (mf * A::NF + nf) * A::NACC;
+        const int row = m0 + wm * A::WTM + mf * 16 + g + ((i >> 1) << 3);
+        const int col = n0 + wn * A::WTN + nf * 8 + 2 * t + (i & 1);
+        if (row >= p.M || col >= p.N || !in_mask(p.uplo, p.diag, row, col)) continue;
+        const size_t idx = (size_t)row + (size_t)col * (size_t)p.ldc;
+        if constexpr (CPLX) {
+          const double xr = a[i], xi = a[4 + i];
+          double vr = p.ar * xr - p.ai * xi;
+          double vi = p.ar * xi + p.ai * xr;
+          if (use_beta) {
+            const double cr = (double)C[2 * idx], ci = (double)C[2 * idx + 1];
+            vr += p.br * cr - p.bi * ci;
+            vi += p.br * ci + p.bi * cr;
+          }
+          if (p.herm_diag && (long)row + p.diag == (long)col) vi = 0.0;
+          C[2 * idx] = static_cast<S>(vr);
+          C[2 * idx + 1] = static_cast<S>(vi);
+        } else {
+          double v = p.ar * a[i];
+          if (use_beta) v = fma(p.br, (double)C[idx], v);
+          C[idx] = static_cast<S>(v);
+        }
+      }
+}
 
 constexpr int kBK = 16;      // k extent of one pipeline stage
 constexpr int kStages = 4;
@@ -74,18 +149,11 @@ __global__ void __launch_bounds__(kThreads, 1)
   uint64_t* full = reinterpret_cast<uint64_t*>(base + kStages * STAGE_BYTES);
   uint64_t* empty = full + kStages;
 
-  // grouped rasterisation: 8 tile rows share a band of B columns in L2
-  const int GROUP = 8;
-  const int span = GROUP * p.tiles_n;
-  const int bid = blockIdx.x;
-  const int first_m = (bid / span) * GROUP;
-  const int gsz = min(p.tiles_m - first_m, GROUP);
-  const int tm = first_m + (bid % span) % gsz;
-  const int tn = (bid % span) / gsz;
-  const int m0 = tm * BM, n0 = tn * BN;
-
-  if (p.uplo == XKB_LOWER && (long)(m0 + BM - 1) + p.diag < (long)n0) return;
-  if (p.uplo == XKB_UPPER && (long)m0 + p.diag > (long)(n0 + BN - 1)) return;
+  const int ntiles = p.tiles_m * p.tiles_n;
+  const int slice = (int)blockIdx.x / ntiles;  // 0 unless split-K
+  const int bid = (int)blockIdx.x - slice * ntiles;
+  int m0, n0;
+  if (!dmma_tile<BM, BN>(p, bid, m0, n0)) return;
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
@@ -97,7 +165,9 @@ __global__ void __launch_bounds__(kThreads, 1)
   }
   __syncthreads();
 
-  const int KT = p.ktiles;
+  // this CTA's k-tiles: [kt0, kt0 + KT)
+  const int kt0 = slice * p.kt_slice;
+  const int KT = p.ksplit > 1 ? max(0, min(p.ktiles - kt0, p.kt_slice)) : p.ktiles;
   // Thread 0 also drives the TMA ring: it fills every stage up front and
   // refills stage s once all eight warps have released it.
   auto issue = [&](int it) {
@@ -105,7 +175,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     uint8_t* sa = base + s * STAGE_BYTES;
     uint8_t* sb = sa + A_BYTES;
     mbar_expect_tx(&full[s], STAGE_BYTES);
-    const int k0 = it * kBK;
+    const int k0 = (kt0 + it) * kBK;
     if (A_KC) tma_load_2d(sa, &tmA, k0 * W, m0, &full[s]);
     else tma_load_2d(sa, &tmA, m0 * W, k0, &full[s]);
     if (B_KC) tma_load_2d(sb, &tmB, k0 * W, n0, &full[s]);
@@ -213,38 +283,40 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
   }
   if (!ok) return;
+  const double* accp = &acc[0][0][0];
+  if (p.ksplit > 1) {
+    // raw partial sums of this slice, register-major: for each register the
+    // block's threads write consecutive doubles (coalesced)
+    constexpr int NREG = AccShape<T, BM, BN>::NREG;
+    double* w = p.ws + ((size_t)slice * ntiles + bid) * (size_t)(NREG * kThreads) + threadIdx.x;
+#pragma unroll
+    for (int r = 0; r < NREG; ++r) w[(size_t)r * kThreads] = accp[r];
+    return;
+  }
+  dmma_epilogue<T, BM, BN>(p, m0, n0, accp);
+}
 
-  // ---------------- epilogue: alpha/beta, mask, store ----------------------
-  S* C = reinterpret_cast<S*>(p.C);
-  const bool use_beta = (p.br != 0.0) || (p.bi != 0.0);
+// Split-K reduction: one block per C tile, the GEMM kernel's thread-to-element
+// map; the slices are summed in slice order (deterministic), then the
+// epilogue runs as in the unsplit kernel.
+template <class T, int BM, int BN>
+__global__ void __launch_bounds__(kThreads) k_gemm_splitk(const GemmParams p) {
+  if (p.run_if && *p.run_if == 0) return;
+  constexpr int NREG = AccShape<T, BM, BN>::NREG;
+  const int ntiles = p.tiles_m * p.tiles_n;
+  const int bid = blockIdx.x;
+  int m0, n0;
+  if (!dmma_tile<BM, BN>(p, bid, m0, n0)) return;
+  double acc[NREG];
 #pragma unroll
-  for (int mf = 0; mf < MF; ++mf)
+  for (int r = 0; r < NREG; ++r) acc[r] = 0.0;
+  for (int sl = 0; sl < p.ksplit; ++sl) {
+    const double* w =
+        p.ws + ((size_t)sl * ntiles + bid) * (size_t)(NREG * kThreads) + threadIdx.x;
 #pragma unroll
-    for (int nf = 0; nf < NF; ++nf)
-#pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        const int row = m0 + wm * WTM + mf * 16 + g + ((i >> 1) << 3);
-        const int col = n0 + wn * WTN + nf * 8 + 2 * t + (i & 1);
-        if (row >= p.M || col >= p.N || !in_mask(p.uplo, p.diag, row, col)) continue;
-        const size_t idx = (size_t)row + (size_t)col * (size_t)p.ldc;
-        if constexpr (CPLX) {
-          const double xr = acc[mf][nf][i], xi = acc[mf][nf][4 + i];
-          double vr = p.ar * xr - p.ai * xi;
-          double vi = p.ar * xi + p.ai * xr;
-          if (use_beta) {
-            const double cr = (double)C[2 * idx], ci = (double)C[2 * idx + 1];
-            vr += p.br * cr - p.bi * ci;
-            vi += p.br * ci + p.bi * cr;
-          }
-          if (p.herm_diag && (long)row + p.diag == (long)col) vi = 0.0;
-          C[2 * idx] = static_cast<S>(vr);
-          C[2 * idx + 1] = static_cast<S>(vi);
-        } else {
-          double v = p.ar * acc[mf][nf][i];
-          if (use_beta) v = fma(p.br, (double)C[idx], v);
-          C[idx] = static_cast<S>(v);
-        }
-      }
+    for (int r = 0; r < NREG; ++r) acc[r] += w[(size_t)r * kThreads];
+  }
+  dmma_epilogue<T, BM, BN>(p, m0, n0, acc);
 }
 
 // C <- beta*C on the masked part (beta == 0 writes zeros without reading).
@@ -278,7 +350,7 @@ __global__ void k_scale(int M, int N, double br, double bi, T* Cv, long ldc, int
 // ---------------------------------------------------------------------------
 // host side
 template <class T, int BM, int BN, bool A_KC, bool B_KC>
-static int launch_dmma(const xkb_gemm_args* a, cudaStream_t st, const int* run_if) {
+static int launch_dmma(const xkb_gemm_args* a, cudaStream_t st, const int* run_if, int ksplit) {
   using S = typename St<T>::S;
   constexpr int W = St<T>::W;
   const int es = (int)sizeof(S);
@@ -311,6 +383,10 @@ static int launch_dmma(const xkb_gemm_args* a, cudaStream_t st, const int* run_i
   p.tiles_n = (a->N + BN - 1) / BN;
   p.ktiles = (a->K + kBK - 1) / kBK;
   p.run_if = run_if;
+  p.ksplit = std::max(1, ksplit);
+  p.kt_slice = (p.ktiles + p.ksplit - 1) / p.ksplit;
+  p.ksplit = (p.ktiles + p.kt_slice - 1) / p.kt_slice;  // no empty slice
+  p.ws = nullptr;
   const size_t smem = kStages * (size_t)(BM + BN) * kBK * sizeof(T) + 2 * kStages * 8 + 128;
   auto kern = k_gemm_dmma<T, BM, BN, A_KC, B_KC>;
   static bool attr_done = false;  // one per instantiation
@@ -320,21 +396,55 @@ static int launch_dmma(const xkb_gemm_args* a, cudaStream_t st, const int* run_i
       return XKB_ECUDA;
     attr_done = true;
   }
-  const long grid = (long)p.tiles_m * p.tiles_n;
-  const long long tv = evlog_kern_begin(st, "k_gemm_dmma");
-  kern<<<(unsigned)grid, kThreads, smem, st>>>(tA, tB, p);
+  const long ntiles = (long)p.tiles_m * p.tiles_n;
+  if (p.ksplit > 1) {
+    const size_t ws = (size_t)p.ksplit * ntiles * AccShape<T, BM, BN>::NREG * kThreads * 8;
+    if (cudaMallocAsync(reinterpret_cast<void**>(&p.ws), ws, st) != cudaSuccess) {
+      cudaGetLastError();
+      return XKB_ENOMEM;
+    }
+  }
+  const long long tv = evlog_kern_begin(st, p.ksplit > 1 ? "k_gemm_dmma+k_gemm_splitk"
+                                                         : "k_gemm_dmma");
+  kern<<<(unsigned)(ntiles * p.ksplit), kThreads, smem, st>>>(tA, tB, p);
+  if (p.ksplit > 1) {
+    k_gemm_splitk<T, BM, BN><<<(unsigned)ntiles, kThreads, 0, st>>>(p);
+    cudaFreeAsync(p.ws, st);
+  }
   evlog_kern_end(tv, st);
-  count_launch();
+  count_launch(p.ksplit > 1 ? 2 : 1);
   return cudaPeekAtLastError() == cudaSuccess ? XKB_OK : XKB_ECUDA;
 }
 
 template <class T, int BM, int BN>
-static int dispatch_ops(const xkb_gemm_args* a, cudaStream_t st, const int* run_if) {
+static int dispatch_ops(const xkb_gemm_args* a, cudaStream_t st, const int* run_if,
+                        int ksplit = 1) {
   const bool akc = a->opA != XKB_OP_N, bkc = a->opB == XKB_OP_N;
-  if (akc && bkc) return launch_dmma<T, BM, BN, true, true>(a, st, run_if);
-  if (akc && !bkc) return launch_dmma<T, BM, BN, true, false>(a, st, run_if);
-  if (!akc && bkc) return launch_dmma<T, BM, BN, false, true>(a, st, run_if);
-  return launch_dmma<T, BM, BN, false, false>(a, st, run_if);
+  if (akc && bkc) return launch_dmma<T, BM, BN, true, true>(a, st, run_if, ksplit);
+  if (akc && !bkc) return launch_dmma<T, BM, BN, true, false>(a, st, run_if, ksplit);
+  if (!akc && bkc) return launch_dmma<T, BM, BN, false, true>(a, st, run_if, ksplit);
+  return launch_dmma<T, BM, BN, false, false>(a, st, run_if, ksplit);
+}
+
+// Split-K factor for big tiles when they alone leave SMs idle: as many
+// slices as keep tiles x slices within one wave, each slice at least
+// gemm_splitk_min_kt k-tiles (tuning key, default 16 = K 256); 1 = no split.
+// Taken when even the small tiles cannot fill the SMs, or when every slice
+// still runs gemm_splitk_long_kt k-tiles (default 64 = K 1024): measured on a
+// B200, split-K 2 over 128x128 tiles beat the 64x64 tiles by 2.2x at
+// 512x512x4096, 1.10x at 768x768x1536 and 1.21x at 2048x512x2048, but lost
+// 4 % at 1024^3 (32 k-tiles per slice).
+static int splitk_factor(long tiles_big, long tiles_small, long ktiles) {
+  const double on = tune("gemm_splitk", 1.0);
+  if (on == 0.0 || tiles_big <= 0) return 1;
+  const long sms = sm_count();
+  const long min_kt = std::max(4L, (long)tune("gemm_splitk_min_kt", 16.0));
+  long s = sms / tiles_big;
+  s = std::min(s, ktiles / min_kt);
+  s = std::max(1L, std::min(s, 32L));
+  if (s > 1 && tiles_small >= sms && ktiles / s < (long)tune("gemm_splitk_long_kt", 64.0))
+    return 1;
+  return (int)s;
 }
 
 template <class T>
@@ -349,6 +459,11 @@ static int dispatch_type(const xkb_gemm_args* a, cudaStream_t st, const int* run
   const bool big = force ? (force[0] == 'b')
                          : (tiles_big >= (long)tune("gemm_big_min_tiles", (double)sm_count()));
   if (big) return dispatch_ops<T, BMb, BNb>(a, st, run_if);
+  // too few big tiles for the SMs: split their k range when K allows
+  const long tiles_small =
+      (long)((a->M + BMb / 2 - 1) / (BMb / 2)) * ((a->N + BNb / 2 - 1) / (BNb / 2));
+  const int ks = force ? 1 : splitk_factor(tiles_big, tiles_small, (a->K + kBK - 1) / kBK);
+  if (ks > 1) return dispatch_ops<T, BMb, BNb>(a, st, run_if, ks);
   return dispatch_ops<T, BMb / 2, BNb / 2>(a, st, run_if);
 }
 

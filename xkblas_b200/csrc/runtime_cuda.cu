@@ -2,6 +2,7 @@
 // through the driver entry point (no link-time libcuda dependency, so the
 // library loads on machines without a GPU driver), stream resolution,
 // launch accounting and the device error word readers.
+#include <algorithm>
 #include <atomic>
 #include <cstdio>
 #include <cstdlib>
@@ -84,9 +85,9 @@ cudaStream_t resolve_stream(void* s) {
 void count_launch(int n) { g_launches.fetch_add((uint64_t)n, std::memory_order_relaxed); }
 
 const SideStream& side_stream(int slot) {
-  static SideStream ss[2];
-  static std::once_flag once[2];
-  slot = slot ? 1 : 0;
+  static SideStream ss[kSideStreams];
+  static std::once_flag once[kSideStreams];
+  slot = std::max(0, std::min(kSideStreams - 1, slot));
   std::call_once(once[slot], [slot] {
     SideStream t;
     if (cudaStreamCreateWithFlags(&t.s, cudaStreamNonBlocking) != cudaSuccess ||

@@ -607,24 +607,38 @@ int trsm_entry(int dtype, int side, int uplo, int trans, int diag, int M, int N,
   }
   c.fwd = c.lower_eff;
   const long n = c.left ? M : N;
-  // Many right-hand sides: two independent halves, the second on a side
-  // stream, so that one half's latency-bound diagonal-block solves overlap
-  // the other half's coupling GEMMs.  Halves are multiples of 64.  In the
-  // Ozaki form each half converts the coupling blocks of A again, which pays
-  // only with more right-hand sides than unknowns.
+  // Many right-hand sides: G independent groups (tuning key
+  // trsm_rhs_groups, default 2; groups of >= 1024 right-hand sides, multiples
+  // of 64), the first on the caller's stream and the others on side
+  // streams, so that one group's latency-bound diagonal-block solves overlap
+  // the other groups' coupling GEMMs.  In the Ozaki form each group converts
+  // the coupling blocks of A again, which pays only with more right-hand
+  // sides than unknowns.
   constexpr long kSplitRhs = 2048;
-  if (split_rhs && c.nrhs >= kSplitRhs && (c.ozaki == 0 || c.nrhs > n)) {
-    const long h = (c.nrhs / 2 + 63) / 64 * 64;
-    TrsmCtx c2 = c;
-    c2.nrhs = c.nrhs - h;
-    c2.B = c.B + (c.left ? h * ldb : h) * (long)c.es;
-    c.nrhs = h;
-    const SideStream& ss = side_stream(1);
-    c2.st = side_fork(ss, c.st);
-    int e = solve(c, 0, n, alpha);
-    const int e2 = solve(c2, 0, n, alpha);
-    if (!side_join(ss, c2.st, c.st) && !e) e = XKB_ECUDA;
-    return e ? e : e2;
+  const long groups = std::min<long>(std::max(1.0, tune("trsm_rhs_groups", 2.0)),
+                                     std::min<long>(4, c.nrhs / (kSplitRhs / 2)));
+  if (split_rhs && c.nrhs >= kSplitRhs && groups >= 2 && (c.ozaki == 0 || c.nrhs > n)) {
+    const long per = (c.nrhs / groups + 63) / 64 * 64;
+    TrsmCtx parts[4];
+    cudaStream_t forked[4];
+    long start = 0;
+    int np = 0;
+    for (long g = 0; g < groups && start < c.nrhs; ++g, ++np) {
+      parts[g] = c;
+      parts[g].nrhs = g == groups - 1 ? c.nrhs - start : std::min(per, c.nrhs - start);
+      parts[g].B = c.B + (c.left ? start * ldb : start) * (long)c.es;
+      forked[g] = g == 0 ? c.st : side_fork(side_stream(g), c.st);
+      parts[g].st = forked[g];
+      start += parts[g].nrhs;
+    }
+    int e = XKB_OK;
+    for (int g = 0; g < np; ++g) {
+      const int eg = solve(parts[g], 0, n, alpha);
+      if (!e) e = eg;
+    }
+    for (int g = 1; g < np; ++g)
+      if (!side_join(side_stream(g), forked[g], c.st) && !e) e = XKB_ECUDA;
+    return e;
   }
   return solve(c, 0, n, alpha);
 }

@@ -137,8 +137,10 @@ void trace_mark(int slot, int k, cudaStream_t st);
 void count_launch(int n = 1);
 // A lazily created non-blocking stream with a fork and a join event, for
 // work that is independent of what the caller's stream runs meanwhile
-// (slot 0: the LU's column-panel solves, slot 1: the TRSM's second half of
-// the right-hand sides).  s is nullptr if CUDA could not create it.
+// (slot 0: the LU's column-panel solves, slots 1-3: the TRSM's groups of
+// right-hand sides after the first).  s is nullptr if CUDA could not create
+// it.
+constexpr int kSideStreams = 4;
 struct SideStream {
   cudaStream_t s = nullptr;
   cudaEvent_t fork = nullptr, join = nullptr;
