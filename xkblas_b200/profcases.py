@@ -1,10 +1,15 @@
 """Small, self-contained cases for profiling single kernels with ncu:
 
-    python -m xkblas_b200.profcases dmma|ozaki|ozaki2|repack|trsm|potrf|getrf|batch|copy
+    python -m xkblas_b200.profcases dmma|ozaki|ozaki2|ozaki8192|splitk|repack|trsm|potrf|getrf|batch|copy
 
 dmma    DGEMM NN 4096^3 through xkb_cuda_gemm (k_gemm_dmma), two calls
 ozaki   the same through xkb_cuda_ozaki_gemm, 16 moduli (k_oz_* kernels)
 ozaki2  the same with the CTA-pair INT8 kernel (tuning key oz_2cta = 1, k_oz_gemm2)
+ozaki8192  DGEMM NN 8192^3, xkb_cuda_ozaki_gemm with the count chosen on the
+        device (nmod = 0: 15 moduli on these inputs), two calls: the DRAM
+        traffic of k_oz_gemm at a size whose residue planes exceed L2
+splitk  DGEMM NN 512 x 512 x 4096 through xkb_cuda_gemm: 16 output tiles,
+        split-K (k_gemm_dmma slices + k_gemm_splitk)
 repack  the DGEMM with lda = ldb = 4097 (k_repack, then k_gemm_dmma)
 trsm    DTRSM L/L/N/N 4096 x 4096, diagonally dominant (k_trsm_block, GEMMs)
 potrf   DPOTRF lower 4096 (k_potrf_block, k_trsm_block, GEMMs)
@@ -43,7 +48,17 @@ def main(case):
     keep = []
     if case == "ozaki2":
         lib.xkb_tune_set(b"oz_2cta", 1.0)
-    if case in ("dmma", "ozaki", "ozaki2", "repack"):
+    if case in ("ozaki8192", "splitk"):
+        m, n, k = (8192, 8192, 8192) if case == "ozaki8192" else (512, 512, 4096)
+        A, B, C = rnd(m, k), rnd(k, n), rnd(m, n)
+        keep += [A, B, C]
+        ga = _GemmArgs(1, 0, 0, m, n, k, A.data_ptr(), m, B.data_ptr(), k, C.data_ptr(), m)
+        ga.alpha[0] = 1.0
+        for _ in range(2):
+            rc = (lib.xkb_cuda_ozaki_gemm(ctypes.byref(ga), 0, sp) if case == "ozaki8192"
+                  else lib.xkb_cuda_gemm(ctypes.byref(ga), sp))
+            assert rc == 0, rc
+    elif case in ("dmma", "ozaki", "ozaki2", "repack"):
         n = 4096
         ld = n + 1 if case == "repack" else n
         A, B, C = rnd(ld, n), rnd(ld, n), rnd(n, n)
