@@ -75,10 +75,11 @@ struct AccShape {
   static constexpr int NREG = MF * NF * NACC;
 };
 
-// alpha/beta, mask, Hermitian diagonal, store of one thread's accumulators.
+// alpha/beta, mask, Hermitian diagonal, store of the fragment (mf, nf) of
+// one thread's accumulators (a: its NACC registers).
 template <class T, int BM, int BN>
-__device__ __forceinline__ void dmma_epilogue(const GemmParams& p, int m0, int n0,
-                                              const double* acc) {
+__device__ __forceinline__ void dmma_store_frag(const GemmParams& p, int m0, int n0, int mf,
+                                                int nf, const double* a) {
   using S = typename St<T>::S;
   using A = AccShape<T, BM, BN>;
   constexpr bool CPLX = St<T>::CPLX;
@@ -88,34 +89,41 @@ __device__ __forceinline__ void dmma_epilogue(const GemmParams& p, int m0, int n
   S* C = reinterpret_cast<S*>(p.C);
   const bool use_beta = (p.br != 0.0) || (p.bi != 0.0);
 #pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int row = m0 + wm * A::WTM + mf * 16 + g + ((i >> 1) << 3);
+    const int col = n0 + wn * A::WTN + nf * 8 + 2 * t + (i & 1);
+    if (row >= p.M || col >= p.N || !in_mask(p.uplo, p.diag, row, col)) continue;
+    const size_t idx = (size_t)row + (size_t)col * (size_t)p.ldc;
+    if constexpr (CPLX) {
+      const double xr = a[i], xi = a[4 + i];
+      double vr = p.ar * xr - p.ai * xi;
+      double vi = p.ar * xi + p.ai * xr;
+      if (use_beta) {
+        const double cr = (double)C[2 * idx], ci = (double)C[2 * idx + 1];
+        vr += p.br * cr - p.bi * ci;
+        vi += p.br * ci + p.bi * cr;
+      }
+      if (p.herm_diag && (long)row + p.diag == (long)col) vi = 0.0;
+      C[2 * idx] = static_cast<S>(vr);
+      C[2 * idx + 1] = static_cast<S>(vi);
+    } else {
+      double v = p.ar * a[i];
+      if (use_beta) v = fma(p.br, (double)C[idx], v);
+      C[idx] = static_cast<S>(v);
+    }
+  }
+}
+
+// alpha/beta, mask, Hermitian diagonal, store of one thread's accumulators.
+template <class T, int BM, int BN>
+__device__ __forceinline__ void dmma_epilogue(const GemmParams& p, int m0, int n0,
+                                              const double* acc) {
+  using A = AccShape<T, BM, BN>;
+#pragma unroll
   for (int mf = 0; mf < A::MF; ++mf)
 #pragma unroll
     for (int nf = 0; nf < A::NF; ++nf)
-#pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        const double* a = acc + (mf * A::NF + nf) * A::NACC;
-        const int row = m0 + wm * A::WTM + mf * 16 + g + ((i >> 1) << 3);
-        const int col = n0 + wn * A::WTN + nf * 8 + 2 * t + (i & 1);
-        if (row >= p.M || col >= p.N || !in_mask(p.uplo, p.diag, row, col)) continue;
-        const size_t idx = (size_t)row + (size_t)col * (size_t)p.ldc;
-        if constexpr (CPLX) {
-          const double xr = a[i], xi = a[4 + i];
-          double vr = p.ar * xr - p.ai * xi;
-          double vi = p.ar * xi + p.ai * xr;
-          if (use_beta) {
-            const double cr = (double)C[2 * idx], ci = (double)C[2 * idx + 1];
-            vr += p.br * cr - p.bi * ci;
-            vi += p.br * ci + p.bi * cr;
-          }
-          if (p.herm_diag && (long)row + p.diag == (long)col) vi = 0.0;
-          C[2 * idx] = static_cast<S>(vr);
-          C[2 * idx + 1] = static_cast<S>(vi);
-        } else {
-          double v = p.ar * a[i];
-          if (use_beta) v = fma(p.br, (double)C[idx], v);
-          C[idx] = static_cast<S>(v);
-        }
-      }
+      dmma_store_frag<T, BM, BN>(p, m0, n0, mf, nf, acc + (mf * A::NF + nf) * A::NACC);
 }
 
 constexpr int kBK = 16;      // k extent of one pipeline stage
@@ -296,27 +304,30 @@ __global__ void __launch_bounds__(kThreads, 1)
   dmma_epilogue<T, BM, BN>(p, m0, n0, accp);
 }
 
-// Split-K reduction: one block per C tile, the GEMM kernel's thread-to-element
-// map; the slices are summed in slice order (deterministic), then the
-// epilogue runs as in the unsplit kernel.
+// Split-K reduction: block (tile, fragment f) sums fragment f of the tile's
+// slices in slice order (deterministic) with the GEMM kernel's
+// thread-to-element map, then stores it as the unsplit epilogue does.  One
+// block per (tile, fragment) spreads the reads of the slices over many SMs.
 template <class T, int BM, int BN>
 __global__ void __launch_bounds__(kThreads) k_gemm_splitk(const GemmParams p) {
   if (p.run_if && *p.run_if == 0) return;
-  constexpr int NREG = AccShape<T, BM, BN>::NREG;
+  using A = AccShape<T, BM, BN>;
+  constexpr int NREG = A::NREG;
   const int ntiles = p.tiles_m * p.tiles_n;
   const int bid = blockIdx.x;
+  const int f = blockIdx.y;  // fragment (mf, nf) = (f / NF, f % NF)
   int m0, n0;
   if (!dmma_tile<BM, BN>(p, bid, m0, n0)) return;
-  double acc[NREG];
+  double acc[A::NACC];
 #pragma unroll
-  for (int r = 0; r < NREG; ++r) acc[r] = 0.0;
+  for (int v = 0; v < A::NACC; ++v) acc[v] = 0.0;
   for (int sl = 0; sl < p.ksplit; ++sl) {
-    const double* w =
-        p.ws + ((size_t)sl * ntiles + bid) * (size_t)(NREG * kThreads) + threadIdx.x;
+    const double* w = p.ws + ((size_t)sl * ntiles + bid) * (size_t)(NREG * kThreads) +
+                      (size_t)(f * A::NACC) * kThreads + threadIdx.x;
 #pragma unroll
-    for (int r = 0; r < NREG; ++r) acc[r] += w[(size_t)r * kThreads];
+    for (int v = 0; v < A::NACC; ++v) acc[v] += w[(size_t)v * kThreads];
   }
-  dmma_epilogue<T, BM, BN>(p, m0, n0, acc);
+  dmma_store_frag<T, BM, BN>(p, m0, n0, f / A::NF, f % A::NF, acc);
 }
 
 // C <- beta*C on the masked part (beta == 0 writes zeros without reading).
@@ -408,7 +419,8 @@ static int launch_dmma(const xkb_gemm_args* a, cudaStream_t st, const int* run_i
                                                          : "k_gemm_dmma");
   kern<<<(unsigned)(ntiles * p.ksplit), kThreads, smem, st>>>(tA, tB, p);
   if (p.ksplit > 1) {
-    k_gemm_splitk<T, BM, BN><<<(unsigned)ntiles, kThreads, 0, st>>>(p);
+    const dim3 rg((unsigned)ntiles, (unsigned)(AccShape<T, BM, BN>::MF * AccShape<T, BM, BN>::NF));
+    k_gemm_splitk<T, BM, BN><<<rg, kThreads, 0, st>>>(p);
     cudaFreeAsync(p.ws, st);
   }
   evlog_kern_end(tv, st);

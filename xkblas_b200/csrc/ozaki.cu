@@ -350,6 +350,34 @@ __global__ void k_oz_pick(const unsigned* rmax, OzSel* sel, const PickP q) {
 // 2. residues: planes[m][l][k] (int8, row stride Kpad) for l < Lpad, k < Kpad
 //    (zero padding), from X (L x K view, KC: k contiguous).  Complex operands
 //    (cplx = 1) are handled by the caller through the concatenated views.
+// Residue planes 1 .. min(CNT, n) - 1 of four consecutive elements whose
+// offset values a' = a + 2^62 have 32-bit halves lo, hi (plane 0 is written
+// by the caller).
+template <int CNT>
+__device__ __forceinline__ void res_planes(const Consts& c, const uint32_t (&lo)[4],
+                                           const uint32_t (&hi)[4], int8_t* dst, size_t plane,
+                                           int n) {
+#pragma unroll
+  for (int m = 1; m < CNT; ++m) {
+    if (m >= n) break;
+    const uint32_t p = (uint32_t)c.p[m];
+    uint32_t r[4];
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      // s = a' mod p + h (mod p) from the bytes of a': offh + sum_t byte_t
+      // (2^(8t) mod p) < 2^21; q = floor(s / p) exactly by the 32-bit
+      // reciprocal ceil(2^32 / p) (error s * 2^-32 < 1/p); s - q p - h is
+      // the symmetric residue in [-h, h]
+      uint32_t sacc = __dp4a(lo[v], c.wlo[m], c.offh[m]);
+      sacc = __dp4a(hi[v], c.whi[m], sacc);
+      const uint32_t q = __umulhi(sacc, c.magic[m]);
+      r[v] = sacc - q * p - (uint32_t)c.half[m];
+    }
+    *reinterpret_cast<uint32_t*>(dst + (size_t)m * plane) =
+        __byte_perm(__byte_perm(r[0], r[1], 0x0040), __byte_perm(r[2], r[3], 0x0040), 0x5410);
+  }
+}
+
 template <bool KC, int NM>
 __global__ void __launch_bounds__(256) k_oz_residues(int L, int K, const double* X, long ld,
                                                       long estride, long eoff, double esign,
@@ -406,25 +434,12 @@ __global__ void __launch_bounds__(256) k_oz_residues(int L, int K, const double*
     // p_0 = 256: the two's complement low byte (the offset 2^62 is 0 mod 256)
     *reinterpret_cast<uint32_t*>(dst) =
         __byte_perm(__byte_perm(lo[0], lo[1], 0x0040), __byte_perm(lo[2], lo[3], 0x0040), 0x5410);
-#pragma unroll
-    for (int m = 1; m < NM; ++m) {
-      if (m >= nm) break;
-      const uint32_t p = (uint32_t)c.p[m];
-      uint32_t r[4];
-#pragma unroll
-      for (int v = 0; v < 4; ++v) {
-        // s = a' mod p + h (mod p) from the bytes of a': offh + sum_t byte_t
-        // (2^(8t) mod p) < 2^21; q = floor(s / p) exactly by the 32-bit
-        // reciprocal ceil(2^32 / p) (error s * 2^-32 < 1/p); s - q p - h is
-        // the symmetric residue in [-h, h]
-        uint32_t sacc = __dp4a(lo[v], c.wlo[m], c.offh[m]);
-        sacc = __dp4a(hi[v], c.whi[m], sacc);
-        const uint32_t q = __umulhi(sacc, c.magic[m]);
-        r[v] = sacc - q * p - (uint32_t)c.half[m];
-      }
-      *reinterpret_cast<uint32_t*>(dst + (size_t)m * plane) =
-          __byte_perm(__byte_perm(r[0], r[1], 0x0040), __byte_perm(r[2], r[3], 0x0040), 0x5410);
-    }
+    // planes 1 .. nm-1, unrolled for the plan's largest count and the one
+    // below it (the data rule's two counts); other counts take a loop
+    if (nm == NM) res_planes<NM>(c, lo, hi, dst, plane, NM);
+    else if (NM > 2 && nm == NM - 1)
+      res_planes<(NM > 2 ? NM - 1 : NM)>(c, lo, hi, dst, plane, NM - 1);
+    else res_planes<NM>(c, lo, hi, dst, plane, nm);
   }
 }
 

@@ -288,50 +288,67 @@ __global__ void __launch_bounds__(kBlkThreads, 2)
     }
   }
 
+  // Each step: every warp forms Y^T = X_s^T inv(T_ss)^T itself -- one DMMA
+  // with M = the CTA's right-hand sides (16; complex 8, rows 8..15 zero),
+  // N = K = the 8 unknowns.  Its accumulator fragment is exactly the B
+  // fragment the rank-8 update needs: lane (g, t) holds Y(2t, c) and
+  // Y(2t+1, c) for c = g (registers 0, 1) and c = g + 8 (registers 2, 3).  So
+  // no warp waits for another between the solve and the update (one barrier
+  // per step).  Warp 0 writes the solved rows back into X after the next
+  // barrier, when no warp reads X_s any more.
+  double pyr[4] = {0.0, 0.0, 0.0, 0.0}, pyi[4] = {0.0, 0.0, 0.0, 0.0};
+  int pb = -1;  // unknowns of the step whose rows warp 0 still holds
+  auto store_y = [&]() {
+    const int k0 = 2 * t;
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      const int c = g + ((v >> 1) << 3), row = pb + k0 + (v & 1);
+      if (c < CW) {
+        Xr[c * XS + row] = pyr[v];
+        if (CP) Xi[c * XS + row] = pyi[v];
+      }
+    }
+  };
   for (int s = 0; s < nsub; ++s) {
     const int b = 8 * sub_of(s), r0 = LOWER ? b : 0;
     // strip s landed (strip s+1 may still be in flight); the barrier also
-    // ends the previous step's update (X, Y free) and the inverses
+    // ends the previous step (its update, its reads of X_s) and the inverses
     asm volatile("cp.async.wait_group 1;" ::: "memory");
     __syncthreads();
+    if (warp == 0 && pb >= 0) store_y();
     strip_issue(s + 2);  // into the buffer step s-1 read
-    // 1. Y = inv(T_ss) X(b..b+7): warp 0, one DMMA per 8 right-hand sides
-    // (rows 8..15 of the 16-row operand are zero)
-    if (warp == 0) {
+    // 1. Y^T = X_s^T inv(T_ss)^T in every warp (k indices 2t, 2t+1 for both
+    //    operands: the same permutation on A and B leaves the sum unchanged)
+    double yr[4] = {0.0, 0.0, 0.0, 0.0}, yi[4] = {0.0, 0.0, 0.0, 0.0};
+    {
       const int m = b / 8, k0 = 2 * t, k1 = k0 + 1;
       const double* vr = Vr + m * 64;
       const double* vi = Vi + m * 64;
-#pragma unroll
-      for (int nt = 0; nt < Sh::NT; ++nt) {
-        const int n0 = nt * 8;
-        const double a_r[4] = {vr[g * 8 + k0], 0.0, vr[g * 8 + k1], 0.0};
-        const double b_r[2] = {Xr[(n0 + g) * XS + b + k0], Xr[(n0 + g) * XS + b + k1]};
-        double yr[4] = {0.0, 0.0, 0.0, 0.0}, yi[4] = {0.0, 0.0, 0.0, 0.0};
-        if constexpr (CP) {
-          const double a_i[4] = {vi[g * 8 + k0], 0.0, vi[g * 8 + k1], 0.0};
-          const double a_ni[4] = {-a_i[0], 0.0, -a_i[2], 0.0};
-          const double b_i[2] = {Xi[(n0 + g) * XS + b + k0], Xi[(n0 + g) * XS + b + k1]};
-          dmma_k8(yr, a_r, b_r);
-          dmma_k8(yr, a_ni, b_i);
-          dmma_k8(yi, a_r, b_i);
-          dmma_k8(yi, a_i, b_r);
-        } else {
-          dmma_k8(yr, a_r, b_r);
-        }
-        // rows 0..7 of the result: (g, n0 + 2t + v)
-#pragma unroll
-        for (int v = 0; v < 2; ++v) {
-          const int c = n0 + 2 * t + v;
-          Yr[g * YW + c] = yr[v];
-          Xr[c * XS + b + g] = yr[v];
-          if (CP) {
-            Yi[g * YW + c] = yi[v];
-            Xi[c * XS + b + g] = yi[v];
-          }
-        }
+      const bool hi = CW > 8;  // right-hand sides g + 8 exist
+      const double a_r[4] = {Xr[g * XS + b + k0], hi ? Xr[(g + 8) * XS + b + k0] : 0.0,
+                             Xr[g * XS + b + k1], hi ? Xr[(g + 8) * XS + b + k1] : 0.0};
+      const double b_r[2] = {vr[g * 8 + k0], vr[g * 8 + k1]};
+      if constexpr (CP) {
+        const double a_i[4] = {Xi[g * XS + b + k0], hi ? Xi[(g + 8) * XS + b + k0] : 0.0,
+                               Xi[g * XS + b + k1], hi ? Xi[(g + 8) * XS + b + k1] : 0.0};
+        const double a_ni[4] = {-a_i[0], -a_i[1], -a_i[2], -a_i[3]};
+        const double b_i[2] = {vi[g * 8 + k0], vi[g * 8 + k1]};
+        dmma_k8(yr, a_r, b_r);
+        dmma_k8(yr, a_ni, b_i);
+        dmma_k8(yi, a_r, b_i);
+        dmma_k8(yi, a_i, b_r);
+      } else {
+        dmma_k8(yr, a_r, b_r);
       }
     }
-    __syncthreads();
+    if (warp == 0) {
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        pyr[v] = yr[v];
+        pyi[v] = yi[v];
+      }
+      pb = b;
+    }
     // 2. rows still to solve -= T(rows, b..b+7) Y: 16 x 8 DMMA tiles
     const S* str = strip_buf(s % Sh::NBUF);
     const S* sti = str + 8 * SRL;
@@ -343,7 +360,7 @@ __global__ void __launch_bounds__(kBlkThreads, 2)
       const int k0 = 2 * t, k1 = k0 + 1;
       const double a_r[4] = {-(double)str[k0 * SRL + ra], -(double)str[k0 * SRL + rb],
                              -(double)str[k1 * SRL + ra], -(double)str[k1 * SRL + rb]};
-      const double b_r[2] = {Yr[k0 * YW + n0 + g], Yr[k1 * YW + n0 + g]};
+      const double b_r[2] = {n0 ? yr[2] : yr[0], n0 ? yr[3] : yr[1]};
       double cr[4], ci[4];
 #pragma unroll
       for (int v = 0; v < 4; ++v) {
@@ -357,7 +374,7 @@ __global__ void __launch_bounds__(kBlkThreads, 2)
         const double a_i[4] = {sg * (double)sti[k0 * SRL + ra], sg * (double)sti[k0 * SRL + rb],
                                sg * (double)sti[k1 * SRL + ra], sg * (double)sti[k1 * SRL + rb]};
         const double a_ni[4] = {-a_i[0], -a_i[1], -a_i[2], -a_i[3]};
-        const double b_i[2] = {Yi[k0 * YW + n0 + g], Yi[k1 * YW + n0 + g]};
+        const double b_i[2] = {n0 ? yi[2] : yi[0], n0 ? yi[3] : yi[1]};
         dmma_k8(cr, a_r, b_r);
         dmma_k8(cr, a_ni, b_i);
         dmma_k8(ci, a_r, b_i);
@@ -376,6 +393,8 @@ __global__ void __launch_bounds__(kBlkThreads, 2)
     }
   }
   asm volatile("cp.async.wait_group 0;" ::: "memory");
+  __syncthreads();
+  if (warp == 0 && pb >= 0) store_y();
   __syncthreads();
 
   // ---- store ----
