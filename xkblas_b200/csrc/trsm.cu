@@ -14,6 +14,7 @@
 // shared memory).  This keeps every flop except O(n * 256 * nrhs) inside
 // large GEMMs.
 #include <algorithm>
+#include <vector>
 
 #include "trsm_leaf.cuh"
 #include "xkb_dev.cuh"
@@ -112,15 +113,31 @@ __device__ __forceinline__ void cp_async_zfill(void* smem, const void* gmem, boo
                : "memory");
 }
 
+// leaves != nullptr: the inverses of several diagonal blocks at once, block
+// y of the grid inverting the block of leaves[2y + 1] unknowns at
+// (leaves[2y], leaves[2y]) into columns y kBlk .. of B (ld kBlk): the
+// right-hand sides are the identity's columns (B is only written).
 template <class T, bool LOWER>
 __global__ void __launch_bounds__(kBlkThreads, 2)
-    k_trsm_block(int nb, int nrhs, const typename St<T>::S* A, long lda, int swap, int conj,
-                 int unit, typename St<T>::S* B, long ldb, int rhs_rows, double ar, double ai) {
+    k_trsm_block(int nb_, int nrhs_, const typename St<T>::S* A_, long lda, int swap, int conj,
+                 int unit, typename St<T>::S* B_, long ldb, int rhs_rows, double ar, double ai,
+                 const int* leaves) {
   using Sh = BlkShape<T>;
   using S = typename St<T>::S;
   constexpr bool CP = Sh::CP;
   constexpr int CW = Sh::CW, XS = Sh::XS, YW = Sh::YW, SRL = Sh::SRL, PE = Sh::PE;
   constexpr int W = CP ? 2 : 1;
+  int nb = nb_, nrhs = nrhs_;
+  const S* A = A_;
+  S* B = B_;
+  const bool ident = leaves != nullptr;
+  if (ident) {
+    const int i0 = leaves[2 * blockIdx.y];
+    nb = nrhs = leaves[2 * blockIdx.y + 1];
+    A = A_ + (size_t)W * ((size_t)i0 + (size_t)i0 * (size_t)lda);
+    B = B_ + (size_t)W * (size_t)blockIdx.y * (size_t)kBlk * (size_t)ldb;
+    if ((int)blockIdx.x * CW >= nb) return;  // the whole CTA is past this block's columns
+  }
   extern __shared__ double sm_blk[];
   double* Xr = sm_blk;  // X[c * XS + row]
   double* Xi = Xr + (CP ? CW * XS : 0);
@@ -182,9 +199,13 @@ __global__ void __launch_bounds__(kBlkThreads, 2)
         const int i = rhs_rows ? e / CW : e % nb, c = rhs_rows ? e % CW : e / nb;
         br[q] = bi[q] = 0.0;
         if (e < nb * CW && c < cols) {
-          const size_t idx = leaf_at(i, c0 + c, ldb, rhs_rows != 0);
-          br[q] = (double)__ldcg(B + W * idx);
-          if (CP) bi[q] = (double)__ldcg(B + 2 * idx + 1);
+          if (ident) {
+            br[q] = (i == c0 + c) ? 1.0 : 0.0;
+          } else {
+            const size_t idx = leaf_at(i, c0 + c, ldb, rhs_rows != 0);
+            br[q] = (double)__ldcg(B + W * idx);
+            if (CP) bi[q] = (double)__ldcg(B + 2 * idx + 1);
+          }
         }
       }
 #pragma unroll
@@ -470,10 +491,12 @@ static unsigned grid_for(size_t total, int per_block = 256) {
 template <class T>
 static int launch_block(int n, int nrhs, const void* A, long lda, int swap, int conj, int lower,
                         int unit, void* B, long ldb, int rhs_rows, const double* al,
-                        cudaStream_t st) {
+                        cudaStream_t st, const int* leaves = nullptr, int nleaves = 0) {
   using S = typename St<T>::S;
   using Sh = BlkShape<T>;
-  const unsigned grid = (unsigned)((nrhs + Sh::CW - 1) / Sh::CW);
+  const dim3 grid(leaves ? (unsigned)((kBlk + Sh::CW - 1) / Sh::CW)
+                         : (unsigned)((nrhs + Sh::CW - 1) / Sh::CW),
+                  leaves ? (unsigned)nleaves : 1u);
   auto kb = lower ? k_trsm_block<T, true> : k_trsm_block<T, false>;
   static bool attr[2] = {false, false};
   if (!attr[lower ? 1 : 0]) {
@@ -484,7 +507,8 @@ static int launch_block(int n, int nrhs, const void* A, long lda, int swap, int 
   }
   const long long tv = evlog_kern_begin(st, "k_trsm_block");
   kb<<<grid, kBlkThreads, Sh::SMEM, st>>>(n, nrhs, static_cast<const S*>(A), lda, swap, conj,
-                                          unit, static_cast<S*>(B), ldb, rhs_rows, al[0], al[1]);
+                                          unit, static_cast<S*>(B), ldb, rhs_rows, al[0], al[1],
+                                          leaves);
   evlog_kern_end(tv, st);
   count_launch();
   return cudaPeekAtLastError() == cudaSuccess ? XKB_OK : XKB_ECUDA;
@@ -511,7 +535,82 @@ struct TrsmCtx {
   int nrhs;
   cudaStream_t st;
   int swap, conj, lower_eff;
+  // inverse leaves (null: every leaf is a block solve): inv(E_l) of the
+  // effective triangle of leaf l at Winv + l kBlk^2 elements (ld kBlk),
+  // leaf l starting at unknown leaf_i0[l]; tmp holds one leaf's product
+  const char* Winv = nullptr;
+  const std::vector<int>* leaf_i0 = nullptr;
+  char* tmp = nullptr;
 };
+
+// Leaves of the recursion below (the same split points): [i0, i1) pairs.
+static void collect_leaves(long i0, long i1, std::vector<int>& out) {
+  const long n = i1 - i0;
+  if (n <= kBlk) {
+    out.push_back((int)i0);
+    out.push_back((int)n);
+    return;
+  }
+  long h = i0 + ((n / 2 + kSplit - 1) / kSplit) * kSplit;
+  if (h >= i1) h = i1 - kSplit;
+  collect_leaves(i0, h, out);
+  collect_leaves(h, i1, out);
+}
+
+// A leaf applied through its inverse: X = alpha inv(E) B (left) or
+// X = alpha B inv(E)^T (right side: E is op(A)^T there), one GEMM into tmp
+// and a copy back into B.
+static int leaf_gemm(const TrsmCtx& c, long i0, long n, const double* alpha) {
+  const auto& L = *c.leaf_i0;
+  long l = 0;
+  while (2 * l < (long)L.size() && L[2 * l] != i0) ++l;
+  if (2 * l >= (long)L.size()) return XKB_EINVAL;
+  xkb_gemm_args g{};
+  g.dtype = c.dt;
+  g.alpha[0] = alpha[0];
+  g.alpha[1] = alpha[1];
+  g.uplo = XKB_FULL;
+  const char* Wl = c.Winv + (size_t)l * kBlk * kBlk * c.es;
+  char* Bk = c.left ? c.B + i0 * (long)c.es : c.B + i0 * c.ldb * (long)c.es;
+  size_t dpitch, spitch, width, height;
+  if (c.left) {
+    g.M = (int)n;
+    g.N = c.nrhs;
+    g.K = (int)n;
+    g.opA = XKB_OP_N;
+    g.A = Wl;
+    g.lda = kBlk;
+    g.opB = XKB_OP_N;
+    g.B = Bk;
+    g.ldb = c.ldb;
+    g.C = c.tmp;
+    g.ldc = kBlk;
+    spitch = kBlk * (size_t)c.es;
+    width = n * (size_t)c.es;
+    height = (size_t)c.nrhs;
+  } else {
+    g.M = c.nrhs;
+    g.N = (int)n;
+    g.K = (int)n;
+    g.opA = XKB_OP_N;
+    g.A = Bk;
+    g.lda = c.ldb;
+    g.opB = XKB_OP_T;
+    g.B = Wl;
+    g.ldb = kBlk;
+    g.C = c.tmp;
+    g.ldc = c.nrhs;
+    spitch = (size_t)c.nrhs * c.es;
+    width = (size_t)c.nrhs * c.es;
+    height = (size_t)n;
+  }
+  dpitch = (size_t)c.ldb * c.es;
+  if (int e = xkb_cuda_gemm(&g, c.st)) return e;
+  return cudaMemcpy2DAsync(Bk, dpitch, c.tmp, spitch, width, height, cudaMemcpyDeviceToDevice,
+                           c.st) == cudaSuccess
+             ? XKB_OK
+             : XKB_ECUDA;
+}
 
 static const char* aptr(const TrsmCtx& c, long r, long col) {
   return c.A + (r + col * c.lda) * (long)c.es;
@@ -567,6 +666,7 @@ static int update(const TrsmCtx& c, long p0, long p1, long q0, long q1, const do
 static int solve(const TrsmCtx& c, long i0, long i1, const double* alpha) {
   const long n = i1 - i0;
   if (n <= kBlk) {
+    if (c.Winv) return leaf_gemm(c, i0, n, alpha);
     // diagonal block of the effective triangle: one launch
     const char* Ad = aptr(c, i0, i0);
     char* Bd = c.left ? c.B + i0 * (long)c.es : c.B + i0 * c.ldb * (long)c.es;
@@ -626,6 +726,64 @@ int trsm_entry(int dtype, int side, int uplo, int trans, int diag, int M, int N,
   }
   c.fwd = c.lower_eff;
   const long n = c.left ? M : N;
+  // Inverse leaves (tuning key trsm_inv_leaves, default 1; FP64 storage,
+  // more than one leaf, >= 64 right-hand sides): the inverses of all the
+  // recursion's diagonal blocks are formed first by ONE launch of the block
+  // kernel (a grid row per block, identity right-hand sides), and each leaf
+  // becomes a GEMM with its inverse -- the latency-bound substitution chains
+  // leave the recursion's critical path.  The products with inv(E_l) carry
+  // the condition number of the <= 256-unknown diagonal blocks, as blocked
+  // solvers with inverted diagonal blocks do.
+  std::vector<int> leaves;
+  void* Wbuf = nullptr;
+  int* dleaves = nullptr;
+  const bool inv = (dtype == XKB_D || dtype == XKB_Z) && n > kBlk && c.nrhs >= 64 &&
+                   tune("trsm_inv_leaves", 1.0) != 0.0;
+  if (inv) {
+    collect_leaves(0, n, leaves);
+    const int nl = (int)leaves.size() / 2;
+    if (cudaMallocAsync(&Wbuf, (size_t)nl * kBlk * kBlk * c.es, st) != cudaSuccess ||
+        cudaMallocAsync(reinterpret_cast<void**>(&dleaves), leaves.size() * sizeof(int), st) !=
+            cudaSuccess) {
+      cudaGetLastError();
+      if (Wbuf) cudaFreeAsync(Wbuf, st);
+      return XKB_ENOMEM;
+    }
+    // pageable source: staged before the call returns
+    cudaMemcpyAsync(dleaves, leaves.data(), leaves.size() * sizeof(int), cudaMemcpyHostToDevice,
+                    st);
+    const double one[2] = {1.0, 0.0};
+    int e = dtype == XKB_D
+                ? launch_block<double>(kBlk, kBlk, A, lda, c.swap, c.conj, c.lower_eff, c.unit,
+                                       Wbuf, kBlk, 0, one, st, dleaves, nl)
+                : launch_block<double2>(kBlk, kBlk, A, lda, c.swap, c.conj, c.lower_eff, c.unit,
+                                        Wbuf, kBlk, 0, one, st, dleaves, nl);
+    if (e) {
+      cudaFreeAsync(Wbuf, st);
+      cudaFreeAsync(dleaves, st);
+      return e;
+    }
+    c.Winv = static_cast<const char*>(Wbuf);
+    c.leaf_i0 = &leaves;
+  }
+  std::vector<void*> tmps;
+  auto give_tmp = [&](TrsmCtx& part) {
+    if (!inv) return XKB_OK;
+    void* t = nullptr;
+    if (cudaMallocAsync(&t, (size_t)kBlk * part.nrhs * c.es, st) != cudaSuccess) {
+      cudaGetLastError();
+      return XKB_ENOMEM;
+    }
+    tmps.push_back(t);
+    part.tmp = static_cast<char*>(t);
+    return XKB_OK;
+  };
+  auto release = [&](int e) {
+    for (void* t : tmps) cudaFreeAsync(t, st);
+    if (Wbuf) cudaFreeAsync(Wbuf, st);
+    if (dleaves) cudaFreeAsync(dleaves, st);
+    return e;
+  };
   // Many right-hand sides: G independent groups (tuning key
   // trsm_rhs_groups, default 2; groups of >= 1024 right-hand sides, multiples
   // of 64), the first on the caller's stream and the others on side
@@ -646,9 +804,12 @@ int trsm_entry(int dtype, int side, int uplo, int trans, int diag, int M, int N,
       parts[g] = c;
       parts[g].nrhs = g == groups - 1 ? c.nrhs - start : std::min(per, c.nrhs - start);
       parts[g].B = c.B + (c.left ? start * ldb : start) * (long)c.es;
+      if (int e = give_tmp(parts[g])) return release(e);
+      start += parts[g].nrhs;
+    }
+    for (int g = 0; g < np; ++g) {
       forked[g] = g == 0 ? c.st : side_fork(side_stream(g), c.st);
       parts[g].st = forked[g];
-      start += parts[g].nrhs;
     }
     int e = XKB_OK;
     for (int g = 0; g < np; ++g) {
@@ -657,9 +818,10 @@ int trsm_entry(int dtype, int side, int uplo, int trans, int diag, int M, int N,
     }
     for (int g = 1; g < np; ++g)
       if (!side_join(side_stream(g), forked[g], c.st) && !e) e = XKB_ECUDA;
-    return e;
+    return release(e);
   }
-  return solve(c, 0, n, alpha);
+  if (int e = give_tmp(c)) return release(e);
+  return release(solve(c, 0, n, alpha));
 }
 }  // namespace xkb
 
