@@ -112,3 +112,34 @@ def test_potrf_argument_codes(xk):
     assert lib.xkblas_dpotrf_async(LO, -1, xk._ptr(A), 4) == -5
     assert lib.xkblas_dpotrf_async(LO, 4, xk._ptr(A), 3) == -8
     assert lib.xkblas_dpotrf_async(LO, 0, xk._ptr(A), 1) == 0
+
+
+@pytest.mark.parametrize("dt", [np.float64, np.complex128])
+@pytest.mark.parametrize("uplo", [LO, UP])
+def test_potrf_blocked_and_recursive_forms(xk, dt, uplo):
+    """The blocked look-ahead form (tuning key potrf_blocked = 1, several
+    block widths, widths shrinking along the factorization, a ragged last
+    block) and the recursive form (= 0) meet the same backward-error bound,
+    and both report a bad pivot in a late block."""
+    lib = xk.lib()
+    n = 1100
+    up = np.complex128 if np.issubdtype(dt, np.complexfloating) else np.float64
+    try:
+        for mode, nb, shrink in ((1, 64, 8), (1, 128, 8), (1, 320, 8), (1, 512, 2), (0, 256, 8)):
+            lib.xkb_tune_set(b"potrf_blocked", float(mode))
+            lib.xkb_tune_set(b"potrf_nb", float(nb))
+            lib.xkb_tune_set(b"potrf_shrink", float(shrink))
+            A0 = _spd(n, dt, 40 + nb)
+            A = A0.copy(order="F")
+            assert _potrf(xk, A, uplo) == 0
+            F = np.tril(A).astype(up) if uplo == LO else np.triu(A).astype(up)
+            R = F @ F.conj().T if uplo == LO else F.conj().T @ F
+            scale = np.abs(A0).max() * n * EPS[dt]
+            assert np.abs(R - A0.astype(up)).max() <= 16 * scale, (mode, nb)
+            B = _spd(n, dt, 41 + nb)
+            B[776, 776] = -5.0
+            assert _potrf(xk, B, uplo) == 777, (mode, nb)
+    finally:
+        lib.xkb_tune_set(b"potrf_blocked", 1.0)
+        lib.xkb_tune_set(b"potrf_nb", 512.0)
+        lib.xkb_tune_set(b"potrf_shrink", 12.0)

@@ -75,55 +75,91 @@ struct AccShape {
   static constexpr int NREG = MF * NF * NACC;
 };
 
-// alpha/beta, mask, Hermitian diagonal, store of the fragment (mf, nf) of
-// one thread's accumulators (a: its NACC registers).
+// Element i (0..3) of fragment (mf, nf) of this thread: its row and column
+// of C; false if outside C or the triangle mask.
 template <class T, int BM, int BN>
-__device__ __forceinline__ void dmma_store_frag(const GemmParams& p, int m0, int n0, int mf,
-                                                int nf, const double* a) {
-  using S = typename St<T>::S;
+__device__ __forceinline__ bool dmma_elem(const GemmParams& p, int m0, int n0, int mf, int nf,
+                                          int i, int& row, int& col) {
   using A = AccShape<T, BM, BN>;
-  constexpr bool CPLX = St<T>::CPLX;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int wm = warp >> 2, wn = warp & 3;
   const int g = lane >> 2, t = lane & 3;
-  S* C = reinterpret_cast<S*>(p.C);
+  row = m0 + wm * A::WTM + mf * 16 + g + ((i >> 1) << 3);
+  col = n0 + wn * A::WTN + nf * 8 + 2 * t + (i & 1);
+  return row < p.M && col < p.N && in_mask(p.uplo, p.diag, row, col);
+}
+
+// The C values of fragment (mf, nf) that beta multiplies (cv[i], imaginary
+// parts at cv[4 + i]; 0 where nothing is stored).  The epilogue loads a
+// whole row of fragments before it stores any: C is read and written
+// through one pointer, so a load placed after a store could not be issued
+// before that store completes.
+template <class T, int BM, int BN>
+__device__ __forceinline__ void dmma_load_frag(const GemmParams& p, int m0, int n0, int mf,
+                                               int nf, double* cv) {
+  using S = typename St<T>::S;
+  constexpr bool CPLX = St<T>::CPLX;
+  const S* C = reinterpret_cast<const S*>(p.C);
   const bool use_beta = (p.br != 0.0) || (p.bi != 0.0);
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
-    const int row = m0 + wm * A::WTM + mf * 16 + g + ((i >> 1) << 3);
-    const int col = n0 + wn * A::WTN + nf * 8 + 2 * t + (i & 1);
-    if (row >= p.M || col >= p.N || !in_mask(p.uplo, p.diag, row, col)) continue;
+    int row, col;
+    cv[i] = 0.0;
+    if (CPLX) cv[4 + i] = 0.0;
+    if (!use_beta || !dmma_elem<T, BM, BN>(p, m0, n0, mf, nf, i, row, col)) continue;
+    const size_t idx = (size_t)row + (size_t)col * (size_t)p.ldc;
+    if constexpr (CPLX) {
+      cv[i] = (double)C[2 * idx];
+      cv[4 + i] = (double)C[2 * idx + 1];
+    } else {
+      cv[i] = (double)C[idx];
+    }
+  }
+}
+
+// alpha/beta, mask, Hermitian diagonal, store of the fragment (mf, nf) of
+// one thread's accumulators (a: its NACC registers; cv: from dmma_load_frag).
+template <class T, int BM, int BN>
+__device__ __forceinline__ void dmma_store_frag(const GemmParams& p, int m0, int n0, int mf,
+                                                int nf, const double* a, const double* cv) {
+  using S = typename St<T>::S;
+  constexpr bool CPLX = St<T>::CPLX;
+  S* C = reinterpret_cast<S*>(p.C);
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    int row, col;
+    if (!dmma_elem<T, BM, BN>(p, m0, n0, mf, nf, i, row, col)) continue;
     const size_t idx = (size_t)row + (size_t)col * (size_t)p.ldc;
     if constexpr (CPLX) {
       const double xr = a[i], xi = a[4 + i];
       double vr = p.ar * xr - p.ai * xi;
       double vi = p.ar * xi + p.ai * xr;
-      if (use_beta) {
-        const double cr = (double)C[2 * idx], ci = (double)C[2 * idx + 1];
-        vr += p.br * cr - p.bi * ci;
-        vi += p.br * ci + p.bi * cr;
-      }
+      vr += p.br * cv[i] - p.bi * cv[4 + i];
+      vi += p.br * cv[4 + i] + p.bi * cv[i];
       if (p.herm_diag && (long)row + p.diag == (long)col) vi = 0.0;
       C[2 * idx] = static_cast<S>(vr);
       C[2 * idx + 1] = static_cast<S>(vi);
     } else {
-      double v = p.ar * a[i];
-      if (use_beta) v = fma(p.br, (double)C[idx], v);
-      C[idx] = static_cast<S>(v);
+      C[idx] = static_cast<S>(fma(p.br, cv[i], p.ar * a[i]));
     }
   }
 }
 
-// alpha/beta, mask, Hermitian diagonal, store of one thread's accumulators.
+// alpha/beta, mask, Hermitian diagonal, store of one thread's accumulators,
+// one row of fragments at a time: all of the row's loads, then its stores.
 template <class T, int BM, int BN>
 __device__ __forceinline__ void dmma_epilogue(const GemmParams& p, int m0, int n0,
                                               const double* acc) {
   using A = AccShape<T, BM, BN>;
 #pragma unroll
-  for (int mf = 0; mf < A::MF; ++mf)
+  for (int mf = 0; mf < A::MF; ++mf) {
+    double cv[A::NF][A::NACC];
+#pragma unroll
+    for (int nf = 0; nf < A::NF; ++nf) dmma_load_frag<T, BM, BN>(p, m0, n0, mf, nf, cv[nf]);
 #pragma unroll
     for (int nf = 0; nf < A::NF; ++nf)
-      dmma_store_frag<T, BM, BN>(p, m0, n0, mf, nf, acc + (mf * A::NF + nf) * A::NACC);
+      dmma_store_frag<T, BM, BN>(p, m0, n0, mf, nf, acc + (mf * A::NF + nf) * A::NACC, cv[nf]);
+  }
 }
 
 constexpr int kBK = 16;      // k extent of one pipeline stage
@@ -327,7 +363,9 @@ __global__ void __launch_bounds__(kThreads) k_gemm_splitk(const GemmParams p) {
 #pragma unroll
     for (int v = 0; v < A::NACC; ++v) acc[v] += w[(size_t)v * kThreads];
   }
-  dmma_store_frag<T, BM, BN>(p, m0, n0, f / A::NF, f % A::NF, acc);
+  double cv[A::NACC];
+  dmma_load_frag<T, BM, BN>(p, m0, n0, f / A::NF, f % A::NF, cv);
+  dmma_store_frag<T, BM, BN>(p, m0, n0, f / A::NF, f % A::NF, acc, cv);
 }
 
 // C <- beta*C on the masked part (beta == 0 writes zeros without reading).

@@ -406,6 +406,136 @@ static int factor(const PotrfCtx& c, long i0, long i1, bool la, bool pend) {
   return factor(c, h, i1, la, s2 != c.st);
 }
 
+// Blocked right-looking Cholesky of rows / columns [i0, i1) with look-ahead,
+// in blocks of nb columns (a multiple of 64); lower storage described (upper
+// is its conjugate transpose).  Step k, with diagonal block D_k factored and
+// the panel below it split into P1 (the next block's nb rows) and P2 (the
+// rest):
+//   critical path (high-priority stream hp):  P1 = P1 D_k^-H, then
+//     D_{k+1} -= P1 P1^H, then factor D_{k+1}, then the next step's P1;
+//   beside it (high-priority stream hp2):     P2 = P2 D_k^-H, then the rest
+//     of block column k+1, B -= P2 P1^H (the next step's panel);
+//   trailing triangle (caller's stream):      T -= P2 P2^H, one
+//     triangle-masked GEMM.
+// The tile-level critical path of the reference's tile loop
+// (blas/zpotrf.c:46-220, potrf -> trsm -> syrk -> potrf per tile column),
+// with nb-wide tiles; the large updates run while the next diagonal block
+// is factored.  Dependencies between the streams are events: D_{k+1}'s
+// update and block column k+1's update wait for the previous trailing
+// update (it wrote both); the next P1 solve waits for block column k+1.
+// The block width shrinks as the factorization proceeds: while the trailing
+// triangle is large its update bounds each step and wider blocks make that
+// GEMM more efficient (larger K); near the end the critical path bounds each
+// step and narrower blocks shorten it.  Width for `m` remaining rows: nb,
+// halved (rounded down to a multiple of 64, at least nmin) while
+// m <= shrink * width (tuning key potrf_shrink, default 12).
+static long block_width(long m, long nb, long nmin) {
+  const double shrink = tune("potrf_shrink", 12.0);
+  long w = nb;
+  while (w > nmin && (double)m <= shrink * (double)w) w = std::max(nmin, (w / 2) / 64 * 64);
+  return w;
+}
+
+static int factor_blocked(const PotrfCtx& c, long i0, long i1, long nb) {
+  const SideStream& hp = side_stream(kHiStream);
+  const SideStream& hp2 = side_stream(kHiStream2);
+  cudaEvent_t* ev = dep_events();
+  if (!hp.s || !hp2.s || !ev) return factor(c, i0, i1, true, false);
+  cudaEvent_t e_diag = ev[0], e_p1 = ev[1], e_p2 = ev[2], e_col = ev[3], e_trail = ev[4];
+  const bool cplx = c.dt == XKB_C || c.dt == XKB_Z;
+  const int ctr = cplx ? XKB_OP_C : XKB_OP_T;
+  const double one[2] = {1.0, 0.0};
+  const long es = c.es, lda = c.lda;
+  auto at = [&](long i, long j) { return c.A + (i + j * lda) * es; };
+  // (rows r, cols q) of the lower-storage picture, mapped to the storage
+  auto blk = [&](long r, long q) { return c.upper ? at(q, r) : at(r, q); };
+  // solve rows [r, r + m) of the panel under block [b, b + nk)
+  auto solve = [&](long b, long nk, long r, long m, cudaStream_t st) {
+    return c.upper ? trsm_entry(c.dt, 0, XKB_UPPER, ctr, 0, (int)nk, (int)m, one, at(b, b), lda,
+                                blk(r, b), lda, 0, st, false)
+                   : trsm_entry(c.dt, 1, XKB_LOWER, ctr, 0, (int)m, (int)nk, one, at(b, b), lda,
+                                blk(r, b), lda, 0, st, false);
+  };
+  // C(rows [r, r + m), cols [q, q + w)) -= P(rows r..) P(rows q..)^H over the
+  // panel of block [b, b + nk); masked to the stored triangle when r == q
+  auto rank_update = [&](long b, long nk, long r, long m, long q, long w, cudaStream_t st,
+                         const PotrfCtx& cx) {
+    xkb_gemm_args g{};
+    g.dtype = c.dt;
+    g.alpha[0] = -1.0;
+    g.beta[0] = 1.0;
+    g.K = (int)nk;
+    g.herm_diag = (cplx && r == q) ? 1 : 0;  // a diagonal block: its diagonal is real
+    g.lda = g.ldb = g.ldc = lda;
+    if (!c.upper) {  // C = A(r.., q..) -= P_r P_q^H, P_x = A(x.., b..)
+      g.opA = XKB_OP_N;
+      g.opB = ctr;
+      g.M = (int)m;
+      g.N = (int)w;
+      g.A = at(r, b);
+      g.B = at(q, b);
+      g.C = at(r, q);
+      g.uplo = r == q ? XKB_LOWER : XKB_FULL;
+    } else {  // C = A(q.., r..) -= P_q^H P_r, P_x = A(b.., x..)
+      g.opA = ctr;
+      g.opB = XKB_OP_N;
+      g.M = (int)w;
+      g.N = (int)m;
+      g.A = at(b, q);
+      g.B = at(b, r);
+      g.C = at(q, r);
+      g.uplo = r == q ? XKB_UPPER : XKB_FULL;
+    }
+    return update(cx, g, st);
+  };
+  PotrfCtx ch = c;
+  ch.st = side_fork(hp, c.st);
+  int e = XKB_OK;
+  auto rec = [&](cudaEvent_t x, cudaStream_t st) {
+    if (!e && cudaEventRecord(x, st) != cudaSuccess) e = XKB_ECUDA;
+  };
+  auto wait = [&](cudaStream_t st, cudaEvent_t x) {
+    if (!e && cudaStreamWaitEvent(st, x, 0) != cudaSuccess) e = XKB_ECUDA;
+  };
+  rec(e_trail, c.st);  // "previous trailing update": the caller's work so far
+  const long nmin = cplx ? PoShape<double2>::NMAX : PoShape<double>::NMAX;
+  long b = i0, nk = std::min(block_width(i1 - i0, nb, nmin), i1 - i0);
+  e = factor(ch, b, b + nk, false, false);
+  rec(e_diag, ch.st);
+  while (!e && b + nk < i1) {
+    const long r0 = b + nk, m2 = i1 - r0;
+    const long n1 = std::min(block_width(m2, nb, nmin), m2), m3 = m2 - n1;  // next block; below it
+    if (m3 > 0) {  // hp2: P2 solve (needs D_k)
+      wait(hp2.s, e_diag);
+      if (!e) e = solve(b, nk, r0 + n1, m3, hp2.s);
+      rec(e_p2, hp2.s);
+    }
+    if (!e) e = solve(b, nk, r0, n1, ch.st);  // hp: P1 solve
+    rec(e_p1, ch.st);
+    if (m3 > 0) {  // hp2: block column k+1 below D_{k+1} (needs P1, previous trailing update)
+      wait(hp2.s, e_p1);
+      wait(hp2.s, e_trail);
+      if (!e) e = rank_update(b, nk, r0 + n1, m3, r0, n1, hp2.s, ch);
+      rec(e_col, hp2.s);
+    }
+    wait(ch.st, e_trail);  // hp: D_{k+1} update (previous trailing update wrote it)
+    if (!e) e = rank_update(b, nk, r0, n1, r0, n1, ch.st, ch);
+    if (m3 > 0) {  // caller's stream: trailing triangle (needs P2)
+      wait(c.st, e_p2);
+      if (!e) e = rank_update(b, nk, r0 + n1, m3, r0 + n1, m3, c.st, c);
+      rec(e_trail, c.st);
+    }
+    if (!e) e = factor(ch, r0, r0 + n1, false, false);  // hp: D_{k+1}
+    rec(e_diag, ch.st);
+    if (m3 > 0) wait(ch.st, e_col);  // the next P1 lies in block column k+1
+    b = r0;
+    nk = n1;
+  }
+  if (!side_join(hp2, hp2.s, c.st) && !e) e = XKB_ECUDA;
+  if (!side_join(hp, ch.st, c.st) && !e) e = XKB_ECUDA;
+  return e;
+}
+
 }  // namespace xkb
 
 using namespace xkb;
@@ -425,5 +555,15 @@ extern "C" int xkb_cuda_potrf(int dtype, int uplo, int N, void* A, long lda, int
   c.info = d_info;
   c.ozaki = (dtype == XKB_D || dtype == XKB_Z) ? std::max(ozaki, 0) : 0;
   c.st = resolve_stream(stream);
+  // Blocked look-ahead form (tuning key potrf_blocked: 0 off, 1 in plain
+  // mode, 2 in both modes; widest block potrf_nb, in tensor-op mode
+  // potrf_nb_oz) or the recursive form.
+  const long nmax = (dtype == XKB_C || dtype == XKB_Z) ? PoShape<double2>::NMAX
+                                                       : PoShape<double>::NMAX;
+  const int mode = (int)tune("potrf_blocked", 1.0);
+  const long nb = std::max(nmax, ((long)tune(c.ozaki ? "potrf_nb_oz" : "potrf_nb",
+                                             c.ozaki ? 2048.0 : 512.0) + 63) / 64 * 64);
+  if (N > 2 * nmax && (mode == 2 || (mode == 1 && c.ozaki == 0)))
+    return factor_blocked(c, 0, N, nb);
   return factor(c, 0, N, true, false);
 }

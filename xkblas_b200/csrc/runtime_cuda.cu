@@ -90,7 +90,13 @@ const SideStream& side_stream(int slot) {
   slot = std::max(0, std::min(kSideStreams - 1, slot));
   std::call_once(once[slot], [slot] {
     SideStream t;
-    if (cudaStreamCreateWithFlags(&t.s, cudaStreamNonBlocking) != cudaSuccess ||
+    int least = 0, greatest = 0;
+    if (slot >= kHiStream && cudaDeviceGetStreamPriorityRange(&least, &greatest) != cudaSuccess) {
+      cudaGetLastError();
+      greatest = 0;
+    }
+    if (cudaStreamCreateWithPriority(&t.s, cudaStreamNonBlocking,
+                                     slot >= kHiStream ? greatest : 0) != cudaSuccess ||
         cudaEventCreateWithFlags(&t.fork, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&t.join, cudaEventDisableTiming) != cudaSuccess) {
       cudaGetLastError();
@@ -99,6 +105,19 @@ const SideStream& side_stream(int slot) {
     ss[slot] = t;
   });
   return ss[slot];
+}
+
+cudaEvent_t* dep_events() {
+  static cudaEvent_t ev[8];
+  static bool ok = false;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    ok = true;
+    for (auto& e : ev)
+      if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) ok = false;
+    if (!ok) cudaGetLastError();
+  });
+  return ok ? ev : nullptr;
 }
 
 cudaStream_t side_fork(const SideStream& side, cudaStream_t st) {

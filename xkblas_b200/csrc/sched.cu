@@ -452,8 +452,29 @@ __device__ __noinline__ void gemm_tile(const Task& t, uint8_t* smem) {
   __syncthreads();  // smem free for the next task
   S* C = reinterpret_cast<S*>(t.C);
   const bool use_beta = (t.br != 0.0) || (t.bi != 0.0);
+  // one row of fragments at a time: all of its C loads, then its stores (C
+  // is read and written through one pointer; a load after a store would
+  // wait for it)
 #pragma unroll
-  for (int mf = 0; mf < MF; ++mf)
+  for (int mf = 0; mf < MF; ++mf) {
+    double cv[NF][CPLX ? 8 : 4];
+#pragma unroll
+    for (int nf = 0; nf < NF; ++nf)
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int row = wm * WTM + mf * 16 + g + ((i >> 1) << 3);
+        const int col = wn * WTN + nf * 8 + 2 * tq + (i & 1);
+        cv[nf][i] = 0.0;
+        if (CPLX) cv[nf][CPLX ? 4 + i : i] = 0.0;
+        if (!use_beta || row >= M || col >= N) continue;
+        const size_t idx = (size_t)row + (size_t)col * (size_t)t.ldc;
+        if constexpr (CPLX) {
+          cv[nf][i] = __ldcg(C + 2 * idx);
+          cv[nf][4 + i] = __ldcg(C + 2 * idx + 1);
+        } else {
+          cv[nf][i] = __ldcg(C + idx);
+        }
+      }
 #pragma unroll
     for (int nf = 0; nf < NF; ++nf)
 #pragma unroll
@@ -464,21 +485,14 @@ __device__ __noinline__ void gemm_tile(const Task& t, uint8_t* smem) {
         const size_t idx = (size_t)row + (size_t)col * (size_t)t.ldc;
         if constexpr (CPLX) {
           const double xr = acc[mf][nf][i], xi = acc[mf][nf][4 + i];
-          double vr = t.ar * xr - t.ai * xi;
-          double vi = t.ar * xi + t.ai * xr;
-          if (use_beta) {
-            const double cr = __ldcg(C + 2 * idx), ci = __ldcg(C + 2 * idx + 1);
-            vr += t.br * cr - t.bi * ci;
-            vi += t.br * ci + t.bi * cr;
-          }
-          C[2 * idx] = vr;
-          C[2 * idx + 1] = vi;
+          const double cr = cv[nf][i], ci = cv[nf][CPLX ? 4 + i : i];
+          C[2 * idx] = t.ar * xr - t.ai * xi + (t.br * cr - t.bi * ci);
+          C[2 * idx + 1] = t.ar * xi + t.ai * xr + (t.br * ci + t.bi * cr);
         } else {
-          double v = t.ar * acc[mf][nf][i];
-          if (use_beta) v = fma(t.br, __ldcg(C + idx), v);
-          C[idx] = v;
+          C[idx] = fma(t.br, cv[nf][i], t.ar * acc[mf][nf][i]);
         }
       }
+  }
 }
 
 template <class T, int BM, int MODE>

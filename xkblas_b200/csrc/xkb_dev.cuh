@@ -138,9 +138,13 @@ void count_launch(int n = 1);
 // A lazily created non-blocking stream with a fork and a join event, for
 // work that is independent of what the caller's stream runs meanwhile
 // (slot 0: the LU's column-panel solves, slots 1-3: the TRSM's groups of
-// right-hand sides after the first).  s is nullptr if CUDA could not create
-// it.
-constexpr int kSideStreams = 4;
+// right-hand sides after the first, slots kHiStream and kHiStream2: the
+// critical path of the blocked factorizations and the panel work beside it,
+// created with the device's greatest stream priority so that their small
+// launches are scheduled ahead of the trailing updates that run meanwhile).
+// s is nullptr if CUDA could not create it.
+constexpr int kSideStreams = 6;
+constexpr int kHiStream = 4, kHiStream2 = 5;
 struct SideStream {
   cudaStream_t s = nullptr;
   cudaEvent_t fork = nullptr, join = nullptr;
@@ -151,6 +155,9 @@ const SideStream& side_stream(int slot);
 cudaStream_t side_fork(const SideStream& side, cudaStream_t st);
 // Join: `st` waits for what the forked stream queued; false on a CUDA error.
 bool side_join(const SideStream& side, cudaStream_t forked, cudaStream_t st);
+// n <= 8 reusable timing-free events of the calling library (created once),
+// for dependencies between the side streams; nullptr if creation failed.
+cudaEvent_t* dep_events();
 // xkb_cuda_trsm with the choice to split many right-hand sides into two
 // concurrent halves (off where the caller already runs solves side by side)
 int trsm_entry(int dtype, int side, int uplo, int trans, int diag, int M, int N,

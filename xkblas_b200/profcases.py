@@ -1,6 +1,6 @@
 """Small, self-contained cases for profiling single kernels with ncu:
 
-    python -m xkblas_b200.profcases dmma|ozaki|ozaki2|ozaki8192|splitk|repack|trsm|potrf|getrf|batch|copy
+    python -m xkblas_b200.profcases dmma|ozaki|ozaki2|ozaki8192|splitk|repack|trsm|potrf|potrf8192|getrf|getrf8192|batch|copy
 
 dmma    DGEMM NN 4096^3 through xkb_cuda_gemm (k_gemm_dmma), two calls
 ozaki   the same through xkb_cuda_ozaki_gemm, 16 moduli (k_oz_* kernels)
@@ -13,8 +13,11 @@ splitk  DGEMM NN 512 x 512 x 4096 through xkb_cuda_gemm: 16 output tiles,
 repack  the DGEMM with lda = ldb = 4097 (k_repack, then k_gemm_dmma)
 trsm    DTRSM L/L/N/N 4096 x 4096, diagonally dominant (k_trsm_block, GEMMs)
 potrf   DPOTRF lower 4096 (k_potrf_block, k_trsm_block, GEMMs)
+potrf8192  DPOTRF lower 8192, two factorizations (the blocked look-ahead
+        form at its default block width)
 getrf   DGETRF without pivoting 4096, diagonally dominant (k_getrf_block,
         k_trsm_block, GEMMs)
+getrf8192  the same at 8192
 copy    beta scaling (k_scale, 8192^2) and the TRMM / SYMM materialisations
         (k_tri_fill, k_copy2d, k_sym_fill, 4096^2)
 batch   150 mixed calls (70% DGEMM, 20% DTRSM, 10% ZGEMM; M, N, K
@@ -79,8 +82,8 @@ def main(case):
             assert lib.xkb_cuda_trsm(1, 0, 1, 0, 0, n, n,
                                      ctypes.cast(al, ctypes.POINTER(ctypes.c_double)),
                                      A.data_ptr(), n, B.data_ptr(), n, 0, sp) == 0
-    elif case == "potrf":
-        n = 4096
+    elif case in ("potrf", "potrf8192"):
+        n = 8192 if case == "potrf8192" else 4096
         Bm = rnd(n, n)
         A0 = Bm @ Bm.t() / n + torch.eye(n, device="cuda", dtype=f64)
         A = A0.clone()
@@ -89,8 +92,8 @@ def main(case):
         for _ in range(2):
             A.copy_(A0)
             assert lib.xkb_cuda_potrf(1, 1, n, A.data_ptr(), n, info.data_ptr(), 0, sp) == 0
-    elif case == "getrf":
-        n = 4096
+    elif case in ("getrf", "getrf8192"):
+        n = 8192 if case == "getrf8192" else 4096
         A0 = rnd(n, n) + n * torch.eye(n, device="cuda", dtype=f64)
         A = A0.clone()
         info = torch.zeros(1, dtype=torch.int32, device="cuda")
