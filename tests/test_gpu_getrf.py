@@ -82,3 +82,34 @@ def test_getrf_nopiv_argument_codes(xk):
     assert lib.xkblas_dgetrf_nopiv_async(4, 3, xk._ptr(A), 4) == -2
     assert lib.xkblas_dgetrf_nopiv_async(4, 4, xk._ptr(A), 3) == -4
     assert lib.xkblas_dgetrf_nopiv_async(0, 0, xk._ptr(A), 1) == 0  # empty: nothing to do
+
+
+@pytest.mark.parametrize("dt", [np.float64, np.complex128])
+def test_getrf_nopiv_blocked_and_recursive_forms(xk, dt):
+    """The blocked look-ahead form (tuning key getrf_blocked = 1, several
+    block widths, widths shrinking along the factorization, a ragged last
+    block) and the recursive form (= 0) meet the same backward-error bound,
+    and both report a zero pivot in a late block."""
+    lib = xk.lib()
+    n = 1100
+    up = np.complex128 if np.issubdtype(dt, np.complexfloating) else np.float64
+    try:
+        for mode, nb, shrink in ((1, 64, 12), (1, 128, 12), (1, 320, 12), (1, 512, 2),
+                                 (0, 256, 12)):
+            lib.xkb_tune_set(b"getrf_blocked", float(mode))
+            lib.xkb_tune_set(b"getrf_nb", float(nb))
+            lib.xkb_tune_set(b"getrf_shrink", float(shrink))
+            A0 = _dd(n, dt, 50 + nb)
+            A = A0.copy(order="F")
+            assert _getrf(xk, A) == 0
+            L = np.tril(A, -1).astype(up) + np.eye(n)
+            U = np.triu(A).astype(up)
+            scale = np.abs(A0).max() * n * EPS[dt]
+            assert np.abs(L @ U - A0.astype(up)).max() <= 16 * scale, (mode, nb)
+            Z = np.asfortranarray((np.eye(n) * 2.0).astype(dt))
+            Z[776, 776] = 0.0
+            assert _getrf(xk, Z) == 777, (mode, nb)
+    finally:
+        lib.xkb_tune_set(b"getrf_blocked", 1.0)
+        lib.xkb_tune_set(b"getrf_nb", 512.0)
+        lib.xkb_tune_set(b"getrf_shrink", 12.0)

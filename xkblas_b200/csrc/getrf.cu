@@ -413,6 +413,124 @@ static int factor(const LuCtx& c, long i0, long i1) {
   return factor(c, h, i1);
 }
 
+// Block width for `m` remaining rows in the blocked form: nb, halved
+// (rounded down to a multiple of 64, at least nmin) while m <= shrink *
+// width (tuning key getrf_shrink, default 12): wide blocks while the
+// trailing update bounds each step, narrow ones once the critical path does.
+static long block_width(long m, long nb, long nmin) {
+  const double shrink = tune("getrf_shrink", 12.0);
+  long w = nb;
+  while (w > nmin && (double)m <= shrink * (double)w) w = std::max(nmin, (w / 2) / 64 * 64);
+  return w;
+}
+
+// Blocked right-looking LU of rows / columns [i0, i1) with look-ahead.  Step
+// k, with diagonal block D_k = L_k U_k factored; its column panel (below) and
+// row panel (to the right) are each split into part 1 (the next block's
+// rows / columns) and part 2 (the rest):
+//   critical path (high-priority stream hp):  column part 1 = . U_k^-1 and
+//     row part 1 = L_k^-1 ., then D_{k+1} -= L1 U1, then factor D_{k+1};
+//   beside it (high-priority stream hp2):     both parts 2, then the rest of
+//     block column k+1 (-= L2 U1) and block row k+1 (-= L1 U2);
+//   trailing block (caller's stream):         -= L2 U2, one GEMM.
+// The tile-level critical path of the reference's tile loop
+// (blas/zgetrf_nopiv.c:48-101: getrf -> trsm -> gemm -> getrf per tile
+// column) with nb-wide tiles.  Dependencies between the streams are events,
+// as in the blocked Cholesky: the next diagonal block's update and block
+// column / row k+1's updates wait for the previous trailing update; the next
+// part-1 solves wait for block column / row k+1.
+static int factor_blocked(const LuCtx& c, long i0, long i1, long nb) {
+  const SideStream& hp = side_stream(kHiStream);
+  const SideStream& hp2 = side_stream(kHiStream2);
+  cudaEvent_t* ev = dep_events();
+  if (!hp.s || !hp2.s || !ev) return factor(c, i0, i1);
+  cudaEvent_t e_diag = ev[0], e_p1 = ev[1], e_p2 = ev[2], e_col = ev[3], e_trail = ev[4];
+  const bool cplx = c.dt == XKB_C || c.dt == XKB_Z;
+  const double one[2] = {1.0, 0.0};
+  const long es = c.es, lda = c.lda;
+  auto at = [&](long i, long j) { return c.A + (i + j * lda) * es; };
+  // rows [r, r + m) of the column panel under block [b, b + nk): L = A U^-1
+  auto solve_col = [&](long b, long nk, long r, long m, cudaStream_t st) {
+    return trsm_entry(c.dt, 1, XKB_UPPER, XKB_OP_N, 0, (int)m, (int)nk, one, at(b, b), lda,
+                      at(r, b), lda, 0, st, false);
+  };
+  // columns [q, q + w) of the row panel right of block [b, b + nk): U = L^-1 A
+  auto solve_row = [&](long b, long nk, long q, long w, cudaStream_t st) {
+    return trsm_entry(c.dt, 0, XKB_LOWER, XKB_OP_N, 1, (int)nk, (int)w, one, at(b, b), lda,
+                      at(b, q), lda, 0, st, false);
+  };
+  // A(r.., q..) (m x w) -= L(r.., b..) U(b.., q..), inner nk
+  auto rank_update = [&](long b, long nk, long r, long m, long q, long w, cudaStream_t st) {
+    xkb_gemm_args g{};
+    g.dtype = c.dt;
+    g.opA = g.opB = XKB_OP_N;
+    g.M = (int)m;
+    g.N = (int)w;
+    g.K = (int)nk;
+    g.alpha[0] = -1.0;
+    g.beta[0] = 1.0;
+    g.A = at(r, b);
+    g.B = at(b, q);
+    g.C = at(r, q);
+    g.lda = g.ldb = g.ldc = lda;
+    g.uplo = XKB_FULL;
+    if (c.ozaki > 0 && std::min(nk, std::min(m, w)) >= c.ozaki) {
+      const int e = xkb_cuda_ozaki_gemm(&g, 0, st);
+      if (e != XKB_ERANGE) return e;
+    }
+    return xkb_cuda_gemm(&g, st);
+  };
+  LuCtx ch = c;
+  ch.st = side_fork(hp, c.st);
+  int e = XKB_OK;
+  auto rec = [&](cudaEvent_t x, cudaStream_t st) {
+    if (!e && cudaEventRecord(x, st) != cudaSuccess) e = XKB_ECUDA;
+  };
+  auto wait = [&](cudaStream_t st, cudaEvent_t x) {
+    if (!e && cudaStreamWaitEvent(st, x, 0) != cudaSuccess) e = XKB_ECUDA;
+  };
+  rec(e_trail, c.st);  // "previous trailing update": the caller's work so far
+  const long nmin = cplx ? LuShape<double2>::NMAX : LuShape<double>::NMAX;
+  long b = i0, nk = std::min(block_width(i1 - i0, nb, nmin), i1 - i0);
+  e = factor(ch, b, b + nk);
+  rec(e_diag, ch.st);
+  while (!e && b + nk < i1) {
+    const long r0 = b + nk, m2 = i1 - r0;
+    const long n1 = std::min(block_width(m2, nb, nmin), m2), m3 = m2 - n1;
+    if (m3 > 0) {  // hp2: both parts 2 (need D_k)
+      wait(hp2.s, e_diag);
+      if (!e) e = solve_col(b, nk, r0 + n1, m3, hp2.s);
+      if (!e) e = solve_row(b, nk, r0 + n1, m3, hp2.s);
+      rec(e_p2, hp2.s);
+    }
+    if (!e) e = solve_col(b, nk, r0, n1, ch.st);  // hp: both parts 1
+    if (!e) e = solve_row(b, nk, r0, n1, ch.st);
+    rec(e_p1, ch.st);
+    if (m3 > 0) {  // hp2: block column and block row k+1 (need parts 1, previous trailing)
+      wait(hp2.s, e_p1);
+      wait(hp2.s, e_trail);
+      if (!e) e = rank_update(b, nk, r0 + n1, m3, r0, n1, hp2.s);
+      if (!e) e = rank_update(b, nk, r0, n1, r0 + n1, m3, hp2.s);
+      rec(e_col, hp2.s);
+    }
+    wait(ch.st, e_trail);  // hp: D_{k+1} update (the previous trailing update wrote it)
+    if (!e) e = rank_update(b, nk, r0, n1, r0, n1, ch.st);
+    if (m3 > 0) {  // caller's stream: trailing block (needs parts 2)
+      wait(c.st, e_p2);
+      if (!e) e = rank_update(b, nk, r0 + n1, m3, r0 + n1, m3, c.st);
+      rec(e_trail, c.st);
+    }
+    if (!e) e = factor(ch, r0, r0 + n1);  // hp: D_{k+1}
+    rec(e_diag, ch.st);
+    if (m3 > 0) wait(ch.st, e_col);  // the next parts 1 lie in block column / row k+1
+    b = r0;
+    nk = n1;
+  }
+  if (!side_join(hp2, hp2.s, c.st) && !e) e = XKB_ECUDA;
+  if (!side_join(hp, ch.st, c.st) && !e) e = XKB_ECUDA;
+  return e;
+}
+
 }  // namespace xkb
 
 using namespace xkb;
@@ -430,5 +548,15 @@ extern "C" int xkb_cuda_getrf_nopiv(int dtype, int N, void* A, long lda, int* d_
   c.lda = lda;
   c.info = d_info;
   c.st = resolve_stream(stream);
+  // Blocked look-ahead form (tuning key getrf_blocked: 0 off, 1 in plain
+  // mode, 2 in both modes; widest block getrf_nb, in tensor-op mode
+  // getrf_nb_oz) or the recursive form.
+  const long nmax = (dtype == XKB_C || dtype == XKB_Z) ? LuShape<double2>::NMAX
+                                                       : LuShape<double>::NMAX;
+  const int mode = (int)tune("getrf_blocked", 1.0);
+  const long nb = std::max(nmax, ((long)tune(c.ozaki ? "getrf_nb_oz" : "getrf_nb",
+                                             c.ozaki ? 2048.0 : 512.0) + 63) / 64 * 64);
+  if (N > 2 * nmax && (mode == 2 || (mode == 1 && c.ozaki == 0)))
+    return factor_blocked(c, 0, N, nb);
   return factor(c, 0, N);
 }
