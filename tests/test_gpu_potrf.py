@@ -63,18 +63,27 @@ def test_potrf_factor(xk, dt, uplo, n):
 
 
 @pytest.mark.parametrize("dt,uplo", [(np.float64, LO), (np.complex128, UP)])
-def test_potrf_tensor_op_mode(xk, dt, uplo):
-    """XKBLAS_TENSOR_OP_MATH: the top-level trailing update and the panel
-    solve's coupling updates (all dimensions >= 2048 at n = 4200) run in the
-    Ozaki INT8 form; same backward-error bound as the plain factorization."""
+@pytest.mark.parametrize("mode", [0, 2])
+def test_potrf_tensor_op_mode(xk, dt, uplo, mode):
+    """XKBLAS_TENSOR_OP_MATH: in the recursive form (tuning key
+    potrf_blocked = 0) the top-level trailing update and the panel solve's
+    coupling updates (all dimensions >= 2048 at n = 4200) run in the Ozaki
+    INT8 form; the blocked form (= 2, the default) is also checked.  Same
+    backward-error bound as the plain factorization."""
     n = 4200
     A0 = _spd(n, dt, 11)
     A = A0.copy(order="F")
+    lib = xk.lib()
     xk.set_modemath(xk.XKBLAS_TENSOR_OP_MATH)
+    lib.xkb_tune_set(b"potrf_blocked", float(mode))
     try:
+        c0 = xk.ozaki_counts()[0]
         assert _potrf(xk, A, uplo) == 0
+        if mode == 0:
+            assert xk.ozaki_counts()[0] > c0  # Ozaki contractions ran
     finally:
         xk.set_modemath(xk.XKBLAS_DEFAULT_MATH)
+        lib.xkb_tune_set(b"potrf_blocked", 2.0)
     up = np.complex128 if np.iscomplexobj(A0) else np.float64
     if uplo == LO:
         L = np.tril(A)
@@ -140,6 +149,6 @@ def test_potrf_blocked_and_recursive_forms(xk, dt, uplo):
             B[776, 776] = -5.0
             assert _potrf(xk, B, uplo) == 777, (mode, nb)
     finally:
-        lib.xkb_tune_set(b"potrf_blocked", 1.0)
+        lib.xkb_tune_set(b"potrf_blocked", 2.0)
         lib.xkb_tune_set(b"potrf_nb", 512.0)
         lib.xkb_tune_set(b"potrf_shrink", 12.0)

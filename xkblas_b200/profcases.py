@@ -1,8 +1,10 @@
 """Small, self-contained cases for profiling single kernels with ncu:
 
-    python -m xkblas_b200.profcases dmma|ozaki|ozaki2|ozaki8192|splitk|repack|trsm|potrf|potrf8192|getrf|getrf8192|batch|copy
+    python -m xkblas_b200.profcases dmma|update256|ozaki|ozaki2|ozaki8192|splitk|repack|trsm|potrf|potrf8192|getrf|getrf8192|batch|copy
 
 dmma    DGEMM NN 4096^3 through xkb_cuda_gemm (k_gemm_dmma), two calls
+update256  the Cholesky's first trailing update at 8192 with 256-wide
+        blocks: C(7680 x 7680, lower) -= P P^T, K = 256, two calls
 ozaki   the same through xkb_cuda_ozaki_gemm, 16 moduli (k_oz_* kernels)
 ozaki2  the same with the CTA-pair INT8 kernel (tuning key oz_2cta = 1, k_oz_gemm2)
 ozaki8192  DGEMM NN 8192^3, xkb_cuda_ozaki_gemm with the count chosen on the
@@ -51,7 +53,15 @@ def main(case):
     keep = []
     if case == "ozaki2":
         lib.xkb_tune_set(b"oz_2cta", 1.0)
-    if case in ("ozaki8192", "splitk"):
+    if case == "update256":
+        m, k = 7680, 256
+        P, C = rnd(m, k), rnd(m, m)
+        keep += [P, C]
+        ga = _GemmArgs(1, 0, 1, m, m, k, P.data_ptr(), m, P.data_ptr(), m, C.data_ptr(), m)
+        ga.alpha[0], ga.beta[0], ga.uplo = -1.0, 1.0, 1
+        for _ in range(2):
+            assert lib.xkb_cuda_gemm(ctypes.byref(ga), sp) == 0
+    elif case in ("ozaki8192", "splitk"):
         m, n, k = (8192, 8192, 8192) if case == "ozaki8192" else (512, 512, 4096)
         A, B, C = rnd(m, k), rnd(k, n), rnd(m, n)
         keep += [A, B, C]
