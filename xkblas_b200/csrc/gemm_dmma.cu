@@ -480,10 +480,11 @@ static int dispatch_ops(const xkb_gemm_args* a, cudaStream_t st, const int* run_
 // slices as keep tiles x slices within one wave, each slice at least
 // gemm_splitk_min_kt k-tiles (tuning key, default 16 = K 256); 1 = no split.
 // Taken when even the small tiles cannot fill the SMs, or when every slice
-// still runs gemm_splitk_long_kt k-tiles (default 64 = K 1024): measured on a
-// B200, split-K 2 over 128x128 tiles beat the 64x64 tiles by 2.2x at
-// 512x512x4096, 1.10x at 768x768x1536 and 1.21x at 2048x512x2048, but lost
-// 4 % at 1024^3 (32 k-tiles per slice).
+// still runs gemm_splitk_long_kt k-tiles (default 16): measured on a B200,
+// split-K 2 over 128x128 tiles beat the 64x64 tiles by 2.2x at
+// 512x512x4096, 1.10x at 768x768x1536, 1.21x at 2048x512x2048, 1.16x at
+// 1024^3 (92.5 vs 107.6 us; 32 k-tiles per slice) and 1.03x at
+// 1024x1024x512 (16 k-tiles per slice).
 static int splitk_factor(long tiles_big, long tiles_small, long ktiles) {
   const double on = tune("gemm_splitk", 1.0);
   if (on == 0.0 || tiles_big <= 0) return 1;
@@ -492,7 +493,7 @@ static int splitk_factor(long tiles_big, long tiles_small, long ktiles) {
   long s = sms / tiles_big;
   s = std::min(s, ktiles / min_kt);
   s = std::max(1L, std::min(s, 32L));
-  if (s > 1 && tiles_small >= sms && ktiles / s < (long)tune("gemm_splitk_long_kt", 64.0))
+  if (s > 1 && tiles_small >= sms && ktiles / s < (long)tune("gemm_splitk_long_kt", 16.0))
     return 1;
   return (int)s;
 }
@@ -503,11 +504,16 @@ static int dispatch_type(const xkb_gemm_args* a, cudaStream_t st, const int* run
   constexpr int BMb = CPLX ? 64 : 128, BNb = 128;
   const long tiles_big = (long)((a->M + BMb - 1) / BMb) * ((a->N + BNb - 1) / BNb);
   // XKBLAS_GEMM_TILE=big|small overrides the size rule (tuning sweeps); the
-  // rule's threshold is the tuning table's gemm_big_min_tiles (default: one
-  // big tile per SM)
+  // rule's threshold is the tuning table's gemm_big_min_tiles (default: more
+  // big tiles than half the SMs).  Small tiles run two CTAs per SM at about
+  // 0.68 of a big tile's time per SM-wave, so one wave of big tiles beats
+  // them once it fills more than half the SMs (2048 x 1024 x 1024: 128 big
+  // tiles 160 us, 512 small tiles 205 us); below that, split-K or the small
+  // tiles.
   static const char* force = getenv("XKBLAS_GEMM_TILE");
   const bool big = force ? (force[0] == 'b')
-                         : (tiles_big >= (long)tune("gemm_big_min_tiles", (double)sm_count()));
+                         : (tiles_big >= (long)tune("gemm_big_min_tiles",
+                                                    (double)(sm_count() / 2 + 1)));
   if (big) return dispatch_ops<T, BMb, BNb>(a, st, run_if);
   // too few big tiles for the SMs: split their k range when K allows
   const long tiles_small =
