@@ -128,6 +128,26 @@ int xkb_cuda_ozaki_gemm_panels(const xkb_gemm_args* a, int nmod, void* stream, i
                                const long* bounds, void* const* wait_ev,
                                void* const* done_ev);
 
+/* Row-block and column-panel form of the real Ozaki contraction (C full):
+ * op(A) in row blocks [rb[i], rb[i+1]) (rb[0] = 0, rb[nr] = M), op(B) and C
+ * in column panels [cb[j], cb[j+1]) (cb[0] = 0, cb[nc] = N); interior
+ * bounds multiples of 256.  seq[0 .. nr+nc) is the order in which the
+ * blocks land: seq[k] >= 0 is column panel seq[k] (the stream first waits on
+ * b_ev[seq[k]], if not NULL), seq[k] < 0 row block -1-seq[k] (waits on
+ * a_ev[-1-seq[k]]); row blocks in increasing order, panels too.  At the k-th
+ * landing the block is converted and multiplied with every block of the
+ * other operand landed before it, which completes the rectangle of C
+ * [row block] x [0, columns landed) or [0, rows landed) x [panel];
+ * done_ev[k] (if not NULL) is recorded once that rectangle is final (an
+ * empty rectangle when nothing of the other operand has landed yet).  Lets
+ * a caller start the arithmetic, and the copy-back of C, before all of
+ * op(A) crossed the host link.  Results are those of
+ * xkb_cuda_ozaki_gemm_panels with the same count.  No counterpart in the
+ * reference. */
+int xkb_cuda_ozaki_gemm_blocks(const xkb_gemm_args* a, int nmod, void* stream, int nr,
+                               const long* rb, int nc, const long* cb, const int* seq,
+                               void* const* a_ev, void* const* b_ev, void* const* done_ev);
+
 /* The same real (XKB_D) Ozaki contraction as xkb_cuda_ozaki_gemm, for
  * callers that cannot allocate device memory at call time (a process whose
  * free GPU memory is held by its own caching allocator, a loop that must not

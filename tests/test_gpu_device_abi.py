@@ -161,3 +161,57 @@ def test_ozaki_panels_ragged(xk):
     bad = (ctypes.c_long * 3)(0, 600, 500)
     assert lib.xkb_cuda_ozaki_gemm_panels(ctypes.byref(ga), 0, None, 2, bad, None, None) != 0
     assert lib.xkb_cuda_take_device_error() == 0
+
+
+@pytest.mark.parametrize("opA", [0, 1])
+def test_ozaki_blocks_match_panels(xk, opA):
+    """xkb_cuda_ozaki_gemm_blocks (row blocks of op(A), column panels of
+    op(B), several landing orders, no events, unaligned operands) gives
+    bit for bit the column-panel form's result with the same moduli count;
+    badly placed bounds and out-of-order landings are EINVAL."""
+    import torch
+    g = torch.Generator(device="cuda").manual_seed(47)
+    M, N, K = 700, 1100, 500
+    ar, ac = (M, K) if opA == 0 else (K, M)
+    bufA, pA, A = _mat(torch, ar, ac, ar + 1, 1, 1, g)
+    bufB, pB, B = _mat(torch, K, N, K + 2, 1, 1, g)
+    bufC, pC, C = _mat(torch, M, N, M + 3, 1, 1, g)
+    C0 = C.clone()
+    lib = xk.lib()
+    L = ctypes.c_long
+    rb = (L * 4)(0, 256, 512, M)
+    cb = (L * 4)(0, 256, 768, N)
+
+    def args():
+        ga = GemmArgs(1, opA, 0, M, N, K, pA, ar + 1, pB, K + 2, pC, M + 3)
+        ga.alpha[0], ga.beta[0] = 1.5, -0.5
+        return ga
+
+    ga = args()
+    torch.cuda.synchronize()
+    assert lib.xkb_cuda_ozaki_gemm_panels(ctypes.byref(ga), 15, None, 3, cb, None, None) == 0
+    xk.sync()
+    want = C.clone()
+    opAm = A if opA == 0 else A.t()
+    ref = 1.5 * (opAm @ B) - 0.5 * C0
+    scale = 1.5 * A.abs().max().item() * B.abs().max().item() * K + 0.5
+    assert (want - ref).abs().max().item() <= 4 * EPS * scale
+    for order in ([-1, -2, -3, 0, 1, 2], [0, 1, 2, -1, -2, -3], [-1, 0, -2, 1, 2, -3]):
+        C.copy_(C0)
+        seq = (ctypes.c_int * 6)(*order)
+        torch.cuda.synchronize()
+        assert lib.xkb_cuda_ozaki_gemm_blocks(ctypes.byref(ga), 15, None, 3, rb, 3, cb, seq,
+                                              None, None, None) == 0
+        xk.sync()
+        assert torch.equal(C, want), order
+    ok = (ctypes.c_int * 6)(-1, -2, -3, 0, 1, 2)
+    bad_rb = (L * 4)(0, 300, 512, M)  # interior bound not a multiple of 256
+    assert lib.xkb_cuda_ozaki_gemm_blocks(ctypes.byref(ga), 15, None, 3, bad_rb, 3, cb, ok,
+                                          None, None, None) != 0
+    swapped = (ctypes.c_int * 6)(-2, -1, -3, 0, 1, 2)  # row blocks out of order
+    assert lib.xkb_cuda_ozaki_gemm_blocks(ctypes.byref(ga), 15, None, 3, rb, 3, cb, swapped,
+                                          None, None, None) != 0
+    twice = (ctypes.c_int * 6)(-1, -2, -2, 0, 1, 2)  # a block missing, another repeated
+    assert lib.xkb_cuda_ozaki_gemm_blocks(ctypes.byref(ga), 15, None, 3, rb, 3, cb, twice,
+                                          None, None, None) != 0
+    assert lib.xkb_cuda_take_device_error() == 0

@@ -169,6 +169,79 @@ int gemm_async(int transA, int transB, int M, int N, int K, const T* alpha, cons
   const size_t NB = auto_tilesize(KERN_GEMM, M, N, K), es = sizeof(T);
   int err;
   const bool need_ab = !is_zero(*alpha) && K > 0;
+  // Large real Ozaki contractions with op(B) = B and beta = 0 run block by
+  // block: op(A) crosses the host link in row blocks and B in column panels,
+  // interleaved so that the landed fractions of both grow together; every
+  // landed block is multiplied with all of the other operand landed before
+  // it, and coherence copies each finished rectangle of C back.  The
+  // arithmetic (and the copy-back) starts after the first row block instead
+  // of after all of op(A).  Tuning key ozaki_row_blocks (default 1; 0: the
+  // column-panel form below), rows per block ozaki_block_rows (1024).
+  if (need_ab && HT<T>::dt == XKB_D && transB == CblasNoTrans && N >= 4096 && M >= 4096 &&
+      is_zero(*beta) && use_ozaki(XKB_D, M, N, K) &&
+      xkb_tune_get("ozaki_row_blocks", 1.0) != 0.0) {
+    if ((err = flush_pending())) return rt_error(err);
+    Desc* dA = get_desc(A, Am, An, LDA, es, NB, &err);
+    if (!dA) return rt_error(err);
+    Desc* dB = get_desc(B, Bm, Bn, LDB, es, NB, &err);
+    if (!dB) return rt_error(err);
+    Desc* dC = get_desc(C, M, N, LDC, es, NB, &err);
+    if (!dC) return rt_error(err);
+    const long h = std::max<long>(256, (long)xkb_tune_get("ozaki_block_rows", 1024.0)) / 256 * 256;
+    const long pc = std::max<long>(256, (long)xkb_tune_get("ozaki_panel_cols", 1024.0));
+    const long np = std::min<long>(32, std::max<long>(2, N / pc));
+    const long w = ((N + np - 1) / np + 255) / 256 * 256;
+    std::vector<long> rb{0}, cb{0};
+    while (rb.back() < M) rb.push_back(std::min<long>(M, rb.back() + h));
+    while (cb.back() < N) cb.push_back(std::min<long>(N, cb.back() + w));
+    const long nr = (long)rb.size() - 1, nc = (long)cb.size() - 1;
+    // landing order: the next row block while the landed fraction of op(A)
+    // does not exceed that of B
+    std::vector<int> seq;
+    for (long i = 0, j = 0; i < nr || j < nc;) {
+      if (i < nr && (j >= nc || i * nc <= j * nr)) seq.push_back((int)(-1 - i++));
+      else seq.push_back((int)j++);
+    }
+    std::vector<EventRef> fin(seq.size());
+    std::vector<cudaEvent_t> ev_a, ev_b, done(seq.size());
+    for (size_t k = 0; k < fin.size(); ++k) {
+      if (!(fin[k] = new_event_ref())) return rt_error(XKB_ECUDA);
+      done[k] = fin[k]->e;
+    }
+    if ((err = make_valid_blocks(dA, transA != CblasNoTrans, (size_t)K, rb, dB, cb, seq, ev_a,
+                                 ev_b)))
+      return rt_error(err);
+    xkb_gemm_args a = base_args<T>(opcode(transA), opcode(transB), M, N, K, alpha, beta);
+    a.A = dev_ptr(dA, 0, 0);
+    a.lda = (long)dA->dld;
+    a.B = dev_ptr(dB, 0, 0);
+    a.ldb = (long)dB->dld;
+    a.C = dev_ptr(dC, 0, 0);
+    a.ldc = (long)dC->dld;
+    const int nm = R.ozaki_moduli ? R.ozaki_moduli : xkb_ozaki_default_moduli(K);
+    err = xkb_cuda_ozaki_gemm_blocks(&a, nm, R.s_comp, (int)nr, rb.data(), (int)nc, cb.data(),
+                                     seq.data(), reinterpret_cast<void* const*>(ev_a.data()),
+                                     reinterpret_cast<void* const*>(ev_b.data()),
+                                     reinterpret_cast<void* const*>(done.data()));
+    if (err) return rt_error(err);
+    mark_full_overwrite(dC, 0, M, 0, N);
+    // the rectangle each landing completed (as xkb_cuda_ozaki_gemm_blocks)
+    long ra = 0, cn = 0;
+    for (size_t k = 0; k < seq.size(); ++k) {
+      long r0, r1, c0, c1;
+      if (seq[k] < 0) {
+        const long i = -1 - seq[k];
+        r0 = rb[i], r1 = rb[i + 1], c0 = 0, c1 = cb[cn];
+        ++ra;
+      } else {
+        r0 = 0, r1 = rb[ra], c0 = cb[seq[k]], c1 = cb[seq[k] + 1];
+        ++cn;
+      }
+      if (r1 > r0 && c1 > c0)
+        dC->ready.push_back({(size_t)r0, (size_t)r1, (size_t)c0, (size_t)c1, fin[k]});
+    }
+    return 0;
+  }
   // Large real Ozaki contractions with op(B) = B run panel by panel: B (and
   // C) cross the host link in column panels, each panel is multiplied as soon
   // as its operands landed, and coherence copies each finished panel back.
@@ -212,7 +285,8 @@ int gemm_async(int transA, int transB, int M, int N, int K, const T* alpha, cons
     if (err) return rt_error(err);
 
     mark_full_overwrite(dC, 0, M, 0, N);
-    for (size_t p = 0; p < fin.size(); ++p) dC->col_ready.emplace_back((size_t)bounds[p + 1], fin[p]);
+    for (size_t p = 0; p < fin.size(); ++p)
+      dC->ready.push_back({0, (size_t)M, (size_t)bounds[p], (size_t)bounds[p + 1], fin[p]});
     return 0;
   }
   Desc *dA = nullptr, *dB = nullptr;

@@ -1252,9 +1252,11 @@ static int launch_pick(CallWords* w, const ModPlan& pl, bool allow_fallback, cud
 // plan's largest count; the per-modulus constants are those of every count).
 static int launch_res(const View& v, int L, int K, const int* code, const OzSel* sel,
                       const Consts* c, int8_t* planes, long Lpad, long Kpad, long kofs,
-                      cudaStream_t st) {
-  // grid covers Lpad x (K rounded to 64); kofs places the block at column kofs
-  dim3 g((unsigned)(Lpad / 64), (unsigned)(rup((size_t)K, 64) / 64));
+                      cudaStream_t st, long grid_rows = 0) {
+  // grid covers Lpad (or grid_rows, for a block of rows of larger planes:
+  // planes stay Lpad rows apart) x (K rounded to 64); kofs places the block
+  // at column kofs; rows from L to the grid's end are written as zeros
+  dim3 g((unsigned)((grid_rows ? grid_rows : Lpad) / 64), (unsigned)(rup((size_t)K, 64) / 64));
 #define XKB_RES_CASE(NM)                                                                     \
   case NM:                                                                                   \
     if (v.kc)                                                                                \
@@ -1280,20 +1282,23 @@ static int launch_res(const View& v, int L, int K, const int* code, const OzSel*
 }
 
 static bool encode_planes(CUtensorMap* m, const int8_t* base, long Kpad, long Lpad, int nmod,
-                          uint32_t box_rows) {
+                          uint32_t box_rows, long plane_rows = 0) {
   return encode_tmap_3d_u8(m, base, (uint64_t)Kpad, (uint64_t)Lpad, (uint64_t)nmod, 128,
-                           box_rows);
+                           box_rows, (uint64_t)plane_rows);
 }
 
 // a_rows / b_rows: rows per plane of the A / B residue buffers (>= Mpad /
-// Npad; equal when one buffer serves both operands).
+// Npad; equal when one buffer serves both operands).  a_stride / b_stride
+// (0: the same): rows between consecutive planes, when Ap / Bp point at a
+// block of rows of larger planes.
 static int launch_gemm(const int8_t* Ap, long a_rows, const int8_t* Bp, long b_rows, long Mpad,
                        long Npad, long Kpad, const Consts* c, const OzSel* sel, uint8_t* R,
-                       int uplo, long diag, cudaStream_t st) {
+                       int uplo, long diag, cudaStream_t st, long a_stride = 0,
+                       long b_stride = 0) {
   CUtensorMap tA, tB;
   if (a_rows < Mpad || b_rows < Npad) return XKB_EINVAL;
-  if (!encode_planes(&tA, Ap, Kpad, a_rows, c->nmod, BM)) return XKB_EINVAL;
-  if (!encode_planes(&tB, Bp, Kpad, b_rows, c->nmod, BN)) return XKB_EINVAL;
+  if (!encode_planes(&tA, Ap, Kpad, a_rows, c->nmod, BM, a_stride)) return XKB_EINVAL;
+  if (!encode_planes(&tB, Bp, Kpad, b_rows, c->nmod, BN, b_stride)) return XKB_EINVAL;
   GemmP p;
   std::memset(&p, 0, sizeof(p));
   p.tiles_m = (int)(Mpad / BM);
@@ -1317,7 +1322,7 @@ static int launch_gemm(const int8_t* Ap, long a_rows, const int8_t* Bp, long b_r
   if (total2 > 0 && tune("oz_2cta", 0.0) != 0.0 && sm_count() >= 2) {
     // CTA pairs: 256 x 256 tiles, each CTA loading 128-row halves of A and B
     CUtensorMap tB2;
-    if (!encode_planes(&tB2, Bp, Kpad, b_rows, c->nmod, 128)) return XKB_EINVAL;
+    if (!encode_planes(&tB2, Bp, Kpad, b_rows, c->nmod, 128, b_stride)) return XKB_EINVAL;
     p.tiles_m = (int)(Mpad / BM2);
     p.tiles_n = (int)(Npad / BN2);
     p.group = std::max(1, std::min(p.tiles_m, (int)tune("oz_group_m", 8.0)));
@@ -1699,6 +1704,177 @@ extern "C" int xkb_cuda_ozaki_gemm_panels(const xkb_gemm_args* a, int nmod, void
       }
     }
     done(q);  // recorded on every path: waiters never hang on an error
+  }
+  trace_mark(slot, 2, st);
+  trace_mark(slot, 3, st);
+  if (Ap) cudaFreeAsync(Ap, st);
+  if (Bp) cudaFreeAsync(Bp, st);
+  if (R) cudaFreeAsync(R, st);
+  if (mu) cudaFreeAsync(mu, st);
+  if (nu) cudaFreeAsync(nu, st);
+  if (pw) cudaFreeAsync(pw, st);
+  return err;
+}
+
+// Row blocks of op(A) and column panels of op(B) landing in the order `seq`
+// names; see include/xkb_cuda.h.  Every block is converted once, when it
+// lands, into residue planes that hold all of op(A) (all of op(B)); the
+// products of the newly landed block with all the blocks of the other
+// operand converted before it form one rectangle of C -- one INT8 launch,
+// one CRT -- whose completion is recorded on done_ev[k].  Row blocks and
+// column panels each land in increasing order, so those rectangles are
+// [row block i] x [0, the columns landed so far) or [0, the rows landed so
+// far) x [panel j], and together they cover C once.
+extern "C" int xkb_cuda_ozaki_gemm_blocks(const xkb_gemm_args* a, int nmod, void* stream, int nr,
+                                          const long* rb, int nc, const long* cb, const int* seq,
+                                          void* const* a_ev, void* const* b_ev,
+                                          void* const* done_ev) {
+  if (!a || a->dtype != XKB_D || a->uplo != XKB_FULL || nr < 1 || nc < 1 || !rb || !cb || !seq)
+    return XKB_EINVAL;
+  if (a->M < 0 || a->N < 0 || a->K < 0) return XKB_EINVAL;
+  if (rb[0] != 0 || rb[nr] != a->M || cb[0] != 0 || cb[nc] != a->N) return XKB_EINVAL;
+  // interior bounds on multiples of 256: block and panel offsets then fall on
+  // INT8 tile and TMA boundaries of the residue planes
+  for (int i = 0; i < nr; ++i)
+    if (rb[i + 1] <= rb[i] || (i > 0 && rb[i] % 256 != 0)) return XKB_EINVAL;
+  for (int j = 0; j < nc; ++j)
+    if (cb[j + 1] <= cb[j] || (j > 0 && cb[j] % 256 != 0)) return XKB_EINVAL;
+  {
+    int ni = 0, nj = 0;  // each block once, row blocks and panels in increasing order
+    for (int k = 0; k < nr + nc; ++k) {
+      if (seq[k] < 0) {
+        if (-1 - seq[k] != ni) return XKB_EINVAL;
+        ++ni;
+      } else {
+        if (seq[k] != nj) return XKB_EINVAL;
+        ++nj;
+      }
+    }
+    if (ni != nr || nj != nc) return XKB_EINVAL;
+  }
+  cudaStream_t st = resolve_stream(stream);
+  const int nseq = nr + nc;
+  auto wait = [&](void* const* evs, int q) {
+    if (evs && evs[q]) cudaStreamWaitEvent(st, static_cast<cudaEvent_t>(evs[q]), 0);
+  };
+  auto done = [&](int k) {
+    if (done_ev && done_ev[k]) cudaEventRecord(static_cast<cudaEvent_t>(done_ev[k]), st);
+  };
+  if (a->M == 0 || a->K == 0 || a->alpha[0] == 0.0 || a->K > 131072) {
+    // nothing to pipeline: every operand, then one plain product
+    for (int k = 0; k < nseq; ++k) wait(seq[k] < 0 ? a_ev : b_ev, seq[k] < 0 ? -1 - seq[k] : seq[k]);
+    const int r = a->K > 131072 ? XKB_ERANGE : (a->M == 0 ? XKB_OK : xkb_cuda_gemm(a, st));
+    for (int k = 0; k < nseq; ++k) done(k);
+    return r;
+  }
+  // blocks are converted before the other operand has landed: the count is
+  // fixed for the call (the tuning table's or the K rule's when nmod == 0)
+  if (nmod == 0) nmod = default_moduli(a->K);
+  ModPlan pl;
+  if (!plan_moduli(nmod, a->K, &pl)) return XKB_ERANGE;
+  const Consts* c = pl.chi;
+  const int M = a->M, N = a->N, K = a->K;
+  const long Kpad = (long)rup(K, BKB), Mpad = (long)rup(M, BM2), Npad = (long)rup(N, BN2);
+  long rmax = 0, cmax = 0;
+  for (int i = 0; i < nr; ++i) rmax = std::max(rmax, rb[i + 1] - rb[i]);
+  for (int j = 0; j < nc; ++j) cmax = std::max(cmax, cb[j + 1] - cb[j]);
+  const bool akc = a->opA != XKB_OP_N, bkc = a->opB == XKB_OP_N;
+  const int nch = (int)((K + kNormChunk - 1) / kNormChunk);
+  int8_t *Ap = nullptr, *Bp = nullptr;
+  uint8_t* R = nullptr;
+  int *mu = nullptr, *nu = nullptr;
+  unsigned char* pw = nullptr;  // CallWords, then the norm partials from byte 256
+  auto alloc = [&](void** p, size_t n) {
+    return cudaMallocAsync(p, std::max<size_t>(n, 256), st) == cudaSuccess;
+  };
+  // the largest rectangle: all rows x one panel, or one row block x all columns
+  const size_t rsz = std::max((size_t)Mpad * rup((size_t)cmax, BN), rup((size_t)rmax, BM) * (size_t)Npad);
+  bool ok = alloc((void**)&Ap, (size_t)nmod * Mpad * Kpad) &&
+            alloc((void**)&Bp, (size_t)nmod * Npad * Kpad) && alloc((void**)&R, (size_t)nmod * rsz) &&
+            alloc((void**)&mu, sizeof(int) * M) && alloc((void**)&nu, sizeof(int) * N) &&
+            alloc((void**)&pw, 256 + sizeof(double4) * (size_t)nch * (size_t)std::max(rmax, cmax));
+  int err = ok ? XKB_OK : XKB_ENOMEM;
+  if (!ok) cudaGetLastError();
+  CallWords* w = reinterpret_cast<CallWords*>(pw);
+  double4* part = reinterpret_cast<double4*>(pw + 256);
+  const OzSel* sel = w ? &w->sel : nullptr;
+  const double* Ad = static_cast<const double*>(a->A);
+  const double* Bd = static_cast<const double*>(a->B);
+  const int slot = trace_begin("ozaki_blocks", a->dtype, M, N, K, nmod, st);
+  if (!err) {
+    if (cudaMemsetAsync(w, 0, sizeof(CallWords), st) != cudaSuccess) err = XKB_ECUDA;
+    if (!err) err = launch_pick(w, pl, false, st);
+    // k columns past K (to the INT8 k-block) are zero in every plane
+    const size_t kz = rup(K, 64);
+    if (!err && Kpad > (long)kz &&
+        (cudaMemset2DAsync(Ap + kz, Kpad, 0, Kpad - kz, (size_t)nmod * Mpad, st) != cudaSuccess ||
+         cudaMemset2DAsync(Bp + kz, Kpad, 0, Kpad - kz, (size_t)nmod * Npad, st) != cudaSuccess))
+      err = XKB_ECUDA;
+  }
+  trace_mark(slot, 1, st);
+  int ra = 0, cn = 0;  // row blocks / panels landed so far
+  for (int k = 0; k < nseq; ++k) {
+    long r0, r1, c0, c1;  // the rectangle of C this landing completes
+    if (seq[k] < 0) {
+      const int i = -1 - seq[k];
+      wait(a_ev, i);
+      r0 = rb[i];
+      r1 = rb[i + 1];
+      c0 = 0;
+      c1 = cb[cn];
+      if (!err) {
+        // rows r0.. of op(A): opA == N -> A[i + k lda]; else A[k + i lda]
+        View va{akc ? Ad + r0 * a->lda : Ad + r0, a->lda, akc, 1, 0, 1.0};
+        const int L = (int)(r1 - r0);
+        err = launch_norm(va, L, K, 0, part, mu + r0, &w->rmax[0], st);
+        if (!err)
+          err = launch_res(va, L, K, mu + r0, sel, c, Ap + r0 * Kpad, Mpad, Kpad, 0, st,
+                           (long)rup((size_t)L, 64));
+      }
+      ++ra;
+    } else {
+      const int j = seq[k];
+      wait(b_ev, j);
+      r0 = 0;
+      r1 = rb[ra];
+      c0 = cb[j];
+      c1 = cb[j + 1];
+      if (!err) {
+        // columns c0.. of op(B): opB == N -> B[k + j ldb]; else B[j + k ldb]
+        View vb{bkc ? Bd + c0 * a->ldb : Bd + c0, a->ldb, bkc, 1, 0, 1.0};
+        const int L = (int)(c1 - c0);
+        err = launch_norm(vb, L, K, 0, part, nu + c0, &w->rmax[1], st);
+        if (!err)
+          err = launch_res(vb, L, K, nu + c0, sel, c, Bp + c0 * Kpad, Npad, Kpad, 0, st,
+                           (long)rup((size_t)L, 64));
+      }
+      ++cn;
+    }
+    if (!err && r1 > r0 && c1 > c0) {
+      const long mp = (long)rup((size_t)(r1 - r0), BM), np = (long)rup((size_t)(c1 - c0), BN);
+      err = launch_gemm(Ap + r0 * Kpad, mp, Bp + c0 * Kpad, np, mp, np, Kpad, c, sel, R, XKB_FULL,
+                        0, st, Mpad, Npad);
+      if (!err) {
+        CrtP cp;
+        std::memset(&cp, 0, sizeof(cp));
+        cp.M = (int)(r1 - r0);
+        cp.N = (int)(c1 - c0);
+        cp.R = R;
+        cp.Mpad = mp;
+        cp.Npad = np;
+        cp.mu = mu + r0;
+        cp.nu = nu + c0;
+        cp.sel = sel;
+        cp.C = static_cast<double*>(a->C) + r0 + c0 * a->ldc;
+        cp.ldc = a->ldc;
+        cp.ar = a->alpha[0];
+        cp.br = a->beta[0];
+        cp.uplo = XKB_FULL;
+        const dim3 cg((unsigned)(((cp.M + 3) / 4 + 255) / 256), (unsigned)std::min<long>(cp.N, 65535));
+        err = launch_crt(cg, st, cp, c, c, nullptr);
+      }
+    }
+    done(k);  // recorded on every path: waiters never hang on an error
   }
   trace_mark(slot, 2, st);
   trace_mark(slot, 3, st);

@@ -524,7 +524,7 @@ static bool tile_in_uplo(const Desc* d, size_t i, size_t j, int uplo) {
 
 void mark_written(Desc* d, size_t r0, size_t r1, size_t c0, size_t c1, int uplo) {
   if (r1 <= r0 || c1 <= c0) return;
-  d->col_ready.clear();  // this write is ordered by the compute stream only
+  d->ready.clear();  // this write is ordered by the compute stream only
   const size_t tr0 = r0 / d->mb, tr1 = (r1 + d->mb - 1) / d->mb;
   const size_t tc0 = c0 / d->nb, tc1 = (c1 + d->nb - 1) / d->nb;
   for (size_t j = tc0; j < tc1; ++j)
@@ -555,7 +555,7 @@ int flush_pending() {
   // work queued after it
   if (EventRef ev = new_event_ref()) {
     cudaEventRecord(ev->e, R.s_comp);
-    for (Desc* d : written) d->col_ready.assign(1, {d->N, ev});
+    for (Desc* d : written) d->ready.assign(1, {0, d->M, 0, d->N, ev});
   }
   return XKB_OK;
 }
@@ -621,7 +621,7 @@ int defer_op(const xkb_batch_op& o, Desc* r0, Desc* r1, Desc* r2, Desc* w) {
   mark(r1, 1);
   mark(r2, 1);
   mark(w, 2);
-  if (w) w->col_ready.clear();  // set again when this call is launched
+  if (w) w->ready.clear();  // set again when this call is launched
   const size_t lim = R.batch_flush_env
                          ? R.batch_flush_env
                          : (size_t)(xkb_tune_get("batch_flush_mb", 2048.0) * 1048576.0);
@@ -681,6 +681,75 @@ int make_valid_panels(const std::vector<std::pair<Desc*, size_t>>& ds,
   return XKB_OK;
 }
 
+int make_valid_blocks(Desc* da, bool a_trans, size_t K, const std::vector<long>& rb, Desc* db,
+                      const std::vector<long>& cb, const std::vector<int>& seq,
+                      std::vector<cudaEvent_t>& ev_a, std::vector<cudaEvent_t>& ev_b) {
+  Runtime& R = rt();
+  const size_t nr = rb.size() - 1, nc = cb.size() - 1;
+  ev_a.assign(nr, nullptr);
+  ev_b.assign(nc, nullptr);
+  // the stored region of a block: rows [r0, r1) x columns [c0, c1)
+  struct Reg {
+    size_t r0, r1, c0, c1;
+  };
+  auto region = [&](int s) -> Reg {
+    if (s >= 0) return {0, K, (size_t)cb[s], (size_t)cb[s + 1]};
+    const size_t i = (size_t)(-1 - s);
+    return a_trans ? Reg{0, K, (size_t)rb[i], (size_t)rb[i + 1]}
+                   : Reg{(size_t)rb[i], (size_t)rb[i + 1], 0, K};
+  };
+  // snapshot of the tiles that need a copy (whole matrices as used)
+  auto snapshot = [&](Desc* d, size_t rows, size_t cols) {
+    std::vector<uint8_t> need(d->mt * d->nt, 0);
+    const size_t tr1 = std::min(d->mt, (rows + d->mb - 1) / d->mb);
+    const size_t tc1 = std::min(d->nt, (cols + d->nb - 1) / d->nb);
+    for (size_t j = 0; j < tc1; ++j)
+      for (size_t i = 0; i < tr1; ++i) {
+        const bool miss = !(d->tile(i, j) & kDevValid);
+        need[i + j * d->mt] = miss;
+        miss ? ++R.stats.misses : ++R.stats.hits;
+      }
+    return need;
+  };
+  const size_t a_rows = a_trans ? K : (size_t)rb.back(), a_cols = a_trans ? (size_t)rb.back() : K;
+  std::vector<uint8_t> need_a = snapshot(da, a_rows, a_cols);
+  std::vector<uint8_t> need_b = snapshot(db, K, (size_t)cb.back());
+  for (int s : seq) {
+    Desc* d = s >= 0 ? db : da;
+    const std::vector<uint8_t>& need = s >= 0 ? need_b : need_a;
+    const Reg g = region(s);
+    // runs of tile rows needing a copy in each tile column, clipped to the block
+    for (size_t tj = g.c0 / d->nb; tj * d->nb < g.c1 && tj < d->nt; ++tj) {
+      const size_t c0 = std::max(g.c0, tj * d->nb), c1 = std::min(g.c1, (tj + 1) * d->nb);
+      const size_t ti1 = std::min(d->mt, (g.r1 + d->mb - 1) / d->mb);
+      size_t i = g.r0 / d->mb;
+      while (i < ti1) {
+        if (!need[i + tj * d->mt]) {
+          ++i;
+          continue;
+        }
+        size_t i1 = i;
+        while (i1 < ti1 && need[i1 + tj * d->mt]) ++i1;
+        if (int e = copy_h2d(d, std::max(g.r0, i * d->mb), std::min(g.r1, i1 * d->mb), c0, c1))
+          return e;
+        i = i1;
+      }
+    }
+    cudaEvent_t ev = next_event();
+    cudaEventRecord(ev, R.s_h2d);
+    (s >= 0 ? ev_b[(size_t)s] : ev_a[(size_t)(-1 - s)]) = ev;
+  }
+  auto mark = [&](Desc* d, size_t rows, size_t cols) {
+    const size_t tr1 = std::min(d->mt, (rows + d->mb - 1) / d->mb);
+    const size_t tc1 = std::min(d->nt, (cols + d->nb - 1) / d->nb);
+    for (size_t j = 0; j < tc1; ++j)
+      for (size_t i = 0; i < tr1; ++i) d->tile(i, j) |= kDevValid;
+  };
+  mark(da, a_rows, a_cols);
+  mark(db, K, (size_t)cb.back());
+  return XKB_OK;
+}
+
 int coherent(Desc* d, int uplo, int memflag) {
   Runtime& R = rt();
   if (int e = flush_pending()) return e;
@@ -694,35 +763,50 @@ int coherent(Desc* d, int uplo, int memflag) {
     if (cudaMemPrefetchAsync(d->host, ((d->N ? d->N - 1 : 0) * d->ld + d->M) * d->esz,
                              cudaCpuDeviceId, R.s_d2h) != cudaSuccess)
       cudaGetLastError();
-    d->col_ready.clear();
+    d->ready.clear();
     return XKB_OK;
   }
-  int e;
-  if (uplo == 0 && !d->col_ready.empty()) {
-    // written panel by panel: copy each panel back once its event fired;
-    // columns past the last panel after all work queued so far
+  int e = XKB_OK;
+  if (uplo == 0 && !d->ready.empty()) {
+    // written rectangle by rectangle: copy each back once its event fired, in
+    // the order they finish; what lies outside them after all work queued
+    // so far
+    const auto stale = [&](uint8_t s, size_t, size_t) { return (s & kHostStale) != 0; };
+    size_t Mc = 0, Nc = 0;
+    for (const auto& r : d->ready) {
+      Mc = std::max(Mc, r.r1);
+      Nc = std::max(Nc, r.c1);
+      bool waited = false;
+      e = for_runs(d, r.r0 / d->mb, std::min(d->mt, (r.r1 + d->mb - 1) / d->mb), r.c0 / d->nb,
+                   std::min(d->nt, (r.c1 + d->nb - 1) / d->nb), stale,
+                   [&](size_t a, size_t b, size_t c, size_t dd) {
+                     const size_t ra = std::max(a, r.r0), rz = std::min(b, r.r1);
+                     const size_t ca = std::max(c, r.c0), cz = std::min(dd, r.c1);
+                     if (ra >= rz || ca >= cz) return XKB_OK;
+                     if (!waited) {
+                       cudaStreamWaitEvent(R.s_d2h, r.ev->e, 0);
+                       waited = true;
+                     }
+                     return copy_d2h(d, ra, rz, ca, cz);
+                   });
+      if (e) break;
+    }
     cudaEvent_t tail = nullptr;
-    e = for_runs(
-        d, 0, d->mt, 0, d->nt, [&](uint8_t s, size_t, size_t) { return (s & kHostStale) != 0; },
-        [&](size_t a, size_t b, size_t c, size_t dd) {
-          size_t from = 0;
-          for (auto& cr : d->col_ready) {
-            const size_t lo = std::max(c, from), hi = std::min(dd, cr.first);
-            from = cr.first;
-            if (lo >= hi) continue;
-            cudaStreamWaitEvent(R.s_d2h, cr.second->e, 0);
-            if (int r = copy_d2h(d, a, b, lo, hi)) return r;
-          }
-          if (dd > std::max(c, from)) {
-            if (!tail) {
-              tail = next_event();
-              cudaEventRecord(tail, R.s_comp);
-            }
-            cudaStreamWaitEvent(R.s_d2h, tail, 0);
-            if (int r = copy_d2h(d, a, b, std::max(c, from), dd)) return r;
-          }
-          return XKB_OK;
-        });
+    auto after_all = [&](size_t a, size_t b, size_t c, size_t dd) {
+      if (a >= b || c >= dd) return XKB_OK;
+      if (!tail) {
+        tail = next_event();
+        cudaEventRecord(tail, R.s_comp);
+        cudaStreamWaitEvent(R.s_d2h, tail, 0);
+      }
+      return copy_d2h(d, a, b, c, dd);
+    };
+    if (!e)
+      e = for_runs(d, 0, d->mt, 0, d->nt, stale, [&](size_t a, size_t b, size_t c, size_t dd) {
+        // the parts of the run outside [0, Mc) x [0, Nc)
+        if (int r = after_all(std::max(a, Mc), b, c, dd)) return r;
+        return after_all(a, std::min(b, Mc), std::max(c, Nc), dd);
+      });
   } else {
     // D2H after everything already queued on the compute stream
     cudaEvent_t ev = next_event();
@@ -736,7 +820,7 @@ int coherent(Desc* d, int uplo, int memflag) {
         [&](size_t a, size_t b, size_t c, size_t dd) { return copy_d2h(d, a, b, c, dd); });
   }
   if (e) return e;
-  d->col_ready.clear();
+  d->ready.clear();
   for (size_t j = 0; j < d->nt; ++j)
     for (size_t i = 0; i < d->mt; ++i) {
       uint8_t& s = d->tile(i, j);

@@ -55,13 +55,19 @@ struct Desc {
   size_t bytes = 0;                       // device buffer size (counted against the cache limit)
   uint64_t last_use = 0;                  // LRU stamp: the runtime's use clock at the last touch
   uint64_t epoch = 0;                     // API call that last touched it (never evicted by it)
-  // columns finished on the compute stream: (end column, event recorded when
-  // columns [previous end, end) are final), ascending.  Set by the panel
-  // contraction (one entry per panel) and by an executor batch (one entry for
-  // the whole matrix); lets coherence copy results back as soon as their
+  // rectangles finished on the compute stream, in the order they finish:
+  // rows [r0, r1) x columns [c0, c1) are final once `ev` fired.  Together
+  // they cover [0, max r1) x [0, max c1) once.  Set by the panel
+  // contraction (one column panel each), the row-block / column-panel
+  // contraction (one rectangle per landed block) and an executor batch (the
+  // whole matrix); lets coherence copy results back as soon as their
   // producer is done instead of after all queued work.  Cleared by any write
   // that does not set it.
-  std::vector<std::pair<size_t, std::shared_ptr<struct SharedEvent>>> col_ready;
+  struct Ready {
+    size_t r0, r1, c0, c1;
+    std::shared_ptr<struct SharedEvent> ev;
+  };
+  std::vector<Ready> ready;
   std::string name;
   uint8_t& tile(size_t i, size_t j) { return st[i + j * mt]; }
 };
@@ -168,6 +174,17 @@ int coherent(Desc* d, int uplo, int memflag);
 // made to wait: the caller waits per panel.  The tiles become valid.
 int make_valid_panels(const std::vector<std::pair<Desc*, size_t>>& ds,
                       const std::vector<long>& bounds, std::vector<cudaEvent_t>& ev);
+// Row-block / column-panel upload for a contraction with inner dimension K:
+// row block i = rows [rb[i], rb[i+1]) of op(A) (rows of the stored `da`, or
+// its columns when a_trans), column panel j = columns [cb[j], cb[j+1]) of
+// the stored `db` (K rows).  The parts of those blocks whose tiles are not
+// valid on the device are copied in the order `seq` names (>= 0: panel,
+// < 0: row block -1 - seq), and ev_a[i] / ev_b[j] recorded on the copy
+// stream once the block has landed.  The compute stream is NOT made to wait.
+// The tiles become valid.
+int make_valid_blocks(Desc* da, bool a_trans, size_t K, const std::vector<long>& rb, Desc* db,
+                      const std::vector<long>& cb, const std::vector<int>& seq,
+                      std::vector<cudaEvent_t>& ev_a, std::vector<cudaEvent_t>& ev_b);
 // The Ozaki crossover in effect (min(M, N, K) at or above it: tensor-op mode
 // uses the Ozaki form).
 long ozaki_min_dim();

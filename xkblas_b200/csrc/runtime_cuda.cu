@@ -59,13 +59,16 @@ bool encode_tmap_2d(CUtensorMap* map, CUtensorMapDataType dtype, int elem_bytes,
 }
 
 bool encode_tmap_3d_u8(CUtensorMap* map, const void* base, uint64_t inner, uint64_t rows,
-                       uint64_t planes, uint32_t box_inner, uint32_t box_rows) {
+                       uint64_t planes, uint32_t box_inner, uint32_t box_rows,
+                       uint64_t plane_rows) {
   PFN_encodeTiled enc = get_encode();
   if (!enc || !base || inner == 0 || rows == 0 || planes == 0) return false;
   if ((reinterpret_cast<uintptr_t>(base) & 15u) != 0 || (inner & 15u) != 0) return false;
   if (box_inner > 128 || box_rows > 256 || (box_inner & 15u) != 0) return false;
   cuuint64_t dims[3] = {inner, rows, planes};
-  cuuint64_t strides[2] = {inner, inner * rows};
+  if (plane_rows == 0) plane_rows = rows;
+  if (plane_rows < rows) return false;
+  cuuint64_t strides[2] = {inner, inner * plane_rows};
   cuuint32_t box[3] = {box_inner, box_rows, 1};
   cuuint32_t estr[3] = {1, 1, 1};
   std::memset(map, 0, sizeof(*map));

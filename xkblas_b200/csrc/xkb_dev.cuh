@@ -127,8 +127,11 @@ bool encode_tmap_2d(CUtensorMap* map, CUtensorMapDataType dtype, int elem_bytes,
                     uint32_t bx, uint32_t by, CUtensorMapSwizzle swz);
 // 3-D byte tensor (planes of rows x inner bytes), 128-byte swizzle, box
 // (box_inner x box_rows x 1): the layout tcgen05 K-major operands use.
+// planes of `rows` x `inner` bytes (inner contiguous), consecutive planes
+// plane_rows * inner bytes apart (0: rows; a view of rows of larger planes)
 bool encode_tmap_3d_u8(CUtensorMap* map, const void* base, uint64_t inner, uint64_t rows,
-                       uint64_t planes, uint32_t box_inner, uint32_t box_rows);
+                       uint64_t planes, uint32_t box_inner, uint32_t box_rows,
+                       uint64_t plane_rows = 0);
 cudaStream_t resolve_stream(void* s);
 // trace: begin a record (returns a slot or -1 when tracing is off) and mark
 // phase boundaries 1..3 (3 = end) on the launching stream.
