@@ -360,9 +360,11 @@ def pinned_empty(shape, dtype):
 
 class _Pinned(np.ndarray):
     def __del__(self):
-        p = getattr(self, "_xkb_ptr", None)
-        if p and self.base is not None and not isinstance(self.base, _Pinned):
-            try:
+        # at interpreter exit module globals may already be gone: then the
+        # process is ending and the pinned block goes with it
+        try:
+            p = getattr(self, "_xkb_ptr", None)
+            if p and self.base is not None and not isinstance(self.base, _Pinned):
                 lib().xkblas_free(ctypes.c_void_p(p), self._xkb_n)
-            except Exception:
-                pass
+        except Exception:
+            pass
