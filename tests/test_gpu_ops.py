@@ -483,3 +483,53 @@ def test_trsm_inverse_leaves(xk, dt, side):
                         assert r <= 10, (flag, uplo, tr, dg, r)
     finally:
         lib.xkb_tune_set(b"trsm_inv_leaves", 1.0)
+
+
+@pytest.mark.parametrize("case", [
+    # (dtype, M, N, K, opA, opB): few output tiles, long K
+    (np.float64, 640, 1280, 2048, T_, N_),
+    (np.float64, 300, 200, 2049, N_, T_),
+    (np.complex128, 320, 256, 3000, C_, N_),
+    (np.float64, 1000, 900, 3000, N_, N_),
+])
+def test_gemm_stream_k(xk, case):
+    """Stream-K (tuning key gemm_sk_fill = 1: taken whenever split-K would
+    be) and split-K (gemm_streamk = 0) on the same operands: both meet the
+    reference bound, and stream-K's fixed order of the pieces makes repeated
+    calls bit-identical."""
+    import ctypes
+    import torch
+    from xkblas_b200 import GemmArgs
+    dt, M, N, K, ta, tb = case
+    cplx = dt == np.complex128
+    A = gen(M, K, 70, dt) if ta == N_ else gen(K, M, 70, dt)
+    B = gen(K, N, 71, dt) if tb == N_ else gen(N, K, 71, dt)
+    C0 = gen(M, N, 72, dt)
+    al, be = (0.5 + 1.25j, 0.75 - 0.5j) if cplx else (0.5, 0.75)
+    dev = lambda X: torch.from_numpy(np.ascontiguousarray(X.T)).cuda()
+    dA, dB = dev(A), dev(B)
+    lib = xk.lib()
+    R = O.gemm(ta, tb, al, A, B, be, C0.copy(order="F"), nb=256)
+    outs = {}
+    try:
+        for mode, (sk, fill) in (("sk", (1.0, 1.0)), ("sk2", (1.0, 1.0)), ("split", (0.0, 0.8))):
+            lib.xkb_tune_set(b"gemm_streamk", sk)
+            lib.xkb_tune_set(b"gemm_sk_fill", fill)
+            dC = dev(C0)
+            g = GemmArgs(3 if cplx else 1, ta - N_, tb - N_, M, N, K, dA.data_ptr(), A.shape[0],
+                         dB.data_ptr(), B.shape[0], dC.data_ptr(), M)
+            g.alpha[0], g.alpha[1] = (al.real, al.imag) if cplx else (al, 0.0)
+            g.beta[0], g.beta[1] = (be.real, be.imag) if cplx else (be, 0.0)
+            torch.cuda.synchronize()
+            k0 = xk.kernel_count()
+            assert lib.xkb_cuda_gemm(ctypes.byref(g), None) == 0
+            assert xk.kernel_count() - k0 == 2  # the pieces and their reduction
+            xk.sync()
+            outs[mode] = np.asfortranarray(dC.cpu().numpy().T)
+    finally:
+        lib.xkb_tune_set(b"gemm_streamk", 1.0)
+        lib.xkb_tune_set(b"gemm_sk_fill", 0.8)
+    assert lib.xkb_cuda_take_device_error() == 0
+    assert np.array_equal(outs["sk"], outs["sk2"])
+    for mode in ("sk", "split"):
+        assert checks.gemm_ratio(outs[mode], R, A, B, C0, al, be, K) <= 3.0, mode

@@ -46,7 +46,20 @@ struct GemmParams {
   // ws and k_gemm_splitk sums the slices in order and runs the epilogue
   int ksplit, kt_slice;
   double* ws;
+  // stream-K (k_gemm_dmma_sk): the ntiles x ktiles k-tiles, tile-major, are
+  // dealt out evenly to sk_ctas CTAs; a tile's pieces land in ws slots
+  // [tile][0 .. sk_slots) in CTA order
+  int sk_ctas, sk_slots;
 };
+
+// The stream-K CTA whose share of the k-tile sequence holds k-tile g (of
+// total T over G CTAs; CTA c holds [c T / G, (c+1) T / G)).
+__host__ __device__ __forceinline__ int sk_cta(long g, long T, int G) {
+  int c = (int)(g * G / T);
+  while (c + 1 < G && (long)(c + 1) * T / G <= g) ++c;
+  while (c > 0 && (long)c * T / G > g) --c;
+  return c;
+}
 
 // Tile of CTA `bid` (< tiles_m tiles_n) in the grouped rasterisation: 8 tile
 // rows share a band of B columns in L2.  False if it lies wholly outside the
@@ -166,6 +179,71 @@ constexpr int kBK = 16;      // k extent of one pipeline stage
 constexpr int kStages = 4;
 constexpr int kConsumerWarps = 8;
 constexpr int kThreads = kConsumerWarps * 32;
+
+// One 16-deep k stage of a consumer warp: DMMAs of its fragments of A (in
+// shared memory at `st`) and B (after A's BM x kBK tile) into acc.
+template <class T, int BM, int BN, bool A_KC, bool B_KC>
+__device__ __forceinline__ void dmma_stage(const uint8_t* st,
+                                           double (&acc)[BM / 32][BN / 32][St<T>::CPLX ? 8 : 4],
+                                           int wm, int wn, int g, int t, double sgnA,
+                                           double sgnB) {
+  using S = typename St<T>::S;
+  constexpr bool CPLX = St<T>::CPLX;
+  constexpr int WTM = BM / 2, WTN = BN / 4;
+  constexpr int MF = WTM / 16, NF = WTN / 8;
+  const S* sa = reinterpret_cast<const S*>(st);
+  const S* sb = reinterpret_cast<const S*>(st + BM * kBK * sizeof(T));
+#pragma unroll
+  for (int kc = 0; kc < kBK / 8; ++kc) {
+    const int k0 = kc * 8 + 2 * t, k1 = k0 + 1;
+    double br[NF][2], bi[NF][2];
+#pragma unroll
+    for (int nf = 0; nf < NF; ++nf) {
+      const int n = wn * WTN + nf * 8 + g;
+      const int o0 = B_KC ? n * kBK + k0 : k0 * BN + n;
+      const int o1 = B_KC ? n * kBK + k1 : k1 * BN + n;
+      ld_elem<T>(sb, o0, br[nf][0], bi[nf][0]);
+      ld_elem<T>(sb, o1, br[nf][1], bi[nf][1]);
+      if (CPLX) {
+        bi[nf][0] *= sgnB;
+        bi[nf][1] *= sgnB;
+      }
+    }
+#pragma unroll
+    for (int mf = 0; mf < MF; ++mf) {
+      const int r0 = wm * WTM + mf * 16 + g, r1 = r0 + 8;
+      double ar[4], ai[4];
+      ld_elem<T>(sa, A_KC ? r0 * kBK + k0 : k0 * BM + r0, ar[0], ai[0]);
+      ld_elem<T>(sa, A_KC ? r1 * kBK + k0 : k0 * BM + r1, ar[1], ai[1]);
+      ld_elem<T>(sa, A_KC ? r0 * kBK + k1 : k1 * BM + r0, ar[2], ai[2]);
+      ld_elem<T>(sa, A_KC ? r1 * kBK + k1 : k1 * BM + r1, ar[3], ai[3]);
+      if constexpr (CPLX) {
+        double nai[4];
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+          ai[v] *= sgnA;
+          nai[v] = -ai[v];
+        }
+#pragma unroll
+        for (int nf = 0; nf < NF; ++nf) {
+          double* a = acc[mf][nf];
+          double (&re)[4] = *reinterpret_cast<double(*)[4]>(a);
+          double (&im)[4] = *reinterpret_cast<double(*)[4]>(a + 4);
+          dmma_k8(re, ar, br[nf]);
+          dmma_k8(re, nai, bi[nf]);
+          dmma_k8(im, ar, bi[nf]);
+          dmma_k8(im, ai, br[nf]);
+        }
+      } else {
+#pragma unroll
+        for (int nf = 0; nf < NF; ++nf) {
+          double (&d)[4] = *reinterpret_cast<double(*)[4]>(acc[mf][nf]);
+          dmma_k8(d, ar, br[nf]);
+        }
+      }
+    }
+  }
+}
 
 // A_KC: op(A) != N, A tile stored [BM][BK] (k contiguous), else [BK][BM].
 // B_KC: op(B) == N, B tile stored [BN][BK], else [BK][BN].
@@ -340,6 +418,152 @@ __global__ void __launch_bounds__(kThreads, 1)
   dmma_epilogue<T, BM, BN>(p, m0, n0, accp);
 }
 
+// Stream-K form of k_gemm_dmma (real or complex, C full, 128x128 tiles):
+// for shapes whose tiles leave SMs idle, every CTA takes an equal share of
+// the tile-major sequence of (tile, k-tile) steps -- pieces of at most a few
+// tiles -- with the TMA ring running on from one piece into the next; each
+// piece's raw accumulators go to a workspace slot, and k_gemm_sk_reduce sums
+// every tile's pieces in CTA order (deterministic) and runs the epilogue.
+template <class T, int BM, int BN, bool A_KC, bool B_KC>
+__global__ void __launch_bounds__(kThreads, 1)
+    k_gemm_dmma_sk(const __grid_constant__ CUtensorMap tmA,
+                   const __grid_constant__ CUtensorMap tmB, const GemmParams p) {
+  if (p.run_if && *p.run_if == 0) return;
+  constexpr int W = St<T>::W;
+  constexpr bool CPLX = St<T>::CPLX;
+  constexpr int MF = BM / 32, NF = BN / 32;
+  constexpr uint32_t A_BYTES = BM * kBK * sizeof(T);
+  constexpr uint32_t B_BYTES = BN * kBK * sizeof(T);
+  constexpr uint32_t STAGE_BYTES = A_BYTES + B_BYTES;
+  constexpr int NACC = CPLX ? 8 : 4;
+  constexpr int NREG = AccShape<T, BM, BN>::NREG;
+
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* base =
+      reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
+  uint64_t* full = reinterpret_cast<uint64_t*>(base + kStages * STAGE_BYTES);
+  uint64_t* empty = full + kStages;
+
+  const int kts = p.ktiles;
+  const long tot = (long)p.tiles_m * p.tiles_n * kts;
+  const int G = p.sk_ctas;
+  const long g0 = (long)blockIdx.x * tot / G, g1 = (long)(blockIdx.x + 1) * tot / G;
+  if (g0 >= g1) return;
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kStages; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], kConsumerWarps);
+    }
+    fence_barrier_init();
+  }
+  __syncthreads();
+
+  // producer (thread 0): the next step gp of [g0, g1) into ring slot gi
+  long gp = g0;
+  uint32_t gi = 0;
+  auto issue_next = [&]() {
+    const int s = gi % kStages;
+    uint8_t* sa = base + s * STAGE_BYTES;
+    uint8_t* sb = sa + A_BYTES;
+    int m0, n0;
+    dmma_tile<BM, BN>(p, (int)(gp / kts), m0, n0);
+    const int k0 = (int)(gp % kts) * kBK;
+    mbar_expect_tx(&full[s], STAGE_BYTES);
+    if (A_KC) tma_load_2d(sa, &tmA, k0 * W, m0, &full[s]);
+    else tma_load_2d(sa, &tmA, m0 * W, k0, &full[s]);
+    if (B_KC) tma_load_2d(sb, &tmB, k0 * W, n0, &full[s]);
+    else tma_load_2d(sb, &tmB, n0 * W, k0, &full[s]);
+    ++gi;
+    ++gp;
+  };
+  if (threadIdx.x == 0) {
+    tma_prefetch(&tmA);
+    tma_prefetch(&tmB);
+    for (int i = 0; i < kStages && gp < g1; ++i) issue_next();
+  }
+
+  const int wm = warp >> 2, wn = warp & 3;
+  const int g = lane >> 2, t = lane & 3;
+  const double sgnA = p.conjA ? -1.0 : 1.0;
+  const double sgnB = p.conjB ? -1.0 : 1.0;
+  uint32_t gc = 0;
+  for (long gs = g0; gs < g1;) {
+    const int tile = (int)(gs / kts);
+    const long gend = (long)(tile + 1) * kts < g1 ? (long)(tile + 1) * kts : g1;
+    const int KT = (int)(gend - gs);
+    double acc[MF][NF][NACC];
+#pragma unroll
+    for (int i = 0; i < MF; ++i)
+#pragma unroll
+      for (int j = 0; j < NF; ++j)
+#pragma unroll
+        for (int v = 0; v < NACC; ++v) acc[i][j][v] = 0.0;
+    bool ok = true;
+    for (int it = 0; it < KT; ++it, ++gc) {
+      const int s = gc % kStages;
+      const uint32_t ph = (gc / kStages) & 1;
+      const bool got = mbar_wait(&full[s], ph, kErrFullWait);
+      if (!__all_sync(0xffffffffu, got)) {
+        ok = false;
+        break;
+      }
+      dmma_stage<T, BM, BN, A_KC, B_KC>(base + s * STAGE_BYTES, acc, wm, wn, g, t, sgnA, sgnB);
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&empty[s]);
+      if (warp == 0) {
+        bool refill_ok = true;
+        if (lane == 0 && gp < g1) {
+          refill_ok = mbar_wait(&empty[s], ph, kErrEmptyWait);
+          if (refill_ok) issue_next();
+        }
+        if (!__all_sync(0xffffffffu, refill_ok)) {
+          ok = false;
+          break;
+        }
+      }
+    }
+    if (!ok) return;  // a bounded wait gave up (error word recorded)
+    // this piece's slot: its CTA's position among the tile's CTAs
+    const int slot = (int)blockIdx.x - sk_cta((long)tile * kts, tot, G);
+    const double* accp = &acc[0][0][0];
+    double* w = p.ws + ((size_t)tile * p.sk_slots + slot) * (size_t)(NREG * kThreads) + threadIdx.x;
+#pragma unroll
+    for (int r = 0; r < NREG; ++r) w[(size_t)r * kThreads] = accp[r];
+    gs += KT;
+  }
+}
+
+// Stream-K reduction: block (tile, fragment f) sums fragment f of the
+// tile's pieces in CTA order, then stores it as the unsplit epilogue does.
+template <class T, int BM, int BN>
+__global__ void __launch_bounds__(kThreads) k_gemm_sk_reduce(const GemmParams p) {
+  if (p.run_if && *p.run_if == 0) return;
+  using A = AccShape<T, BM, BN>;
+  constexpr int NREG = A::NREG;
+  const int kts = p.ktiles;
+  const long tot = (long)p.tiles_m * p.tiles_n * kts;
+  const int bid = blockIdx.x, f = blockIdx.y;
+  int m0, n0;
+  if (!dmma_tile<BM, BN>(p, bid, m0, n0)) return;
+  const int c0 = sk_cta((long)bid * kts, tot, p.sk_ctas);
+  const int c1 = sk_cta((long)(bid + 1) * kts - 1, tot, p.sk_ctas);
+  double acc[A::NACC];
+#pragma unroll
+  for (int v = 0; v < A::NACC; ++v) acc[v] = 0.0;
+  for (int sl = 0; sl <= c1 - c0; ++sl) {
+    const double* w = p.ws + ((size_t)bid * p.sk_slots + sl) * (size_t)(NREG * kThreads) +
+                      (size_t)(f * A::NACC) * kThreads + threadIdx.x;
+#pragma unroll
+    for (int v = 0; v < A::NACC; ++v) acc[v] += w[(size_t)v * kThreads];
+  }
+  double cv[A::NACC];
+  dmma_load_frag<T, BM, BN>(p, m0, n0, f / A::NF, f % A::NF, cv);
+  dmma_store_frag<T, BM, BN>(p, m0, n0, f / A::NF, f % A::NF, acc, cv);
+}
+
 // Split-K reduction: block (tile, fragment f) sums fragment f of the tile's
 // slices in slice order (deterministic) with the GEMM kernel's
 // thread-to-element map, then stores it as the unsplit epilogue does.  One
@@ -399,7 +623,10 @@ __global__ void k_scale(int M, int N, double br, double bi, T* Cv, long ldc, int
 // ---------------------------------------------------------------------------
 // host side
 template <class T, int BM, int BN, bool A_KC, bool B_KC>
-static int launch_dmma(const xkb_gemm_args* a, cudaStream_t st, const int* run_if, int ksplit) {
+// ksplit > 1: split-K over that many slices; sk_ctas > 0: stream-K over
+// that many CTAs (C full only).
+static int launch_dmma(const xkb_gemm_args* a, cudaStream_t st, const int* run_if, int ksplit,
+                       int sk_ctas = 0) {
   using S = typename St<T>::S;
   constexpr int W = St<T>::W;
   const int es = (int)sizeof(S);
@@ -436,7 +663,43 @@ static int launch_dmma(const xkb_gemm_args* a, cudaStream_t st, const int* run_i
   p.kt_slice = (p.ktiles + p.ksplit - 1) / p.ksplit;
   p.ksplit = (p.ktiles + p.kt_slice - 1) / p.kt_slice;  // no empty slice
   p.ws = nullptr;
+  p.sk_ctas = 0;
+  p.sk_slots = 0;
   const size_t smem = kStages * (size_t)(BM + BN) * kBK * sizeof(T) + 2 * kStages * 8 + 128;
+  if constexpr (BN == 128) {  // stream-K: the big tiles only
+  if (sk_ctas > 0) {
+    if (a->uplo != XKB_FULL) return XKB_EINVAL;
+    const long ntiles = (long)p.tiles_m * p.tiles_n;
+    const long tot = ntiles * p.ktiles;
+    p.ksplit = 1;
+    p.sk_ctas = (int)std::max<long>(1, std::min<long>(sk_ctas, tot));
+    // a tile meets at most ceil(ktiles / shortest share) + 1 CTAs
+    const long share = std::max<long>(1, tot / p.sk_ctas);
+    p.sk_slots = (int)((p.ktiles + share - 1) / share + 1);
+    auto kern = k_gemm_dmma_sk<T, BM, BN, A_KC, B_KC>;
+    static bool sk_attr = false;  // one per instantiation
+    if (!sk_attr) {
+      if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+          cudaSuccess)
+        return XKB_ECUDA;
+      sk_attr = true;
+    }
+    const size_t ws =
+        (size_t)ntiles * p.sk_slots * AccShape<T, BM, BN>::NREG * kThreads * sizeof(double);
+    if (cudaMallocAsync(reinterpret_cast<void**>(&p.ws), ws, st) != cudaSuccess) {
+      cudaGetLastError();
+      return XKB_ENOMEM;
+    }
+    const long long tv = evlog_kern_begin(st, "k_gemm_dmma_sk+k_gemm_sk_reduce");
+    kern<<<(unsigned)p.sk_ctas, kThreads, smem, st>>>(tA, tB, p);
+    const dim3 rg((unsigned)ntiles, (unsigned)(AccShape<T, BM, BN>::MF * AccShape<T, BM, BN>::NF));
+    k_gemm_sk_reduce<T, BM, BN><<<rg, kThreads, 0, st>>>(p);
+    cudaFreeAsync(p.ws, st);
+    evlog_kern_end(tv, st);
+    count_launch(2);
+    return cudaPeekAtLastError() == cudaSuccess ? XKB_OK : XKB_ECUDA;
+  }
+  }
   auto kern = k_gemm_dmma<T, BM, BN, A_KC, B_KC>;
   static bool attr_done = false;  // one per instantiation
   if (!attr_done) {
@@ -468,12 +731,12 @@ static int launch_dmma(const xkb_gemm_args* a, cudaStream_t st, const int* run_i
 
 template <class T, int BM, int BN>
 static int dispatch_ops(const xkb_gemm_args* a, cudaStream_t st, const int* run_if,
-                        int ksplit = 1) {
+                        int ksplit = 1, int sk_ctas = 0) {
   const bool akc = a->opA != XKB_OP_N, bkc = a->opB == XKB_OP_N;
-  if (akc && bkc) return launch_dmma<T, BM, BN, true, true>(a, st, run_if, ksplit);
-  if (akc && !bkc) return launch_dmma<T, BM, BN, true, false>(a, st, run_if, ksplit);
-  if (!akc && bkc) return launch_dmma<T, BM, BN, false, true>(a, st, run_if, ksplit);
-  return launch_dmma<T, BM, BN, false, false>(a, st, run_if, ksplit);
+  if (akc && bkc) return launch_dmma<T, BM, BN, true, true>(a, st, run_if, ksplit, sk_ctas);
+  if (akc && !bkc) return launch_dmma<T, BM, BN, true, false>(a, st, run_if, ksplit, sk_ctas);
+  if (!akc && bkc) return launch_dmma<T, BM, BN, false, true>(a, st, run_if, ksplit, sk_ctas);
+  return launch_dmma<T, BM, BN, false, false>(a, st, run_if, ksplit, sk_ctas);
 }
 
 // Split-K factor for big tiles when they alone leave SMs idle: as many
@@ -518,8 +781,22 @@ static int dispatch_type(const xkb_gemm_args* a, cudaStream_t st, const int* run
   // too few big tiles for the SMs: split their k range when K allows
   const long tiles_small =
       (long)((a->M + BMb / 2 - 1) / (BMb / 2)) * ((a->N + BNb / 2 - 1) / (BNb / 2));
-  const int ks = force ? 1 : splitk_factor(tiles_big, tiles_small, (a->K + kBK - 1) / kBK);
-  if (ks > 1) return dispatch_ops<T, BMb, BNb>(a, st, run_if, ks);
+  const long ktiles = (a->K + kBK - 1) / kBK;
+  const int ks = force ? 1 : splitk_factor(tiles_big, tiles_small, ktiles);
+  if (ks > 1) {
+    // Stream-K instead when C is full (tuning key gemm_streamk, default 1)
+    // and split-K's ks x tiles CTAs fill less than gemm_sk_fill (0.8) of the
+    // SMs: one CTA per SM, each with an equal share of the tiles' k-steps (at
+    // least gemm_sk_min_kt of them).  Measured on a B200: 640 x 1280 x 2048
+    // (50 tiles, split-K 2 on 100 CTAs) 168 -> 136 us; where split-K already
+    // filled 86-97 % of the SMs the two were within 5 % either way.
+    const long min_kt = std::max(1L, (long)tune("gemm_sk_min_kt", 8.0));
+    const long sk = std::min<long>(sm_count(), tiles_big * ktiles / min_kt);
+    if (a->uplo == XKB_FULL && tune("gemm_streamk", 1.0) != 0.0 && sk > tiles_big * ks &&
+        (double)(tiles_big * ks) < tune("gemm_sk_fill", 0.8) * (double)sm_count())
+      return dispatch_ops<T, BMb, BNb>(a, st, run_if, 1, (int)sk);
+    return dispatch_ops<T, BMb, BNb>(a, st, run_if, ks);
+  }
   return dispatch_ops<T, BMb / 2, BNb / 2>(a, st, run_if);
 }
 
