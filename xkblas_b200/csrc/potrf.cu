@@ -107,7 +107,7 @@ __global__ void __launch_bounds__(kPoThreads, 1)
     for (int j = 0; j < 8; ++j) {
       const double d = __shfl_sync(0xffffffffu, ar[j], j);
       if (!(d > 0.0) && lane == 0 && j < w && info) atomicCAS(info, 0, col0 + b + j + 1);
-      const double ljj = sqrt(d), r = 1.0 / ljj;
+      const double r = rsqrt(d), ljj = d * r;  // one long-latency operation on the chain
       rinv[j] = r;
       if (l == j) {
         ar[j] = ljj;
