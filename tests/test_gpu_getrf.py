@@ -51,17 +51,25 @@ def test_getrf_nopiv_factor(xk, dt, n):
     assert np.abs(A.astype(up) - ref).max() <= 64 * n * EPS[dt] * max(1.0, np.abs(ref).max())
 
 
-def test_getrf_nopiv_tensor_op_mode(xk):
+@pytest.mark.parametrize("mode", [1, 3])
+def test_getrf_nopiv_tensor_op_mode(xk, mode):
     """Tensor-op mode: couplings with all dimensions >= 2048 run in the Ozaki
-    form; same backward-error bound."""
+    form, in the recursive form (tuning key getrf_blocked = 1) and in the
+    hybrid (= 3: the top coupling in the Ozaki form, the halves blocked);
+    same backward-error bound."""
     n = 4200
     A0 = _dd(n, np.float64, 37)
     A = A0.copy(order="F")
+    lib = xk.lib()
     xk.set_modemath(xk.XKBLAS_TENSOR_OP_MATH)
+    lib.xkb_tune_set(b"getrf_blocked", float(mode))
     try:
+        c0 = xk.ozaki_counts()[0]
         assert _getrf(xk, A) == 0
+        assert xk.ozaki_counts()[0] > c0
     finally:
         xk.set_modemath(xk.XKBLAS_DEFAULT_MATH)
+        lib.xkb_tune_set(b"getrf_blocked", 3.0)
     L = np.tril(A, -1) + np.eye(n)
     U = np.triu(A)
     assert np.abs(L @ U - A0).max() <= 16 * np.abs(A0).max() * n * EPS[np.float64]
@@ -110,6 +118,6 @@ def test_getrf_nopiv_blocked_and_recursive_forms(xk, dt):
             Z[776, 776] = 0.0
             assert _getrf(xk, Z) == 777, (mode, nb)
     finally:
-        lib.xkb_tune_set(b"getrf_blocked", 1.0)
+        lib.xkb_tune_set(b"getrf_blocked", 3.0)
         lib.xkb_tune_set(b"getrf_nb", 512.0)
         lib.xkb_tune_set(b"getrf_shrink", 12.0)

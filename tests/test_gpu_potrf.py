@@ -63,13 +63,14 @@ def test_potrf_factor(xk, dt, uplo, n):
 
 
 @pytest.mark.parametrize("dt,uplo", [(np.float64, LO), (np.complex128, UP)])
-@pytest.mark.parametrize("mode", [0, 2])
+@pytest.mark.parametrize("mode", [0, 2, 3])
 def test_potrf_tensor_op_mode(xk, dt, uplo, mode):
     """XKBLAS_TENSOR_OP_MATH: in the recursive form (tuning key
     potrf_blocked = 0) the top-level trailing update and the panel solve's
     coupling updates (all dimensions >= 2048 at n = 4200) run in the Ozaki
-    INT8 form; the blocked form (= 2, the default) is also checked.  Same
-    backward-error bound as the plain factorization."""
+    INT8 form; the blocked form (= 2) and the hybrid (= 3: the recursion's
+    top update in the Ozaki form, the two halves blocked) are also checked.
+    Same backward-error bound as the plain factorization."""
     n = 4200
     A0 = _spd(n, dt, 11)
     A = A0.copy(order="F")
@@ -79,11 +80,11 @@ def test_potrf_tensor_op_mode(xk, dt, uplo, mode):
     try:
         c0 = xk.ozaki_counts()[0]
         assert _potrf(xk, A, uplo) == 0
-        if mode == 0:
+        if mode in (0, 3):  # the recursion (3: down to 4096 rows, blocked below)
             assert xk.ozaki_counts()[0] > c0  # Ozaki contractions ran
     finally:
         xk.set_modemath(xk.XKBLAS_DEFAULT_MATH)
-        lib.xkb_tune_set(b"potrf_blocked", 2.0)
+        lib.xkb_tune_set(b"potrf_blocked", 3.0)
     up = np.complex128 if np.iscomplexobj(A0) else np.float64
     if uplo == LO:
         L = np.tril(A)
@@ -149,6 +150,6 @@ def test_potrf_blocked_and_recursive_forms(xk, dt, uplo):
             B[776, 776] = -5.0
             assert _potrf(xk, B, uplo) == 777, (mode, nb)
     finally:
-        lib.xkb_tune_set(b"potrf_blocked", 2.0)
+        lib.xkb_tune_set(b"potrf_blocked", 3.0)
         lib.xkb_tune_set(b"potrf_nb", 512.0)
         lib.xkb_tune_set(b"potrf_shrink", 12.0)

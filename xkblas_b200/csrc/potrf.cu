@@ -276,7 +276,12 @@ struct PotrfCtx {
   long lda;
   int* info;
   cudaStream_t st;
+  // hybrid form: the recursion hands sub-problems of at most blk_leaf rows to
+  // the blocked look-ahead form (widest block blk_nb); 0: recursion only
+  long blk_leaf = 0, blk_nb = 0;
 };
+
+static int factor_blocked(const PotrfCtx& c, long i0, long i1, long nb);
 
 template <class T>
 static int launch_leaf(const PotrfCtx& c, char* Ad, long n, long i0) {
@@ -339,6 +344,15 @@ static int factor(const PotrfCtx& c, long i0, long i1, bool la, bool pend) {
   const bool cplx = c.dt == XKB_C || c.dt == XKB_Z;
   const long nmax = cplx ? PoShape<double2>::NMAX : PoShape<double>::NMAX;
   if (n <= nmax) return leaf(c, i0, n);  // never pending: callers fork only above nmax
+  if (c.blk_leaf > 0 && n <= c.blk_leaf && n > 2 * nmax) {
+    // hybrid: this sub-problem in the blocked form, after the caller's
+    // pending update of it
+    const SideStream& ss0 = side_stream(0);
+    if (pend && !side_join(ss0, ss0.s, c.st)) return XKB_ECUDA;
+    PotrfCtx cb = c;
+    cb.blk_leaf = 0;
+    return factor_blocked(cb, i0, i1, c.blk_nb);
+  }
   const long h = split_point(i0, i1);
   const long n1 = h - i0, n2 = i1 - h;
   int e;
@@ -556,18 +570,26 @@ extern "C" int xkb_cuda_potrf(int dtype, int uplo, int N, void* A, long lda, int
   c.ozaki = (dtype == XKB_D || dtype == XKB_Z) ? std::max(ozaki, 0) : 0;
   c.st = resolve_stream(stream);
   // Blocked look-ahead form (tuning key potrf_blocked: 0 off, 1 in plain
-  // mode, 2 in both modes, the default; widest block potrf_nb, in tensor-op
-  // mode potrf_nb_oz) or the recursive form.  In tensor-op mode the blocked
+  // mode, 2 in both modes; 3, the default: in plain mode, and in tensor-op
+  // mode the hybrid -- the recursion with Ozaki updates down to
+  // potrf_oz_leaf rows (4096), the blocked form below; widest block
+  // potrf_nb, in tensor-op mode potrf_nb_oz) or the recursive form.
+  // Measured on a B200, tensor-op DPOTRF 8192: hybrid 9.37 ms, blocked
+  // 10.14, recursive 12.64; 16384: 35.8, 58.2, 42.2 ms.  In tensor-op mode the blocked
   // form's updates (inner dimension = block width, 512) stay below the Ozaki
   // threshold; measured on a B200 it still beat the recursive form with
   // Ozaki updates at 8192 (10.2 vs 13.3 ms), whose panel solves and leaf
   // chain are exposed.
   const long nmax = (dtype == XKB_C || dtype == XKB_Z) ? PoShape<double2>::NMAX
                                                        : PoShape<double>::NMAX;
-  const int mode = (int)tune("potrf_blocked", 2.0);
+  const int mode = (int)tune("potrf_blocked", 3.0);
   const long nb = std::max(nmax, ((long)tune(c.ozaki ? "potrf_nb_oz" : "potrf_nb", 512.0) + 63) /
                                      64 * 64);
-  if (N > 2 * nmax && (mode == 2 || (mode == 1 && c.ozaki == 0)))
+  if (N > 2 * nmax && (mode == 2 || ((mode == 1 || mode == 3) && c.ozaki == 0)))
     return factor_blocked(c, 0, N, nb);
+  if (mode == 3 && c.ozaki > 0) {
+    c.blk_leaf = std::max(2 * nmax + 1, (long)tune("potrf_oz_leaf", 4096.0));
+    c.blk_nb = nb;
+  }
   return factor(c, 0, N, true, false);
 }
