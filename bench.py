@@ -238,6 +238,9 @@ def other_configs(lib, torch, dev, sp, stream):
     def timed(fn, reps, reset=None):
         ev0 = torch.cuda.Event(enable_timing=True)
         ev1 = torch.cuda.Event(enable_timing=True)
+        # the inputs were made on torch's default stream; the library's calls
+        # (and the resets) run on `stream`
+        torch.cuda.synchronize()
         if reset:
             reset()
         assert fn() == 0
