@@ -121,3 +121,57 @@ def test_concurrent_threads_sync_their_own_work(xk):
             assert _gemm_ratio(*g) <= 3.0
             R = O.trsm(O.LEFT, O.LOWER, O.NOTRANS, O.NONUNIT, 2.0, A, B0.copy(order="F"), nb=64)
             assert checks.trsm_ratio(B, R, A, A.shape[0], B.shape[1]) <= 10
+
+
+def test_concurrent_device_abi_factorizations(xk):
+    """Three threads, each on its own CUDA stream, call xkb_cuda_potrf (the
+    blocked form: side streams ordered by events) and xkb_cuda_trsm (two
+    groups of right-hand sides on side streams) at the same time, several
+    times over; every result is right.  The side streams are shared by the
+    threads, the events that order them are each thread's own."""
+    import ctypes
+    import torch
+    lib = xk.lib()
+    n, nrhs = 1100, 2304
+    work = []
+    for k in range(3):
+        g = torch.Generator(device="cuda").manual_seed(500 + k)
+        Bm = torch.rand(n, n, generator=g, device="cuda", dtype=torch.float64) - 0.5
+        A0 = Bm @ Bm.t() / n + torch.eye(n, device="cuda", dtype=torch.float64)
+        T = torch.tril(torch.rand(n, n, generator=g, device="cuda", dtype=torch.float64) - 0.5)
+        T += n * torch.eye(n, device="cuda", dtype=torch.float64)
+        Tcm = T.t().contiguous()  # column-major lower
+        R0 = torch.rand(nrhs, n, generator=g, device="cuda", dtype=torch.float64) - 0.5
+        work.append({"A0": A0, "A": A0.clone(), "Tcm": Tcm, "T": T, "R0": R0, "R": R0.clone(),
+                     "info": torch.zeros(1, dtype=torch.int32, device="cuda"),
+                     "st": torch.cuda.Stream()})
+    torch.cuda.synchronize()
+    al = (ctypes.c_double * 2)(1.0, 0.0)
+    alp = ctypes.cast(al, ctypes.POINTER(ctypes.c_double))
+
+    def worker(w):
+        def run():
+            sp = ctypes.c_void_p(w["st"].cuda_stream)
+            with torch.cuda.stream(w["st"]):
+                for _ in range(4):
+                    w["A"].copy_(w["A0"])
+                    w["R"].copy_(w["R0"])
+                    assert lib.xkb_cuda_potrf(1, 1, n, ctypes.c_void_p(w["A"].data_ptr()), n,
+                                              ctypes.c_void_p(w["info"].data_ptr()), 0, sp) == 0
+                    assert lib.xkb_cuda_trsm(1, 0, 1, 0, 0, n, nrhs, alp, w["Tcm"].data_ptr(), n,
+                                             w["R"].data_ptr(), n, 0, sp) == 0
+            w["st"].synchronize()
+        return run
+
+    errs = _run_threads([worker(w) for w in work])
+    assert not errs, errs
+    torch.cuda.synchronize()
+    assert lib.xkb_cuda_take_device_error() == 0
+    for w in work:
+        L = torch.triu(w["A"])  # column-major lower factor = row-major upper
+        r = (L.t() @ L - w["A0"]).abs().max().item() / w["A0"].abs().max().item()
+        assert r <= 16 * n * 2.0 ** -53, r
+        assert int(w["info"].item()) == 0
+        X = w["R"].t()  # column-major n x nrhs solution of T X = R0^T
+        res = (w["T"] @ X - w["R0"].t()).abs().max().item()
+        assert res <= 16 * n * 2.0 ** -53 * (n + 0.5) * max(1.0, X.abs().max().item()), res

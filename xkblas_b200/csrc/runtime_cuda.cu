@@ -87,40 +87,75 @@ cudaStream_t resolve_stream(void* s) {
 
 void count_launch(int n) { g_launches.fetch_add((uint64_t)n, std::memory_order_relaxed); }
 
+// Events of one host thread (created on its first use, destroyed when it
+// exits): the fork / join events of the side streams and the dependency
+// events of the blocked factorizations.  Per thread, so that calls made from
+// several threads at once never record over each other's events; the
+// streams themselves are shared.
+namespace {
+struct ThreadEvents {
+  cudaEvent_t side[kSideStreams][2] = {};
+  cudaEvent_t dep[8] = {};
+  bool side_ok[kSideStreams] = {}, dep_ok = false, dep_tried = false;
+  bool side_tried[kSideStreams] = {};
+  ~ThreadEvents() {
+    for (auto& p : side)
+      for (cudaEvent_t e : p)
+        if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : dep)
+      if (e) cudaEventDestroy(e);
+    cudaGetLastError();  // at process exit the runtime may already be gone
+  }
+};
+ThreadEvents& thread_events() {
+  thread_local ThreadEvents te;
+  return te;
+}
+}  // namespace
+
 const SideStream& side_stream(int slot) {
-  static SideStream ss[kSideStreams];
+  static cudaStream_t streams[kSideStreams] = {};
   static std::once_flag once[kSideStreams];
   slot = std::max(0, std::min(kSideStreams - 1, slot));
   std::call_once(once[slot], [slot] {
-    SideStream t;
     int least = 0, greatest = 0;
     if (slot >= kHiStream && cudaDeviceGetStreamPriorityRange(&least, &greatest) != cudaSuccess) {
       cudaGetLastError();
       greatest = 0;
     }
-    if (cudaStreamCreateWithPriority(&t.s, cudaStreamNonBlocking,
-                                     slot >= kHiStream ? greatest : 0) != cudaSuccess ||
-        cudaEventCreateWithFlags(&t.fork, cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&t.join, cudaEventDisableTiming) != cudaSuccess) {
+    if (cudaStreamCreateWithPriority(&streams[slot], cudaStreamNonBlocking,
+                                     slot >= kHiStream ? greatest : 0) != cudaSuccess) {
       cudaGetLastError();
-      return;
+      streams[slot] = nullptr;
     }
-    ss[slot] = t;
   });
-  return ss[slot];
+  // the calling thread's fork / join events for this stream
+  thread_local SideStream ss[kSideStreams];
+  ThreadEvents& te = thread_events();
+  if (!te.side_tried[slot]) {
+    te.side_tried[slot] = true;
+    te.side_ok[slot] =
+        cudaEventCreateWithFlags(&te.side[slot][0], cudaEventDisableTiming) == cudaSuccess &&
+        cudaEventCreateWithFlags(&te.side[slot][1], cudaEventDisableTiming) == cudaSuccess;
+    if (!te.side_ok[slot]) cudaGetLastError();
+  }
+  SideStream& t = ss[slot];
+  t.s = te.side_ok[slot] ? streams[slot] : nullptr;
+  t.fork = te.side[slot][0];
+  t.join = te.side[slot][1];
+  return t;
 }
 
 cudaEvent_t* dep_events() {
-  static cudaEvent_t ev[8];
-  static bool ok = false;
-  static std::once_flag once;
-  std::call_once(once, [] {
-    ok = true;
-    for (auto& e : ev)
-      if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) ok = false;
-    if (!ok) cudaGetLastError();
-  });
-  return ok ? ev : nullptr;
+  ThreadEvents& te = thread_events();
+  if (!te.dep_tried) {
+    te.dep_tried = true;
+    te.dep_ok = true;
+    for (auto& e : te.dep)
+      if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) te.dep_ok = false;
+    if (!te.dep_ok) cudaGetLastError();
+  }
+  return te.dep_ok ? te.dep : nullptr;
 }
 
 cudaStream_t side_fork(const SideStream& side, cudaStream_t st) {
