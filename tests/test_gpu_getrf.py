@@ -51,14 +51,15 @@ def test_getrf_nopiv_factor(xk, dt, n):
     assert np.abs(A.astype(up) - ref).max() <= 64 * n * EPS[dt] * max(1.0, np.abs(ref).max())
 
 
+@pytest.mark.parametrize("dt", [np.float64, np.complex128])
 @pytest.mark.parametrize("mode", [1, 3])
-def test_getrf_nopiv_tensor_op_mode(xk, mode):
+def test_getrf_nopiv_tensor_op_mode(xk, mode, dt):
     """Tensor-op mode: couplings with all dimensions >= 2048 run in the Ozaki
     form, in the recursive form (tuning key getrf_blocked = 1) and in the
     hybrid (= 3: the top coupling in the Ozaki form, the halves blocked);
     same backward-error bound."""
     n = 4200
-    A0 = _dd(n, np.float64, 37)
+    A0 = _dd(n, dt, 37)
     A = A0.copy(order="F")
     lib = xk.lib()
     xk.set_modemath(xk.XKBLAS_TENSOR_OP_MATH)
