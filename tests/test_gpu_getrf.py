@@ -97,15 +97,17 @@ def test_getrf_nopiv_argument_codes(xk):
 def test_getrf_nopiv_blocked_and_recursive_forms(xk, dt):
     """The blocked look-ahead form (tuning key getrf_blocked = 1, several
     block widths, widths shrinking along the factorization, a ragged last
-    block) and the recursive form (= 0) meet the same backward-error bound,
-    and both report a zero pivot in a late block."""
+    block), the recursive form (= 0) and the hybrid (= 3 with getrf_oz_leaf
+    = 512: the recursion's top coupling, blocked halves) meet the same
+    backward-error bound, and all report a zero pivot in a late block."""
     lib = xk.lib()
     n = 1100
     up = np.complex128 if np.issubdtype(dt, np.complexfloating) else np.float64
     try:
         for mode, nb, shrink in ((1, 64, 12), (1, 128, 12), (1, 320, 12), (1, 512, 2),
-                                 (0, 256, 12)):
+                                 (0, 256, 12), (3, 256, 12)):
             lib.xkb_tune_set(b"getrf_blocked", float(mode))
+            lib.xkb_tune_set(b"getrf_oz_leaf", 512.0 if mode == 3 else 4096.0)
             lib.xkb_tune_set(b"getrf_nb", float(nb))
             lib.xkb_tune_set(b"getrf_shrink", float(shrink))
             A0 = _dd(n, dt, 50 + nb)
@@ -122,3 +124,4 @@ def test_getrf_nopiv_blocked_and_recursive_forms(xk, dt):
         lib.xkb_tune_set(b"getrf_blocked", 3.0)
         lib.xkb_tune_set(b"getrf_nb", 512.0)
         lib.xkb_tune_set(b"getrf_shrink", 12.0)
+        lib.xkb_tune_set(b"getrf_oz_leaf", 4096.0)

@@ -559,8 +559,8 @@ extern "C" int xkb_cuda_getrf_nopiv(int dtype, int N, void* A, long lda, int* d_
   c.info = d_info;
   c.st = resolve_stream(stream);
   // Blocked look-ahead form (tuning key getrf_blocked: 0 off, 1 in plain
-  // mode, 2 in both modes; 3, the default: in plain mode, and in tensor-op
-  // mode the hybrid -- the recursion with Ozaki updates down to
+  // mode, 2 in both modes; 3, the default: the hybrid in both modes -- the
+  // recursion (its couplings in the Ozaki form in tensor-op mode) down to
   // getrf_oz_leaf rows (4096), the blocked form below; widest block
   // getrf_nb, in tensor-op mode getrf_nb_oz) or the recursive form.
   // Measured on a B200, tensor-op DGETRF 8192: hybrid 14.4 ms, recursive
@@ -570,9 +570,9 @@ extern "C" int xkb_cuda_getrf_nopiv(int dtype, int N, void* A, long lda, int* d_
   const int mode = (int)tune("getrf_blocked", 3.0);
   const long nb = std::max(nmax, ((long)tune(c.ozaki ? "getrf_nb_oz" : "getrf_nb",
                                              c.ozaki ? 2048.0 : 512.0) + 63) / 64 * 64);
-  if (N > 2 * nmax && (mode == 2 || ((mode == 1 || mode == 3) && c.ozaki == 0)))
+  if (N > 2 * nmax && (mode == 2 || (mode == 1 && c.ozaki == 0)))
     return factor_blocked(c, 0, N, nb);
-  if (mode == 3 && c.ozaki > 0) {
+  if (mode == 3) {  // in plain mode too: DMMA couplings (8192: 18.3 against 18.9 ms)
     c.blk_leaf = std::max(2 * nmax + 1, (long)tune("getrf_oz_leaf", 4096.0));
     c.blk_nb = std::max(nmax, ((long)tune("getrf_nb", 512.0) + 63) / 64 * 64);
   }
