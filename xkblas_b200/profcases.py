@@ -1,6 +1,6 @@
 """Small, self-contained cases for profiling single kernels with ncu:
 
-    python -m xkblas_b200.profcases dmma|update256|ozaki|ozaki2|ozaki8192|splitk|repack|trsm|potrf|potrf8192|getrf|getrf8192|batch|copy
+    python -m xkblas_b200.profcases dmma|update256|ozaki|ozaki2|ozaki8192|splitk|streamk|repack|trsm|potrf|potrf8192|getrf|getrf8192|batch|copy
 
 dmma    DGEMM NN 4096^3 through xkb_cuda_gemm (k_gemm_dmma), two calls
 update256  the Cholesky's first trailing update at 8192 with 256-wide
@@ -12,6 +12,8 @@ ozaki8192  DGEMM NN 8192^3, xkb_cuda_ozaki_gemm with the count chosen on the
         traffic of k_oz_gemm at a size whose residue planes exceed L2
 splitk  DGEMM NN 512 x 512 x 4096 through xkb_cuda_gemm: 16 output tiles,
         split-K (k_gemm_dmma slices + k_gemm_splitk)
+streamk DGEMM TN 640 x 1280 x 2048 through xkb_cuda_gemm: 50 output tiles,
+        stream-K (k_gemm_dmma_sk pieces + k_gemm_sk_reduce), two calls
 repack  the DGEMM with lda = ldb = 4097 (k_repack, then k_gemm_dmma)
 trsm    DTRSM L/L/N/N 4096 x 4096, diagonally dominant (k_trsm_block, GEMMs)
 potrf   DPOTRF lower 4096 (k_potrf_block, k_trsm_block, GEMMs)
@@ -59,6 +61,14 @@ def main(case):
         keep += [P, C]
         ga = _GemmArgs(1, 0, 1, m, m, k, P.data_ptr(), m, P.data_ptr(), m, C.data_ptr(), m)
         ga.alpha[0], ga.beta[0], ga.uplo = -1.0, 1.0, 1
+        for _ in range(2):
+            assert lib.xkb_cuda_gemm(ctypes.byref(ga), sp) == 0
+    elif case == "streamk":
+        m, n, k = 640, 1280, 2048
+        A, B, C = rnd(k, m), rnd(k, n), rnd(m, n)  # op(A) = A^T: A stored k x m
+        keep += [A, B, C]
+        ga = _GemmArgs(1, 1, 0, m, n, k, A.data_ptr(), k, B.data_ptr(), k, C.data_ptr(), m)
+        ga.alpha[0] = ga.beta[0] = 1.0
         for _ in range(2):
             assert lib.xkb_cuda_gemm(ctypes.byref(ga), sp) == 0
     elif case in ("ozaki8192", "splitk"):
