@@ -16,6 +16,7 @@
 // blocks become NaN as in LAPACK's unchecked use -- but the first failing
 // column (1-based, over the whole matrix) is recorded in *d_info (0 = none).
 #include <algorithm>
+#include <type_traits>
 
 #include "dmma_common.cuh"
 #include "xkb_dev.cuh"
@@ -24,16 +25,24 @@ namespace xkb {
 
 // Diagonal blocks of up to NMAX (128 real, 64 complex) columns are factored
 // by one CTA with the block in shared memory (FP64), 8 columns per step:
-//   1. warp 0 factors the 8 x 8 diagonal block in registers (lane l holds row
-//      l; per column: pivot by shuffle, square root, reciprocal, rank-1
-//      update by shuffles) and forms the inverse of that factor (lane c
-//      solves for column c);
-//   2. all warps solve the panel below, L(rows, s) = A(rows, s) L_ss^-H,
-//      with FP64 DMMA (16 x 8 tiles, K = 8);
-//   3. all warps apply the rank-8 update to the trailing lower triangle,
-//      A(i, j) -= L(i, s) L(j, s)^H, with DMMA tiles that meet the triangle.
-// Same operations as the blocked right-looking Cholesky; the 8 x 8 panel
-// solve goes through the explicit inverse of the 8 x 8 factor.
+//   1. warp 0 factors the 8 x 8 diagonal block in registers: lane
+//      (r, k) = (lane >> 3, lane & 7) holds entries (r, k) and (r + 4, k);
+//      per column j the pivot and the column come by shuffles, then the
+//      reciprocal square root, the scaling and the rank-1 update of the
+//      entries right of j;
+//   2. the panel below, L(i, s) = A(i, s) L_ss^-H, by substitution, one
+//      thread per row (8 dependent steps, products with the reciprocal
+//      pivots);
+//   3. the rank-8 update of the trailing lower triangle,
+//      A(i, j) -= L(i, s) L(j, s)^H, with DMMA 16 x 8 tiles that meet the
+//      triangle, two tiles per warp in flight; warp 0 updates the tile
+//      holding the next diagonal block and factors that block while warps
+//      1..7 update the rest (look-ahead).
+// Same operations as the blocked right-looking Cholesky.  The loops over
+// columns are not unrolled: the kernel runs once per launch on an SM whose
+// instruction cache is cold, and a fully unrolled 8 x 8 factor paid about
+// 19k cycles of instruction fetch on its first pass (clock64 stamps: 22.5k
+// cycles cold, 3.75k warm).
 constexpr int kPoThreads = 256;
 
 template <class T>
@@ -55,20 +64,41 @@ __global__ void __launch_bounds__(kPoThreads, 1)
   constexpr bool CP = Sh::CP;
   constexpr int LD = Sh::LD;
   constexpr int W = CP ? 2 : 1;
+  constexpr unsigned FULL = 0xffffffffu;
   extern __shared__ double sm_po[];
   double* Xr = sm_po;  // L(i, k) at X[k * LD + i], lower part only
   double* Xi = Xr + (CP ? Sh::COLS * LD : 0);
   double* Lsr = sm_po + (size_t)Sh::PL * Sh::COLS * LD;  // 8 x 8 factor, [i][k]
   double* Lsi = Lsr + 64;
-  double* Vr = Lsr + Sh::PL * 64;  // its inverse, [i][k]
-  double* Vi = Vr + 64;
+  double* Rv = Lsr + Sh::PL * 64;  // reciprocals of its diagonal
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int g = lane >> 2, t = lane & 3;
 
-  // ---- load the effective lower triangle (upper: L = U^H); loads in
-  // groups of 8 per thread before their stores ----
+  // ---- load the effective lower triangle (upper: L = U^H) ----
+  // Real lower blocks with 16-byte aligned columns: every 16-byte piece of
+  // the lower triangle's columns is copied by cp.async at once (one memory
+  // latency for the whole block); the rows and columns past n are zeroed.
+  // Pieces that straddle the diagonal also bring the element above it,
+  // which nothing reads (every tile update stores only its lower part).
+  // Other blocks: loads in groups of 8 per thread before their stores.
+  bool fast = false;
+  if constexpr (!CP && std::is_same<S, double>::value) {
+    fast = !upper && (n % 2) == 0 && (lda % 2) == 0 &&
+           (reinterpret_cast<uintptr_t>(A) % 16) == 0;
+  }
+  if constexpr (!CP && std::is_same<S, double>::value) if (fast) {
+    for (int k = warp; k < n; k += kPoThreads / 32)
+      for (int i = (k & ~1) + 2 * lane; i < n; i += 64)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(Xr + k * LD + i)),
+                     "l"(A + (size_t)i + (size_t)k * lda)
+                     : "memory");
+    asm volatile("cp.async.commit_group;" ::: "memory");
+    for (int k = warp; k < Sh::COLS; k += kPoThreads / 32)
+      for (int i = (k < n ? n : 0) + lane; i < LD; i += 32) Xr[k * LD + i] = 0.0;
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+  }
   constexpr int GRP = 8;
-  for (int e0 = 0; e0 < Sh::COLS * LD; e0 += kPoThreads * GRP) {
+  for (int e0 = 0; !fast && e0 < Sh::COLS * LD; e0 += kPoThreads * GRP) {
     double vr[GRP], vi[GRP];
 #pragma unroll
     for (int q = 0; q < GRP; ++q) {
@@ -91,182 +121,204 @@ __global__ void __launch_bounds__(kPoThreads, 1)
     }
   }
 
-  // warp 0: factor the 8 x 8 diagonal block at b (final values in X) and
-  // invert the factor into V
+  // warp 0: factor the 8 x 8 diagonal block at b (final values in X, the
+  // strictly lower part of the factor in Ls, the reciprocals of its diagonal
+  // in Rv).  Every lane holds the whole triangle and computes the same
+  // factor, so the chain per column is the reciprocal square root, one
+  // product and one update (no shuffles); lane 0 stores.  Rows past the block
+  // (w < 8) are identity rows.
   auto diag_factor = [&](int b) {
     const int w = min(8, n - b);
-    const int l = lane & 7;  // lanes 8..31 mirror lanes 0..7 (shuffles span the warp)
-    double ar[8], ai[8], rinv[8];
+    double ar[8][8], ai[8][8];
 #pragma unroll
-    for (int k = 0; k < 8; ++k) {
-      const bool in = k <= l && l < w;
-      ar[k] = in ? Xr[(b + k) * LD + b + l] : (k == l ? 1.0 : 0.0);
-      ai[k] = (in && CP) ? Xi[(b + k) * LD + b + l] : 0.0;
-    }
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+      for (int k = 0; k <= i; ++k) {
+        ar[i][k] = i < w ? Xr[(b + k) * LD + b + i] : (k == i ? 1.0 : 0.0);
+        ai[i][k] = (CP && i < w && k < i) ? Xi[(b + k) * LD + b + i] : 0.0;
+      }
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
-      const double d = __shfl_sync(0xffffffffu, ar[j], j);
+      const double d = ar[j][j];
       if (!(d > 0.0) && lane == 0 && j < w && info) atomicCAS(info, 0, col0 + b + j + 1);
-      const double r = rsqrt(d), ljj = d * r;  // one long-latency operation on the chain
-      rinv[j] = r;
-      if (l == j) {
-        ar[j] = ljj;
-        ai[j] = 0.0;
-      } else if (l > j) {
-        ar[j] *= r;
-        ai[j] *= r;
+      const double rj = rsqrt(d);
+      ar[j][j] = d * rj;
+      if (lane == 0) Rv[j] = rj;
+#pragma unroll
+      for (int i = j + 1; i < 8; ++i) {
+        ar[i][j] *= rj;
+        if (CP) ai[i][j] *= rj;
       }
 #pragma unroll
-      for (int k = j + 1; k < 8; ++k) {
-        const double vr = __shfl_sync(0xffffffffu, ar[j], k);  // L(k, j)
-        const double vi = CP ? __shfl_sync(0xffffffffu, ai[j], k) : 0.0;
-        if (l >= k) {  // A(l, k) -= L(l, j) conj(L(k, j))
-          ar[k] -= ar[j] * vr + ai[j] * vi;
-          if (CP) ai[k] -= ai[j] * vr - ar[j] * vi;
+      for (int k = j + 1; k < 8; ++k)
+#pragma unroll
+        for (int i = k; i < 8; ++i) {  // A(i, k) -= L(i, j) conj(L(k, j))
+          ar[i][k] -= ar[i][j] * ar[k][j] + (CP ? ai[i][j] * ai[k][j] : 0.0);
+          if (CP) ai[i][k] -= ai[i][j] * ar[k][j] - ar[i][j] * ai[k][j];
         }
-      }
     }
-    if (lane < 8) {
+    if (lane == 0) {
 #pragma unroll
-      for (int k = 0; k < 8; ++k) {
-        Lsr[l * 8 + k] = k <= l ? ar[k] : 0.0;
-        if (CP) Lsi[l * 8 + k] = k <= l ? ai[k] : 0.0;
-        if (k <= l && l < w) {
-          Xr[(b + k) * LD + b + l] = ar[k];
-          if (CP) Xi[(b + k) * LD + b + l] = ai[k];
-        }
-      }
-    }
-    __syncwarp();
-    if (lane < 8) {
-      // column c = lane of inv(L_ss): L_ss z = e_c, column form
-      const int c = lane;
-      double zr[8], zi[8];
+      for (int i = 0; i < 8; ++i)
 #pragma unroll
-      for (int i = 0; i < 8; ++i) {
-        zr[i] = i == c ? 1.0 : 0.0;
-        zi[i] = 0.0;
-      }
-#pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        if (j >= c) {
-          zr[j] *= rinv[j];  // the diagonal of the factor is real
-          zi[j] *= rinv[j];
-#pragma unroll
-          for (int i = j + 1; i < 8; ++i) {
-            const double lr = Lsr[i * 8 + j], li = CP ? Lsi[i * 8 + j] : 0.0;
-            zr[i] -= lr * zr[j] - li * zi[j];
-            if (CP) zi[i] -= lr * zi[j] + li * zr[j];
+        for (int k = 0; k <= i; ++k) {
+          if (k < i) {
+            Lsr[i * 8 + k] = ar[i][k];
+            if (CP) Lsi[i * 8 + k] = ai[i][k];
+          }
+          if (i < w) {
+            Xr[(b + k) * LD + b + i] = ar[i][k];
+            if (CP) Xi[(b + k) * LD + b + i] = k < i ? ai[i][k] : 0.0;
           }
         }
-      }
-#pragma unroll
-      for (int i = 0; i < 8; ++i) {
-        Vr[i * 8 + c] = zr[i];
-        if (CP) Vi[i * 8 + c] = zi[i];
-      }
     }
   };
 
   __syncthreads();
-  if (warp == 0) diag_factor(0);
-  __syncthreads();
+  // step -1 factors block 0; step s >= 0 solves panel s, updates the trailing
+  // triangle and factors block s + 1 (one call site of the unrolled factor:
+  // its code is fetched once)
   const int nsteps = (n + 7) / 8;
-  for (int s = 0; s < nsteps; ++s) {
+  for (int s = -1; s < nsteps; ++s) {
     const int b = 8 * s;
     const int r0 = b + 8, R = n - r0;
     if (R <= 0) break;
-    const int mt = (R + 15) / 16;
-    const int k0 = 2 * t, k1 = k0 + 1;
-    // 1. panel: L(i, b..b+7) = A(i, b..b+7) inv(L_ss)^H, in place
-    //    B operand (k, c) = conj(V(c, k))
-    for (int tile = warp; tile < mt; tile += kPoThreads / 32) {
-      const int m0 = r0 + tile * 16;
-      const double a_r[4] = {Xr[(b + k0) * LD + m0 + g], Xr[(b + k0) * LD + m0 + g + 8],
-                             Xr[(b + k1) * LD + m0 + g], Xr[(b + k1) * LD + m0 + g + 8]};
-      const double b_r[2] = {Vr[g * 8 + k0], Vr[g * 8 + k1]};
-      double dr[4] = {0.0, 0.0, 0.0, 0.0}, di[4] = {0.0, 0.0, 0.0, 0.0};
-      if constexpr (CP) {
-        const double a_i[4] = {Xi[(b + k0) * LD + m0 + g], Xi[(b + k0) * LD + m0 + g + 8],
-                               Xi[(b + k1) * LD + m0 + g], Xi[(b + k1) * LD + m0 + g + 8]};
-        const double a_ni[4] = {-a_i[0], -a_i[1], -a_i[2], -a_i[3]};
-        const double b_i[2] = {-Vi[g * 8 + k0], -Vi[g * 8 + k1]};  // conj
-        dmma_k8(dr, a_r, b_r);
-        dmma_k8(dr, a_ni, b_i);
-        dmma_k8(di, a_r, b_i);
-        dmma_k8(di, a_i, b_r);
-      } else {
-        dmma_k8(dr, a_r, b_r);
-      }
-      __syncwarp();  // all lanes read the tile before any lane writes it
+    if (s >= 0) {
+    // 1. panel: L(i, s) = A(i, s) L_ss^-H, in place, one thread per row:
+    //    x_j = (a_j - sum_{m<j} x_m conj(L(j, m))) / L(j, j)
+    for (int i = r0 + tid; i < n; i += kPoThreads) {
+      double xr[8], xi[8];
 #pragma unroll
-      for (int v = 0; v < 4; ++v) {
-        const int row = m0 + g + ((v >> 1) << 3), col = b + 2 * t + (v & 1);
-        Xr[col * LD + row] = dr[v];
-        if (CP) Xi[col * LD + row] = di[v];
+      for (int j = 0; j < 8; ++j) {
+        xr[j] = Xr[(b + j) * LD + i];
+        xi[j] = CP ? Xi[(b + j) * LD + i] : 0.0;
+      }
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const double rj = Rv[j];
+        xr[j] *= rj;
+        if (CP) xi[j] *= rj;
+#pragma unroll
+        for (int q = j + 1; q < 8; ++q) {
+          const double lr = Lsr[q * 8 + j], li = CP ? Lsi[q * 8 + j] : 0.0;
+          xr[q] -= xr[j] * lr + xi[j] * li;
+          if (CP) xi[q] -= xi[j] * lr - xr[j] * li;
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        Xr[(b + j) * LD + i] = xr[j];
+        if (CP) Xi[(b + j) * LD + i] = xi[j];
       }
     }
     __syncthreads();
+    }
     // 2. trailing update of the lower triangle: A(i, j) -= L(i, s) L(j, s)^H
-    //    over 16 x 8 tiles (i rows, j columns) meeting the triangle.  Tile 0
-    //    holds the next diagonal block: warp 0 updates it and factors that
-    //    block while warps 1..7 update the rest (look-ahead).
-    const int nt = (R + 7) / 8;
-    auto upd_tile = [&](int tile) {
-      const int ti = tile / nt, tj = tile % nt;
-      if (8 * tj > 16 * ti + 15) return;  // wholly above the diagonal (warp-uniform)
-      const int m0 = r0 + 16 * ti, n0 = r0 + 8 * tj;
-      const double a_r[4] = {-Xr[(b + k0) * LD + m0 + g], -Xr[(b + k0) * LD + m0 + g + 8],
-                             -Xr[(b + k1) * LD + m0 + g], -Xr[(b + k1) * LD + m0 + g + 8]};
+    //    over the 16 x 8 tiles (ti, tj) that meet it (tj < min(nt, 2 ti + 2)),
+    //    numbered row by row.  Tile 0 holds the next diagonal block: warp 0
+    //    updates it and factors that block while warps 1..7 take tiles
+    //    warp, warp + 7, ... (look-ahead).
+    const int mt = (R + 15) / 16, nt = (R + 7) / 8;
+    const int k0 = 2 * t, k1 = k0 + 1;
+    auto advance = [&](int& ti, int& tj, int step) {
+      tj += step;
+      while (ti < mt) {
+        const int cnt = min(nt, 2 * ti + 2);
+        if (tj < cnt) break;
+        tj -= cnt;
+        ++ti;
+      }
+    };
+    struct Frag {
+      double ar[4], ai[4], br[2], bi[2], cr[4], ci[4];
+      int m0, n0;
+    };
+    auto frag_load = [&](Frag& f, int ti, int tj) {
+      f.m0 = r0 + 16 * ti;
+      f.n0 = r0 + 8 * tj;
+      const int m0 = f.m0, n0 = f.n0;
+      f.ar[0] = -Xr[(b + k0) * LD + m0 + g];
+      f.ar[1] = -Xr[(b + k0) * LD + m0 + g + 8];
+      f.ar[2] = -Xr[(b + k1) * LD + m0 + g];
+      f.ar[3] = -Xr[(b + k1) * LD + m0 + g + 8];
       // B (k, c) = conj(L(n0 + c, b + k))
-      const double b_r[2] = {Xr[(b + k0) * LD + n0 + g], Xr[(b + k1) * LD + n0 + g]};
-      double cr[4], ci[4];
+      f.br[0] = Xr[(b + k0) * LD + n0 + g];
+      f.br[1] = Xr[(b + k1) * LD + n0 + g];
 #pragma unroll
       for (int v = 0; v < 4; ++v) {
         const int row = m0 + g + ((v >> 1) << 3), col = n0 + 2 * t + (v & 1);
-        cr[v] = Xr[col * LD + row];
-        ci[v] = CP ? Xi[col * LD + row] : 0.0;
+        f.cr[v] = Xr[col * LD + row];
+        f.ci[v] = CP ? Xi[col * LD + row] : 0.0;
       }
       if constexpr (CP) {
-        // C += (-L_i)(conj L_j)
-        const double a_i[4] = {-Xi[(b + k0) * LD + m0 + g], -Xi[(b + k0) * LD + m0 + g + 8],
-                               -Xi[(b + k1) * LD + m0 + g], -Xi[(b + k1) * LD + m0 + g + 8]};
-        const double a_ni[4] = {-a_i[0], -a_i[1], -a_i[2], -a_i[3]};
-        const double b_i[2] = {-Xi[(b + k0) * LD + n0 + g], -Xi[(b + k1) * LD + n0 + g]};
-        dmma_k8(cr, a_r, b_r);
-        dmma_k8(cr, a_ni, b_i);
-        dmma_k8(ci, a_r, b_i);
-        dmma_k8(ci, a_i, b_r);
-      } else {
-        dmma_k8(cr, a_r, b_r);
+        f.ai[0] = -Xi[(b + k0) * LD + m0 + g];
+        f.ai[1] = -Xi[(b + k0) * LD + m0 + g + 8];
+        f.ai[2] = -Xi[(b + k1) * LD + m0 + g];
+        f.ai[3] = -Xi[(b + k1) * LD + m0 + g + 8];
+        f.bi[0] = -Xi[(b + k0) * LD + n0 + g];
+        f.bi[1] = -Xi[(b + k1) * LD + n0 + g];
       }
+    };
+    auto frag_mma = [&](Frag& f) {
+      if constexpr (CP) {
+        // C += (-L_i)(conj L_j)
+        const double a_ni[4] = {-f.ai[0], -f.ai[1], -f.ai[2], -f.ai[3]};
+        dmma_k8(f.cr, f.ar, f.br);
+        dmma_k8(f.cr, a_ni, f.bi);
+        dmma_k8(f.ci, f.ar, f.bi);
+        dmma_k8(f.ci, f.ai, f.br);
+      } else {
+        dmma_k8(f.cr, f.ar, f.br);
+      }
+    };
+    auto frag_store = [&](const Frag& f) {
 #pragma unroll
       for (int v = 0; v < 4; ++v) {
-        const int row = m0 + g + ((v >> 1) << 3), col = n0 + 2 * t + (v & 1);
+        const int row = f.m0 + g + ((v >> 1) << 3), col = f.n0 + 2 * t + (v & 1);
         if (row >= col) {  // lower part only (the diagonal's imaginary part is dropped at the end)
-          Xr[col * LD + row] = cr[v];
-          if (CP) Xi[col * LD + row] = ci[v];
+          Xr[col * LD + row] = f.cr[v];
+          if (CP) Xi[col * LD + row] = f.ci[v];
         }
       }
     };
     if (warp == 0) {
-      upd_tile(0);
-      __syncwarp();
-      diag_factor(r0);  // step s + 1 (its block is final after tile 0)
-    } else {
-      for (int tile = 1 + (warp - 1); tile < mt * nt; tile += kPoThreads / 32 - 1) upd_tile(tile);
+      if (s >= 0) {
+        Frag f;
+        frag_load(f, 0, 0);
+        frag_mma(f);
+        frag_store(f);
+        __syncwarp();
+      }
+      diag_factor(r0);  // block s + 1 (final after tile 0)
+    } else if (s >= 0) {
+      int ti = 0, tj = 0;
+      advance(ti, tj, warp);
+      while (ti < mt) {
+        int ti2 = ti, tj2 = tj;
+        advance(ti2, tj2, kPoThreads / 32 - 1);
+        const bool two = ti2 < mt;  // warp-uniform
+        Frag f0, f1;
+        frag_load(f0, ti, tj);
+        if (two) frag_load(f1, ti2, tj2);
+        frag_mma(f0);
+        if (two) frag_mma(f1);
+        frag_store(f0);
+        if (two) frag_store(f1);
+        ti = ti2;
+        tj = tj2;
+        if (two) advance(ti, tj, kPoThreads / 32 - 1);
+      }
     }
     __syncthreads();
   }
 
-  // ---- store the factor (the stored triangle only) ----
-  for (int e = tid; e < n * n; e += kPoThreads) {
-    const int i = e % n, k = e / n;
-    if (i < k) continue;
-    const size_t idx = upper ? (size_t)k + (size_t)i * lda : (size_t)i + (size_t)k * lda;
-    A[W * idx] = static_cast<S>(Xr[k * LD + i]);
-    if (CP) A[2 * idx + 1] = static_cast<S>(i == k ? 0.0 : (upper ? -Xi[k * LD + i] : Xi[k * LD + i]));
-  }
+  // ---- store the factor (the stored triangle only), column by column ----
+  for (int k = warp; k < n; k += kPoThreads / 32)
+    for (int i = k + lane; i < n; i += 32) {
+      const size_t idx = upper ? (size_t)k + (size_t)i * lda : (size_t)i + (size_t)k * lda;
+      A[W * idx] = static_cast<S>(Xr[k * LD + i]);
+      if (CP) A[2 * idx + 1] = static_cast<S>(i == k ? 0.0 : (upper ? -Xi[k * LD + i] : Xi[k * LD + i]));
+    }
 }
 
 struct PotrfCtx {

@@ -663,28 +663,46 @@ static int update(const TrsmCtx& c, long p0, long p1, long q0, long q1, const do
   return xkb_cuda_gemm(&g, c.st);
 }
 
-static int solve(const TrsmCtx& c, long i0, long i1, const double* alpha) {
+// The recursion below as a flat list of operations in issue order: a leaf
+// (diagonal block [i0, i0 + n)) or a coupling update (rows [p0, p1) from
+// the solved rows [q0, q1)); `scaled` marks the operations that apply the
+// caller's alpha (the others use 1).
+struct SolveOp {
+  bool leaf, scaled;
+  long p0, p1, q0, q1;  // leaf: [p0, p1) only
+};
+
+static void plan_solve(const TrsmCtx& c, long i0, long i1, bool scaled,
+                       std::vector<SolveOp>& ops) {
   const long n = i1 - i0;
   if (n <= kBlk) {
-    if (c.Winv) return leaf_gemm(c, i0, n, alpha);
-    // diagonal block of the effective triangle: one launch
-    const char* Ad = aptr(c, i0, i0);
-    char* Bd = c.left ? c.B + i0 * (long)c.es : c.B + i0 * c.ldb * (long)c.es;
-    return block_dispatch(c.dt, (int)n, c.nrhs, Ad, c.lda, c.swap, c.conj, c.lower_eff, c.unit,
-                          Bd, c.ldb, c.left ? 0 : 1, alpha, c.st);
+    ops.push_back({true, scaled, i0, i1, 0, 0});
+    return;
   }
   long h = i0 + ((n / 2 + kSplit - 1) / kSplit) * kSplit;
   if (h >= i1) h = i1 - kSplit;
-  const double one[2] = {1.0, 0.0};
-  int e;
   if (c.fwd) {
-    if ((e = solve(c, i0, h, alpha))) return e;
-    if ((e = update(c, h, i1, i0, h, alpha))) return e;
-    return solve(c, h, i1, one);
+    plan_solve(c, i0, h, scaled, ops);
+    ops.push_back({false, scaled, h, i1, i0, h});
+    plan_solve(c, h, i1, false, ops);
+    return;
   }
-  if ((e = solve(c, h, i1, alpha))) return e;
-  if ((e = update(c, i0, h, h, i1, alpha))) return e;
-  return solve(c, i0, h, one);
+  plan_solve(c, h, i1, scaled, ops);
+  ops.push_back({false, scaled, i0, h, h, i1});
+  plan_solve(c, i0, h, false, ops);
+}
+
+static int issue(const TrsmCtx& c, const SolveOp& op, const double* alpha) {
+  const double one[2] = {1.0, 0.0};
+  const double* al = op.scaled ? alpha : one;
+  if (!op.leaf) return update(c, op.p0, op.p1, op.q0, op.q1, al);
+  const long i0 = op.p0, n = op.p1 - op.p0;
+  if (c.Winv) return leaf_gemm(c, i0, n, al);
+  // diagonal block of the effective triangle: one launch
+  const char* Ad = aptr(c, i0, i0);
+  char* Bd = c.left ? c.B + i0 * (long)c.es : c.B + i0 * c.ldb * (long)c.es;
+  return block_dispatch(c.dt, (int)n, c.nrhs, Ad, c.lda, c.swap, c.conj, c.lower_eff, c.unit,
+                        Bd, c.ldb, c.left ? 0 : 1, al, c.st);
 }
 
 }  // namespace xkb
@@ -811,17 +829,25 @@ int trsm_entry(int dtype, int side, int uplo, int trans, int diag, int M, int N,
       forked[g] = g == 0 ? c.st : side_fork(side_stream(g), c.st);
       parts[g].st = forked[g];
     }
+    // the groups' operations are issued interleaved, one operation of every
+    // group in turn, so that all groups start together and run side by side
+    // to the end (issued group after group, the last group started one
+    // group's host issue time late and finished alone)
+    std::vector<SolveOp> ops;
+    plan_solve(c, 0, n, true, ops);
     int e = XKB_OK;
-    for (int g = 0; g < np; ++g) {
-      const int eg = solve(parts[g], 0, n, alpha);
-      if (!e) e = eg;
-    }
+    for (const SolveOp& op : ops)
+      for (int g = 0; g < np && !e; ++g) e = issue(parts[g], op, alpha);
     for (int g = 1; g < np; ++g)
       if (!side_join(side_stream(g), forked[g], c.st) && !e) e = XKB_ECUDA;
     return release(e);
   }
   if (int e = give_tmp(c)) return release(e);
-  return release(solve(c, 0, n, alpha));
+  std::vector<SolveOp> ops;
+  plan_solve(c, 0, n, true, ops);
+  for (const SolveOp& op : ops)
+    if (int e = issue(c, op, alpha)) return release(e);
+  return release(XKB_OK);
 }
 }  // namespace xkb
 
