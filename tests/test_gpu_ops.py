@@ -485,6 +485,36 @@ def test_trsm_inverse_leaves(xk, dt, side):
         lib.xkb_tune_set(b"trsm_inv_leaves", 1.0)
 
 
+@pytest.mark.parametrize("dt", [np.float64, np.complex128])
+def test_trsm_pair_leaves(xk, dt):
+    """Left, lower, op(A) = A with >= 2048 unknowns: with the tuning key
+    trsm_pair_leaves = 1 (default) every node of two diagonal blocks but the
+    first is applied through the inverse of its triangle (formed on a side
+    stream), = 0 keeps leaf, coupling update, leaf.  Ragged split points
+    (2148 unknowns), unit and non-unit diagonals: both meet the reference
+    bound."""
+    cplx = np.issubdtype(dt, np.complexfloating)
+    lib = xk.lib()
+    M, N = 2148, 160
+    seed = 1700
+    try:
+        for flag in (1.0, 0.0):
+            lib.xkb_tune_set(b"trsm_pair_leaves", flag)
+            for dg in (NONUNIT, UNIT):
+                A = np.asfortranarray((O.plrnt(M, M, seed, cplx) / M + np.eye(M)).astype(dt))
+                B0 = gen(M, N, seed + 1, dt)
+                seed += 2
+                alpha = scal(2.0 + 0.5j, dt)
+                B = B0.copy(order="F")
+                xk.trsm(LEFT, LO, N_, dg, alpha, A, B)
+                xk.invalidate_caches()
+                R = O.trsm(LEFT, LO, N_, dg, alpha, up(A), up(B0), nb=64)
+                r = checks.trsm_ratio(B, R, A, M, N)
+                assert r <= 10, (flag, dg, r)
+    finally:
+        lib.xkb_tune_set(b"trsm_pair_leaves", 1.0)
+
+
 @pytest.mark.parametrize("case", [
     # (dtype, M, N, K, opA, opB): few output tiles, long K
     (np.float64, 640, 1280, 2048, T_, N_),

@@ -114,8 +114,8 @@ __device__ __forceinline__ void cp_async_zfill(void* smem, const void* gmem, boo
 }
 
 // leaves != nullptr: the inverses of several diagonal blocks at once, block
-// y of the grid inverting the block of leaves[2y + 1] unknowns at
-// (leaves[2y], leaves[2y]) into columns y kBlk .. of B (ld kBlk): the
+// y of the grid inverting the block of leaves[3y + 1] unknowns at
+// (leaves[3y], leaves[3y]) into B + leaves[3y + 2] elements (ld ldb): the
 // right-hand sides are the identity's columns (B is only written).
 template <class T, bool LOWER>
 __global__ void __launch_bounds__(kBlkThreads, 2)
@@ -132,10 +132,10 @@ __global__ void __launch_bounds__(kBlkThreads, 2)
   S* B = B_;
   const bool ident = leaves != nullptr;
   if (ident) {
-    const int i0 = leaves[2 * blockIdx.y];
-    nb = nrhs = leaves[2 * blockIdx.y + 1];
+    const int i0 = leaves[3 * blockIdx.y];
+    nb = nrhs = leaves[3 * blockIdx.y + 1];
     A = A_ + (size_t)W * ((size_t)i0 + (size_t)i0 * (size_t)lda);
-    B = B_ + (size_t)W * (size_t)blockIdx.y * (size_t)kBlk * (size_t)ldb;
+    B = B_ + (size_t)W * (size_t)(unsigned)leaves[3 * blockIdx.y + 2];
     if ((int)blockIdx.x * CW >= nb) return;  // the whole CTA is past this block's columns
   }
   extern __shared__ double sm_blk[];
@@ -536,41 +536,31 @@ struct TrsmCtx {
   cudaStream_t st;
   int swap, conj, lower_eff;
   // inverse leaves (null: every leaf is a block solve): inv(E_l) of the
-  // effective triangle of leaf l at Winv + l kBlk^2 elements (ld kBlk),
-  // leaf l starting at unknown leaf_i0[l]; tmp holds one leaf's product
+  // effective triangle of the leaf (or pair of leaves) starting at unknown
+  // inv_at[2q] at Winv + inv_at[2q + 1] elements (ld ldw); tmp holds one
+  // leaf's product (ldw rows); pair p's inverse is complete once pair_ev[p]
+  // has fired
   const char* Winv = nullptr;
-  const std::vector<int>* leaf_i0 = nullptr;
+  long ldw = kBlk;
+  const std::vector<long>* inv_at = nullptr;
+  const cudaEvent_t* pair_ev = nullptr;
   char* tmp = nullptr;
 };
-
-// Leaves of the recursion below (the same split points): [i0, i1) pairs.
-static void collect_leaves(long i0, long i1, std::vector<int>& out) {
-  const long n = i1 - i0;
-  if (n <= kBlk) {
-    out.push_back((int)i0);
-    out.push_back((int)n);
-    return;
-  }
-  long h = i0 + ((n / 2 + kSplit - 1) / kSplit) * kSplit;
-  if (h >= i1) h = i1 - kSplit;
-  collect_leaves(i0, h, out);
-  collect_leaves(h, i1, out);
-}
 
 // A leaf applied through its inverse: X = alpha inv(E) B (left) or
 // X = alpha B inv(E)^T (right side: E is op(A)^T there), one GEMM into tmp
 // and a copy back into B.
 static int leaf_gemm(const TrsmCtx& c, long i0, long n, const double* alpha) {
-  const auto& L = *c.leaf_i0;
-  long l = 0;
-  while (2 * l < (long)L.size() && L[2 * l] != i0) ++l;
-  if (2 * l >= (long)L.size()) return XKB_EINVAL;
+  const auto& L = *c.inv_at;
+  size_t q = 0;
+  while (2 * q < L.size() && L[2 * q] != i0) ++q;
+  if (2 * q >= L.size()) return XKB_EINVAL;
   xkb_gemm_args g{};
   g.dtype = c.dt;
   g.alpha[0] = alpha[0];
   g.alpha[1] = alpha[1];
   g.uplo = XKB_FULL;
-  const char* Wl = c.Winv + (size_t)l * kBlk * kBlk * c.es;
+  const char* Wl = c.Winv + (size_t)L[2 * q + 1] * c.es;
   char* Bk = c.left ? c.B + i0 * (long)c.es : c.B + i0 * c.ldb * (long)c.es;
   size_t dpitch, spitch, width, height;
   if (c.left) {
@@ -579,13 +569,13 @@ static int leaf_gemm(const TrsmCtx& c, long i0, long n, const double* alpha) {
     g.K = (int)n;
     g.opA = XKB_OP_N;
     g.A = Wl;
-    g.lda = kBlk;
+    g.lda = c.ldw;
     g.opB = XKB_OP_N;
     g.B = Bk;
     g.ldb = c.ldb;
     g.C = c.tmp;
-    g.ldc = kBlk;
-    spitch = kBlk * (size_t)c.es;
+    g.ldc = c.ldw;
+    spitch = (size_t)c.ldw * c.es;
     width = n * (size_t)c.es;
     height = (size_t)c.nrhs;
   } else {
@@ -597,7 +587,7 @@ static int leaf_gemm(const TrsmCtx& c, long i0, long n, const double* alpha) {
     g.lda = c.ldb;
     g.opB = XKB_OP_T;
     g.B = Wl;
-    g.ldb = kBlk;
+    g.ldb = c.ldw;
     g.C = c.tmp;
     g.ldc = c.nrhs;
     spitch = (size_t)c.nrhs * c.es;
@@ -667,29 +657,37 @@ static int update(const TrsmCtx& c, long p0, long p1, long q0, long q1, const do
 // (diagonal block [i0, i0 + n)) or a coupling update (rows [p0, p1) from
 // the solved rows [q0, q1)); `scaled` marks the operations that apply the
 // caller's alpha (the others use 1).
+// With pairs on (forward solves), a node of two leaves other than the first
+// is one operation: a leaf over both (q0 = the split point, pair = its
+// index), applied through the inverse of the pair's triangle.
 struct SolveOp {
   bool leaf, scaled;
   long p0, p1, q0, q1;  // leaf: [p0, p1) only
+  int pair;             // >= 0: a pair of leaves split at q0
 };
 
 static void plan_solve(const TrsmCtx& c, long i0, long i1, bool scaled,
-                       std::vector<SolveOp>& ops) {
+                       std::vector<SolveOp>& ops, bool pairs, int& npairs) {
   const long n = i1 - i0;
   if (n <= kBlk) {
-    ops.push_back({true, scaled, i0, i1, 0, 0});
+    ops.push_back({true, scaled, i0, i1, 0, 0, -1});
     return;
   }
   long h = i0 + ((n / 2 + kSplit - 1) / kSplit) * kSplit;
   if (h >= i1) h = i1 - kSplit;
-  if (c.fwd) {
-    plan_solve(c, i0, h, scaled, ops);
-    ops.push_back({false, scaled, h, i1, i0, h});
-    plan_solve(c, h, i1, false, ops);
+  if (pairs && c.fwd && i0 > 0 && h - i0 <= kBlk && i1 - h <= kBlk) {
+    ops.push_back({true, scaled, i0, i1, h, 0, npairs++});
     return;
   }
-  plan_solve(c, h, i1, scaled, ops);
-  ops.push_back({false, scaled, i0, h, h, i1});
-  plan_solve(c, i0, h, false, ops);
+  if (c.fwd) {
+    plan_solve(c, i0, h, scaled, ops, pairs, npairs);
+    ops.push_back({false, scaled, h, i1, i0, h, -1});
+    plan_solve(c, h, i1, false, ops, pairs, npairs);
+    return;
+  }
+  plan_solve(c, h, i1, scaled, ops, pairs, npairs);
+  ops.push_back({false, scaled, i0, h, h, i1, -1});
+  plan_solve(c, i0, h, false, ops, pairs, npairs);
 }
 
 static int issue(const TrsmCtx& c, const SolveOp& op, const double* alpha) {
@@ -697,6 +695,8 @@ static int issue(const TrsmCtx& c, const SolveOp& op, const double* alpha) {
   const double* al = op.scaled ? alpha : one;
   if (!op.leaf) return update(c, op.p0, op.p1, op.q0, op.q1, al);
   const long i0 = op.p0, n = op.p1 - op.p0;
+  if (op.pair >= 0 && c.pair_ev && cudaStreamWaitEvent(c.st, c.pair_ev[op.pair], 0) != cudaSuccess)
+    return XKB_ECUDA;
   if (c.Winv) return leaf_gemm(c, i0, n, al);
   // diagonal block of the effective triangle: one launch
   const char* Ad = aptr(c, i0, i0);
@@ -752,43 +752,144 @@ int trsm_entry(int dtype, int side, int uplo, int trans, int diag, int M, int N,
   // leave the recursion's critical path.  The products with inv(E_l) carry
   // the condition number of the <= 256-unknown diagonal blocks, as blocked
   // solvers with inverted diagonal blocks do.
-  std::vector<int> leaves;
-  void* Wbuf = nullptr;
-  int* dleaves = nullptr;
+  // Pairs of leaves (tuning key trsm_pair_leaves, default 1; left side,
+  // forward, op(A) = A, >= 2048 unknowns): every node of two leaves but the
+  // first becomes ONE product with the inverse of its <= 512-unknown
+  // triangle, [inv(E_00) 0; Z inv(E_11)] with Z = -inv(E_11) E_10 inv(E_00)
+  // (two GEMMs per pair, formed on a side stream while the solve runs; a
+  // pair's product waits for its event), instead of leaf, coupling update,
+  // leaf -- three dependent small GEMMs on the critical path.  The products
+  // then carry the condition number of the pairs' triangles.
   const bool inv = (dtype == XKB_D || dtype == XKB_Z) && n > kBlk && c.nrhs >= 64 &&
                    tune("trsm_inv_leaves", 1.0) != 0.0;
+  const bool pairs = inv && c.left && c.trans == XKB_OP_N && c.fwd && n >= 2048 &&
+                     tune("trsm_pair_leaves", 1.0) != 0.0;
+  int npairs = 0;
+  std::vector<SolveOp> ops;
+  plan_solve(c, 0, n, true, ops, pairs, npairs);
+  std::vector<long> inv_at;  // (first unknown, element offset) per leaf or pair
+  void* Wbuf = nullptr;
+  int* dtab = nullptr;
+  void* Wtmp = nullptr;
+  std::vector<cudaEvent_t> pev;
+  cudaStream_t pst = st;  // the stream that forms the pairs' inverses
+  auto release_inv = [&]() {
+    if (pst != st) side_join(side_stream(kTrsmInvStream), pst, st);
+    for (cudaEvent_t ev : pev)
+      if (ev) cudaEventDestroy(ev);
+    if (Wtmp) cudaFreeAsync(Wtmp, st);
+    if (Wbuf) cudaFreeAsync(Wbuf, st);
+    if (dtab) cudaFreeAsync(dtab, st);
+  };
   if (inv) {
-    collect_leaves(0, n, leaves);
-    const int nl = (int)leaves.size() / 2;
-    if (cudaMallocAsync(&Wbuf, (size_t)nl * kBlk * kBlk * c.es, st) != cudaSuccess ||
-        cudaMallocAsync(reinterpret_cast<void**>(&dleaves), leaves.size() * sizeof(int), st) !=
-            cudaSuccess) {
+    const long ldw = npairs > 0 ? 2 * kBlk : kBlk;
+    std::vector<int> table;  // inverse launch: (first unknown, size, offset) per block
+    long slot = 0;
+    for (const SolveOp& op : ops) {
+      if (!op.leaf) continue;
+      const long off = slot++ * ldw * ldw;
+      inv_at.push_back(op.p0);
+      inv_at.push_back(off);
+      if (op.pair >= 0) {
+        const long h = op.q0 - op.p0;
+        table.insert(table.end(), {(int)op.p0, (int)h, (int)off});
+        table.insert(table.end(), {(int)op.q0, (int)(op.p1 - op.q0), (int)(off + h + h * ldw)});
+      } else {
+        table.insert(table.end(), {(int)op.p0, (int)(op.p1 - op.p0), (int)off});
+      }
+    }
+    const int nl = (int)table.size() / 3;
+    const size_t wbytes = (size_t)slot * ldw * ldw * c.es;
+    if (cudaMallocAsync(&Wbuf, wbytes, st) != cudaSuccess ||
+        cudaMallocAsync(reinterpret_cast<void**>(&dtab), table.size() * sizeof(int), st) !=
+            cudaSuccess ||
+        (npairs > 0 && cudaMallocAsync(&Wtmp, (size_t)kBlk * kBlk * c.es, st) != cudaSuccess)) {
       cudaGetLastError();
-      if (Wbuf) cudaFreeAsync(Wbuf, st);
+      release_inv();
       return XKB_ENOMEM;
     }
-    // pageable source: staged before the call returns
-    cudaMemcpyAsync(dleaves, leaves.data(), leaves.size() * sizeof(int), cudaMemcpyHostToDevice,
-                    st);
+    // a pair's upper-right block is zero; pageable source: staged before the
+    // call returns
+    if ((npairs > 0 && cudaMemsetAsync(Wbuf, 0, wbytes, st) != cudaSuccess) ||
+        cudaMemcpyAsync(dtab, table.data(), table.size() * sizeof(int), cudaMemcpyHostToDevice,
+                        st) != cudaSuccess) {
+      release_inv();
+      return XKB_ECUDA;
+    }
     const double one[2] = {1.0, 0.0};
     int e = dtype == XKB_D
                 ? launch_block<double>(kBlk, kBlk, A, lda, c.swap, c.conj, c.lower_eff, c.unit,
-                                       Wbuf, kBlk, 0, one, st, dleaves, nl)
+                                       Wbuf, ldw, 0, one, st, dtab, nl)
                 : launch_block<double2>(kBlk, kBlk, A, lda, c.swap, c.conj, c.lower_eff, c.unit,
-                                        Wbuf, kBlk, 0, one, st, dleaves, nl);
+                                        Wbuf, ldw, 0, one, st, dtab, nl);
     if (e) {
-      cudaFreeAsync(Wbuf, st);
-      cudaFreeAsync(dleaves, st);
+      release_inv();
       return e;
     }
     c.Winv = static_cast<const char*>(Wbuf);
-    c.leaf_i0 = &leaves;
+    c.ldw = ldw;
+    c.inv_at = &inv_at;
+    if (npairs > 0) {
+      pev.assign((size_t)npairs, nullptr);
+      for (cudaEvent_t& ev : pev)
+        if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) {
+          cudaGetLastError();
+          ev = nullptr;
+          release_inv();
+          return XKB_ECUDA;
+        }
+      pst = side_fork(side_stream(kTrsmInvStream), st);
+      size_t q = 0;
+      for (const SolveOp& op : ops) {
+        if (!op.leaf) continue;
+        const long off = inv_at[2 * q + 1];
+        ++q;
+        if (op.pair < 0) continue;
+        const long n0 = op.q0 - op.p0, n1 = op.p1 - op.q0;
+        char* P = static_cast<char*>(Wbuf) + (size_t)off * c.es;
+        xkb_gemm_args g{};
+        g.dtype = dtype;
+        g.uplo = XKB_FULL;
+        g.opA = g.opB = XKB_OP_N;
+        // W = E_10 inv(E_00), n1 x n0
+        g.M = (int)n1;
+        g.N = (int)n0;
+        g.K = (int)n0;
+        g.alpha[0] = 1.0;
+        g.A = aptr(c, op.q0, op.p0);
+        g.lda = lda;
+        g.B = P;
+        g.ldb = ldw;
+        g.C = Wtmp;
+        g.ldc = kBlk;
+        if ((e = xkb_cuda_gemm(&g, pst))) break;
+        // Z = -inv(E_11) W into the pair's lower-left block
+        g.K = (int)n1;
+        g.alpha[0] = -1.0;
+        g.A = P + (size_t)(n0 + n0 * ldw) * c.es;
+        g.lda = ldw;
+        g.B = Wtmp;
+        g.ldb = kBlk;
+        g.C = P + (size_t)n0 * c.es;
+        g.ldc = ldw;
+        if ((e = xkb_cuda_gemm(&g, pst))) break;
+        if (cudaEventRecord(pev[(size_t)op.pair], pst) != cudaSuccess) {
+          e = XKB_ECUDA;
+          break;
+        }
+      }
+      if (e) {
+        release_inv();
+        return e;
+      }
+      c.pair_ev = pev.data();
+    }
   }
   std::vector<void*> tmps;
   auto give_tmp = [&](TrsmCtx& part) {
     if (!inv) return XKB_OK;
     void* t = nullptr;
-    if (cudaMallocAsync(&t, (size_t)kBlk * part.nrhs * c.es, st) != cudaSuccess) {
+    if (cudaMallocAsync(&t, (size_t)c.ldw * part.nrhs * c.es, st) != cudaSuccess) {
       cudaGetLastError();
       return XKB_ENOMEM;
     }
@@ -797,9 +898,8 @@ int trsm_entry(int dtype, int side, int uplo, int trans, int diag, int M, int N,
     return XKB_OK;
   };
   auto release = [&](int e) {
+    release_inv();
     for (void* t : tmps) cudaFreeAsync(t, st);
-    if (Wbuf) cudaFreeAsync(Wbuf, st);
-    if (dleaves) cudaFreeAsync(dleaves, st);
     return e;
   };
   // Many right-hand sides: G independent groups (tuning key
@@ -833,8 +933,6 @@ int trsm_entry(int dtype, int side, int uplo, int trans, int diag, int M, int N,
     // group in turn, so that all groups start together and run side by side
     // to the end (issued group after group, the last group started one
     // group's host issue time late and finished alone)
-    std::vector<SolveOp> ops;
-    plan_solve(c, 0, n, true, ops);
     int e = XKB_OK;
     for (const SolveOp& op : ops)
       for (int g = 0; g < np && !e; ++g) e = issue(parts[g], op, alpha);
@@ -843,8 +941,6 @@ int trsm_entry(int dtype, int side, int uplo, int trans, int diag, int M, int N,
     return release(e);
   }
   if (int e = give_tmp(c)) return release(e);
-  std::vector<SolveOp> ops;
-  plan_solve(c, 0, n, true, ops);
   for (const SolveOp& op : ops)
     if (int e = issue(c, op, alpha)) return release(e);
   return release(XKB_OK);

@@ -143,11 +143,12 @@ void count_launch(int n = 1);
 // (slot 0: the LU's column-panel solves, slots 1-3: the TRSM's groups of
 // right-hand sides after the first, slots kHiStream and kHiStream2: the
 // critical path of the blocked factorizations and the panel work beside it,
-// created with the device's greatest stream priority so that their small
-// launches are scheduled ahead of the trailing updates that run meanwhile).
-// s is nullptr if CUDA could not create it.
-constexpr int kSideStreams = 6;
-constexpr int kHiStream = 4, kHiStream2 = 5;
+// slot kTrsmInvStream: the TRSM's inverses of pairs of diagonal blocks;
+// slots from kHiStream on are created with the device's greatest stream
+// priority so that their small launches are scheduled ahead of the trailing
+// updates that run meanwhile).  s is nullptr if CUDA could not create it.
+constexpr int kSideStreams = 7;
+constexpr int kHiStream = 4, kHiStream2 = 5, kTrsmInvStream = 6;
 struct SideStream {
   cudaStream_t s = nullptr;
   cudaEvent_t fork = nullptr, join = nullptr;
