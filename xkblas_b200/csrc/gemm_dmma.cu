@@ -536,6 +536,31 @@ __global__ void __launch_bounds__(kThreads, 1)
   }
 }
 
+// Sum of n partial-sum slots (slot q at w0 + q * stride, NACC values
+// kThreads apart) in slot order, loaded four slots at a time so that one
+// memory latency covers four slots (the order of the additions, and so the
+// result, is that of a slot-by-slot loop).
+template <int NACC>
+__device__ __forceinline__ void sum_slots(const double* w0, size_t stride, int n,
+                                          double (&acc)[NACC]) {
+#pragma unroll
+  for (int v = 0; v < NACC; ++v) acc[v] = 0.0;
+  for (int s0 = 0; s0 < n; s0 += 4) {
+    double wv[4][NACC];
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+      for (int v = 0; v < NACC; ++v)
+        wv[q][v] = s0 + q < n ? w0[(size_t)(s0 + q) * stride + (size_t)v * kThreads] : 0.0;
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+      if (s0 + q < n) {
+#pragma unroll
+        for (int v = 0; v < NACC; ++v) acc[v] += wv[q][v];
+      }
+  }
+}
+
 // Stream-K reduction: block (tile, fragment f) sums fragment f of the
 // tile's pieces in CTA order, then stores it as the unsplit epilogue does.
 template <class T, int BM, int BN>
@@ -550,17 +575,11 @@ __global__ void __launch_bounds__(kThreads) k_gemm_sk_reduce(const GemmParams p)
   if (!dmma_tile<BM, BN>(p, bid, m0, n0)) return;
   const int c0 = sk_cta((long)bid * kts, tot, p.sk_ctas);
   const int c1 = sk_cta((long)(bid + 1) * kts - 1, tot, p.sk_ctas);
-  double acc[A::NACC];
-#pragma unroll
-  for (int v = 0; v < A::NACC; ++v) acc[v] = 0.0;
-  for (int sl = 0; sl <= c1 - c0; ++sl) {
-    const double* w = p.ws + ((size_t)bid * p.sk_slots + sl) * (size_t)(NREG * kThreads) +
-                      (size_t)(f * A::NACC) * kThreads + threadIdx.x;
-#pragma unroll
-    for (int v = 0; v < A::NACC; ++v) acc[v] += w[(size_t)v * kThreads];
-  }
-  double cv[A::NACC];
-  dmma_load_frag<T, BM, BN>(p, m0, n0, f / A::NF, f % A::NF, cv);
+  double cv[A::NACC], acc[A::NACC];
+  dmma_load_frag<T, BM, BN>(p, m0, n0, f / A::NF, f % A::NF, cv);  // in flight meanwhile
+  const double* w0 = p.ws + (size_t)bid * p.sk_slots * (size_t)(NREG * kThreads) +
+                     (size_t)(f * A::NACC) * kThreads + threadIdx.x;
+  sum_slots<A::NACC>(w0, (size_t)NREG * kThreads, c1 - c0 + 1, acc);
   dmma_store_frag<T, BM, BN>(p, m0, n0, f / A::NF, f % A::NF, acc, cv);
 }
 
@@ -578,17 +597,11 @@ __global__ void __launch_bounds__(kThreads) k_gemm_splitk(const GemmParams p) {
   const int f = blockIdx.y;  // fragment (mf, nf) = (f / NF, f % NF)
   int m0, n0;
   if (!dmma_tile<BM, BN>(p, bid, m0, n0)) return;
-  double acc[A::NACC];
-#pragma unroll
-  for (int v = 0; v < A::NACC; ++v) acc[v] = 0.0;
-  for (int sl = 0; sl < p.ksplit; ++sl) {
-    const double* w = p.ws + ((size_t)sl * ntiles + bid) * (size_t)(NREG * kThreads) +
-                      (size_t)(f * A::NACC) * kThreads + threadIdx.x;
-#pragma unroll
-    for (int v = 0; v < A::NACC; ++v) acc[v] += w[(size_t)v * kThreads];
-  }
-  double cv[A::NACC];
-  dmma_load_frag<T, BM, BN>(p, m0, n0, f / A::NF, f % A::NF, cv);
+  double cv[A::NACC], acc[A::NACC];
+  dmma_load_frag<T, BM, BN>(p, m0, n0, f / A::NF, f % A::NF, cv);  // in flight meanwhile
+  const double* w0 =
+      p.ws + (size_t)bid * (size_t)(NREG * kThreads) + (size_t)(f * A::NACC) * kThreads + threadIdx.x;
+  sum_slots<A::NACC>(w0, (size_t)ntiles * NREG * kThreads, p.ksplit, acc);
   dmma_store_frag<T, BM, BN>(p, m0, n0, f / A::NF, f % A::NF, acc, cv);
 }
 
@@ -786,14 +799,19 @@ static int dispatch_type(const xkb_gemm_args* a, cudaStream_t st, const int* run
   if (ks > 1) {
     // Stream-K instead when C is full (tuning key gemm_streamk, default 1)
     // and split-K's ks x tiles CTAs fill less than gemm_sk_fill (0.8) of the
-    // SMs: one CTA per SM, each with an equal share of the tiles' k-steps (at
-    // least gemm_sk_min_kt of them).  Measured on a B200: 640 x 1280 x 2048
-    // (50 tiles, split-K 2 on 100 CTAs) 168 -> 136 us; where split-K already
-    // filled 86-97 % of the SMs the two were within 5 % either way.
+    // SMs, or leave any SM idle while every tile has at least gemm_sk_long_kt
+    // (64) k-steps: one CTA per SM, each with an equal share of the tiles'
+    // k-steps (at least gemm_sk_min_kt of them).  Measured on a B200: 640 x
+    // 1280 x 2048 (50 tiles, split-K 2 on 100 CTAs) 168 -> 136 us; 1024^3
+    // (split-K 2 on 128 CTAs, 64 k-steps per tile) 97.8-98.9 -> 94.5-95.3 us
+    // (alternating, same box); at 16-32 k-steps per tile and 86-97 % of the
+    // SMs filled the two were within 5 % either way.
     const long min_kt = std::max(1L, (long)tune("gemm_sk_min_kt", 8.0));
     const long sk = std::min<long>(sm_count(), tiles_big * ktiles / min_kt);
+    const double split_fill = (double)(tiles_big * ks) / (double)sm_count();
     if (a->uplo == XKB_FULL && tune("gemm_streamk", 1.0) != 0.0 && sk > tiles_big * ks &&
-        (double)(tiles_big * ks) < tune("gemm_sk_fill", 0.8) * (double)sm_count())
+        (split_fill < tune("gemm_sk_fill", 0.8) ||
+         (split_fill < 1.0 && ktiles >= (long)tune("gemm_sk_long_kt", 64.0))))
       return dispatch_ops<T, BMb, BNb>(a, st, run_if, 1, (int)sk);
     return dispatch_ops<T, BMb, BNb>(a, st, run_if, ks);
   }

@@ -494,9 +494,11 @@ static int factor(const PotrfCtx& c, long i0, long i1, bool la, bool pend) {
 // GEMM more efficient (larger K); near the end the critical path bounds each
 // step and narrower blocks shorten it.  Width for `m` remaining rows: nb,
 // halved (rounded down to a multiple of 64, at least nmin) while
-// m <= shrink * width (tuning key potrf_shrink, default 12).
-static long block_width(long m, long nb, long nmin) {
-  const double shrink = tune("potrf_shrink", 12.0);
+// m <= shrink * width (tuning keys potrf_shrink, default 8, and in tensor-op
+// mode potrf_shrink_oz, default 12; DPOTRF 8192 plain, shrink 8 / 12 / 16 /
+// 24: 9.88 / 10.05 / 10.88 / 11.69 ms).
+static long block_width(long m, long nb, long nmin, bool oz) {
+  const double shrink = oz ? tune("potrf_shrink_oz", 12.0) : tune("potrf_shrink", 8.0);
   long w = nb;
   while (w > nmin && (double)m <= shrink * (double)w) w = std::max(nmin, (w / 2) / 64 * 64);
   return w;
@@ -565,12 +567,12 @@ static int factor_blocked(const PotrfCtx& c, long i0, long i1, long nb) {
   };
   rec(e_trail, c.st);  // "previous trailing update": the caller's work so far
   const long nmin = cplx ? PoShape<double2>::NMAX : PoShape<double>::NMAX;
-  long b = i0, nk = std::min(block_width(i1 - i0, nb, nmin), i1 - i0);
+  long b = i0, nk = std::min(block_width(i1 - i0, nb, nmin, c.ozaki > 0), i1 - i0);
   e = factor(ch, b, b + nk, false, false);
   rec(e_diag, ch.st);
   while (!e && b + nk < i1) {
     const long r0 = b + nk, m2 = i1 - r0;
-    const long n1 = std::min(block_width(m2, nb, nmin), m2), m3 = m2 - n1;  // next block; below it
+    const long n1 = std::min(block_width(m2, nb, nmin, c.ozaki > 0), m2), m3 = m2 - n1;  // next block; below it
     if (m3 > 0) {  // hp2: P2 solve (needs D_k)
       wait(hp2.s, e_diag);
       if (!e) e = solve(b, nk, r0 + n1, m3, hp2.s);
