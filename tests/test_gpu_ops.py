@@ -490,16 +490,18 @@ def test_trsm_pair_leaves(xk, dt):
     """Left, lower, op(A) = A with >= 2048 unknowns: with the tuning key
     trsm_pair_leaves = 1 (default) every node of two diagonal blocks but the
     first is applied through the inverse of its triangle (formed on a side
-    stream), = 0 keeps leaf, coupling update, leaf.  Ragged split points
-    (2148 unknowns), unit and non-unit diagonals: both meet the reference
-    bound."""
+    stream; trsm_pair_split = 0, default, multiplies by the whole inverse,
+    = 1 skips its zero block in two products), = 0 keeps leaf,
+    coupling update, leaf.  Ragged split points (2148 unknowns), unit and
+    non-unit diagonals: every form meets the reference bound."""
     cplx = np.issubdtype(dt, np.complexfloating)
     lib = xk.lib()
     M, N = 2148, 160
     seed = 1700
     try:
-        for flag in (1.0, 0.0):
+        for flag, split in ((1.0, 0.0), (1.0, 1.0), (0.0, 0.0)):
             lib.xkb_tune_set(b"trsm_pair_leaves", flag)
+            lib.xkb_tune_set(b"trsm_pair_split", split)
             for dg in (NONUNIT, UNIT):
                 A = np.asfortranarray((O.plrnt(M, M, seed, cplx) / M + np.eye(M)).astype(dt))
                 B0 = gen(M, N, seed + 1, dt)
@@ -510,9 +512,10 @@ def test_trsm_pair_leaves(xk, dt):
                 xk.invalidate_caches()
                 R = O.trsm(LEFT, LO, N_, dg, alpha, up(A), up(B0), nb=64)
                 r = checks.trsm_ratio(B, R, A, M, N)
-                assert r <= 10, (flag, dg, r)
+                assert r <= 10, (flag, split, dg, r)
     finally:
         lib.xkb_tune_set(b"trsm_pair_leaves", 1.0)
+        lib.xkb_tune_set(b"trsm_pair_split", 0.0)
 
 
 @pytest.mark.parametrize("case", [

@@ -549,8 +549,14 @@ struct TrsmCtx {
 
 // A leaf applied through its inverse: X = alpha inv(E) B (left) or
 // X = alpha B inv(E)^T (right side: E is op(A)^T there), one GEMM into tmp
-// and a copy back into B.
-static int leaf_gemm(const TrsmCtx& c, long i0, long n, const double* alpha) {
+// and a copy back into B.  A pair split at mid (> 0; left side only) may
+// skip the zero upper-right block of its inverse (tuning key
+// trsm_pair_split, default 0): X_0 = alpha inv(E_00) B_0 and X_1 = alpha
+// [Z inv(E_11)] [B_0; B_1], two GEMMs into tmp.  Measured on a B200 (DTRSM
+// 4096, alternating): 2.83 -> 2.86 ms plain, 2.30 -> 2.32 tensor-op -- the
+// second launch on the chain costs more than the quarter of the product's
+// flops it saves.
+static int leaf_gemm(const TrsmCtx& c, long i0, long n, const double* alpha, long mid = 0) {
   const auto& L = *c.inv_at;
   size_t q = 0;
   while (2 * q < L.size() && L[2 * q] != i0) ++q;
@@ -595,6 +601,16 @@ static int leaf_gemm(const TrsmCtx& c, long i0, long n, const double* alpha) {
     height = (size_t)n;
   }
   dpitch = (size_t)c.ldb * c.es;
+  if (c.left && mid > 0 && tune("trsm_pair_split", 0.0) != 0.0) {
+    const long n0 = mid - i0;
+    xkb_gemm_args g0 = g;  // X_0: rows [0, n0) of the product
+    g0.M = (int)n0;
+    g0.K = (int)n0;
+    if (int e = xkb_cuda_gemm(&g0, c.st)) return e;
+    g.M = (int)(n - n0);  // X_1: rows [n0, n), all n columns of the inverse
+    g.A = Wl + (size_t)n0 * c.es;
+    g.C = c.tmp + (size_t)n0 * c.es;
+  }
   if (int e = xkb_cuda_gemm(&g, c.st)) return e;
   return cudaMemcpy2DAsync(Bk, dpitch, c.tmp, spitch, width, height, cudaMemcpyDeviceToDevice,
                            c.st) == cudaSuccess
@@ -697,7 +713,7 @@ static int issue(const TrsmCtx& c, const SolveOp& op, const double* alpha) {
   const long i0 = op.p0, n = op.p1 - op.p0;
   if (op.pair >= 0 && c.pair_ev && cudaStreamWaitEvent(c.st, c.pair_ev[op.pair], 0) != cudaSuccess)
     return XKB_ECUDA;
-  if (c.Winv) return leaf_gemm(c, i0, n, al);
+  if (c.Winv) return leaf_gemm(c, i0, n, al, op.pair >= 0 ? op.q0 : 0);
   // diagonal block of the effective triangle: one launch
   const char* Ad = aptr(c, i0, i0);
   char* Bd = c.left ? c.B + i0 * (long)c.es : c.B + i0 * c.ldb * (long)c.es;
